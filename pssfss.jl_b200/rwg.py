@@ -1,0 +1,199 @@
+"""RWG basis-function topology (PSSFSS.jl ``src/RWG.jl:27-324``).
+
+``setup_rwg(sheet)`` returns the same ``bfe``, ``bff``, ``ebf``, ``eci``, ``ufpm``,
+``ufp2fp`` and ``nufp`` as the reference (1-based values, Julia column-major meaning).
+
+Unique face pairs (``RWG.jl:287-319``): the reference puts face pairs (m, n) (match m,
+source n) whose 6-vectors ``(c_m - r1_n, c_m - r2_n, c_m - r3_n)`` lie within
+``1e-6*|c_1 - c_2|`` of each other into one class, numbered in column-major order of
+their first member.  Here the same classes are formed by exact grouping of the
+quantised key ``(source-triangle shape, c_m - r1_n)`` on a grid of that radius: the
+three vectors are determined by ``c_m - r1_n`` and the source triangle's edge vectors,
+and translation-equivalent pairs agree to rounding error, far inside the radius.  A
+pair whose key straddles a grid line would form its own class; its integrals then
+equal the class's to rounding error, so results are unchanged.
+"""
+import math
+
+import numpy as np
+
+
+class RWGData:
+    def __init__(self, bfe, bff, ebf, eci, ufpm, ufp_rep, nufp):
+        self.bfe = bfe            # (2, nbf) int64, 1-based edge numbers
+        self.bff = bff            # (2, nbf) int64, 1-based face numbers (plus, minus)
+        self.ebf = ebf            # (nedge,) int64, basis function of each edge or 0
+        self.eci = eci            # (nedge,) int64 in 0..4, unit-cell boundary code
+        self.ufpm = ufpm          # (nface, nface) int64, ufpm[m, n] = class of (match m, source n)
+        self.ufp_rep = ufp_rep    # (nufp,) int64, 1-based column-major index of each class's first pair
+        self.nufp = nufp
+
+    @property
+    def nbf(self):
+        return self.bfe.shape[1]
+
+    @property
+    def ufp2fp(self):
+        """List of 1-based column-major face-pair indices per class (``RWG.jl:69``)."""
+        flat = self.ufpm.ravel(order="F")
+        order = np.argsort(flat, kind="stable")
+        counts = np.bincount(flat, minlength=self.nufp + 1)[1:]
+        ptr = np.concatenate([[0], np.cumsum(counts)])
+        return [order[ptr[i]:ptr[i + 1]] + 1 for i in range(self.nufp)]
+
+
+def _xieta(sheet, node):
+    p = sheet.rho[node - 1]
+    b1, b2 = sheet.beta1, sheet.beta2
+    return (b1[0] * p[0] + b1[1] * p[1]) / (2 * math.pi), (b2[0] * p[0] + b2[1] * p[1]) / (2 * math.pi)
+
+
+def get_ie_xieta(ie, sheet):
+    """``get_ie_ξη`` (``RWG.jl:388-398``) for 1-based edge ``ie``."""
+    xi0, eta0 = _xieta(sheet, int(sheet.e1[ie - 1]))
+    xi1, eta1 = _xieta(sheet, int(sheet.e2[ie - 1]))
+    return xi0, xi1, eta0, eta1
+
+
+def setup_rwg(sheet):
+    """Basis functions, boundary codes and unique face pairs of ``sheet`` (``RWG.jl:90``)."""
+    tol = 1.0e-5
+    nface = sheet.nface
+    nedge = sheet.nedge
+    fe = sheet.fe
+    eci = np.zeros(nedge, np.int64)
+    ie_xi0, ie_xi1, ie_eta0, ie_eta1 = [], [], [], []
+
+    # Interior basis functions: each pair of faces (fp < fm) sharing an edge, ordered by
+    # (fp, fm, local edge slot in fp, local edge slot in fm) like the reference's loops.
+    edge_faces = [[] for _ in range(nedge + 1)]
+    for f in range(nface):
+        for k in range(3):
+            edge_faces[int(fe[k, f])].append((f + 1, k))
+    pairs = []
+    for e in range(1, nedge + 1):
+        fl = edge_faces[e]
+        for a in range(len(fl)):
+            for b in range(a + 1, len(fl)):
+                (fa, ka), (fb, kb) = fl[a], fl[b]
+                if fa > fb:
+                    (fa, ka), (fb, kb) = (fb, kb), (fa, ka)
+                pairs.append((fa, fb, ka, kb, e))
+    pairs.sort()
+    nbf_int = len(pairs)
+
+    nbf = nbf_int
+    if sheet.xi_eta_check:
+        for gep in range(1, nedge + 1):
+            xi0, xi1, eta0, eta1 = get_ie_xieta(gep, sheet)
+            if abs(xi0) < tol and abs(xi1) < tol:
+                nbf += 1
+                eci[gep - 1] = 1
+                ie_xi0.append(gep)
+            elif abs(xi0 - 1) < tol and abs(xi1 - 1) < tol:
+                eci[gep - 1] = 2
+                ie_xi1.append(gep)
+            elif abs(eta0) < tol and abs(eta1) < tol:
+                nbf += 1
+                eci[gep - 1] = 3
+                ie_eta0.append(gep)
+            elif abs(eta0 - 1) < tol and abs(eta1 - 1) < tol:
+                eci[gep - 1] = 4
+                ie_eta1.append(gep)
+    if len(ie_xi0) != len(ie_xi1):
+        raise ValueError("Inconsistent # edges at ξ=0 and ξ=1")
+    if len(ie_eta0) != len(ie_eta1):
+        raise ValueError("Inconsistent # edges at η=0 and η=1")
+
+    bfe = np.zeros((2, nbf), np.int64)
+    bff = np.zeros((2, nbf), np.int64)
+    ebf = np.zeros(nedge, np.int64)
+    for i, (fa, fb, ka, kb, e) in enumerate(pairs):
+        bfe[:, i] = (e, e)
+        bff[:, i] = (fa, fb)
+        ebf[e - 1] = i + 1
+    i = nbf_int
+
+    def first_face(ge):
+        fl = edge_faces[ge]
+        if not fl:
+            return 0
+        return min(f for f, _ in fl)
+
+    def pair_boundary(list0, list1, use_xi):
+        nonlocal i
+        for ge0 in list0:
+            face0 = first_face(ge0)
+            if face0 == 0:
+                raise ValueError(f"Unable to locate face containing boundary edge {ge0}")
+            x0 = get_ie_xieta(ge0, sheet)
+            v0 = (x0[0], x0[1]) if use_xi else (x0[2], x0[3])
+            mn0, mx0 = min(v0), max(v0)
+            ge1 = 0
+            for ge in list1:
+                x1 = get_ie_xieta(ge, sheet)
+                v1 = (x1[0], x1[1]) if use_xi else (x1[2], x1[3])
+                if abs(min(v1) - mn0) < tol and abs(max(v1) - mx0) < tol:
+                    ge1 = ge
+                    break
+            if ge1 == 0:
+                raise ValueError(f"Unable to locate edge corresponding to edge {ge0}")
+            face1 = first_face(ge1)
+            if face1 == 0:
+                raise ValueError(f"Unable to locate face containing boundary edge {ge1}")
+            bfe[:, i] = (ge0, ge1)
+            bff[:, i] = (face0, face1)
+            ebf[ge0 - 1] = i + 1
+            ebf[ge1 - 1] = i + 1
+            i += 1
+
+    pair_boundary(ie_eta0, ie_eta1, use_xi=True)   # η=0 ↔ η=1 edges matched on ξ extent
+    pair_boundary(ie_xi0, ie_xi1, use_xi=False)    # ξ=0 ↔ ξ=1 edges matched on η extent
+    if i != nbf:
+        raise ValueError("Inconsistent number of basis functions")
+
+    if not sheet.fufp:
+        nufp = nface * nface
+        ufpm = np.arange(1, nufp + 1, dtype=np.int64).reshape((nface, nface), order="F")
+        return RWGData(bfe, bff, ebf, eci, ufpm, np.arange(1, nufp + 1, dtype=np.int64), nufp)
+    ufpm, rep, nufp = unique_face_pairs(sheet)
+    return RWGData(bfe, bff, ebf, eci, ufpm, rep, nufp)
+
+
+def unique_face_pairs(sheet):
+    """Translation-equivalence classes of face pairs (``RWG.jl:287-319``)."""
+    nface = sheet.nface
+    rho = sheet.rho
+    r1 = rho[sheet.fv[0] - 1]
+    r2 = rho[sheet.fv[1] - 1]
+    r3 = rho[sheet.fv[2] - 1]
+    cen = (r1 + r2 + r3) / 3
+    d = cen[0] - cen[1]
+    rad = 1e-6 * math.sqrt(d[0] * d[0] + d[1] * d[1])
+    g = rad
+    # Source-triangle shape classes (edge vectors quantised on the same grid).
+    shape_key = np.round(np.hstack([r2 - r1, r3 - r1]) / g).astype(np.int64)
+    _, shape_id = np.unique(shape_key, axis=0, return_inverse=True)
+    shape_id = shape_id.ravel().astype(np.int64)
+    # Column-major face pairs: match m fastest, source n slowest.
+    dx = np.round((cen[:, None, 0] - r1[None, :, 0]) / g).astype(np.int64)  # [m, n]
+    dy = np.round((cen[:, None, 1] - r1[None, :, 1]) / g).astype(np.int64)
+    sid = np.broadcast_to(shape_id[None, :], (nface, nface))
+    k0 = sid.ravel(order="F")
+    k1 = dx.ravel(order="F")
+    k2 = dy.ravel(order="F")
+    del dx, dy
+    order = np.lexsort((k2, k1, k0))
+    ks0, ks1, ks2 = k0[order], k1[order], k2[order]
+    newgrp = np.ones(len(order), bool)
+    newgrp[1:] = (ks0[1:] != ks0[:-1]) | (ks1[1:] != ks1[:-1]) | (ks2[1:] != ks2[:-1])
+    starts = np.flatnonzero(newgrp)
+    grp_sorted = np.cumsum(newgrp) - 1
+    rep = np.minimum.reduceat(order, starts)      # smallest column-major index per group
+    rank = np.empty(len(rep), np.int64)
+    rank[np.argsort(rep, kind="stable")] = np.arange(len(rep))
+    cls = np.empty(len(order), np.int64)
+    cls[order] = rank[grp_sorted] + 1
+    ufpm = cls.reshape((nface, nface), order="F")
+    rep_sorted = np.sort(rep) + 1
+    return ufpm, rep_sorted.astype(np.int64), len(rep)

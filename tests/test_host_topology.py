@@ -1,0 +1,132 @@
+"""Host-side geometry, topology, modes and GSM algebra against the reference's tests.
+
+test/RWGData_test.jl, test/RWGSheet_test.jl, test/Elements_test.jl, test/Rings_test.jl,
+test/GSMs_test.jl (cascade identities).
+"""
+import math
+
+import numpy as np
+
+import oracle
+from pssfss_b200.elements import meander, meander_counts, rectstrip
+from pssfss_b200.gsms import GSM, cascade, cascade_layer
+from pssfss_b200.layers import Layer
+from pssfss_b200.rings import Ring
+from pssfss_b200.rwg import setup_rwg
+from pssfss_b200.sheets import combine, recttri
+from pssfss_b200.units import Length, inch, mm
+
+
+def test_rings():
+    assert list(Ring(0)) == [(0, 0)]
+    assert list(Ring(1)) == [(1, -1), (1, 0), (1, 1), (-1, -1), (-1, 0), (-1, 1), (0, -1), (0, 1)]
+    assert list(Ring(2)) == [(2, -2), (2, -1), (2, 0), (2, 1), (2, 2), (-2, -2), (-2, -1), (-2, 0),
+                             (-2, 1), (-2, 2), (-1, -2), (0, -2), (1, -2), (-1, 2), (0, 2), (1, 2)]
+    assert len(list(Ring(10))) == len(Ring(10)) == 80
+    assert all(max(abs(m), abs(n)) == 100 for m, n in Ring(100))
+
+
+def test_recttri_and_combine():
+    sh1 = recttri([0., 0.], [1., 1.], 1, 1)
+    assert sh1.rho.tolist() == [[0, 0], [1, 0], [0, 1], [1, 1]]
+    assert sh1.e1.tolist() == [1, 3, 1, 2, 1] and sh1.e2.tolist() == [2, 4, 3, 4, 4]
+    assert sh1.fe.ravel(order="F").tolist() == [2, 3, 5, 4, 5, 1]
+    assert sh1.fv.ravel(order="F").tolist() == [1, 4, 3, 1, 2, 4]
+    sh3 = combine(sh1, recttri([1., 0.], [2., 1.], 1, 1), "x", 1)
+    assert sh3.rho.tolist() == [[0, 0], [1, 0], [0, 1], [1, 1], [2, 0], [2, 1]]
+    assert sh3.e1.tolist() == [1, 3, 1, 2, 1, 2, 4, 5, 2]
+    assert sh3.e2.tolist() == [2, 4, 3, 4, 4, 5, 6, 6, 6]
+    assert sh3.fv.ravel(order="F").tolist() == [1, 4, 3, 1, 2, 4, 2, 6, 4, 2, 5, 6]
+    assert sh3.fe.ravel(order="F").tolist() == [2, 3, 5, 4, 5, 1, 7, 4, 9, 8, 9, 6]
+    sh3 = combine(sh1, recttri([0., 1.], [1., 2.], 1, 1), "y", 1.0)
+    assert sh3.e1.tolist() == [1, 3, 1, 2, 1, 5, 3, 4, 3]
+    assert sh3.fe.tolist() == [[2, 4, 6, 8], [3, 5, 7, 9], [5, 1, 9, 2]]
+    assert sh3.fv.tolist() == [[1, 1, 3, 3], [4, 2, 6, 4], [3, 4, 5, 6]]
+    sh3 = combine(sh1, recttri([1., 1.], [2., 2.], 1, 1), "y", 1.0)
+    assert sh3.rho.tolist() == [[0, 0], [1, 0], [0, 1], [1, 1], [2, 1], [1, 2], [2, 2]]
+    assert sh3.e1.tolist() == [1, 3, 1, 2, 1, 4, 6, 4, 5, 4]
+    assert sh3.e2.tolist() == [2, 4, 3, 4, 4, 5, 7, 6, 7, 7]
+    assert sh3.fe.tolist() == [[2, 4, 7, 9], [3, 5, 8, 10], [5, 1, 10, 6]]
+    assert sh3.fv.tolist() == [[1, 1, 4, 4], [4, 2, 7, 5], [3, 4, 6, 7]]
+    sh3 = combine(sh1, recttri([2., 0.], [3., 1.], 1, 1), " ", float("nan"))
+    assert sh3.e1.tolist() == [1, 3, 1, 2, 1, 5, 7, 5, 6, 5]
+    assert sh3.fv.tolist() == [[1, 1, 5, 5], [4, 2, 8, 6], [3, 4, 7, 8]]
+
+
+def test_rectstrip_fields():
+    sh = rectstrip(Lx=1, Ly=1.0, Nx=1, Ny=1, Px=1, Py=1, units=inch)
+    assert (sh.rho[1] - sh.rho[0]).tolist() == [1, 0]
+    assert sh.fufp and sh.cls == "J" and sh.units == inch
+    assert np.allclose(sh.beta1, [2 * math.pi, 0]) and np.allclose(sh.beta2, [0, 2 * math.pi])
+
+
+def test_rwgdata_fufp_true_false():
+    for fufp in (True, False):
+        r = setup_rwg(rectstrip(Lx=1, Ly=1, Px=1, Py=1, Nx=2, Ny=1, units=mm, fufp=fufp))
+        assert r.bfe.tolist() == [[8, 6, 9, 1, 2, 5], [8, 6, 9, 3, 4, 7]]
+        assert r.bff.tolist() == [[1, 2, 3, 2, 4, 1], [2, 3, 4, 1, 3, 4]]
+        assert r.ebf.tolist() == [4, 5, 4, 5, 6, 2, 6, 1, 3]
+        assert r.eci.tolist() == [3, 3, 4, 4, 1, 0, 2, 0, 0]
+        if fufp:
+            assert r.ufpm.tolist() == [[1, 5, 9, 11], [2, 6, 10, 12], [3, 7, 1, 5], [4, 8, 2, 6]]
+            assert [list(x) for x in r.ufp2fp] == [[1, 11], [2, 12], [3], [4], [5, 15], [6, 16],
+                                                    [7], [8], [9], [10], [13], [14]]
+            assert r.nufp == 12
+        else:
+            assert (r.ufpm.ravel(order="F") == np.arange(1, 17)).all() and r.nufp == 16
+
+
+def test_rwgbfft_golden():
+    # test/RWGData_test.jl:39-58
+    sh = rectstrip(Lx=1, Ly=1, Px=1, Py=1, Nx=2, Ny=1, units=mm, fufp=False)
+    ft = oracle.rwgbfft(setup_rwg(sh), sh, [0., 0.], 0.0, 0.0)
+    gold = [[0.0001666666666666667, -0.0003333333333333334],
+            [0.0003333333333333334, 0.0003333333333333334],
+            [0.00016666666666666663, -0.0003333333333333334]]
+    assert np.allclose(ft[:3], gold, rtol=1e-12, atol=0)
+    sh = rectstrip(Lx=1, Ly=1, Px=1, Py=1, Nx=2, Ny=1, units=inch, fufp=False)
+    ft = oracle.rwgbfft(setup_rwg(sh), sh, [20.0, -30.3], 0.8, -0.7)
+    gold = [[0.003986416685586114 - 0.0010511300702857503j, -0.008079847138694855 + 0.0021304773084817956j],
+            [0.008263557134402535 - 0.0010871639073400372j, 0.008284527320353664 - 0.0010899227712197804j],
+            [0.004122638196063312 - 1.5707327530113332e-5j, -0.008355946971820058 + 3.1836312009155855e-5j]]
+    assert np.allclose(ft[:3], gold, rtol=1e-12, atol=0)
+
+
+def test_meander_counts_and_topology():
+    nx1, nx2, ny1, ny2, nt = meander_counts(5, 10, 6, 0.3, 0.3, 3000)
+    sh = meander(a=5, b=10, h=6, w1=0.3, w2=0.3, ntri=3000, units=mm)
+    assert sh.nface == nt == 2840
+    r = setup_rwg(sh)
+    assert r.nbf == 3976
+    # every edge used by <= 2 faces, every face's edges distinct
+    assert all(len(set(sh.fe[:, f])) == 3 for f in range(sh.nface))
+
+
+def test_cascade_identities():
+    # test/GSMs_test.jl:17-95
+    c = cascade(GSM.identity(10, 20), GSM.identity(20, 15))
+    assert np.linalg.norm(c.s11) == np.linalg.norm(c.s22) == 0
+    off = ~np.eye(*c.s12.shape, dtype=bool)
+    assert (np.diag(c.s12) == 1).all() and (c.s12[off] == 0).all()
+    assert (np.diag(c.s21) == 1).all() and (c.s21[~np.eye(*c.s21.shape, dtype=bool)] == 0).all()
+    al, be = 0.35, math.sqrt(1 - 0.35 ** 2)
+    ga, de = 0.23, math.sqrt(1 - 0.23 ** 2)
+    a = GSM.identity(1, 1)
+    b = GSM.identity(1, 1)
+    b.s11[:] = b.s22[:] = ga
+    b.s12[:] = b.s21[:] = de
+    c = cascade(a, b)
+    D = 1 / (1 - a.s22[0, 0] * b.s11[0, 0])
+    assert abs(c.s11[0, 0] - (a.s11 + a.s12 * a.s21 * b.s11 / D)[0, 0]) <= 1e-16
+    assert abs(c.s12[0, 0] - (a.s12 * b.s12 / D)[0, 0]) <= 1e-16
+    a = GSM.identity(1, 1)
+    a.s11[:] = a.s22[:] = al
+    a.s12[:] = a.s21[:] = be
+    layer = Layer(width=Length(25, mm))
+    layer.gamma = np.array([1.0j])
+    prop = np.exp(-1.0j * 0.025)
+    b = a.copy()
+    cascade_layer(a, layer, 25)
+    cascade_layer(b, layer)
+    for x, y in ((a.s12, be * prop), (a.s22, al * prop ** 2), (b.s21, be * prop)):
+        assert abs(x[0, 0] - y) <= 1e-16

@@ -1,0 +1,160 @@
+"""Pin the CPU oracle to the golden values hard-coded in the reference's own tests.
+
+Reference tests (PSSFSS.jl v0.1.4): test/FillZY_test.jl, test/PGF_test.jl,
+test/full_test.jl.  The reference tolerances are kept as the assertion bound where the
+golden value itself is a truncated series (PGF), and tightened where the golden value was
+produced by the reference's own fill (FillZY): the restatement matches those to ~1e-13
+relative, so 1e-10 relative is asserted.
+"""
+import cmath
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+from pssfss_b200.elements import rectstrip
+from pssfss_b200.layers import Layer
+from pssfss_b200.rwg import setup_rwg
+from pssfss_b200.sheets import s1s2_to_b1b2
+from pssfss_b200.units import Length, inch, mil
+
+
+def _fillzy_case(cls):
+    FGHz = 2.0
+    wl_inch = 11.80285 / FGHz
+    k0 = 2 * math.pi / (wl_inch * 2.54 / 100)
+    layers = [Layer(), Layer(epsr=3.4, tandel=0.003, width=Length(1, mil)),
+              Layer(epsr=3.4, tandel=0.003, width=Length(1, mil))]
+    sheet = rectstrip(Nx=20, Ny=20, Lx=20, Ly=50, Px=100, Py=100, units=mil, **{"class": cls})
+    upm = sheet.units.units_per_meter
+    u = 0.5 * max(np.linalg.norm(sheet.beta1), np.linalg.norm(sheet.beta2)) * upm
+    rwg = setup_rwg(sheet)
+    Z, info = oracle.fill(k0, u, layers, 2, 0.0, 0.0, sheet, rwg)
+    return Z, info
+
+
+def test_fillz_golden():
+    # test/FillZY_test.jl:45-46 (reference tolerances 0.005 and 0.01 absolute)
+    Z, info = _fillzy_case("J")
+    assert info["converged"]
+    for (i, j), ref in (((20, 30), 0.8990238712012797 - 354.1682770720877j),
+                        ((100, 100), 110.95156005861463 - 37529.820828933574j)):
+        assert abs(Z[i - 1, j - 1] - ref) / abs(ref) < 1e-10
+
+
+def test_filly_golden():
+    # test/FillZY_test.jl:77-78 (reference tolerance 1e-4 absolute)
+    Y, info = _fillzy_case("M")
+    for (i, j), ref in (((20, 30), 1.2168396602563192e-6 - 0.02476973884018213j),
+                        ((100, 100), 2.2127855040521283e-6 - 3.5131557304457406j)):
+        assert abs(Y[i - 1, j - 1] - ref) / abs(ref) < 1e-10
+
+
+PGF_GOLD = {  # test/PGF_test.jl:126-129, 142-146
+    0.1: ((-232.15311689927114 - 10.286495939161526j, -11.778556545589899 - 160.87504453495308j),
+          (-5905.287097073966 - 116.24899221632135j, -65.290894751642 - 115.6027231717079j)),
+    0.9: ((-86.47040978143367 - 9.887172408455307j, 133.51945406766538 - 160.47675058617088j),
+          (-2516.511258383936 - 111.36619289656556j, 138.66489521333057 - 115.0436702287188j)),
+}
+
+
+def _pgf_setup():
+    FGHz = 2.0
+    inch2m = 2.54 / 100
+    k0 = 2 * math.pi / (11.80285 / FGHz * inch2m)
+    layers = [Layer(), Layer(width=Length(20, mil), epsr=3.6, tandel=0.0013, mur=5.0),
+              Layer(width=Length(10, mil), epsr=8.0, tandel=0.0013, mur=2.0),
+              Layer(width=Length(50, mil), epsr=2.6, tandel=0.0003), Layer()]
+    psi1, psi2 = 0.4, -0.6
+    s1 = np.array([1.14 * inch2m, 0.0])
+    s2 = np.array([0.5707, 0.9885]) * inch2m
+    b1, b2 = s1s2_to_b1b2(s1, s2)
+    b00 = (psi1 * b1 + psi2 * b2) / (2 * math.pi)
+    rho = np.array([2.0, 6.0]) / 1000 * inch2m
+    return k0, layers, psi1, psi2, s1, s2, b1, b2, b00, rho
+
+
+@pytest.mark.parametrize("ufact", [0.1, 0.9])
+def test_modal_series_golden(ufact):
+    # test/PGF_test.jl:157-171, relative tolerance 2e-4
+    k0, layers, psi1, psi2, s1, s2, b1, b2, b00, rho = _pgf_setup()
+    u = ufact * max(np.linalg.norm(b1), np.linalg.norm(b2))
+    for mag in (0, 1):
+        tb = oracle.modal_tables(mag, k0, u, psi1, psi2, layers, 2, b1, b2, b00)
+        g1, g2 = PGF_GOLD[ufact][mag]
+        assert abs(tb.sigma(1, rho) - g1) / abs(g1) < 2e-4
+        assert abs(tb.sigma(2, rho) - g2) / abs(g2) < 2e-4
+
+
+def test_full_pgf_u_invariance():
+    # test/PGF_test.jl:174-212: spectral + spatial parts are independent of u
+    k0, layers, psi1, psi2, s1, s2, b1, b2, b00, rho = _pgf_setup()
+    s = 2
+    out = []
+    for ufact in (0.1, 0.9):
+        u = ufact * max(np.linalg.norm(b1), np.linalg.norm(b2))
+        S1, S2 = oracle.jksums(u * rho, psi1, psi2, u * s1, u * s2, True)
+        te = oracle.modal_tables(0, k0, u, psi1, psi2, layers, s, b1, b2, b00)
+        tm = oracle.modal_tables(1, k0, u, psi1, psi2, layers, s, b1, b2, b00)
+        m1, m2 = te.sigma(1, rho), te.sigma(2, rho)
+        pm1, pm2 = tm.sigma(1, rho), tm.sigma(2, rho)
+        ls, ls1 = layers[s - 1], layers[s]
+        mut = 2 * ls.mur * ls1.mur / (ls.mur + ls1.mur)
+        eb = (ls.epsr + ls1.epsr) / 2
+
+        def c3(m1_, e1_, m2_, e2_):
+            w1 = k0 * k0 * m1_ * e1_ + u * u
+            w2 = k0 * k0 * m2_ * e2_ + u * u
+            return (m1_ * w2 + m2_ * w1) / (2 * (m1_ + m2_))
+
+        def d3(m1_, e1_, m2_, e2_):
+            w1 = k0 * k0 * m1_ * e1_ + u * u
+            w2 = k0 * k0 * m2_ * e2_ + u * u
+            num = m1_ * (w2 * (2 * e1_ + e2_) - w1 * e1_) + m2_ * (w1 * (2 * e2_ + e1_) - w2 * e2_)
+            return num / (2 * (m1_ + m2_) * (e1_ + e2_))
+
+        C3 = c3(ls.mur, ls.epsr, ls1.mur, ls1.epsr)
+        D3 = d3(ls.mur, ls.epsr, ls1.mur, ls1.epsr)
+        GA = mut * (m1 + u / (4 * math.pi) * (S1 + C3 / u ** 2 * S2))
+        GP = 1 / eb * (m2 + u / (4 * math.pi) * (S1 + D3 / u ** 2 * S2))
+        c3s = c3(ls.epsr, ls.mur, ls.epsr, ls.mur)
+        c3p = c3(ls1.epsr, ls1.mur, ls1.epsr, ls1.mur)
+        d3s = d3(ls.epsr, ls.mur, ls.epsr, ls.mur)
+        d3p = d3(ls1.epsr, ls1.mur, ls1.epsr, ls1.mur)
+        GF = -(pm1 + u * eb / math.pi * S1 + (c3s * ls.epsr + c3p * ls1.epsr) / (2 * math.pi * u) * S2)
+        GPsi = pm2 + u / (math.pi * mut) * S1 + (d3s / ls.mur + d3p / ls1.mur) / (2 * math.pi * u) * S2
+        out.append((GA, GP, GF, GPsi))
+    for a, b in zip(out[0], out[1]):
+        assert 2 * abs(b - a) / abs(a + b) < 2e-4
+
+
+def _grating(kP, nterms=30):
+    """Collin's strip-grating closed form (test/full_test.jl:27-42)."""
+    sum1, sum3 = 1.3862943611198906, 7.2123414189575710
+    x = kP / (4 * math.pi)
+    th = x * sum1 + x ** 3 / 6 * sum3
+    for n in range(1, nterms + 1):
+        a, b = x / (n - 0.5), x / n
+        th += math.asin(a) - (a + a ** 3 / 6) - (math.asin(b) - (b + b ** 3 / 6))
+    G = math.sin(th) * cmath.exp(1j * (-math.pi / 2 - th))
+    return G, 1 + G
+
+
+@pytest.mark.parametrize("cls", ["J", "M"])
+def test_strip_grating_analytic(cls):
+    # test/full_test.jl:65-93: full GSM within 0.01 (inf-norm) of the closed form
+    F = 0.8
+    r, t = _grating(2 * math.pi * F)
+    ex = {(1, 1): np.array([[r, 0], [0, -t]]), (2, 1): np.array([[t, 0], [0, -r]])}
+    ex[(2, 2)], ex[(1, 2)] = ex[(1, 1)], ex[(2, 1)]
+    period = 299792458.0 * 100 / 2.54 * 1e-9
+    Py, Ly = period, period / 2
+    Px = Lx = Ly / 10
+    Ny = 40
+    Nx = round(Ny * Lx / Ly)
+    sh = rectstrip(Px=Px, Py=Py, Lx=Lx, Ly=Ly, Nx=Nx, Ny=Ny, units=inch, **{"class": cls})
+    res = oracle.analyze([Layer(), sh, Layer()], F, {"θ": 0, "ϕ": 0})
+    g = res[0].gsm
+    for k in ex:
+        assert np.abs(g[k] - ex[k]).max() < 0.01
