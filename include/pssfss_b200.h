@@ -1,0 +1,118 @@
+/*
+ * pssfss_b200 -- C ABI of the B200 (sm_100a) periodic method-of-moments fill-and-solve
+ * library.  Plain pointers and sizes only; every entry point returns 0 on success or a
+ * negative code (message via pss_last_error()).  No entry point aborts or traps.
+ *
+ * Conventions (chosen so a Julia caller passes its arrays unchanged):
+ *   - index arrays are int64 with 1-based values, laid out column-major exactly like the
+ *     reference's Julia arrays (fv/fe are 3 x nface, bff 2 x nbf, ufpm nface x nface);
+ *   - complex numbers are interleaved (re, im) doubles;
+ *   - lengths in sheet units unless stated; wavenumbers in 1/m.
+ *
+ * Reference interfaces replaced (PSSFSS.jl v0.1.4):
+ *   pss_sheet_create   <- RWGSheet + RWGData fields used by the fill (src/Sheets.jl:19-58,
+ *                          src/RWG.jl:27-76); the J/K cache of Sheets.jl:35-47 lives on the
+ *                          device inside the sheet object, keyed as in FillZY.jl:97-99.
+ *   pss_partial_gsms   <- the hot body of calculate_jtype_gsm / calculate_mtype_gsm
+ *                          (src/PSSFSS.jl:391-457, 516-584): fillz/filly (src/FillZY.jl:50,273),
+ *                          lu! (PSSFSS.jl:401,526), rwgbfft! (src/RWG.jl:428), ldiv!
+ *                          (PSSFSS.jl:439,566) and the modal projection (Eqs. 6.18/6.37),
+ *                          batched over all frequency / steering points of a sweep.
+ *   pss_fill_matrix    <- fillz / filly alone (src/FillZY.jl:50-245, 273-457).
+ *   pss_modal_tables   <- electric_/magnetic_modal_sum_funcs tables (src/PGF.jl:196, 478).
+ *   pss_face_integrals <- filljk! (src/Zint.jl:117-242).
+ *   pss_lu_solve       <- lu! followed by ldiv! on a caller matrix (LinearAlgebra).
+ */
+#ifndef PSSFSS_B200_H
+#define PSSFSS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct pss_ctx pss_ctx;
+typedef struct pss_sheet pss_sheet;
+
+/* precision of the dense solve */
+#define PSS_FP64 0        /* complex128 LU and solves */
+#define PSS_FP32_REFINE 1 /* complex64 LU, FP64 residuals and iterative refinement */
+
+/* per-point status bits */
+#define PSS_STATUS_TABLE_NOCONV 1   /* modal tables reached mmax = 2048 (PGF.jl:300 warning) */
+#define PSS_STATUS_JK_NOCONV 2      /* a spatial lattice sum reached 65 rings (PGF.jl:104) */
+#define PSS_STATUS_SINGULAR 4       /* exactly zero pivot */
+#define PSS_STATUS_REFINE_NOCONV 8  /* refinement stopped before its tolerance */
+#define PSS_STATUS_NONFINITE 16     /* NaN or Inf in the solution */
+#define PSS_STATUS_FP64_FALLBACK 32 /* PSS_FP32_REFINE only: refinement stalled (cond(Z) too
+                                       large for FP32 factors), point recomputed in FP64 */
+
+const char *pss_last_error(void);
+int pss_version(void);
+/* Total number of CUDA kernels this library has launched in the process so far. */
+int64_t pss_kernel_launches(void);
+
+/* One context per device; nworkers CUDA streams process frequency points concurrently. */
+int pss_ctx_create(int device, int nworkers, pss_ctx **out);
+int pss_ctx_destroy(pss_ctx *ctx);
+
+/* Upload a triangulated sheet and its basis-function topology.
+ * cls: 'J' (conductor, fillz) or 'M' (aperture, filly).  s1, s2, beta1, beta2 in sheet
+ * units (and 1/sheet units); rho: 2 x nnode; fv, fe: 3 x nface (fe[k] opposite fv[k]);
+ * fr: nface sheet resistances (ohm/sq); bff: 2 x nbf plus/minus faces; ebf, eci: nedge;
+ * ufpm: nface x nface unique-face-pair class numbers (match index fastest);
+ * ufp_rep: nufp column-major face-pair index of each class's first member. */
+int pss_sheet_create(pss_ctx *ctx, char cls, double units_per_meter, const double *s1, const double *s2,
+                     const double *beta1, const double *beta2, int64_t nnode, const double *rho,
+                     int64_t nface, const int64_t *fv, const int64_t *fe, const double *fr, int64_t nedge,
+                     int64_t nbf, const int64_t *bff, const int64_t *ebf, const int64_t *eci, int64_t nufp,
+                     const int64_t *ufpm, const int64_t *ufp_rep, pss_sheet **out);
+int pss_sheet_destroy(pss_sheet *sheet);
+
+/* Scattered part of the sheet's partial GSM at npts points.
+ * Region layers: nl layers, eps/mu complex (2*nl doubles), width in metres; s = 1-based
+ * interface of the sheet; u = smoothing parameter (1/m).
+ * Per point i: k0[i] (1/m), psi[2i], psi[2i+1] (rad).  Per point and mode j
+ * (nmodes, region-1 modes first): kvec[(i*nmodes+j)*2 + 0..1] (1/m), src (2 complex),
+ * tobs (2 real), wobs (1 complex) such that
+ *     rhs[n, j] = conj(F_j[n]) . src_j,   Z x = rhs,
+ *     dS[i][a + b*nmodes] = wobs_a * sum_n (tobs_a . F_a[n]) x[n, b],
+ * where F_j is the basis-function transform at kvec_j (RWG.jl:428).  dS: npts *
+ * nmodes^2 complex (column-major per point); status: npts (PSS_STATUS_* bits). */
+int pss_partial_gsms(pss_sheet *sheet, int nl, const double *eps, const double *mu, const double *width,
+                     int s, double u, int npts, const double *k0, const double *psi, int nmodes,
+                     const double *kvec, const double *src, const double *tobs, const double *wobs,
+                     int precision, double *dS, int *status);
+
+/* The MoM matrix of one point: Z (nbf x nbf complex, column-major like zorymat). */
+int pss_fill_matrix(pss_sheet *sheet, int nl, const double *eps, const double *mu, const double *width, int s,
+                    double u, double k0, double psi1, double psi2, double *Z, int *mmax_out);
+
+/* Padded modal tables (capacity cap entries each, (mmax+2)^2 used, column-major). */
+int pss_modal_tables(pss_ctx *ctx, int magnetic, int nl, const double *eps, const double *mu,
+                     const double *width, int s, double k0, double u, double psi1, double psi2,
+                     const double *b1, const double *b2, double convtest, int64_t cap, double *t1,
+                     double *t2, int *mmax_out, int *status);
+
+/* Frequency-independent face-pair integrals of every unique pair (ulocal in 1/sheet units).
+ * Outputs (nufp entries each): J, Jxi, Jeta, K, Kxi, Keta complex; rho_r 2*nufp; rinv. */
+int pss_face_integrals(pss_sheet *sheet, double ulocal, double psi1, double psi2, double *J, double *Jxi,
+                       double *Jeta, double *K, double *Kxi, double *Keta, double *rho_r, double *rinv,
+                       int *nonconv);
+
+/* Basis-function transforms at nmodes transform variables: F (nmodes x nbf x 2 complex). */
+int pss_basis_transforms(pss_sheet *sheet, int nmodes, const double *kvec, double psi1, double psi2, double *F);
+
+/* Solve Z X = B with Z n x n complex column-major, B/X n x nrhs column-major. */
+int pss_lu_solve(pss_ctx *ctx, int n, const double *Z, int nrhs, const double *B, int precision, double *X,
+                 int *status);
+
+/* Accumulated per-phase device milliseconds of the last pss_partial_gsms call on worker 0:
+ * [tables, face_integrals, fill, factor, transforms+rhs, solve+refine, projection, total]. */
+int pss_last_timings(pss_ctx *ctx, double *ms8);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

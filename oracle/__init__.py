@@ -255,7 +255,8 @@ def partial_dS(sheet, rwg, region, s, k0, u, io):
 def analyze(strata, flist, steering):
     """Oracle ``analyze`` (PSSFSS.jl:114-334): the package's host plan and cascade with the
     hot path (fill, LU/solve, transforms, projection) done by this restatement."""
-    from pssfss_b200 import analyze as A
+    import importlib
+    A = importlib.import_module("pssfss_b200.analyze")
     plan = A.make_plan(strata, flist, steering)
     partial = {}
     for ig, (i1, i2), isht, s in A.sheet_gblocks(plan):

@@ -1,0 +1,862 @@
+// C ABI of the library: contexts, device-resident sheets and the batched sweep.
+//
+// pss_partial_gsms is the drop-in for the hot body of calculate_jtype_gsm /
+// calculate_mtype_gsm (PSSFSS.jl:391-457, 516-584) over a whole sweep:
+//   1. modal tables of every point (K1; the only phase with host synchronisation, to
+//      read back each point's mmax);
+//   2. the J/K face-pair integrals (K2) when (ψ1, ψ2, u) differ from the cached key
+//      (FillZY.jl:97-99): once per sweep at normal incidence or fixed ψ, per point for
+//      θ steering;
+//   3. per point on one of nworkers CUDA streams: pair terms (K3a), gather assembly (K3b),
+//      LU (K4), basis transforms and right-hand sides (K6), solves (K5) with FP64
+//      iterative refinement in the FP32 form, modal projection (K6);
+//   4. one synchronisation, then dS and status are copied to the caller.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstring>
+#include <vector>
+
+#include "pss_internal.cuh"
+#include "pssfss_b200.h"
+
+#include <atomic>
+
+static thread_local char g_err[1024];
+static std::atomic<long long> g_launches{0};
+
+void pss_count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+void pss_set_error(const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+namespace {
+
+constexpr int kRing0 = 160;  // ring budget of the first table pass (mmax <= 320)
+constexpr int kTableChunk = 16;
+constexpr int kMaxRefine = 40;  // steps after convergence are no-ops (device flag)
+constexpr double kRefineTol = 1e-13;
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t n = 0;
+  int ensure(size_t bytes) {
+    if (bytes <= n) return 0;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    if (bytes == 0) return 0;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+      pss_set_error("cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+      p = nullptr;
+      return -3;
+    }
+    n = bytes;
+    return 0;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  template <class T>
+  T *as() const { return (T *)p; }
+};
+
+struct JKBufs {
+  DevBuf buf;
+  JKDev jk{};
+  int ensure(int nufp) {
+    size_t c = (size_t)nufp * sizeof(cd), d = (size_t)nufp * sizeof(double);
+    if (buf.ensure(6 * c + 3 * d + 64)) return -3;
+    char *b = (char *)buf.p;
+    jk.J = (cd *)b; jk.Jxi = (cd *)(b + c); jk.Jeta = (cd *)(b + 2 * c);
+    jk.K = (cd *)(b + 3 * c); jk.Kxi = (cd *)(b + 4 * c); jk.Keta = (cd *)(b + 5 * c);
+    jk.rho_r = (double *)(b + 6 * c);
+    jk.rinv = (double *)(b + 6 * c + 2 * d);
+    return 0;
+  }
+};
+
+struct Worker {
+  cudaStream_t st = nullptr;
+  DevBuf zb, z64, zr, zi, ipiv, info, bf, rhs, X, R, norms, done, nonconv;
+  JKBufs jk;
+};
+
+__global__ void k_info_to_status(int *info, int *status) {
+  if (*info) *status |= PSS_ST_SINGULAR;
+  *info = 0;
+}
+__global__ void k_nonconv_to_status(int *nonconv, int *status) {
+  if (*nonconv) *status |= PSS_ST_JK_NOCONV;
+  *nonconv = 0;
+}
+
+// c3_calc / d3_calc (PGF.jl:138-162)
+cd c3_calc(double k0, double u, cd mu1, cd eps1, cd mu2, cd eps2) {
+  cd w1 = ((k0 * k0) * mu1) * eps1 + mkcd(u * u, 0);
+  cd w2 = ((k0 * k0) * mu2) * eps2 + mkcd(u * u, 0);
+  return (mu1 * w2 + mu2 * w1) / (2.0 * (mu1 + mu2));
+}
+cd d3_calc(double k0, double u, cd mu1, cd eps1, cd mu2, cd eps2) {
+  cd w1 = ((k0 * k0) * mu1) * eps1 + mkcd(u * u, 0);
+  cd w2 = ((k0 * k0) * mu2) * eps2 + mkcd(u * u, 0);
+  cd num = mu1 * (w2 * (2.0 * eps1 + eps2) - w1 * eps1) + mu2 * (w1 * (2.0 * eps2 + eps1) - w2 * eps2);
+  return num / ((2.0 * (mu1 + mu2)) * (eps1 + eps2));
+}
+cd hcis(double a) { return mkcd(std::cos(a), std::sin(a)); }
+
+}  // namespace
+
+struct pss_ctx {
+  int device = 0;
+  int nworkers = 1;
+  std::vector<Worker> w;
+  DevBuf params, dense, conv, mm, stage, tables, bigdense, modes, dS, status;
+  std::vector<DevBuf> bigtables;
+  double last_ms[8] = {0};
+};
+
+struct pss_sheet {
+  pss_ctx *ctx = nullptr;
+  char cls = 'J';
+  double upm = 1.0;
+  double s1[2], s2[2], b1[2], b2[2];
+  int nnode = 0, nface = 0, nbf = 0, nufp = 0;
+  DevBuf rho, fv, ufpm, rep, fr, ls, a48, inc_cnt, inc_face, inc_loc, inc_sgn, inc_eci;
+  SheetDev G{};
+  JKBufs cache;
+  bool jk_valid = false;
+  double jk_psi1 = 0, jk_psi2 = 0, jk_u = 0;
+  int jk_nonconv = 0;
+};
+
+namespace {
+
+int set_device(pss_ctx *c) {
+  PSS_CUDA_TRY(cudaSetDevice(c->device));
+  return 0;
+}
+
+template <class T>
+int upload(DevBuf &b, const T *h, size_t n) {
+  if (b.ensure(std::max<size_t>(n, 1) * sizeof(T))) return -3;
+  if (n) PSS_CUDA_TRY(cudaMemcpy(b.p, h, n * sizeof(T), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+int make_stack(int nl, const double *eps, const double *mu, const double *width, int s, StackParams &S) {
+  if (nl < 2 || nl > PSS_MAXLAYERS) { pss_set_error("layer count %d outside 2..%d", nl, PSS_MAXLAYERS); return -1; }
+  if (s < 1 || s >= nl) { pss_set_error("interface %d outside 1..%d", s, nl - 1); return -1; }
+  S.nl = nl;
+  S.s = s;
+  for (int i = 0; i < nl; ++i) {
+    S.eps[i] = mkcd(eps[2 * i], eps[2 * i + 1]);
+    S.mu[i] = mkcd(mu[2 * i], mu[2 * i + 1]);
+    S.width[i] = width[i];
+    if (!std::isfinite(eps[2 * i]) || !std::isfinite(eps[2 * i + 1]) || !std::isfinite(mu[2 * i]) ||
+        !std::isfinite(mu[2 * i + 1]) || !std::isfinite(width[i])) {
+      pss_set_error("non-finite layer parameter in layer %d", i + 1);
+      return -1;
+    }
+  }
+  return 0;
+}
+
+// Per-point scalars: FillZY.jl:60-77 / 282-322 and PGF.jl:202-210 / 483-499.
+void make_params(int magnetic, const StackParams &S, const double b1m[2], const double b2m[2], double u,
+                 double k0, double psi1, double psi2, PointParams &P) {
+  memset(&P, 0, sizeof(P));
+  P.magnetic = magnetic;
+  P.k0 = k0;
+  P.u = u;
+  P.psi1 = psi1;
+  P.psi2 = psi2;
+  P.omega = k0 * PSS_C0;
+  for (int d = 0; d < 2; ++d) {
+    P.b1[d] = b1m[d];
+    P.b2[d] = b2m[d];
+    P.b00[d] = (psi1 * b1m[d] + psi2 * b2m[d]) / PSS_TWOPI;
+  }
+  double cr = b1m[0] * b2m[1] - b1m[1] * b2m[0];
+  P.area = 4.0 * (PSS_PI * PSS_PI) / std::fabs(cr);
+  P.k0sq = k0 * k0;
+  P.b2min = 1e-10 * P.k0sq;
+  const int s = S.s;
+  cd mus = S.mu[s - 1], mus1 = S.mu[s], epss = S.eps[s - 1], epss1 = S.eps[s];
+  P.mutilde = ((2.0 * mus) * mus1) / (mus + mus1);
+  P.epsbar = (epss + epss1) / 2.0;
+  if (!magnetic) {
+    P.c3 = c3_calc(k0, u, mus, epss, mus1, epss1);
+    P.d3 = d3_calc(k0, u, mus, epss, mus1, epss1);
+  } else {
+    cd c3s = c3_calc(k0, u, epss, mus, epss, mus);
+    cd c3sp1 = c3_calc(k0, u, epss1, mus1, epss1, mus1);
+    cd d3s = d3_calc(k0, u, epss, mus, epss, mus);
+    cd d3sp1 = d3_calc(k0, u, epss1, mus1, epss1, mus1);
+    P.f1 = 2.0 * P.epsbar;
+    P.f3 = epss * c3s + epss1 * c3sp1;
+    P.p1 = mkcd(2.0, 0) / P.mutilde;
+    P.p3 = d3s / mus + d3sp1 / mus1;
+    cd fc3s = c3_calc(k0, u, mus, epss, mus, epss);
+    cd fc3sp1 = c3_calc(k0, u, mus1, epss1, mus1, epss1);
+    cd fd3s = d3_calc(k0, u, mus, epss, mus, epss);
+    cd fd3sp1 = d3_calc(k0, u, mus1, epss1, mus1, epss1);
+    P.I1fact = mkcd(PSS_PI, 0) / P.epsbar;
+    P.KFfact = (fc3s * epss + fc3sp1 * epss1) / (u * (2.0 * P.epsbar));
+    P.I2fact = PSS_PI * P.mutilde;
+    P.KPfact = (P.mutilde / (2 * u)) * (fd3s / mus + fd3sp1 / mus1);
+  }
+  P.ff[0] = P.ff[1] = P.ff[3] = mkcd(1, 0);
+  P.ff[2] = hcis(-psi1);
+  P.ff[4] = hcis(-psi2);
+}
+
+// Tables of npts points (params already on the device at dP).  Fills tabs[i] and ORs
+// PSS_ST_TABLE_NOCONV into hstatus[i].  Synchronises the ctx's first stream.
+int build_tables(pss_ctx *c, const StackParams &S, const PointParams *dP, int npts, double convtest,
+                 std::vector<TableDev> &tabs, std::vector<int> &hstatus) {
+  cudaStream_t st = c->w[0].st;
+  const int R0 = kRing0;
+  const size_t W0 = 2 * (size_t)R0 + 1;
+  const size_t pstride = 2 * W0 * W0;
+  const int chunk = std::min(npts, kTableChunk);
+  const size_t cap0 = (size_t)(2 * R0 + 2) * (2 * R0 + 2);
+  if (c->dense.ensure((size_t)chunk * pstride * sizeof(cd))) return -3;
+  if (c->conv.ensure((size_t)chunk * (R0 + 1) + 64)) return -3;
+  if (c->mm.ensure(2 * sizeof(int) * (size_t)chunk + 64)) return -3;
+  if (c->stage.ensure(2 * (size_t)(2 * R0) * (2 * R0) * sizeof(cd))) return -3;
+  if (c->tables.ensure((size_t)npts * 2 * cap0 * sizeof(cd))) return -3;
+  c->bigtables.resize(npts);
+  tabs.assign(npts, TableDev{});
+  std::vector<int> hm(2 * chunk);
+  for (int c0 = 0; c0 < npts; c0 += chunk) {
+    const int nc = std::min(chunk, npts - c0);
+    int *dmm = c->mm.as<int>();
+    pss_tables_ring_fill(S, dP + c0, nc, R0, c->dense.as<cd>(), pstride, st);
+    pss_tables_ring_sums(dP + c0, nc, R0, c->dense.as<cd>(), pstride, convtest, c->conv.as<unsigned char>(), st);
+    pss_tables_find_mmax(nc, R0, c->conv.as<unsigned char>(), dmm, dmm + chunk, st);
+    PSS_CUDA_TRY(cudaMemcpyAsync(hm.data(), dmm, 2 * chunk * sizeof(int), cudaMemcpyDeviceToHost, st));
+    PSS_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int q = 0; q < nc; ++q) {
+      const int i = c0 + q;
+      int mmax = hm[q], flag = hm[chunk + q];
+      if (flag == 2) {
+        // rings beyond the first budget: full-size pass for this point only
+        const int R1 = PSS_MMAX_CAP / 2;
+        const size_t W1 = 2 * (size_t)R1 + 1;
+        if (c->bigdense.ensure(2 * W1 * W1 * sizeof(cd))) return -3;
+        if (c->conv.ensure((size_t)(R1 + 1) + 64)) return -3;
+        pss_tables_ring_fill(S, dP + i, 1, R1, c->bigdense.as<cd>(), 0, st);
+        pss_tables_ring_sums(dP + i, 1, R1, c->bigdense.as<cd>(), 0, convtest, c->conv.as<unsigned char>(), st);
+        pss_tables_find_mmax(1, R1, c->conv.as<unsigned char>(), dmm, dmm + 1, st);
+        int h2[2];
+        PSS_CUDA_TRY(cudaMemcpyAsync(h2, dmm, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+        PSS_CUDA_TRY(cudaStreamSynchronize(st));
+        mmax = h2[0];
+        if (h2[1] == 1) hstatus[i] |= PSS_ST_TABLE_NOCONV;
+        size_t cap = pss_table_cap(mmax);
+        if (c->bigtables[i].ensure(2 * cap * sizeof(cd))) return -3;
+        if (c->stage.ensure(2 * (size_t)mmax * mmax * sizeof(cd))) return -3;
+        tabs[i].t1 = c->bigtables[i].as<cd>();
+        tabs[i].t2 = tabs[i].t1 + cap;
+        tabs[i].mmax = mmax;
+        int rc = pss_tables_finish(c->bigdense.as<cd>(), R1, mmax, dP + i, c->stage.as<cd>(), tabs[i].t1,
+                                   tabs[i].t2, st);
+        if (rc) return rc;
+        continue;
+      }
+      if (flag == 1) hstatus[i] |= PSS_ST_TABLE_NOCONV;
+      tabs[i].t1 = c->tables.as<cd>() + (size_t)i * 2 * cap0;
+      tabs[i].t2 = tabs[i].t1 + cap0;
+      tabs[i].mmax = mmax;
+      int rc = pss_tables_finish(c->dense.as<cd>() + (size_t)q * pstride, R0, mmax, dP + i, c->stage.as<cd>(),
+                                 tabs[i].t1, tabs[i].t2, st);
+      if (rc) return rc;
+    }
+  }
+  PSS_CUDA_TRY(cudaStreamSynchronize(st));
+  return 0;
+}
+
+bool jk_key_stale(const pss_sheet *sh, double psi1, double psi2, double ulocal) {
+  return !sh->jk_valid || psi1 != sh->jk_psi1 || psi2 != sh->jk_psi2 || sh->jk_u == 0 ||
+         std::fabs((ulocal - sh->jk_u) / sh->jk_u) > 1e-4;
+}
+
+int refresh_jk_cache(pss_sheet *sh, double psi1, double psi2, double ulocal, cudaStream_t st) {
+  if (!jk_key_stale(sh, psi1, psi2, ulocal)) return 0;
+  if (sh->cache.ensure(sh->nufp)) return -3;
+  DevBuf nc;
+  if (nc.ensure(sizeof(int))) return -3;
+  PSS_CUDA_TRY(cudaMemsetAsync(nc.p, 0, sizeof(int), st));
+  pss_filljk(sh->G, ulocal, psi1, psi2, sh->s1, sh->s2, sh->cache.jk, nc.as<int>(), st);
+  int h = 0;
+  PSS_CUDA_TRY(cudaMemcpyAsync(&h, nc.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  PSS_CUDA_TRY(cudaStreamSynchronize(st));
+  nc.release();
+  sh->jk_valid = true;
+  sh->jk_psi1 = psi1;
+  sh->jk_psi2 = psi2;
+  sh->jk_u = ulocal;
+  sh->jk_nonconv = h;
+  return 0;
+}
+
+int ensure_worker(Worker &w, const pss_sheet *sh, int nm, int precision, bool own_jk) {
+  const size_t n = sh->nbf;
+  if (w.zb.ensure((size_t)sh->nufp * 9 * sizeof(cd))) return -3;
+  if (w.z64.ensure(n * n * sizeof(cd))) return -3;
+  if (precision == PSS_FP32_REFINE) {
+    if (w.zr.ensure(n * n * sizeof(float)) || w.zi.ensure(n * n * sizeof(float))) return -3;
+  }
+  if (w.ipiv.ensure(n * sizeof(int)) || w.info.ensure(sizeof(int)) || w.nonconv.ensure(sizeof(int))) return -3;
+  if (w.bf.ensure((size_t)nm * n * 2 * sizeof(cd))) return -3;
+  if (w.rhs.ensure((size_t)nm * n * sizeof(cd)) || w.X.ensure((size_t)nm * n * sizeof(cd)) ||
+      w.R.ensure((size_t)nm * n * sizeof(cd)))
+    return -3;
+  if (w.norms.ensure(2 * sizeof(double)) || w.done.ensure(sizeof(int))) return -3;
+  if (own_jk && w.jk.ensure(sh->nufp)) return -3;
+  PSS_CUDA_TRY(cudaMemsetAsync(w.info.p, 0, sizeof(int), w.st));
+  PSS_CUDA_TRY(cudaMemsetAsync(w.nonconv.p, 0, sizeof(int), w.st));
+  return 0;
+}
+
+}  // namespace
+
+size_t pss_table_cap(int mmax) { return (size_t)(mmax + 2) * (mmax + 2); }
+
+extern "C" {
+
+const char *pss_last_error(void) { return g_err; }
+int pss_version(void) { return 100; }
+int64_t pss_kernel_launches(void) { return (int64_t)g_launches.load(); }
+
+int pss_ctx_create(int device, int nworkers, pss_ctx **out) {
+  if (!out) { pss_set_error("null output pointer"); return -1; }
+  *out = nullptr;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) {
+    pss_set_error("no CUDA device available: %s", cudaGetErrorString(e));
+    return -3;
+  }
+  if (device < 0 || device >= ndev) { pss_set_error("device %d outside 0..%d", device, ndev - 1); return -1; }
+  pss_ctx *c = new pss_ctx();
+  c->device = device;
+  c->nworkers = std::max(1, std::min(nworkers, 16));
+  if (set_device(c)) { delete c; return -3; }
+  c->w.resize(c->nworkers);
+  for (auto &w : c->w) {
+    if (cudaStreamCreateWithFlags(&w.st, cudaStreamNonBlocking) != cudaSuccess) {
+      pss_set_error("cudaStreamCreate failed");
+      delete c;
+      return -3;
+    }
+  }
+  *out = c;
+  return 0;
+}
+
+int pss_ctx_destroy(pss_ctx *c) {
+  if (!c) return 0;
+  cudaSetDevice(c->device);
+  cudaDeviceSynchronize();
+  for (auto &w : c->w) {
+    for (DevBuf *b : {&w.zb, &w.z64, &w.zr, &w.zi, &w.ipiv, &w.info, &w.bf, &w.rhs, &w.X, &w.R, &w.norms, &w.done,
+                      &w.nonconv})
+      b->release();
+    w.jk.buf.release();
+    if (w.st) cudaStreamDestroy(w.st);
+  }
+  for (DevBuf *b : {&c->params, &c->dense, &c->conv, &c->mm, &c->stage, &c->tables, &c->bigdense, &c->modes,
+                    &c->dS, &c->status})
+    b->release();
+  for (auto &b : c->bigtables) b.release();
+  delete c;
+  return 0;
+}
+
+int pss_sheet_create(pss_ctx *ctx, char cls, double units_per_meter, const double *s1, const double *s2,
+                     const double *beta1, const double *beta2, int64_t nnode, const double *rho,
+                     int64_t nface, const int64_t *fv, const int64_t *fe, const double *fr, int64_t nedge,
+                     int64_t nbf, const int64_t *bff, const int64_t *ebf, const int64_t *eci, int64_t nufp,
+                     const int64_t *ufpm, const int64_t *ufp_rep, pss_sheet **out) {
+  if (!ctx || !out) { pss_set_error("null argument"); return -1; }
+  *out = nullptr;
+  if (cls != 'J' && cls != 'M') { pss_set_error("sheet class must be 'J' or 'M'"); return -1; }
+  if (nface <= 0 || nbf <= 0 || nnode <= 0 || nufp <= 0 || nface > 46000 || nbf > 100000) {
+    pss_set_error("invalid sizes nnode=%lld nface=%lld nbf=%lld nufp=%lld", (long long)nnode, (long long)nface,
+                  (long long)nbf, (long long)nufp);
+    return -1;
+  }
+  if (!(units_per_meter > 0)) { pss_set_error("units_per_meter must be positive"); return -1; }
+  if (set_device(ctx)) return -3;
+  pss_sheet *sh = new pss_sheet();
+  sh->ctx = ctx;
+  sh->cls = cls;
+  sh->upm = units_per_meter;
+  for (int d = 0; d < 2; ++d) {
+    sh->s1[d] = s1[d]; sh->s2[d] = s2[d]; sh->b1[d] = beta1[d]; sh->b2[d] = beta2[d];
+  }
+  sh->nnode = (int)nnode; sh->nface = (int)nface; sh->nbf = (int)nbf; sh->nufp = (int)nufp;
+  // host conversion to 0-based int32 + validation
+  std::vector<int> hfv(3 * nface);
+  for (int64_t i = 0; i < 3 * nface; ++i) {
+    if (fv[i] < 1 || fv[i] > nnode) { pss_set_error("fv[%lld] out of range", (long long)i); delete sh; return -1; }
+    hfv[i] = (int)(fv[i] - 1);
+    if (fe[i] < 1 || fe[i] > nedge) { pss_set_error("fe[%lld] out of range", (long long)i); delete sh; return -1; }
+  }
+  std::vector<int> hufpm((size_t)nface * nface);
+  for (size_t i = 0; i < hufpm.size(); ++i) {
+    if (ufpm[i] < 1 || ufpm[i] > nufp) { pss_set_error("ufpm entry out of range"); delete sh; return -1; }
+    hufpm[i] = (int)(ufpm[i] - 1);
+  }
+  std::vector<int> hrep(nufp);
+  for (int64_t i = 0; i < nufp; ++i) {
+    if (ufp_rep[i] < 1 || ufp_rep[i] > nface * nface) { pss_set_error("ufp_rep out of range"); delete sh; return -1; }
+    hrep[i] = (int)(ufp_rep[i] - 1);
+  }
+  // basis-function incidences: (face, local edge, sign, edge code), fixed order
+  std::vector<int> icnt(nbf, 0), iface(4 * nbf, 0), iloc(4 * nbf, 0), isgn(4 * nbf, 0), ieci(4 * nbf, 0);
+  for (int64_t f = 0; f < nface; ++f)
+    for (int k = 0; k < 3; ++k) {
+      int64_t e = fe[3 * f + k];
+      int64_t b = ebf[e - 1];
+      if (b == 0) continue;
+      if (b < 1 || b > nbf) { pss_set_error("ebf entry out of range"); delete sh; return -1; }
+      int sgn;
+      if (bff[2 * (b - 1)] - 1 == f) sgn = 1;
+      else if (bff[2 * (b - 1) + 1] - 1 == f) sgn = -1;
+      else { pss_set_error("Impossible situation in edge loop (face %lld, bf %lld)", (long long)f + 1, (long long)b); delete sh; return -1; }
+      int &cnt = icnt[b - 1];
+      if (cnt >= 4) { pss_set_error("basis function %lld has more than 4 face incidences", (long long)b); delete sh; return -1; }
+      int64_t code = eci[e - 1];
+      if (code < 0 || code > 4) { pss_set_error("eci entry out of range"); delete sh; return -1; }
+      iface[4 * (b - 1) + cnt] = (int)f;
+      iloc[4 * (b - 1) + cnt] = k;
+      isgn[4 * (b - 1) + cnt] = sgn;
+      ieci[4 * (b - 1) + cnt] = (int)code;
+      ++cnt;
+    }
+  // per-face edge lengths (m) and 48|area| (m^2) for the surface-resistance terms
+  std::vector<double> hls(3 * nface), ha48(nface);
+  for (int64_t f = 0; f < nface; ++f) {
+    double r[3][2];
+    for (int k = 0; k < 3; ++k) {
+      int64_t v = fv[3 * f + k] - 1;
+      r[k][0] = rho[2 * v] / units_per_meter;
+      r[k][1] = rho[2 * v + 1] / units_per_meter;
+    }
+    double a32x = r[2][0] - r[1][0], a32y = r[2][1] - r[1][1];
+    double a12x = r[0][0] - r[1][0], a12y = r[0][1] - r[1][1];
+    double a13x = r[0][0] - r[2][0], a13y = r[0][1] - r[2][1];
+    hls[3 * f] = std::sqrt(a32x * a32x + a32y * a32y);
+    hls[3 * f + 1] = std::sqrt(a13x * a13x + a13y * a13y);
+    hls[3 * f + 2] = std::sqrt(a12x * a12x + a12y * a12y);
+    ha48[f] = 48 * std::fabs(0.5 * (a32x * a12y - a32y * a12x));
+  }
+  std::vector<double> hfr(fr, fr + nface);
+  int rc = 0;
+  rc |= upload(sh->rho, rho, 2 * (size_t)nnode);
+  rc |= upload(sh->fv, hfv.data(), hfv.size());
+  rc |= upload(sh->ufpm, hufpm.data(), hufpm.size());
+  rc |= upload(sh->rep, hrep.data(), hrep.size());
+  rc |= upload(sh->fr, hfr.data(), hfr.size());
+  rc |= upload(sh->ls, hls.data(), hls.size());
+  rc |= upload(sh->a48, ha48.data(), ha48.size());
+  rc |= upload(sh->inc_cnt, icnt.data(), icnt.size());
+  rc |= upload(sh->inc_face, iface.data(), iface.size());
+  rc |= upload(sh->inc_loc, iloc.data(), iloc.size());
+  rc |= upload(sh->inc_sgn, isgn.data(), isgn.size());
+  rc |= upload(sh->inc_eci, ieci.data(), ieci.size());
+  if (rc) { delete sh; return -3; }
+  SheetDev &G = sh->G;
+  G.nface = sh->nface; G.nbf = sh->nbf; G.nufp = sh->nufp; G.nnode = sh->nnode; G.upm = units_per_meter;
+  G.rho = sh->rho.as<double>(); G.fv = sh->fv.as<int>(); G.ufpm = sh->ufpm.as<int>(); G.ufp_rep = sh->rep.as<int>();
+  G.fr = sh->fr.as<double>(); G.face_ls = sh->ls.as<double>(); G.face_a48 = sh->a48.as<double>();
+  G.inc_cnt = sh->inc_cnt.as<int>(); G.inc_face = sh->inc_face.as<int>(); G.inc_loc = sh->inc_loc.as<int>();
+  G.inc_sgn = sh->inc_sgn.as<int>(); G.inc_eci = sh->inc_eci.as<int>();
+  *out = sh;
+  return 0;
+}
+
+int pss_sheet_destroy(pss_sheet *sh) {
+  if (!sh) return 0;
+  cudaSetDevice(sh->ctx->device);
+  cudaDeviceSynchronize();
+  for (DevBuf *b : {&sh->rho, &sh->fv, &sh->ufpm, &sh->rep, &sh->fr, &sh->ls, &sh->a48, &sh->inc_cnt,
+                    &sh->inc_face, &sh->inc_loc, &sh->inc_sgn, &sh->inc_eci})
+    b->release();
+  sh->cache.buf.release();
+  delete sh;
+  return 0;
+}
+
+int pss_partial_gsms(pss_sheet *sh, int nl, const double *eps, const double *mu, const double *width, int s,
+                     double u, int npts, const double *k0, const double *psi, int nmodes, const double *kvec,
+                     const double *src, const double *tobs, const double *wobs, int precision, double *dS,
+                     int *status) {
+  if (!sh || !k0 || !psi || !dS || !status) { pss_set_error("null argument"); return -1; }
+  if (npts <= 0 || nmodes <= 0 || nmodes > 4096) { pss_set_error("invalid npts/nmodes"); return -1; }
+  if (precision != PSS_FP64 && precision != PSS_FP32_REFINE) { pss_set_error("unknown precision %d", precision); return -1; }
+  if (!(u > 0)) { pss_set_error("smoothing parameter u must be positive"); return -1; }
+  pss_ctx *c = sh->ctx;
+  if (set_device(c)) return -3;
+  StackParams S;
+  if (make_stack(nl, eps, mu, width, s, S)) return -1;
+  const int magnetic = sh->cls == 'M';
+  const double b1m[2] = {sh->b1[0] * sh->upm, sh->b1[1] * sh->upm};
+  const double b2m[2] = {sh->b2[0] * sh->upm, sh->b2[1] * sh->upm};
+  std::vector<PointParams> hP(npts);
+  for (int i = 0; i < npts; ++i) {
+    if (!(k0[i] > 0) || !std::isfinite(psi[2 * i]) || !std::isfinite(psi[2 * i + 1])) {
+      pss_set_error("invalid k0/psi at point %d", i);
+      return -1;
+    }
+    make_params(magnetic, S, b1m, b2m, u, k0[i], psi[2 * i], psi[2 * i + 1], hP[i]);
+  }
+  if (upload(c->params, hP.data(), hP.size())) return -3;
+  const PointParams *dP = c->params.as<PointParams>();
+  // device-time span of the whole batch (start on worker 0; every worker joins it at the end)
+  cudaEvent_t span0, span1;
+  PSS_CUDA_TRY(cudaEventCreate(&span0));
+  PSS_CUDA_TRY(cudaEventCreate(&span1));
+  PSS_CUDA_TRY(cudaEventRecord(span0, c->w[0].st));
+  std::vector<int> hstatus(npts, 0);
+  std::vector<TableDev> tabs;
+  int rc = build_tables(c, S, dP, npts, 1e-7, tabs, hstatus);
+  if (rc) return rc;
+  float tables_ms = 0;
+  {
+    cudaEvent_t t;
+    PSS_CUDA_TRY(cudaEventCreate(&t));
+    PSS_CUDA_TRY(cudaEventRecord(t, c->w[0].st));
+    PSS_CUDA_TRY(cudaEventSynchronize(t));
+    cudaEventElapsedTime(&tables_ms, span0, t);
+    cudaEventDestroy(t);
+  }
+
+  // mode data for all points
+  const size_t nmp = (size_t)npts * nmodes;
+  size_t off_k = 0, off_s = off_k + nmp * 2 * sizeof(double), off_t = off_s + nmp * 2 * sizeof(cd),
+         off_w = off_t + nmp * 2 * sizeof(double), tot = off_w + nmp * sizeof(cd);
+  if (c->modes.ensure(tot)) return -3;
+  char *mb = c->modes.as<char>();
+  PSS_CUDA_TRY(cudaMemcpy(mb + off_k, kvec, nmp * 2 * sizeof(double), cudaMemcpyHostToDevice));
+  PSS_CUDA_TRY(cudaMemcpy(mb + off_s, src, nmp * 2 * sizeof(cd), cudaMemcpyHostToDevice));
+  PSS_CUDA_TRY(cudaMemcpy(mb + off_t, tobs, nmp * 2 * sizeof(double), cudaMemcpyHostToDevice));
+  PSS_CUDA_TRY(cudaMemcpy(mb + off_w, wobs, nmp * sizeof(cd), cudaMemcpyHostToDevice));
+  const size_t nm2 = (size_t)nmodes * nmodes;
+  if (c->dS.ensure((size_t)npts * nm2 * sizeof(cd)) || c->status.ensure((size_t)npts * sizeof(int))) return -3;
+  PSS_CUDA_TRY(cudaMemset(c->status.p, 0, (size_t)npts * sizeof(int)));
+  int *dstatus = c->status.as<int>();
+
+  // J/K face-pair integrals: shared cache when every point has the same (ψ1, ψ2)
+  const double ulocal = u / sh->upm;
+  bool same_psi = true;
+  for (int i = 1; i < npts; ++i)
+    same_psi = same_psi && psi[2 * i] == psi[0] && psi[2 * i + 1] == psi[1];
+  if (same_psi) {
+    if ((rc = refresh_jk_cache(sh, psi[0], psi[1], ulocal, c->w[0].st))) return rc;
+    if (sh->jk_nonconv)
+      for (int i = 0; i < npts; ++i) hstatus[i] |= PSS_ST_JK_NOCONV;
+  }
+  const int nw = c->nworkers;
+  for (int k = 0; k < nw; ++k)
+    if ((rc = ensure_worker(c->w[k], sh, nmodes, precision, !same_psi))) return rc;
+
+  const int n = sh->nbf;
+  const long long ld = n;
+  std::vector<cudaEvent_t> ev;
+  // One point through fill, LU, transforms, solve(s) and projection on worker w's stream.
+  auto run_point = [&](int i, int prec, Worker &w, bool rec) -> int {
+    cudaStream_t st = w.st;
+    const PointParams *Pi = dP + i;
+    const double p1 = psi[2 * i], p2 = psi[2 * i + 1];
+    cudaEvent_t e[8];
+    if (rec) {
+      for (int q = 0; q < 8; ++q) { cudaEventCreate(&e[q]); ev.push_back(e[q]); }
+      cudaEventRecord(e[0], st);
+    }
+    JKDev jk;
+    if (same_psi) {
+      jk = sh->cache.jk;
+    } else {
+      jk = w.jk.jk;
+      pss_filljk(sh->G, ulocal, p1, p2, sh->s1, sh->s2, jk, w.nonconv.as<int>(), st);
+      pss_count_launch();
+      k_nonconv_to_status<<<1, 1, 0, st>>>(w.nonconv.as<int>(), dstatus + i);
+    }
+    if (rec) cudaEventRecord(e[1], st);
+    pss_fill_pairs(sh->G, Pi, jk, tabs[i].t1, tabs[i].t2, tabs[i].mmax, w.zb.as<cd>(), st);
+    float *zr = prec == PSS_FP32_REFINE ? w.zr.as<float>() : nullptr;
+    float *zi = prec == PSS_FP32_REFINE ? w.zi.as<float>() : nullptr;
+    pss_fill_assemble(sh->G, Pi, w.zb.as<cd>(), w.z64.as<cd>(), zr, zi, ld, st);
+    if (rec) cudaEventRecord(e[2], st);
+    int rc2;
+    if (prec == PSS_FP64) rc2 = pss_lu64(n, w.z64.as<cd>(), ld, w.ipiv.as<int>(), w.info.as<int>(), nullptr, 0, st);
+    else rc2 = pss_lu32(n, zr, zi, ld, w.ipiv.as<int>(), w.info.as<int>(), nullptr, 0, st);
+    if (rc2) return rc2;
+    pss_count_launch();
+    k_info_to_status<<<1, 1, 0, st>>>(w.info.as<int>(), dstatus + i);
+    if (rec) cudaEventRecord(e[3], st);
+    const double *kv = (const double *)(mb + off_k) + (size_t)i * nmodes * 2;
+    const cd *sv = (const cd *)(mb + off_s) + (size_t)i * nmodes * 2;
+    const double *tv = (const double *)(mb + off_t) + (size_t)i * nmodes * 2;
+    const cd *wv = (const cd *)(mb + off_w) + (size_t)i * nmodes;
+    pss_bfft(sh->G, nmodes, kv, p1, p2, w.bf.as<cd>(), st);
+    pss_rhs(n, nmodes, w.bf.as<cd>(), sv, w.rhs.as<cd>(), st);
+    PSS_CUDA_TRY(cudaMemcpyAsync(w.X.p, w.rhs.p, (size_t)n * nmodes * sizeof(cd), cudaMemcpyDeviceToDevice, st));
+    if (rec) cudaEventRecord(e[4], st);
+    if (prec == PSS_FP64) {
+      pss_solve64(n, w.z64.as<cd>(), ld, w.ipiv.as<int>(), nmodes, w.X.as<cd>(), nullptr, st);
+    } else {
+      pss_solve32(n, zr, zi, ld, w.ipiv.as<int>(), nmodes, w.X.as<cd>(), nullptr, st);
+      PSS_CUDA_TRY(cudaMemsetAsync(w.done.p, 0, sizeof(int), st));
+      PSS_CUDA_TRY(cudaMemsetAsync(w.norms.p, 0, 2 * sizeof(double), st));
+      for (int it = 0; it < kMaxRefine; ++it) {
+        pss_residual64(n, w.z64.as<cd>(), ld, nmodes, w.X.as<cd>(), w.rhs.as<cd>(), w.R.as<cd>(), w.done.as<int>(), st);
+        pss_solve32(n, zr, zi, ld, w.ipiv.as<int>(), nmodes, w.R.as<cd>(), w.done.as<int>(), st);
+        pss_axpy_norms(n, nmodes, w.X.as<cd>(), w.R.as<cd>(), w.norms.as<double>(), w.done.as<int>(), st);
+        pss_refine_check(w.norms.as<double>(), kRefineTol, w.done.as<int>(), dstatus + i, it == kMaxRefine - 1, st);
+      }
+    }
+    if (rec) cudaEventRecord(e[5], st);
+    pss_project(n, nmodes, w.bf.as<cd>(), tv, wv, w.X.as<cd>(), c->dS.as<cd>() + (size_t)i * nm2, st);
+    if (rec) { cudaEventRecord(e[6], st); cudaEventRecord(e[7], st); }
+    PSS_CUDA_TRY(cudaGetLastError());
+    return 0;
+  };
+  for (int i = 0; i < npts; ++i) {
+    if ((rc = run_point(i, precision, c->w[i % nw], (i % nw) == 0))) return rc;
+  }
+  for (auto &w : c->w) PSS_CUDA_TRY(cudaStreamSynchronize(w.st));
+  PSS_CUDA_TRY(cudaMemcpy(status, c->status.p, (size_t)npts * sizeof(int), cudaMemcpyDeviceToHost));
+  // FP32 points whose refinement stalled (cond(Z) * eps32 too close to 1) or went
+  // non-finite are recomputed with the FP64 LU; the status keeps a record of it.
+  if (precision == PSS_FP32_REFINE) {
+    std::vector<int> redo;
+    for (int i = 0; i < npts; ++i)
+      if (status[i] & (PSS_ST_REFINE_NOCONV | PSS_ST_NONFINITE)) redo.push_back(i);
+    if (!redo.empty()) {
+      std::vector<int> cleared(npts);
+      for (int i = 0; i < npts; ++i) cleared[i] = status[i] & ~(PSS_ST_REFINE_NOCONV | PSS_ST_NONFINITE);
+      PSS_CUDA_TRY(cudaMemcpy(c->status.p, cleared.data(), (size_t)npts * sizeof(int), cudaMemcpyHostToDevice));
+      for (size_t q = 0; q < redo.size(); ++q)
+        if ((rc = run_point(redo[q], PSS_FP64, c->w[q % nw], false))) return rc;
+      for (auto &w : c->w) PSS_CUDA_TRY(cudaStreamSynchronize(w.st));
+      PSS_CUDA_TRY(cudaMemcpy(status, c->status.p, (size_t)npts * sizeof(int), cudaMemcpyDeviceToHost));
+      for (int i : redo) status[i] |= PSS_ST_FP64_FALLBACK;
+    }
+  }
+  for (size_t k = 1; k < c->w.size(); ++k) {
+    cudaEvent_t j;
+    PSS_CUDA_TRY(cudaEventCreate(&j));
+    PSS_CUDA_TRY(cudaEventRecord(j, c->w[k].st));
+    PSS_CUDA_TRY(cudaStreamWaitEvent(c->w[0].st, j, 0));
+    cudaEventDestroy(j);
+  }
+  PSS_CUDA_TRY(cudaEventRecord(span1, c->w[0].st));
+  PSS_CUDA_TRY(cudaEventSynchronize(span1));
+  float span_ms = 0;
+  cudaEventElapsedTime(&span_ms, span0, span1);
+  cudaEventDestroy(span0);
+  cudaEventDestroy(span1);
+  PSS_CUDA_TRY(cudaMemcpy(dS, c->dS.p, (size_t)npts * nm2 * sizeof(cd), cudaMemcpyDeviceToHost));
+  for (int i = 0; i < npts; ++i) status[i] |= hstatus[i];
+  for (int q = 0; q < 8; ++q) c->last_ms[q] = 0;
+  for (size_t b = 0; b + 8 <= ev.size(); b += 8) {
+    float ms;
+    const int map[6][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 4}, {4, 5}, {5, 6}};
+    for (int q = 0; q < 6; ++q) {
+      cudaEventElapsedTime(&ms, ev[b + map[q][0]], ev[b + map[q][1]]);
+      c->last_ms[q + 1] += ms;
+    }
+  }
+  c->last_ms[0] = tables_ms;
+  c->last_ms[7] = span_ms;
+  for (auto e : ev) cudaEventDestroy(e);
+  return 0;
+}
+
+int pss_last_timings(pss_ctx *c, double *ms8) {
+  if (!c || !ms8) return -1;
+  for (int q = 0; q < 8; ++q) ms8[q] = c->last_ms[q];
+  return 0;
+}
+
+int pss_fill_matrix(pss_sheet *sh, int nl, const double *eps, const double *mu, const double *width, int s,
+                    double u, double k0, double psi1, double psi2, double *Z, int *mmax_out) {
+  if (!sh || !Z) { pss_set_error("null argument"); return -1; }
+  pss_ctx *c = sh->ctx;
+  if (set_device(c)) return -3;
+  StackParams S;
+  if (make_stack(nl, eps, mu, width, s, S)) return -1;
+  const double b1m[2] = {sh->b1[0] * sh->upm, sh->b1[1] * sh->upm};
+  const double b2m[2] = {sh->b2[0] * sh->upm, sh->b2[1] * sh->upm};
+  PointParams P;
+  make_params(sh->cls == 'M', S, b1m, b2m, u, k0, psi1, psi2, P);
+  if (upload(c->params, &P, 1)) return -3;
+  std::vector<int> hs(1, 0);
+  std::vector<TableDev> tabs;
+  int rc = build_tables(c, S, c->params.as<PointParams>(), 1, 1e-7, tabs, hs);
+  if (rc) return rc;
+  Worker &w = c->w[0];
+  if ((rc = refresh_jk_cache(sh, psi1, psi2, u / sh->upm, w.st))) return rc;
+  if ((rc = ensure_worker(w, sh, 1, PSS_FP64, false))) return rc;
+  pss_fill_pairs(sh->G, c->params.as<PointParams>(), sh->cache.jk, tabs[0].t1, tabs[0].t2, tabs[0].mmax,
+                 w.zb.as<cd>(), w.st);
+  pss_fill_assemble(sh->G, c->params.as<PointParams>(), w.zb.as<cd>(), w.z64.as<cd>(), nullptr, nullptr, sh->nbf,
+                    w.st);
+  PSS_CUDA_TRY(cudaStreamSynchronize(w.st));
+  const size_t n = sh->nbf;
+  std::vector<cd> h(n * n);
+  PSS_CUDA_TRY(cudaMemcpy(h.data(), w.z64.p, n * n * sizeof(cd), cudaMemcpyDeviceToHost));
+  for (size_t m = 0; m < n; ++m)
+    for (size_t q = 0; q < n; ++q) {  // row-major device -> column-major caller
+      Z[2 * (m + q * n)] = h[m * n + q].x;
+      Z[2 * (m + q * n) + 1] = h[m * n + q].y;
+    }
+  if (mmax_out) *mmax_out = tabs[0].mmax;
+  return 0;
+}
+
+int pss_modal_tables(pss_ctx *c, int magnetic, int nl, const double *eps, const double *mu, const double *width,
+                     int s, double k0, double u, double psi1, double psi2, const double *b1, const double *b2,
+                     double convtest, int64_t cap, double *t1, double *t2, int *mmax_out, int *status) {
+  if (!c || !t1 || !t2 || !mmax_out) { pss_set_error("null argument"); return -1; }
+  if (set_device(c)) return -3;
+  StackParams S;
+  if (make_stack(nl, eps, mu, width, s, S)) return -1;
+  PointParams P;
+  make_params(magnetic, S, b1, b2, u, k0, psi1, psi2, P);
+  if (upload(c->params, &P, 1)) return -3;
+  std::vector<int> hs(1, 0);
+  std::vector<TableDev> tabs;
+  int rc = build_tables(c, S, c->params.as<PointParams>(), 1, convtest, tabs, hs);
+  if (rc) return rc;
+  size_t need = pss_table_cap(tabs[0].mmax);
+  *mmax_out = tabs[0].mmax;
+  if (status) *status = hs[0];
+  if ((int64_t)need > cap) { pss_set_error("table capacity %lld < %zu", (long long)cap, need); return -2; }
+  PSS_CUDA_TRY(cudaMemcpy(t1, tabs[0].t1, need * sizeof(cd), cudaMemcpyDeviceToHost));
+  PSS_CUDA_TRY(cudaMemcpy(t2, tabs[0].t2, need * sizeof(cd), cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int pss_face_integrals(pss_sheet *sh, double ulocal, double psi1, double psi2, double *J, double *Jxi,
+                       double *Jeta, double *K, double *Kxi, double *Keta, double *rho_r, double *rinv,
+                       int *nonconv) {
+  if (!sh) { pss_set_error("null argument"); return -1; }
+  if (set_device(sh->ctx)) return -3;
+  sh->jk_valid = false;
+  int rc = refresh_jk_cache(sh, psi1, psi2, ulocal, sh->ctx->w[0].st);
+  if (rc) return rc;
+  const size_t c = (size_t)sh->nufp * sizeof(cd), d = (size_t)sh->nufp * sizeof(double);
+  const JKDev &jk = sh->cache.jk;
+  PSS_CUDA_TRY(cudaMemcpy(J, jk.J, c, cudaMemcpyDeviceToHost));
+  PSS_CUDA_TRY(cudaMemcpy(Jxi, jk.Jxi, c, cudaMemcpyDeviceToHost));
+  PSS_CUDA_TRY(cudaMemcpy(Jeta, jk.Jeta, c, cudaMemcpyDeviceToHost));
+  PSS_CUDA_TRY(cudaMemcpy(K, jk.K, c, cudaMemcpyDeviceToHost));
+  PSS_CUDA_TRY(cudaMemcpy(Kxi, jk.Kxi, c, cudaMemcpyDeviceToHost));
+  PSS_CUDA_TRY(cudaMemcpy(Keta, jk.Keta, c, cudaMemcpyDeviceToHost));
+  PSS_CUDA_TRY(cudaMemcpy(rho_r, jk.rho_r, 2 * d, cudaMemcpyDeviceToHost));
+  PSS_CUDA_TRY(cudaMemcpy(rinv, jk.rinv, d, cudaMemcpyDeviceToHost));
+  if (nonconv) *nonconv = sh->jk_nonconv;
+  return 0;
+}
+
+int pss_basis_transforms(pss_sheet *sh, int nmodes, const double *kvec, double psi1, double psi2, double *F) {
+  if (!sh || !kvec || !F || nmodes <= 0) { pss_set_error("invalid argument"); return -1; }
+  pss_ctx *c = sh->ctx;
+  if (set_device(c)) return -3;
+  Worker &w = c->w[0];
+  DevBuf kb;
+  if (upload(kb, kvec, 2 * (size_t)nmodes)) return -3;
+  if (w.bf.ensure((size_t)nmodes * sh->nbf * 2 * sizeof(cd))) return -3;
+  pss_bfft(sh->G, nmodes, kb.as<double>(), psi1, psi2, w.bf.as<cd>(), w.st);
+  PSS_CUDA_TRY(cudaStreamSynchronize(w.st));
+  PSS_CUDA_TRY(cudaMemcpy(F, w.bf.p, (size_t)nmodes * sh->nbf * 2 * sizeof(cd), cudaMemcpyDeviceToHost));
+  kb.release();
+  return 0;
+}
+
+int pss_lu_solve(pss_ctx *c, int n, const double *Z, int nrhs, const double *B, int precision, double *X,
+                 int *status) {
+  if (!c || !Z || !B || !X || n <= 0 || nrhs <= 0) { pss_set_error("invalid argument"); return -1; }
+  if (set_device(c)) return -3;
+  Worker &w = c->w[0];
+  cudaStream_t st = w.st;
+  const size_t nn = (size_t)n * n;
+  std::vector<cd> h(nn);
+  for (size_t m = 0; m < (size_t)n; ++m)
+    for (size_t q = 0; q < (size_t)n; ++q) h[m * n + q] = mkcd(Z[2 * (m + q * n)], Z[2 * (m + q * n) + 1]);
+  if (w.z64.ensure(nn * sizeof(cd)) || w.ipiv.ensure(n * sizeof(int)) || w.info.ensure(sizeof(int)) ||
+      w.rhs.ensure((size_t)n * nrhs * sizeof(cd)) || w.X.ensure((size_t)n * nrhs * sizeof(cd)) ||
+      w.R.ensure((size_t)n * nrhs * sizeof(cd)) || w.norms.ensure(2 * sizeof(double)) || w.done.ensure(sizeof(int)))
+    return -3;
+  DevBuf st_buf;
+  if (st_buf.ensure(sizeof(int))) return -3;
+  PSS_CUDA_TRY(cudaMemset(st_buf.p, 0, sizeof(int)));
+  PSS_CUDA_TRY(cudaMemset(w.info.p, 0, sizeof(int)));
+  PSS_CUDA_TRY(cudaMemcpy(w.z64.p, h.data(), nn * sizeof(cd), cudaMemcpyHostToDevice));
+  PSS_CUDA_TRY(cudaMemcpy(w.rhs.p, B, (size_t)n * nrhs * sizeof(cd), cudaMemcpyHostToDevice));
+  PSS_CUDA_TRY(cudaMemcpy(w.X.p, B, (size_t)n * nrhs * sizeof(cd), cudaMemcpyHostToDevice));
+  int rc;
+  if (precision == PSS_FP64) {
+    rc = pss_lu64(n, w.z64.as<cd>(), n, w.ipiv.as<int>(), w.info.as<int>(), nullptr, 0, st);
+    if (rc) return rc;
+    pss_solve64(n, w.z64.as<cd>(), n, w.ipiv.as<int>(), nrhs, w.X.as<cd>(), nullptr, st);
+  } else {
+    if (w.zr.ensure(nn * sizeof(float)) || w.zi.ensure(nn * sizeof(float))) return -3;
+    std::vector<float> hr(nn), hi(nn);
+    for (size_t i = 0; i < nn; ++i) { hr[i] = (float)h[i].x; hi[i] = (float)h[i].y; }
+    PSS_CUDA_TRY(cudaMemcpy(w.zr.p, hr.data(), nn * sizeof(float), cudaMemcpyHostToDevice));
+    PSS_CUDA_TRY(cudaMemcpy(w.zi.p, hi.data(), nn * sizeof(float), cudaMemcpyHostToDevice));
+    rc = pss_lu32(n, w.zr.as<float>(), w.zi.as<float>(), n, w.ipiv.as<int>(), w.info.as<int>(), nullptr, 0, st);
+    if (rc) return rc;
+    pss_solve32(n, w.zr.as<float>(), w.zi.as<float>(), n, w.ipiv.as<int>(), nrhs, w.X.as<cd>(), nullptr, st);
+    PSS_CUDA_TRY(cudaMemsetAsync(w.done.p, 0, sizeof(int), st));
+    PSS_CUDA_TRY(cudaMemsetAsync(w.norms.p, 0, 2 * sizeof(double), st));
+    for (int it = 0; it < kMaxRefine; ++it) {
+      pss_residual64(n, w.z64.as<cd>(), n, nrhs, w.X.as<cd>(), w.rhs.as<cd>(), w.R.as<cd>(), w.done.as<int>(), st);
+      pss_solve32(n, w.zr.as<float>(), w.zi.as<float>(), n, w.ipiv.as<int>(), nrhs, w.R.as<cd>(), w.done.as<int>(), st);
+      pss_axpy_norms(n, nrhs, w.X.as<cd>(), w.R.as<cd>(), w.norms.as<double>(), w.done.as<int>(), st);
+      pss_refine_check(w.norms.as<double>(), kRefineTol, w.done.as<int>(), st_buf.as<int>(), it == kMaxRefine - 1, st);
+    }
+  }
+  pss_count_launch();
+  k_info_to_status<<<1, 1, 0, st>>>(w.info.as<int>(), st_buf.as<int>());
+  PSS_CUDA_TRY(cudaStreamSynchronize(st));
+  PSS_CUDA_TRY(cudaGetLastError());
+  int hs = 0;
+  PSS_CUDA_TRY(cudaMemcpy(&hs, st_buf.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (precision == PSS_FP32_REFINE && (hs & (PSS_ST_REFINE_NOCONV | PSS_ST_NONFINITE))) {
+    // stalled refinement: FP64 factorisation of the original matrix
+    PSS_CUDA_TRY(cudaMemset(w.info.p, 0, sizeof(int)));
+    PSS_CUDA_TRY(cudaMemset(st_buf.p, 0, sizeof(int)));
+    PSS_CUDA_TRY(cudaMemcpy(w.z64.p, h.data(), nn * sizeof(cd), cudaMemcpyHostToDevice));
+    PSS_CUDA_TRY(cudaMemcpy(w.X.p, B, (size_t)n * nrhs * sizeof(cd), cudaMemcpyHostToDevice));
+    rc = pss_lu64(n, w.z64.as<cd>(), n, w.ipiv.as<int>(), w.info.as<int>(), nullptr, 0, st);
+    if (rc) return rc;
+    pss_solve64(n, w.z64.as<cd>(), n, w.ipiv.as<int>(), nrhs, w.X.as<cd>(), nullptr, st);
+    pss_count_launch();
+    k_info_to_status<<<1, 1, 0, st>>>(w.info.as<int>(), st_buf.as<int>());
+    PSS_CUDA_TRY(cudaStreamSynchronize(st));
+    PSS_CUDA_TRY(cudaMemcpy(&hs, st_buf.p, sizeof(int), cudaMemcpyDeviceToHost));
+    hs |= PSS_ST_FP64_FALLBACK;
+  }
+  PSS_CUDA_TRY(cudaMemcpy(X, w.X.p, (size_t)n * nrhs * sizeof(cd), cudaMemcpyDeviceToHost));
+  if (status) *status = hs;
+  st_buf.release();
+  return 0;
+}
+
+}  // extern "C"

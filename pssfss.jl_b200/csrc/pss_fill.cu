@@ -1,0 +1,314 @@
+// K2 + K3: face-pair integrals and the MoM matrix fill.
+//
+// K2 k_filljk   restates Zint.jl:117-242 (filljk!) with PGF.jl:67-106 (jksums):
+//               one thread per unique face pair, the 7-point rule and each lattice
+//               ring summed in the reference's order, FP64.
+// K3a k_pairs   restates Zint.jl:281-308 (zint) and the per-edge algebra of
+//               FillZY.jl:141-197 / 362-419: one thread per unique face pair computes
+//               the 3x3 unflagged edge-pair terms  zA*(ρc2[iml]·a_isl) - zP*φ.
+// K3b k_assemble replaces the spin-locked scatter of FillZY.jl:160-239 by a gather:
+//               each Z entry sums, in a fixed order, the <=2x2 face incidences of its
+//               test and source basis functions, applying the Floquet/sign flags and the
+//               surface-resistance terms of Eqs. 7-34/7-35 (FillZY.jl:221-230).
+//               Deterministic, atomic-free; writes FP64 and/or split FP32 planes.
+#include "pss_internal.cuh"
+
+namespace {
+
+__device__ __forceinline__ int jksums_dev(double urx, double ury, double psi1, double psi2, double us1x,
+                                          double us1y, double us2x, double us2y, cd &jout, cd &kout) {
+  const int rmin = 5;
+  const double small = 1e-5, convtest = 1e-8;
+  double arg = sqrt(urx * urx + ury * ury);
+  double rterm = exp(-arg);
+  cd ksum = mkcd(rterm, 0.0), jsum;
+  if (arg <= small) jsum = mkcd((-arg / 6 + 0.5) * arg - 1, 0.0);
+  else jsum = mkcd((rterm - 1) / arg, 0.0);
+  const bool nophase = (psi1 == 0.0 && psi2 == 0.0);
+  int converged = 0;
+  for (int r = 1; r <= PSS_JKRINGMAX; ++r) {
+    cd jring = mkcd(0, 0), kring = mkcd(0, 0);
+    const int len = 8 * r;
+    for (int t = 0; t < len; ++t) {
+      int m, n;
+      ring_mn(r, t, m, n);
+      double dx = urx - ((double)m * us1x + (double)n * us2x);
+      double dy = ury - ((double)m * us1y + (double)n * us2y);
+      double a = sqrt(dx * dx + dy * dy);
+      double er = exp(-a);
+      cd term;
+      if (nophase) {
+        term = mkcd(er, 0.0);
+      } else {
+        double ph = (double)m * psi1 + (double)n * psi2;
+        if (ph == 0.0) term = mkcd(er, -ph);
+        else {
+          double s, c;
+          sincos(-ph, &s, &c);
+          term = mkcd(er * c, er * s);
+        }
+      }
+      jring = jring + term / a;
+      kring = kring + term;
+    }
+    jsum = jsum + jring;
+    ksum = ksum + kring;
+    if (r > rmin) {
+      double c1 = cabsd(jring / jsum), c2 = cabsd(kring / ksum);
+      if (fmax(c1, c2) < convtest) { converged = 1; break; }
+    }
+  }
+  jout = jsum;
+  kout = ksum;
+  return converged;
+}
+
+__device__ __forceinline__ void face_vtx(const SheetDev &G, int f, double r[3][2], double scale) {
+  for (int k = 0; k < 3; ++k) {
+    int v = G.fv[3 * f + k];
+    r[k][0] = G.rho[2 * v] * scale;
+    r[k][1] = G.rho[2 * v + 1] * scale;
+  }
+}
+
+__global__ void k_filljk(SheetDev G, double ul, double psi1, double psi2, double us1x, double us1y,
+                         double us2x, double us2y, JKDev jk, int *nonconv) {
+  int iu = blockIdx.x * blockDim.x + threadIdx.x;
+  if (iu >= G.nufp) return;
+  int fp = G.ufp_rep[iu];
+  int ifm = fp % G.nface, ifs = fp / G.nface;
+  double rs[3][2], rm[3][2];
+  face_vtx(G, ifs, rs, 1.0);
+  face_vtx(G, ifm, rm, 1.0);
+  double rs32[2] = {rs[2][0] - rs[1][0], rs[2][1] - rs[1][1]};
+  double rs12[2] = {rs[0][0] - rs[1][0], rs[0][1] - rs[1][1]};
+  double area2 = (-rs32[1]) * rs12[0] + rs32[0] * rs12[1];
+  double unz = 1.0;
+  if (area2 < 0) { area2 = fabs(area2); unz = -1.0; }
+  double rs31[2] = {rs[2][0] - rs[0][0], rs[2][1] - rs[0][1]};
+  double rs21[2] = {-rs12[0], -rs12[1]};
+  double rmc[2] = {((rm[0][0] + rm[1][0]) + rm[2][0]) / 3, ((rm[0][1] + rm[1][1]) + rm[2][1]) / 3};
+  cd aJ = mkcd(0, 0), aJx = aJ, aJe = aJ, aK = aJ, aKx = aJ, aKe = aJ;
+  int bad = 0;
+  for (int i = 0; i < 7; ++i) {
+    double rtx = (rs[0][0] + rs21[0] * c_qxi[i]) + rs31[0] * c_qeta[i];
+    double rty = (rs[0][1] + rs21[1] * c_qxi[i]) + rs31[1] * c_qeta[i];
+    cd js, ks;
+    if (!jksums_dev(ul * (rmc[0] - rtx), ul * (rmc[1] - rty), psi1, psi2, us1x, us1y, us2x, us2y, js, ks))
+      bad = 1;
+    cd jw = c_qw[i] * js;
+    aJx = aJx + c_qxi[i] * jw;
+    aJe = aJe + c_qeta[i] * jw;
+    aJ = aJ + jw;
+    cd kw = c_qw[i] * ks;
+    aKx = aKx + c_qxi[i] * kw;
+    aKe = aKe + c_qeta[i] * kw;
+    aK = aK + kw;
+  }
+  const int nxt[3] = {1, 2, 0};
+  double rr0 = 0, rr1 = 0, ri = 0;
+  for (int i = 0; i < 3; ++i) {
+    int ip1 = nxt[i];
+    double lx = rs[ip1][0] - rs[i][0], ly = rs[ip1][1] - rs[i][1];
+    double ln = sqrt(lx * lx + ly * ly);
+    lx /= ln;
+    ly /= ln;
+    double ux = (-unz) * (-ly), uy = (-unz) * lx;
+    double d0x = rs[i][0] - rmc[0], d0y = rs[i][1] - rmc[1];
+    double d1x = rs[ip1][0] - rmc[0], d1y = rs[ip1][1] - rmc[1];
+    double p0 = ux * d0x + uy * d0y;
+    double p0sq = p0 * p0;
+    double lp = lx * d1x + ly * d1y;
+    double lm = lx * d0x + ly * d0y;
+    double ledge = lp - lm;
+    double pplus = sqrt(p0sq + lp * lp);
+    double pminus = sqrt(p0sq + lm * lm);
+    double factor;
+    if (fabs(p0 / ledge) < 1e-4) {
+      factor = lp * pplus - lm * pminus;
+    } else {
+      factor = p0 * log((pplus + lp) / (pminus + lm));
+      ri += factor;
+      factor = (factor * p0 + pplus * lp) - pminus * lm;
+    }
+    rr0 += ux * factor;
+    rr1 += uy * factor;
+  }
+  rr0 *= 0.5;
+  rr1 *= 0.5;
+  rr0 /= area2;
+  rr1 /= area2;
+  ri /= (area2 * ul);
+  jk.J[iu] = aJ; jk.Jxi[iu] = aJx; jk.Jeta[iu] = aJe;
+  jk.K[iu] = aK; jk.Kxi[iu] = aKx; jk.Keta[iu] = aKe;
+  jk.rho_r[2 * iu] = rr0;
+  jk.rho_r[2 * iu + 1] = rr1;
+  jk.rinv[iu] = ri;
+  if (bad) atomicAdd(nonconv, 1);
+}
+
+// Per-point coefficients that turn the face-pair integrals into Z terms:
+//   a_isl = cI1*I1_i + sing + u*J_i + cK*K_i,   φ = cI2*I2 + u*(rinv + J) + cKP*K,
+//   term(isl, iml) = zA*(ρc2[iml]·a_isl) - zP*φ.
+struct PairCoef {
+  cd cI1, cK, cI2, cKP, zA, zP;
+};
+
+__device__ __forceinline__ PairCoef pair_coef(const PointParams &P) {
+  PairCoef c;
+  const double eps0 = 1.0 / (PSS_MU0 * (PSS_C0 * PSS_C0));
+  const double u = P.u, w = P.omega;
+  if (!P.magnetic) {
+    c.cI1 = mkcd(PSS_FOURPI, 0);
+    c.cK = P.c3 / u;
+    c.cI2 = mkcd(PSS_FOURPI, 0);
+    c.cKP = P.d3 / u;
+    c.zA = mkcd(0.0, w) * ((PSS_MU0 / PSS_FOURPI) * P.mutilde);
+    c.zP = (mkcd(0.0, 1.0) / P.epsbar) * mkcd(1.0 / (PSS_TWOPI * w * eps0), 0.0);
+  } else {
+    c.cI1 = P.I1fact;
+    c.cK = P.KFfact;
+    c.cI2 = P.I2fact;
+    c.cKP = P.KPfact;
+    c.zA = mkcd(0.0, -w) * ((-eps0 / PSS_PI) * P.epsbar);
+    c.zP = mkcd(0.0, 2.0) / ((PSS_PI * w * PSS_MU0) * P.mutilde);
+  }
+  return c;
+}
+
+__global__ void __launch_bounds__(128) k_pairs(SheetDev G, const PointParams *__restrict__ Pp, JKDev jk,
+                                               const cd *__restrict__ t1, const cd *__restrict__ t2, int mmax,
+                                               cd *__restrict__ zb) {
+  int iu = blockIdx.x * blockDim.x + threadIdx.x;
+  if (iu >= G.nufp) return;
+  const PointParams &P = *Pp;
+  const PairCoef C = pair_coef(P);
+  int fp = G.ufp_rep[iu];
+  int ifm = fp % G.nface, ifs = fp / G.nface;
+  const double inv = 1.0 / G.upm;
+  double rs[3][2], rm[3][2];
+  for (int k = 0; k < 3; ++k) {
+    int vs = G.fv[3 * ifs + k], vm = G.fv[3 * ifm + k];
+    rs[k][0] = G.rho[2 * vs] / G.upm;
+    rs[k][1] = G.rho[2 * vs + 1] / G.upm;
+    rm[k][0] = G.rho[2 * vm] / G.upm;
+    rm[k][1] = G.rho[2 * vm + 1] / G.upm;
+  }
+  (void)inv;
+  double rmc[2] = {((rm[0][0] + rm[1][0]) + rm[2][0]) / 3, ((rm[0][1] + rm[1][1]) + rm[2][1]) / 3};
+  cd I1 = mkcd(0, 0), I1x = I1, I1e = I1, I2 = I1;
+  for (int i = 0; i < 7; ++i) {
+    double rtx = (rs[0][0] + (rs[1][0] - rs[0][0]) * c_qxi[i]) + (rs[2][0] - rs[0][0]) * c_qeta[i];
+    double rty = (rs[0][1] + (rs[1][1] - rs[0][1]) * c_qxi[i]) + (rs[2][1] - rs[0][1]) * c_qeta[i];
+    double dx = rmc[0] - rtx, dy = rmc[1] - rty;
+    cd g1 = sigma_interp(t1, mmax, P, dx, dy);
+    cd g2 = sigma_interp(t2, mmax, P, dx, dy);
+    cd g1w = c_qw[i] * g1;
+    I1x = I1x + c_qxi[i] * g1w;
+    I1e = I1e + c_qeta[i] * g1w;
+    I1 = I1 + g1w;
+    I2 = I2 + c_qw[i] * g2;
+  }
+  cd J = jk.J[iu], Jx = jk.Jxi[iu], Je = jk.Jeta[iu];
+  cd K = jk.K[iu], Kx = jk.Kxi[iu], Ke = jk.Keta[iu];
+  double rinv = jk.rinv[iu], rr0 = jk.rho_r[2 * iu], rr1 = jk.rho_r[2 * iu + 1];
+  cd I1z = (I1 - I1x) - I1e, Jz = (J - Jx) - Je, Kz = (K - Kx) - Ke;
+  const double u = P.u;
+  cd phi = (C.cI2 * I2 + u * (mkcd(rinv, 0) + J)) + C.cKP * K;
+  cd zphi = C.zP * phi;
+  double rc2[3][2];
+  for (int i = 0; i < 3; ++i) {
+    rc2[i][0] = 0.5 * (rmc[0] - rm[i][0]);
+    rc2[i][1] = 0.5 * (rmc[1] - rm[i][1]);
+  }
+  cd *out = zb + (size_t)iu * 9;
+  for (int isl = 0; isl < 3; ++isl) {
+    double sing0 = rr0 + (u * rinv) * (rmc[0] - rs[isl][0]);
+    double sing1 = rr1 + (u * rinv) * (rmc[1] - rs[isl][1]);
+    cd av[2];
+    for (int d = 0; d < 2; ++d) {
+      cd Ii = ((rs[0][d] * I1x + rs[1][d] * I1e) + rs[2][d] * I1z) - rs[isl][d] * I1;
+      cd Ji = ((rs[0][d] * Jx + rs[1][d] * Je) + rs[2][d] * Jz) - rs[isl][d] * J;
+      cd Ki = ((rs[0][d] * Kx + rs[1][d] * Ke) + rs[2][d] * Kz) - rs[isl][d] * K;
+      double sg = d == 0 ? sing0 : sing1;
+      av[d] = ((C.cI1 * Ii + mkcd(sg, 0)) + u * Ji) + C.cK * Ki;
+    }
+    for (int iml = 0; iml < 3; ++iml) {
+      cd dp = rc2[iml][0] * av[0] + rc2[iml][1] * av[1];
+      out[3 * isl + iml] = C.zA * dp - zphi;
+    }
+  }
+}
+
+// Z[m, n] (m = test / match basis function, n = source).  Row-major, leading dimension ld.
+__global__ void __launch_bounds__(256) k_assemble(SheetDev G, const PointParams *__restrict__ Pp,
+                                                  const cd *__restrict__ zb, cd *__restrict__ z64,
+                                                  float *__restrict__ zr, float *__restrict__ zi, long long ld) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  int m = blockIdx.y * blockDim.y + threadIdx.y;
+  if (m >= G.nbf || n >= G.nbf) return;
+  const PointParams &P = *Pp;
+  const int nx[3] = {1, 2, 0}, pv[3] = {2, 0, 1};
+  const int third[3][3] = {{0, 2, 1}, {2, 0, 0}, {1, 0, 0}};
+  cd acc = mkcd(0, 0);
+  const int cm = G.inc_cnt[m], cn = G.inc_cnt[n];
+  for (int a = 0; a < cm; ++a) {
+    const int fa = G.inc_face[4 * m + a], ka = G.inc_loc[4 * m + a];
+    const cd ffa = P.ff[G.inc_eci[4 * m + a]];
+    const cd mflag = G.inc_sgn[4 * m + a] > 0 ? conjd(ffa) : -conjd(ffa);
+    for (int b = 0; b < cn; ++b) {
+      const int fb = G.inc_face[4 * n + b], kb = G.inc_loc[4 * n + b];
+      const cd ffb = P.ff[G.inc_eci[4 * n + b]];
+      const cd sflag = G.inc_sgn[4 * n + b] > 0 ? ffb : -ffb;
+      const int iu = G.ufpm[(size_t)fa + (size_t)fb * G.nface];
+      const cd v = zb[(size_t)iu * 9 + 3 * kb + ka];
+      acc = acc + (mflag * sflag) * v;
+      if (!P.magnetic && fa == fb) {
+        const double fr = G.fr[fa];
+        if (fr != 0.0) {
+          const double *ls = G.face_ls + 3 * fa;
+          const double g = fr / G.face_a48[fa];
+          if (ka == kb) {
+            double l1 = ls[nx[kb]], l2 = ls[pv[kb]], l0 = ls[kb];
+            acc = acc + mkcd(g * (3 * (l1 * l1 + l2 * l2) - l0 * l0), 0.0);
+          } else {
+            double lt = ls[third[kb][ka]];
+            double geo = ls[kb] * ls[kb] + ls[ka] * ls[ka] - 3 * (lt * lt);
+            acc = acc + geo * ((g * sflag) * mflag);
+          }
+        }
+      }
+    }
+  }
+  size_t o = (size_t)m * ld + n;
+  if (z64) z64[o] = acc;
+  if (zr) {
+    zr[o] = (float)acc.x;
+    zi[o] = (float)acc.y;
+  }
+}
+
+}  // namespace
+
+void pss_filljk(const SheetDev &G, double ulocal, double psi1, double psi2, const double s1[2], const double s2[2],
+                JKDev jk, int *nonconv, cudaStream_t st) {
+  if (G.nufp == 0) return;
+  pss_count_launch();
+  k_filljk<<<cdiv_u(G.nufp, 128), 128, 0, st>>>(G, ulocal, psi1, psi2, ulocal * s1[0], ulocal * s1[1],
+                                                 ulocal * s2[0], ulocal * s2[1], jk, nonconv);
+}
+
+void pss_fill_pairs(const SheetDev &G, const PointParams *dP1, const JKDev &jk, const cd *t1, const cd *t2,
+                    int mmax, cd *zb, cudaStream_t st) {
+  if (G.nufp == 0) return;
+  pss_count_launch();
+  k_pairs<<<cdiv_u(G.nufp, 128), 128, 0, st>>>(G, dP1, jk, t1, t2, mmax, zb);
+}
+
+void pss_fill_assemble(const SheetDev &G, const PointParams *dP1, const cd *zb, cd *z64, float *zr, float *zi,
+                       long long ld, cudaStream_t st) {
+  dim3 blk(64, 4);
+  dim3 grd(cdiv_u(G.nbf, 64), cdiv_u(G.nbf, 4));
+  pss_count_launch();
+  k_assemble<<<grd, blk, 0, st>>>(G, dP1, zb, z64, zr, zi, ld);
+}

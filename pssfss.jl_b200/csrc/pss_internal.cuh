@@ -1,0 +1,132 @@
+// Internal declarations shared by the library's translation units.
+#pragma once
+#include "pss_common.cuh"
+
+// Layer stack of one Gblock region (same for every frequency point of a batch).
+struct StackParams {
+  int nl, s;  // number of layers, 1-based interface index of the sheet
+  cd eps[PSS_MAXLAYERS], mu[PSS_MAXLAYERS];
+  double width[PSS_MAXLAYERS];  // metres
+};
+
+// Per frequency-point scalars (computed on the host, read by the kernels).
+struct PointParams {
+  double k0, u, psi1, psi2, omega;
+  double b1[2], b2[2], b00[2];  // reciprocal lattice (1/m) and principal Floquet vector
+  double area;                  // 4π²/|β1×β2|  (m²)
+  double k0sq, b2min;
+  cd mutilde, epsbar, c3, d3;       // electric (PGF.jl:205-210, FillZY.jl:60-61)
+  cd f1, f3, p1, p3;                // magnetic summand factors (PGF.jl:496-499)
+  cd I1fact, KFfact, I2fact, KPfact;  // filly factors (FillZY.jl:319-322)
+  cd ff[5];                         // Floquet factors by edge code (FillZY.jl:72-77)
+  int magnetic;
+};
+
+// Device-resident sheet topology (0-based indices).
+struct SheetDev {
+  int nface, nbf, nufp, nnode;
+  double upm;  // sheet units per metre
+  const double *rho;     // 2*nnode, sheet units
+  const int *fv;         // 3*nface
+  const int *ufpm;       // nface*nface, column-major (match fastest), 0-based class
+  const int *ufp_rep;    // nufp, 0-based column-major face pair of the class representative
+  const double *fr;      // nface
+  const double *face_ls; // 3*nface edge lengths (m): |r3-r2|, |r1-r3|, |r1-r2|
+  const double *face_a48;// nface: 48*|area| (m²)
+  const int *inc_cnt;    // nbf
+  const int *inc_face;   // 4*nbf
+  const int *inc_loc;    // 4*nbf local edge slot 0..2
+  const int *inc_sgn;    // 4*nbf +1 plus / -1 minus
+  const int *inc_eci;    // 4*nbf edge boundary code 0..4
+};
+
+// J/K cache (Zint.jl:117-242), SoA over unique face pairs.
+struct JKDev {
+  cd *J, *Jxi, *Jeta, *K, *Kxi, *Keta;
+  double *rho_r;  // 2*nufp
+  double *rinv;   // nufp
+};
+
+// Modal tables of one point: padded (mmax+2)^2 column-major, index (m,n) in -1..mmax.
+struct TableDev {
+  cd *t1, *t2;
+  int mmax;
+};
+
+// Six-point interpolation of a padded table (PGF.jl:396-441).
+__device__ __forceinline__ cd sigma_interp(const cd *__restrict__ T, int mmax, const PointParams &P,
+                                           double rx, double ry) {
+  double x1o = (P.b1[0] * rx + P.b1[1] * ry) / PSS_TWOPI;
+  if (fabs(x1o) < 1e-8) x1o = 0.0;
+  double x2o = (P.b2[0] * rx + P.b2[1] * ry) / PSS_TWOPI;
+  if (fabs(x2o) < 1e-8) x2o = 0.0;
+  double r1 = fmod(x1o, 1.0), r2 = fmod(x2o, 1.0);
+  double x1 = (r1 == 0.0) ? 0.0 : (r1 < 0.0 ? r1 + 1.0 : r1);
+  double x2 = (r2 == 0.0) ? 0.0 : (r2 < 0.0 ? r2 + 1.0 : r2);
+  double ms = rint(x1o - x1), ns = rint(x2o - x2);
+  int m = (int)trunc(mmax * x1);
+  double p = mmax * x1 - m;
+  int n = (int)trunc(mmax * x2);
+  double q = mmax * x2 - n;
+  // x < 1 always, but mmax*x can round up to mmax; the stencil then must stay inside
+  // the padded table (same point, one cell to the left).
+  if (m >= mmax) { m = mmax - 1; p = mmax * x1 - m; }
+  if (n >= mmax) { n = mmax - 1; q = mmax * x2 - n; }
+  double p2 = p * p, q2 = q * q, pq = p * q;
+  const int L = mmax + 2;
+#define TX(a, b) T[(size_t)((a) + 1) + (size_t)((b) + 1) * L]
+  cd s = (0.5 * (q2 - q)) * TX(m, n - 1);
+  s = s + (0.5 * (p2 - p)) * TX(m - 1, n);
+  s = s + (((1.0 + pq) - p2) - q2) * TX(m, n);
+  s = s + (0.5 * ((p2 - 2.0 * pq) + p)) * TX(m + 1, n);
+  s = s + (0.5 * ((q2 - 2.0 * pq) + q)) * TX(m, n + 1);
+  s = s + pq * TX(m + 1, n + 1);
+#undef TX
+  if (ms != 0.0 || ns != 0.0) s = s * cisd(-(ms * P.psi1 + ns * P.psi2));
+  return s;
+}
+
+// Counts every kernel the library launches (reported by pss_kernel_launches()).
+void pss_count_launch();
+
+// ---- host launchers (return 0 or a negative error code; errors via pss_set_error) ----
+// Modal tables (pss_tables.cu)
+void pss_tables_ring_fill(const StackParams &S, const PointParams *dP, int npts, int R, cd *dense,
+                          size_t point_stride, cudaStream_t st);
+void pss_tables_ring_sums(const PointParams *dP, int npts, int R, const cd *dense, size_t point_stride,
+                          double convtest, unsigned char *conv, cudaStream_t st);
+void pss_tables_find_mmax(int npts, int R, const unsigned char *conv, int *mmax, int *flag, cudaStream_t st);
+int pss_tables_finish(const cd *dense, int R, int mmax, const PointParams *dP1, cd *stage, cd *t1, cd *t2,
+                      cudaStream_t st);
+size_t pss_table_cap(int mmax);  // (mmax+2)^2 entries per padded table
+
+// Face-pair integrals and matrix fill (pss_fill.cu)
+void pss_filljk(const SheetDev &G, double ulocal, double psi1, double psi2, const double s1[2],
+                const double s2[2], JKDev jk, int *nonconv, cudaStream_t st);
+void pss_fill_pairs(const SheetDev &G, const PointParams *dP1, const JKDev &jk, const cd *t1, const cd *t2,
+                    int mmax, cd *zb, cudaStream_t st);
+// Assemble Z (row-major, ld columns).  z64 and/or (zr, zi) may be null.
+void pss_fill_assemble(const SheetDev &G, const PointParams *dP1, const cd *zb, cd *z64, float *zr, float *zi,
+                       long long ld, cudaStream_t st);
+
+// Basis-function transforms, right-hand sides, projection (pss_bfft.cu)
+void pss_bfft(const SheetDev &G, int nmodes, const double *kvec, double psi1, double psi2, cd *bf,
+              cudaStream_t st);
+void pss_rhs(int nbf, int nmodes, const cd *bf, const cd *src, cd *rhs, cudaStream_t st);
+void pss_project(int nbf, int nmodes, const cd *bf, const double *tobs, const cd *wobs, const cd *X, cd *dS,
+                 cudaStream_t st);
+
+// Dense complex LU and solves (pss_lu.cu); matrices row-major with leading dimension ld.
+int pss_lu64(int n, cd *A, long long ld, int *ipiv, int *info, void *ws, size_t ws_bytes, cudaStream_t st);
+int pss_lu32(int n, float *Ar, float *Ai, long long ld, int *ipiv, int *info, void *ws, size_t ws_bytes,
+             cudaStream_t st);
+size_t pss_lu_ws_bytes(int n, int precision);
+// ``done`` (device flag, may be null) makes the refinement kernels no-ops once converged.
+void pss_solve64(int n, const cd *LU, long long ld, const int *ipiv, int nrhs, cd *B, const int *done,
+                 cudaStream_t st);
+void pss_solve32(int n, const float *Lr, const float *Li, long long ld, const int *ipiv, int nrhs, cd *B,
+                 const int *done, cudaStream_t st);
+void pss_residual64(int n, const cd *A, long long ld, int nrhs, const cd *X, const cd *B, cd *Rout,
+                    const int *done, cudaStream_t st);
+void pss_axpy_norms(int n, int nrhs, cd *X, const cd *D, double *norms, const int *done, cudaStream_t st);
+void pss_refine_check(double *norms, double tol, int *done, int *status, int last, cudaStream_t st);

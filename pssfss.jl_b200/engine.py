@@ -1,0 +1,248 @@
+"""ctypes binding of ``libpssfss_b200.so`` (the CUDA hot path; C ABI in include/pssfss_b200.h).
+
+There is no CPU fallback: if the library cannot be loaded or no CUDA device is present,
+every call raises ``RuntimeError``.
+"""
+import ctypes
+import os
+import threading
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "libpssfss_b200.so")
+
+PSS_FP64 = 0
+PSS_FP32_REFINE = 1
+PRECISIONS = {"fp64": PSS_FP64, "fp32r": PSS_FP32_REFINE}
+
+STATUS_BITS = {1: "table_noconv", 2: "jk_noconv", 4: "singular", 8: "refine_noconv", 16: "nonfinite",
+               32: "fp64_fallback"}
+
+_lib = None
+_lock = threading.Lock()
+_ctx = {}
+_sheets = {}
+
+_P = ctypes.c_void_p
+_D = ctypes.c_double
+_I = ctypes.c_int
+_L = ctypes.c_int64
+_C = ctypes.c_char
+
+# name -> (restype, argtypes); every function declared in include/pssfss_b200.h
+SIGNATURES = {
+    "pss_last_error": (ctypes.c_char_p, []),
+    "pss_version": (_I, []),
+    "pss_kernel_launches": (_L, []),
+    "pss_ctx_create": (_I, [_I, _I, _P]),
+    "pss_ctx_destroy": (_I, [_P]),
+    "pss_sheet_create": (_I, [_P, _C, _D, _P, _P, _P, _P, _L, _P, _L, _P, _P, _P, _L, _L, _P, _P, _P, _L,
+                              _P, _P, _P]),
+    "pss_sheet_destroy": (_I, [_P]),
+    "pss_partial_gsms": (_I, [_P, _I, _P, _P, _P, _I, _D, _I, _P, _P, _I, _P, _P, _P, _P, _I, _P, _P]),
+    "pss_fill_matrix": (_I, [_P, _I, _P, _P, _P, _I, _D, _D, _D, _D, _P, _P]),
+    "pss_modal_tables": (_I, [_P, _I, _I, _P, _P, _P, _I, _D, _D, _D, _D, _P, _P, _D, _L, _P, _P, _P, _P]),
+    "pss_face_integrals": (_I, [_P, _D, _D, _D, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "pss_basis_transforms": (_I, [_P, _I, _P, _D, _D, _P]),
+    "pss_lu_solve": (_I, [_P, _I, _P, _I, _P, _I, _P, _P]),
+    "pss_last_timings": (_I, [_P, _P]),
+}
+
+
+def lib():
+    """Load the library (raises if it is missing: the CUDA path is the only path)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIBPATH):
+                raise RuntimeError(f"{LIBPATH} not built; run __graft_entry__.build() (nvcc, sm_100a)")
+            L = ctypes.CDLL(LIBPATH)
+            for name, (res, args) in SIGNATURES.items():
+                f = getattr(L, name)
+                f.restype = res
+                f.argtypes = args
+            _lib = L
+    return _lib
+
+
+def _check(rc, what):
+    if rc != 0:
+        msg = lib().pss_last_error().decode(errors="replace")
+        raise RuntimeError(f"{what} failed ({rc}): {msg}")
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _f64(x):
+    return np.ascontiguousarray(np.asarray(x, dtype=np.float64))
+
+
+def _c2d(x):
+    """complex array -> contiguous interleaved float64 view."""
+    a = np.ascontiguousarray(np.asarray(x, dtype=np.complex128))
+    return a
+
+
+def _i64(x):
+    return np.ascontiguousarray(np.asarray(x, dtype=np.int64))
+
+
+def context(device=0, nworkers=None):
+    """Per-device ``pss_ctx`` (created once)."""
+    if nworkers is None:
+        nworkers = int(os.environ.get("PSS_WORKERS", "4"))
+    key = (device, nworkers)
+    with _lock:
+        c = _ctx.get(key)
+    if c is None:
+        h = ctypes.c_void_p()
+        _check(lib().pss_ctx_create(device, nworkers, ctypes.byref(h)), "pss_ctx_create")
+        c = h
+        with _lock:
+            _ctx[key] = c
+    return c
+
+
+def region_arrays(layers):
+    eps = _c2d([l.epsr for l in layers])
+    mu = _c2d([l.mur for l in layers])
+    w = _f64([l.width for l in layers])
+    return eps, mu, w
+
+
+class DeviceSheet:
+    """A sheet uploaded to one device context (``pss_sheet``)."""
+
+    def __init__(self, ctx, sheet, rwg):
+        self.sheet, self.rwg = sheet, rwg
+        h = ctypes.c_void_p()
+        rho = _f64(sheet.rho)
+        fv = _i64(sheet.fv.ravel(order="F"))
+        fe = _i64(sheet.fe.ravel(order="F"))
+        fr = _f64(sheet.fr)
+        bff = _i64(rwg.bff.ravel(order="F"))
+        ebf = _i64(rwg.ebf)
+        eci = _i64(rwg.eci)
+        ufpm = _i64(rwg.ufpm.ravel(order="F"))
+        rep = _i64(rwg.ufp_rep)
+        _check(lib().pss_sheet_create(ctx, sheet.cls.encode(), sheet.units.units_per_meter, _p(_f64(sheet.s1)),
+                                      _p(_f64(sheet.s2)), _p(_f64(sheet.beta1)), _p(_f64(sheet.beta2)),
+                                      sheet.nnode, _p(rho), sheet.nface, _p(fv), _p(fe), _p(fr), sheet.nedge,
+                                      rwg.nbf, _p(bff), _p(ebf), _p(eci), rwg.nufp, _p(ufpm), _p(rep),
+                                      ctypes.byref(h)), "pss_sheet_create")
+        self.h = h
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().pss_sheet_destroy(self.h)
+        except Exception:
+            pass
+
+
+def device_sheet(sheet, rwg, device=0, nworkers=None):
+    ctx = context(device, nworkers)
+    key = (id(sheet), id(rwg), ctx.value)
+    ds = _sheets.get(key)
+    if ds is None or ds.sheet is not sheet or ds.rwg is not rwg:
+        ds = DeviceSheet(ctx, sheet, rwg)
+        _sheets[key] = ds
+    return ds
+
+
+def partial_gsms(sheet, rwg, points, region_rng, s, u, ios, precision="fp64", device=0, stats=None,
+                 nworkers=None):
+    """Scattered partial GSMs of one sheet at every point (``pss_partial_gsms``)."""
+    i1, i2 = region_rng
+    region = points[0].layers[i1 - 1:i2]
+    eps, mu, w = region_arrays(region)
+    npts = len(points)
+    nm = len(ios[0].wobs)
+    k0 = _f64([pt.k0 for pt in points])
+    psi = _f64([[io.psi1, io.psi2] for io in ios])
+    kvec = _f64(np.stack([io.kvec for io in ios]))
+    src = _c2d(np.stack([io.src for io in ios]))
+    tobs = _f64(np.stack([io.tobs for io in ios]))
+    wobs = _c2d(np.stack([io.wobs for io in ios]))
+    dS = np.zeros((npts, nm, nm), complex)       # per point column-major -> transpose below
+    status = np.zeros(npts, np.int32)
+    ds = device_sheet(sheet, rwg, device, nworkers)
+    _check(lib().pss_partial_gsms(ds.h, len(region), _p(eps), _p(mu), _p(w), s, float(u), npts, _p(k0),
+                                  _p(psi), nm, _p(kvec), _p(src), _p(tobs), _p(wobs), PRECISIONS[precision],
+                                  _p(dS), _p(status)), "pss_partial_gsms")
+    if stats is not None:
+        t = np.zeros(8)
+        lib().pss_last_timings(context(device, nworkers), _p(t))
+        stats.setdefault("status", []).extend(status.tolist())
+        stats["timings_ms"] = dict(zip(["tables", "face_integrals", "fill", "factor", "transforms", "solve",
+                                        "project", "total"], t.tolist()))
+    bad = status & (4 | 16)
+    if bad.any():
+        raise RuntimeError(f"solver status {status.tolist()} (singular or non-finite)")
+    return [d.T.copy() for d in dS]
+
+
+def fill_matrix(sheet, rwg, layers, s, u, k0, psi1, psi2, device=0):
+    ds = device_sheet(sheet, rwg, device)
+    eps, mu, w = region_arrays(layers)
+    n = rwg.nbf
+    Z = np.zeros((n, n), complex, order="F")
+    mm = ctypes.c_int()
+    _check(lib().pss_fill_matrix(ds.h, len(layers), _p(eps), _p(mu), _p(w), s, float(u), float(k0), float(psi1),
+                                 float(psi2), Z.ctypes.data_as(ctypes.c_void_p), ctypes.byref(mm)),
+           "pss_fill_matrix")
+    return Z, mm.value
+
+
+def modal_tables(magnetic, k0, u, psi1, psi2, layers, s, b1, b2, convtest=1e-7, device=0):
+    ctx = context(device)
+    eps, mu, w = region_arrays(layers)
+    cap = (2048 + 2) ** 2
+    t1 = np.zeros(cap, complex)
+    t2 = np.zeros(cap, complex)
+    mm = ctypes.c_int()
+    st = ctypes.c_int()
+    _check(lib().pss_modal_tables(ctx, int(magnetic), len(layers), _p(eps), _p(mu), _p(w), s, float(k0), float(u),
+                                  float(psi1), float(psi2), _p(_f64(b1)), _p(_f64(b2)), float(convtest), cap,
+                                  _p(t1), _p(t2), ctypes.byref(mm), ctypes.byref(st)), "pss_modal_tables")
+    L = (mm.value + 2) ** 2
+    return mm.value, t1[:L].copy(), t2[:L].copy(), st.value
+
+
+def face_integrals(sheet, rwg, ulocal, psi1, psi2, device=0):
+    ds = device_sheet(sheet, rwg, device)
+    n = rwg.nufp
+    out = {k: np.zeros(n, complex) for k in ("J", "Jxi", "Jeta", "K", "Kxi", "Keta")}
+    rho_r = np.zeros(2 * n)
+    rinv = np.zeros(n)
+    nc = ctypes.c_int()
+    _check(lib().pss_face_integrals(ds.h, float(ulocal), float(psi1), float(psi2), _p(out["J"]), _p(out["Jxi"]),
+                                    _p(out["Jeta"]), _p(out["K"]), _p(out["Kxi"]), _p(out["Keta"]), _p(rho_r),
+                                    _p(rinv), ctypes.byref(nc)), "pss_face_integrals")
+    out["rho_r"], out["rinv"], out["nonconv"] = rho_r, rinv, nc.value
+    return out
+
+
+def basis_transforms(sheet, rwg, kvecs, psi1, psi2, device=0):
+    ds = device_sheet(sheet, rwg, device)
+    kv = _f64(np.atleast_2d(kvecs))
+    nm = kv.shape[0]
+    F = np.zeros((nm, rwg.nbf, 2), complex)
+    _check(lib().pss_basis_transforms(ds.h, nm, _p(kv), float(psi1), float(psi2), _p(F)), "pss_basis_transforms")
+    return F
+
+
+def lu_solve(Z, B, precision="fp64", device=0):
+    ctx = context(device)
+    Z = np.asfortranarray(np.asarray(Z, complex))
+    B = np.asfortranarray(np.asarray(B, complex).reshape(Z.shape[0], -1))
+    n, nrhs = B.shape
+    X = np.zeros((n, nrhs), complex, order="F")
+    st = ctypes.c_int()
+    _check(lib().pss_lu_solve(ctx, n, Z.ctypes.data_as(ctypes.c_void_p), nrhs, B.ctypes.data_as(ctypes.c_void_p),
+                              PRECISIONS[precision], X.ctypes.data_as(ctypes.c_void_p), ctypes.byref(st)),
+           "pss_lu_solve")
+    return X, st.value

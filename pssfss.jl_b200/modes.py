@@ -23,7 +23,9 @@ def setup_modes(layer, k0, kvec):
     """Fill ``β``, ``γ``, ``Y``, ``c`` and ``tvec`` of ``layer`` (Modes.jl:298-322)."""
     b00 = np.array([kvec[0], kvec[1]], float)
     b1, b2 = layer.beta1, layer.beta2
-    area = TWOPI ** 2 / abs(b1[0] * b2[1] - b1[1] * b2[0])
+    cross = abs(b1[0] * b2[1] - b1[1] * b2[0])
+    # layers inside a Gblock carry no modes and no lattice: their area is never used
+    area = TWOPI ** 2 / cross if cross != 0 else math.inf
     ksq = _rmulc(k0 * k0, layer.epsr) * layer.mur
     n = len(layer.M)
     layer.beta = np.zeros((n, 2))
