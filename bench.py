@@ -1,0 +1,321 @@
+#!/usr/bin/env python
+"""Frequency points per second of the periodic-MoM fill + solve sweep on B200.
+
+Workload (the precision form of the meanderline polarizer): meander(a=5, b=10, h=6,
+w1=w2=0.3 mm, ntri=3000) -> 2840 triangles, N = 3976 RWG unknowns, on a 1 mm eps_r=2.2
+substrate between half-spaces, normal incidence, 101 frequencies 8..18 GHz.  One step =
+the whole 101-point sweep of the sheet's partial GSM: modal tables, face-pair integrals,
+fill, LU, basis transforms, solves (+ FP64 refinement) and modal projection.
+
+value  = sweep points / s from the library's CUDA-event span of each step (inputs already
+         on the device: mesh, topology and J/K cache resident);
+e2e    = the same through the C ABI call with host buffers (per-point inputs copied in,
+         dS copied out), CUDA events on the caller's stream around the call.
+The FP64 form is timed too (fp64_value) and its results give max|dS| of the FP32 form.
+
+--impl reference: the CPU oracle (C restatement + LAPACK) on the host cores, one point
+per step with the sweep's J/K pass amortised over the 101 points.
+
+Multi-GPU (torchrun): weak scaling, each rank runs its own 101-point sweep (frequency
+band shifted by rank); no collectives on the data path; device time max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+NFREQ = 101
+WORKLOAD = ("meanderline a=5 b=10 h=6 w1=w2=0.3 mm ntri=3000 (2840 faces, N=3976) on 1 mm eps_r=2.2, "
+            "normal incidence, 101 freqs 8-18 GHz")
+METRIC = "freq-points/sec fill+solve, FP32+refine vs FP64 on GPU at max|dS|<=1e-6; grads/s"
+GEMM_KERNEL = "k_gemm32 (complex Schur update, FP32 planes)"
+GEMM_TRAFFIC = None  # DRAM bytes per launch from the ncu capture in profiles/ (None until captured)
+
+
+def load_package():
+    import importlib.util
+    if "pssfss_b200" in sys.modules:
+        return sys.modules["pssfss_b200"]
+    pkgdir = os.path.join(ROOT, "pssfss.jl_b200")
+    spec = importlib.util.spec_from_file_location(
+        "pssfss_b200", os.path.join(pkgdir, "__init__.py"), submodule_search_locations=[pkgdir])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["pssfss_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def build_case(rank=0, npts=NFREQ):
+    pkg = load_package()
+    from pssfss_b200.analyze import make_plan, sheet_gblocks, sheet_io
+    sheet = pkg.meander(a=5, b=10, h=6, w1=0.3, w2=0.3, ntri=3000, units=pkg.mm)
+    strata = [pkg.Layer(), sheet, pkg.Layer(epsr=2.2, width=pkg.Length(1, pkg.mm)), pkg.Layer()]
+    shift = 0.01 * rank
+    freqs = np.linspace(8.0 + shift, 18.0 + shift, NFREQ)[:npts]
+    plan = make_plan(strata, freqs, {"θ": 0.0, "ϕ": 0.0})
+    (ig, (i1, i2), isht, s), = sheet_gblocks(plan)
+    rwg = plan.rwgdat[isht - 1]
+    u = plan.uvec[isht - 1]
+    ios = [sheet_io(pt.layers[i1 - 1:i2], sheet, s, pt.k0, pt.beta00) for pt in plan.points]
+    return dict(plan=plan, sheet=sheet, rwg=rwg, rng=(i1, i2), s=s, u=u, ios=ios)
+
+
+class ClockSampler:
+    """nvidia-smi sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p, "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def run_reference(args, rank, world):
+    """CPU oracle on the host cores (bounded sample: one sweep point per step)."""
+    if rank != 0:
+        return
+    sys.path.insert(0, ROOT)
+    import oracle
+    case = build_case(0)
+    sheet, rwg, (i1, i2), s, u = case["sheet"], case["rwg"], case["rng"], case["s"], case["u"]
+    pts = case["plan"].points
+    t0 = time.perf_counter()
+    io0 = case["ios"][0]
+    jk = oracle.filljk(sheet, rwg, u / sheet.units.units_per_meter, io0.psi1, io0.psi2)
+    oracle._jk_cache[id(sheet)] = jk
+    t_jk = time.perf_counter() - t0
+    times = []
+    for step in range(args.warmup + args.steps):
+        i = (step * 37) % len(pts)
+        pt = pts[i]
+        region = pt.layers[i1 - 1:i2]
+        t = time.perf_counter()
+        oracle.partial_dS(sheet, rwg, region, s, pt.k0, u, case["ios"][i])
+        dt = time.perf_counter() - t
+        if step >= args.warmup:
+            times.append(dt)
+    per_point = statistics.mean(times) + t_jk / NFREQ
+    value = 1.0 / per_point
+    cores = os.cpu_count()
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "freq-points/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_point * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "data": "synthetic (structured meander mesh built from the reference's element recipe)",
+            "config": {"workload": WORKLOAD, "sample": "1 sweep point per step (fill+LU+solve+projection), "
+                                                       "J/K pass amortised over 101 points",
+                       "l2": "working set > L2 (host run)"},
+            "cpu_baseline": {"value": value, "unit": "freq-points/s", "cores": cores, "kind": "port",
+                             "sample": f"{args.steps} points of the sweep + one J/K pass ({t_jk:.1f} s)"},
+            "e2e": {"value": value, "unit": "freq-points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_sample(case):
+    """Bounded CPU-oracle sample for the report line (~10-30 s on the host cores)."""
+    sys.path.insert(0, ROOT)
+    import oracle
+    sheet, rwg, (i1, i2), s, u = case["sheet"], case["rwg"], case["rng"], case["s"], case["u"]
+    pt = case["plan"].points[NFREQ // 2]
+    io = case["ios"][NFREQ // 2]
+    t0 = time.perf_counter()
+    jk = oracle.filljk(sheet, rwg, u / sheet.units.units_per_meter, io.psi1, io.psi2)
+    t_jk = time.perf_counter() - t0
+    oracle._jk_cache[id(sheet)] = jk
+    t1 = time.perf_counter()
+    oracle.partial_dS(sheet, rwg, pt.layers[i1 - 1:i2], s, pt.k0, u, io)
+    t_pt = time.perf_counter() - t1
+    return {"value": 1.0 / (t_pt + t_jk / NFREQ), "unit": "freq-points/s", "cores": os.cpu_count(),
+            "kind": "port", "sample": f"1 sweep point (fill+LU+solve+projection {t_pt:.2f} s) + J/K pass "
+                                      f"({t_jk:.1f} s) amortised over {NFREQ} points"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--npts", type=int, default=NFREQ,
+                    help="sweep points per step (default: the full 101-point sweep; fewer only for profiling)")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+    pkg = load_package()
+    from pssfss_b200 import engine
+    case = build_case(rank, args.npts)
+    dev = local
+    call_args = (case["sheet"], case["rwg"], case["plan"].points, case["rng"], case["s"], case["u"], case["ios"])
+
+    def step(precision):
+        st = {}
+        dS = engine.partial_gsms(*call_args, precision=precision, device=dev, stats=st)
+        return dS, st
+
+    for _ in range(args.warmup):
+        dS32, _ = step("fp32r")
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(dev)
+    sampler.start()
+    l0 = engine.lib().pss_kernel_launches()
+    spans, e2e_ms, statuses = [], [], []
+    gemm = {"launches": 0, "ms": 0.0, "flops": 0.0}
+    phases = {}
+    engine.set_profiling(True, device=dev)
+    for _ in range(args.steps):
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        dS32, st = step("fp32r")
+        ev1.record()
+        ev1.synchronize()
+        e2e_ms.append(ev0.elapsed_time(ev1))
+        spans.append(st["timings_ms"]["total"])
+        statuses.extend(st["status"])
+        g = engine.profile_result(device=dev)
+        for k in gemm:
+            gemm[k] += g[k]
+        for k, v in st["timings_ms"].items():
+            phases[k] = phases.get(k, 0.0) + v / args.steps
+    engine.set_profiling(False, device=dev)
+    torch.cuda.synchronize()
+    launches = engine.lib().pss_kernel_launches() - l0
+    clocks = sampler.stop()
+    if dist:
+        dist.barrier()
+    # FP64 form (same sweep) for the speed-up and the accuracy gate
+    spans64 = []
+    for _ in range(max(1, args.fp64_steps)):
+        dS64, st64 = step("fp64")
+        spans64.append(st64["timings_ms"]["total"])
+    max_dS = float(max(np.max(np.abs(a - b)) for a, b in zip(dS32, dS64)))
+
+    tot_ms = sum(spans)
+    tot_e2e = sum(e2e_ms)
+    if dist:
+        t = torch.tensor([tot_ms, tot_e2e, float(np.mean(spans64)), max_dS], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot_ms, tot_e2e, mean64, max_dS = t.tolist()
+    else:
+        mean64 = float(np.mean(spans64))
+    npts = len(case["plan"].points)
+    value = world * npts * args.steps / (tot_ms / 1e3)
+    e2e = world * npts * args.steps / (tot_e2e / 1e3)
+    fp64_value = world * npts / (mean64 / 1e3)
+    nm = len(case["ios"][0].wobs)
+    h2d = npts * (8 + 16 + nm * (16 + 32 + 16 + 16))
+    d2h = npts * (nm * nm * 16 + 4)
+    if rank == 0:
+        pk, pk_kind = peaks()
+        line = {"metric": METRIC, "value": value, "unit": "freq-points/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "c64+c128-refine",
+                "data": "synthetic (structured meander mesh built from the reference's element recipe)",
+                "config": {"workload": WORKLOAD, "points_per_step": npts, "precision": "fp32r",
+                           "l2": "working set > L2 (Z is 253 MB FP64 + 126 MB FP32 per point)",
+                           "parallelism": f"weak x{world}: independent sweeps per GPU"},
+                "fp64_value": fp64_value, "fp32r_speedup_vs_fp64": value / fp64_value / world * world,
+                "max_abs_dS_fp32r_vs_fp64": max_dS,
+                "refine_fallbacks": int(sum(1 for s in statuses if s & 32)),
+                "e2e": {"value": e2e, "unit": "freq-points/s", "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h},
+                "gpu_launches": int(launches), "clocks": clocks,
+                "phase_ms_per_step_worker0": phases, "peaks_source": pk_kind}
+        # Dominant kernel: the Schur-complement GEMM of the LU, timed per launch with CUDA
+        # events on its own stream during the timed steps; achieved = algorithmic flops
+        # (8*M*N*K per complex update) / summed launch time.
+        if gemm["ms"] > 0:
+            achieved = gemm["flops"] / (gemm["ms"] / 1e3) / 1e12
+            peak = float(pk.get("bf16_tflops_sustained", pk["bf16_tflops"]))
+            line["roofline"] = {"kernel": GEMM_KERNEL, "bound": "tensor", "achieved": achieved, "peak": peak,
+                                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": GEMM_TRAFFIC,
+                                "launches": gemm["launches"], "avg_launch_us": 1e3 * gemm["ms"] / gemm["launches"],
+                                "peak_note": f"{pk_kind} dense bf16 (sustained) tensor peak"}
+        else:
+            line["roofline"] = None
+        if not args.no_cpu_baseline:
+            try:
+                line["cpu_baseline"] = cpu_baseline_sample(case)
+            except Exception as e:  # report, never fake
+                line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -112,6 +112,12 @@ int pss_lu_solve(pss_ctx *ctx, int n, const double *Z, int nrhs, const double *B
  * [tables, face_integrals, fill, factor, transforms+rhs, solve+refine, projection, total]. */
 int pss_last_timings(pss_ctx *ctx, double *ms8);
 
+/* Per-launch CUDA-event timing of the Schur-complement GEMM (the dominant kernel) during
+ * pss_partial_gsms calls while enabled.  out3 = [launches, summed ms, summed algorithmic
+ * flops (8*M*N*K per complex update)] of the last call. */
+int pss_profile(pss_ctx *ctx, int enable);
+int pss_profile_result(pss_ctx *ctx, double *out3);
+
 #ifdef __cplusplus
 }
 #endif

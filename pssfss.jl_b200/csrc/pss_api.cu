@@ -27,6 +27,32 @@ static std::atomic<long long> g_launches{0};
 
 void pss_count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
+namespace {
+struct KProf {
+  std::vector<cudaEvent_t> e0, e1;
+  std::vector<double> flops;
+};
+thread_local KProf *g_kprof = nullptr;
+}  // namespace
+
+int pss_prof_begin(cudaStream_t st) {
+  if (!g_kprof) return -1;
+  cudaEvent_t a;
+  if (cudaEventCreate(&a) != cudaSuccess) return -1;
+  cudaEventRecord(a, st);
+  g_kprof->e0.push_back(a);
+  return (int)g_kprof->e0.size() - 1;
+}
+
+void pss_prof_end(int token, cudaStream_t st, double flops) {
+  if (token < 0 || !g_kprof) return;
+  cudaEvent_t b;
+  cudaEventCreate(&b);
+  cudaEventRecord(b, st);
+  g_kprof->e1.push_back(b);
+  g_kprof->flops.push_back(flops);
+}
+
 void pss_set_error(const char *fmt, ...) {
   va_list ap;
   va_start(ap, fmt);
@@ -38,8 +64,7 @@ namespace {
 
 constexpr int kRing0 = 160;  // ring budget of the first table pass (mmax <= 320)
 constexpr int kTableChunk = 16;
-constexpr int kMaxRefine = 40;  // steps after convergence are no-ops (device flag)
-constexpr double kRefineTol = 1e-13;
+constexpr int kMaxRefine = 10;  // refinement steps before the FP64 fallback (zcgesv allows 30)
 
 struct DevBuf {
   void *p = nullptr;
@@ -83,10 +108,43 @@ struct JKBufs {
   }
 };
 
+__global__ void k_info_to_status(int *info, int *status);
+
 struct Worker {
   cudaStream_t st = nullptr;
-  DevBuf zb, z64, zr, zi, ipiv, info, bf, rhs, X, R, norms, done, nonconv;
+  DevBuf zb, z64, zr, zi, ipiv, info, bf, rhs, X, R, D, nonconv, luws, solvews;
   JKBufs jk;
+  SolveWS sws;
+  int ensure_solver(int n, int nrhs) {
+    if (ipiv.ensure((size_t)n * sizeof(int)) || info.ensure(sizeof(int))) return -3;
+    if (luws.ensure(std::max(pss_lu_ws_bytes(n, 0), pss_lu_ws_bytes(n, 1)))) return -3;
+    if (solvews.ensure(pss_solve_ws_bytes(n))) return -3;
+    sws.bind(solvews.p, n);
+    const size_t v = (size_t)n * nrhs * sizeof(cd);
+    if (rhs.ensure(v) || X.ensure(v) || R.ensure(v) || D.ensure(v)) return -3;
+    return 0;
+  }
+  // LU of the worker's matrix (FP64 in z64, or FP32 planes zr/zi) and solve rhs -> X,
+  // refined against z64 in FP32 mode.  Status bits go to *status (device).
+  int factor_solve(int n, long long ld, int prec, int nrhs, int maxit, int *status) {
+    int rc;
+    if (prec == PSS_FP64) rc = pss_lu64(n, z64.as<cd>(), ld, ipiv.as<int>(), info.as<int>(), luws.p, luws.n, st);
+    else rc = pss_lu32(n, zr.as<float>(), zi.as<float>(), ld, ipiv.as<int>(), info.as<int>(), luws.p, luws.n, st);
+    if (rc) return rc;
+    pss_count_launch();
+    k_info_to_status<<<1, 1, 0, st>>>(info.as<int>(), status);
+    const cd *L64 = prec == PSS_FP64 ? z64.as<cd>() : nullptr;
+    const float *Lr = prec == PSS_FP64 ? nullptr : zr.as<float>();
+    const float *Li = prec == PSS_FP64 ? nullptr : zi.as<float>();
+    if ((rc = pss_solve_prepare(sws, L64, Lr, Li, ld, ipiv.as<int>(), st))) return rc;
+    if ((rc = pss_solve_lu(sws, L64, Lr, Li, ld, nrhs, rhs.as<cd>(), X.as<cd>(), nullptr, st))) return rc;
+    if (prec == PSS_FP32_REFINE &&
+        (rc = pss_refine(sws, z64.as<cd>(), ld, Lr, Li, nrhs, rhs.as<cd>(), X.as<cd>(), R.as<cd>(), D.as<cd>(),
+                         maxit, status, st)))
+      return rc;
+    pss_solve_status(sws, status, st);
+    return 0;
+  }
 };
 
 __global__ void k_info_to_status(int *info, int *status) {
@@ -121,6 +179,8 @@ struct pss_ctx {
   DevBuf params, dense, conv, mm, stage, tables, bigdense, modes, dS, status;
   std::vector<DevBuf> bigtables;
   double last_ms[8] = {0};
+  bool prof_on = false;
+  double prof[3] = {0, 0, 0};  // GEMM launches, summed ms, summed algorithmic flops
 };
 
 struct pss_sheet {
@@ -316,12 +376,9 @@ int ensure_worker(Worker &w, const pss_sheet *sh, int nm, int precision, bool ow
   if (precision == PSS_FP32_REFINE) {
     if (w.zr.ensure(n * n * sizeof(float)) || w.zi.ensure(n * n * sizeof(float))) return -3;
   }
-  if (w.ipiv.ensure(n * sizeof(int)) || w.info.ensure(sizeof(int)) || w.nonconv.ensure(sizeof(int))) return -3;
+  if (w.nonconv.ensure(sizeof(int))) return -3;
   if (w.bf.ensure((size_t)nm * n * 2 * sizeof(cd))) return -3;
-  if (w.rhs.ensure((size_t)nm * n * sizeof(cd)) || w.X.ensure((size_t)nm * n * sizeof(cd)) ||
-      w.R.ensure((size_t)nm * n * sizeof(cd)))
-    return -3;
-  if (w.norms.ensure(2 * sizeof(double)) || w.done.ensure(sizeof(int))) return -3;
+  if (w.ensure_solver((int)n, nm)) return -3;
   if (own_jk && w.jk.ensure(sh->nufp)) return -3;
   PSS_CUDA_TRY(cudaMemsetAsync(w.info.p, 0, sizeof(int), w.st));
   PSS_CUDA_TRY(cudaMemsetAsync(w.nonconv.p, 0, sizeof(int), w.st));
@@ -369,8 +426,8 @@ int pss_ctx_destroy(pss_ctx *c) {
   cudaSetDevice(c->device);
   cudaDeviceSynchronize();
   for (auto &w : c->w) {
-    for (DevBuf *b : {&w.zb, &w.z64, &w.zr, &w.zi, &w.ipiv, &w.info, &w.bf, &w.rhs, &w.X, &w.R, &w.norms, &w.done,
-                      &w.nonconv})
+    for (DevBuf *b : {&w.zb, &w.z64, &w.zr, &w.zi, &w.ipiv, &w.info, &w.bf, &w.rhs, &w.X, &w.R, &w.D, &w.nonconv,
+                      &w.luws, &w.solvews})
       b->release();
     w.jk.buf.release();
     if (w.st) cudaStreamDestroy(w.st);
@@ -575,6 +632,8 @@ int pss_partial_gsms(pss_sheet *sh, int nl, const double *eps, const double *mu,
   const int n = sh->nbf;
   const long long ld = n;
   std::vector<cudaEvent_t> ev;
+  KProf kprof;
+  g_kprof = c->prof_on ? &kprof : nullptr;
   // One point through fill, LU, transforms, solve(s) and projection on worker w's stream.
   auto run_point = [&](int i, int prec, Worker &w, bool rec) -> int {
     cudaStream_t st = w.st;
@@ -600,34 +659,15 @@ int pss_partial_gsms(pss_sheet *sh, int nl, const double *eps, const double *mu,
     float *zi = prec == PSS_FP32_REFINE ? w.zi.as<float>() : nullptr;
     pss_fill_assemble(sh->G, Pi, w.zb.as<cd>(), w.z64.as<cd>(), zr, zi, ld, st);
     if (rec) cudaEventRecord(e[2], st);
-    int rc2;
-    if (prec == PSS_FP64) rc2 = pss_lu64(n, w.z64.as<cd>(), ld, w.ipiv.as<int>(), w.info.as<int>(), nullptr, 0, st);
-    else rc2 = pss_lu32(n, zr, zi, ld, w.ipiv.as<int>(), w.info.as<int>(), nullptr, 0, st);
-    if (rc2) return rc2;
-    pss_count_launch();
-    k_info_to_status<<<1, 1, 0, st>>>(w.info.as<int>(), dstatus + i);
-    if (rec) cudaEventRecord(e[3], st);
     const double *kv = (const double *)(mb + off_k) + (size_t)i * nmodes * 2;
     const cd *sv = (const cd *)(mb + off_s) + (size_t)i * nmodes * 2;
     const double *tv = (const double *)(mb + off_t) + (size_t)i * nmodes * 2;
     const cd *wv = (const cd *)(mb + off_w) + (size_t)i * nmodes;
     pss_bfft(sh->G, nmodes, kv, p1, p2, w.bf.as<cd>(), st);
     pss_rhs(n, nmodes, w.bf.as<cd>(), sv, w.rhs.as<cd>(), st);
-    PSS_CUDA_TRY(cudaMemcpyAsync(w.X.p, w.rhs.p, (size_t)n * nmodes * sizeof(cd), cudaMemcpyDeviceToDevice, st));
-    if (rec) cudaEventRecord(e[4], st);
-    if (prec == PSS_FP64) {
-      pss_solve64(n, w.z64.as<cd>(), ld, w.ipiv.as<int>(), nmodes, w.X.as<cd>(), nullptr, st);
-    } else {
-      pss_solve32(n, zr, zi, ld, w.ipiv.as<int>(), nmodes, w.X.as<cd>(), nullptr, st);
-      PSS_CUDA_TRY(cudaMemsetAsync(w.done.p, 0, sizeof(int), st));
-      PSS_CUDA_TRY(cudaMemsetAsync(w.norms.p, 0, 2 * sizeof(double), st));
-      for (int it = 0; it < kMaxRefine; ++it) {
-        pss_residual64(n, w.z64.as<cd>(), ld, nmodes, w.X.as<cd>(), w.rhs.as<cd>(), w.R.as<cd>(), w.done.as<int>(), st);
-        pss_solve32(n, zr, zi, ld, w.ipiv.as<int>(), nmodes, w.R.as<cd>(), w.done.as<int>(), st);
-        pss_axpy_norms(n, nmodes, w.X.as<cd>(), w.R.as<cd>(), w.norms.as<double>(), w.done.as<int>(), st);
-        pss_refine_check(w.norms.as<double>(), kRefineTol, w.done.as<int>(), dstatus + i, it == kMaxRefine - 1, st);
-      }
-    }
+    if (rec) { cudaEventRecord(e[3], st); cudaEventRecord(e[4], st); }
+    int rc2 = w.factor_solve(n, ld, prec, nmodes, kMaxRefine, dstatus + i);
+    if (rc2) return rc2;
     if (rec) cudaEventRecord(e[5], st);
     pss_project(n, nmodes, w.bf.as<cd>(), tv, wv, w.X.as<cd>(), c->dS.as<cd>() + (size_t)i * nm2, st);
     if (rec) { cudaEventRecord(e[6], st); cudaEventRecord(e[7], st); }
@@ -680,6 +720,17 @@ int pss_partial_gsms(pss_sheet *sh, int nl, const double *eps, const double *mu,
       c->last_ms[q + 1] += ms;
     }
   }
+  g_kprof = nullptr;
+  c->prof[0] = c->prof[1] = c->prof[2] = 0;
+  for (size_t q = 0; q < kprof.e1.size(); ++q) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, kprof.e0[q], kprof.e1[q]);
+    c->prof[0] += 1;
+    c->prof[1] += ms;
+    c->prof[2] += kprof.flops[q];
+  }
+  for (auto e : kprof.e0) cudaEventDestroy(e);
+  for (auto e : kprof.e1) cudaEventDestroy(e);
   c->last_ms[0] = tables_ms;
   c->last_ms[7] = span_ms;
   for (auto e : ev) cudaEventDestroy(e);
@@ -689,6 +740,18 @@ int pss_partial_gsms(pss_sheet *sh, int nl, const double *eps, const double *mu,
 int pss_last_timings(pss_ctx *c, double *ms8) {
   if (!c || !ms8) return -1;
   for (int q = 0; q < 8; ++q) ms8[q] = c->last_ms[q];
+  return 0;
+}
+
+int pss_profile(pss_ctx *c, int enable) {
+  if (!c) { pss_set_error("null context"); return -1; }
+  c->prof_on = enable != 0;
+  return 0;
+}
+
+int pss_profile_result(pss_ctx *c, double *out3) {
+  if (!c || !out3) { pss_set_error("null argument"); return -1; }
+  for (int q = 0; q < 3; ++q) out3[q] = c->prof[q];
   return 0;
 }
 
@@ -798,57 +861,31 @@ int pss_lu_solve(pss_ctx *c, int n, const double *Z, int nrhs, const double *B, 
   std::vector<cd> h(nn);
   for (size_t m = 0; m < (size_t)n; ++m)
     for (size_t q = 0; q < (size_t)n; ++q) h[m * n + q] = mkcd(Z[2 * (m + q * n)], Z[2 * (m + q * n) + 1]);
-  if (w.z64.ensure(nn * sizeof(cd)) || w.ipiv.ensure(n * sizeof(int)) || w.info.ensure(sizeof(int)) ||
-      w.rhs.ensure((size_t)n * nrhs * sizeof(cd)) || w.X.ensure((size_t)n * nrhs * sizeof(cd)) ||
-      w.R.ensure((size_t)n * nrhs * sizeof(cd)) || w.norms.ensure(2 * sizeof(double)) || w.done.ensure(sizeof(int)))
-    return -3;
+  if (w.z64.ensure(nn * sizeof(cd)) || w.ensure_solver(n, nrhs)) return -3;
   DevBuf st_buf;
   if (st_buf.ensure(sizeof(int))) return -3;
   PSS_CUDA_TRY(cudaMemset(st_buf.p, 0, sizeof(int)));
   PSS_CUDA_TRY(cudaMemset(w.info.p, 0, sizeof(int)));
   PSS_CUDA_TRY(cudaMemcpy(w.z64.p, h.data(), nn * sizeof(cd), cudaMemcpyHostToDevice));
   PSS_CUDA_TRY(cudaMemcpy(w.rhs.p, B, (size_t)n * nrhs * sizeof(cd), cudaMemcpyHostToDevice));
-  PSS_CUDA_TRY(cudaMemcpy(w.X.p, B, (size_t)n * nrhs * sizeof(cd), cudaMemcpyHostToDevice));
   int rc;
-  if (precision == PSS_FP64) {
-    rc = pss_lu64(n, w.z64.as<cd>(), n, w.ipiv.as<int>(), w.info.as<int>(), nullptr, 0, st);
-    if (rc) return rc;
-    pss_solve64(n, w.z64.as<cd>(), n, w.ipiv.as<int>(), nrhs, w.X.as<cd>(), nullptr, st);
-  } else {
+  if (precision == PSS_FP32_REFINE) {
     if (w.zr.ensure(nn * sizeof(float)) || w.zi.ensure(nn * sizeof(float))) return -3;
     std::vector<float> hr(nn), hi(nn);
     for (size_t i = 0; i < nn; ++i) { hr[i] = (float)h[i].x; hi[i] = (float)h[i].y; }
     PSS_CUDA_TRY(cudaMemcpy(w.zr.p, hr.data(), nn * sizeof(float), cudaMemcpyHostToDevice));
     PSS_CUDA_TRY(cudaMemcpy(w.zi.p, hi.data(), nn * sizeof(float), cudaMemcpyHostToDevice));
-    rc = pss_lu32(n, w.zr.as<float>(), w.zi.as<float>(), n, w.ipiv.as<int>(), w.info.as<int>(), nullptr, 0, st);
-    if (rc) return rc;
-    pss_solve32(n, w.zr.as<float>(), w.zi.as<float>(), n, w.ipiv.as<int>(), nrhs, w.X.as<cd>(), nullptr, st);
-    PSS_CUDA_TRY(cudaMemsetAsync(w.done.p, 0, sizeof(int), st));
-    PSS_CUDA_TRY(cudaMemsetAsync(w.norms.p, 0, 2 * sizeof(double), st));
-    for (int it = 0; it < kMaxRefine; ++it) {
-      pss_residual64(n, w.z64.as<cd>(), n, nrhs, w.X.as<cd>(), w.rhs.as<cd>(), w.R.as<cd>(), w.done.as<int>(), st);
-      pss_solve32(n, w.zr.as<float>(), w.zi.as<float>(), n, w.ipiv.as<int>(), nrhs, w.R.as<cd>(), w.done.as<int>(), st);
-      pss_axpy_norms(n, nrhs, w.X.as<cd>(), w.R.as<cd>(), w.norms.as<double>(), w.done.as<int>(), st);
-      pss_refine_check(w.norms.as<double>(), kRefineTol, w.done.as<int>(), st_buf.as<int>(), it == kMaxRefine - 1, st);
-    }
   }
-  pss_count_launch();
-  k_info_to_status<<<1, 1, 0, st>>>(w.info.as<int>(), st_buf.as<int>());
+  if ((rc = w.factor_solve(n, n, precision, nrhs, kMaxRefine, st_buf.as<int>()))) return rc;
   PSS_CUDA_TRY(cudaStreamSynchronize(st));
   PSS_CUDA_TRY(cudaGetLastError());
   int hs = 0;
   PSS_CUDA_TRY(cudaMemcpy(&hs, st_buf.p, sizeof(int), cudaMemcpyDeviceToHost));
   if (precision == PSS_FP32_REFINE && (hs & (PSS_ST_REFINE_NOCONV | PSS_ST_NONFINITE))) {
     // stalled refinement: FP64 factorisation of the original matrix
-    PSS_CUDA_TRY(cudaMemset(w.info.p, 0, sizeof(int)));
     PSS_CUDA_TRY(cudaMemset(st_buf.p, 0, sizeof(int)));
     PSS_CUDA_TRY(cudaMemcpy(w.z64.p, h.data(), nn * sizeof(cd), cudaMemcpyHostToDevice));
-    PSS_CUDA_TRY(cudaMemcpy(w.X.p, B, (size_t)n * nrhs * sizeof(cd), cudaMemcpyHostToDevice));
-    rc = pss_lu64(n, w.z64.as<cd>(), n, w.ipiv.as<int>(), w.info.as<int>(), nullptr, 0, st);
-    if (rc) return rc;
-    pss_solve64(n, w.z64.as<cd>(), n, w.ipiv.as<int>(), nrhs, w.X.as<cd>(), nullptr, st);
-    pss_count_launch();
-    k_info_to_status<<<1, 1, 0, st>>>(w.info.as<int>(), st_buf.as<int>());
+    if ((rc = w.factor_solve(n, n, PSS_FP64, nrhs, 0, st_buf.as<int>()))) return rc;
     PSS_CUDA_TRY(cudaStreamSynchronize(st));
     PSS_CUDA_TRY(cudaMemcpy(&hs, st_buf.p, sizeof(int), cudaMemcpyDeviceToHost));
     hs |= PSS_ST_FP64_FALLBACK;

@@ -88,6 +88,10 @@ __device__ __forceinline__ cd sigma_interp(const cd *__restrict__ T, int mmax, c
 
 // Counts every kernel the library launches (reported by pss_kernel_launches()).
 void pss_count_launch();
+// Optional CUDA-event timing of the Schur-complement GEMM launches (pss_profile): returns
+// a token (-1 when profiling is off) to pass to pss_prof_end with the launch's flops.
+int pss_prof_begin(cudaStream_t st);
+void pss_prof_end(int token, cudaStream_t st, double flops);
 
 // ---- host launchers (return 0 or a negative error code; errors via pss_set_error) ----
 // Modal tables (pss_tables.cu)
@@ -121,12 +125,22 @@ int pss_lu64(int n, cd *A, long long ld, int *ipiv, int *info, void *ws, size_t 
 int pss_lu32(int n, float *Ar, float *Ai, long long ld, int *ipiv, int *info, void *ws, size_t ws_bytes,
              cudaStream_t st);
 size_t pss_lu_ws_bytes(int n, int precision);
-// ``done`` (device flag, may be null) makes the refinement kernels no-ops once converged.
-void pss_solve64(int n, const cd *LU, long long ld, const int *ipiv, int nrhs, cd *B, const int *done,
-                 cudaStream_t st);
-void pss_solve32(int n, const float *Lr, const float *Li, long long ld, const int *ipiv, int nrhs, cd *B,
-                 const int *done, cudaStream_t st);
-void pss_residual64(int n, const cd *A, long long ld, int nrhs, const cd *X, const cd *B, cd *Rout,
-                    const int *done, cudaStream_t st);
-void pss_axpy_norms(int n, int nrhs, cd *X, const cd *D, double *norms, const int *done, cudaStream_t st);
-void pss_refine_check(double *norms, double tol, int *done, int *status, int last, cudaStream_t st);
+
+// Triangular solves and refinement (pss_trsv.cu).  The factor is either FP64 (LU64) or
+// FP32 planes (Lr, Li); pass the other as null.
+struct SolveWS {
+  int n = 0, nblk = 0, epoch = 0;
+  cd *Dinv = nullptr;      // inverses of the 64x64 diagonal blocks (L and U)
+  int *perm = nullptr;     // pivot permutation
+  int *ctrl = nullptr;     // ticket, error flag, done flag, per-block epoch flags
+  double *norms = nullptr; // refinement norms
+  void bind(void *base, int n_);
+};
+size_t pss_solve_ws_bytes(int n);
+int pss_solve_prepare(SolveWS &ws, const cd *LU64, const float *Lr, const float *Li, long long ld, const int *ipiv,
+                      cudaStream_t st);
+int pss_solve_lu(SolveWS &ws, const cd *LU64, const float *Lr, const float *Li, long long ld, int nrhs, const cd *B,
+                 cd *X, const int *done, cudaStream_t st);
+int pss_refine(SolveWS &ws, const cd *A, long long ld, const float *Lr, const float *Li, int nrhs, const cd *B,
+               cd *X, cd *R, cd *D, int maxit, int *status, cudaStream_t st);
+void pss_solve_status(SolveWS &ws, int *status, cudaStream_t st);

@@ -1,20 +1,21 @@
-// K4/K5: dense complex LU with partial pivoting and the multi-RHS solves.
+// K4: dense complex LU with partial pivoting (replaces LAPACK zgetrf behind lu!,
+// PSSFSS.jl:401, 526).
 //
-// Replaces LAPACK zgetrf / zgetrs (LinearAlgebra.lu! / ldiv!, PSSFSS.jl:401,439).
-// Matrices are row-major (row swaps are contiguous).  Blocked right-looking LU with a
-// two-level panel:
-//   * the narrow panel (W columns) is factored by one thread-block cluster: its rows are
-//     spread over the CTAs' shared memory, each column's pivot is found by a CTA-local
-//     argmax plus an exchange of candidates through distributed shared memory, and the
-//     pivot row is broadcast the same way (two cluster barriers per column);
-//   * pivots follow LAPACK izamax: largest |re|+|im|, first index on ties;
-//   * row interchanges, the unit-lower TRSM of the block row and the Schur-complement
-//     GEMM run as separate kernels.  In FP32 mode the matrix is two float planes
-//     (real, imaginary) and the Schur update is the complex product written as real
-//     products C_r -= L_r U_r - L_i U_i, C_i -= L_r U_i + L_i U_r.
-// Solves: one CTA per right-hand-side set (latency-bound; batches of frequency points
-// run concurrently on other SMs), FP64 arithmetic even with FP32 factors, so iterative
-// refinement against the FP64 matrix recovers FP64 accuracy.
+// Matrices are row-major (row interchanges are contiguous).  Blocked right-looking LU,
+// two-level: an outer block of NB columns is factored as panels of W columns.
+//   * k_panel: one thread-block cluster (8 CTAs) owns a W-column panel; its rows are
+//     spread over the CTAs' shared memory and never move during the factorisation.  For
+//     each column every CTA pushes its local pivot candidate (|re|+|im| as LAPACK izamax,
+//     the row index, and the candidate row itself) into every CTA's shared memory, one
+//     cluster barrier makes them visible, and every CTA picks the same winner and applies
+//     the rank-1 update to its own active rows - one barrier and no remote round trip per
+//     column.  At the end the LAPACK swap sequence (ipiv) is replayed once and each CTA
+//     writes its rows to their final positions.
+//   * k_laswp applies the panel's interchanges to the other columns.
+//   * the block-row triangular solve U12 = L11^{-1} A12 uses the explicit inverse of the
+//     unit-lower diagonal block (k_tri_inv, then k_trsm_apply, a small dense product).
+//   * the Schur complement A22 -= L21 U12 is the GEMM (k_gemm64 / k_gemm32).
+// In FP32 mode the matrix is two float planes (real, imaginary).
 #include <cooperative_groups.h>
 #include "pss_internal.cuh"
 
@@ -39,6 +40,8 @@ template <class E>
 __device__ __forceinline__ E cmulE(E a, E b) { return E{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x}; }
 template <class E>
 __device__ __forceinline__ E csubE(E a, E b) { return E{a.x - b.x, a.y - b.y}; }
+template <class E>
+__device__ __forceinline__ E caddE(E a, E b) { return E{a.x + b.x, a.y + b.y}; }
 
 // Matrix accessor: FP64 interleaved (A), FP32 planes (Ar, Ai).
 template <bool F32>
@@ -56,48 +59,44 @@ struct Mat {
   }
 };
 
-constexpr int kPanelThreads = 512;
+constexpr int kPanelThreads = 512;  // one panel row per thread
+constexpr int kMaxCluster = 16;
+constexpr int kMaxW = 32;
 
-template <bool F32>
+// Panel of W columns (w <= W used), rows row0..row0+nrows-1, factored by a cluster of
+// cs = gridDim.x CTAs; thread t of CTA q holds row q*512 + t in registers.
+template <bool F32, int W>
 __global__ void __launch_bounds__(kPanelThreads) k_panel(Mat<F32> M, int row0, int nrows, int col0, int w,
-                                                         int *ipiv, int *info) {
+                                                         int *ipiv, int *info, int *scratch) {
   using E = typename Prec<F32>::E;
   using Rl = typename Prec<F32>::R;
   cg::cluster_group cluster = cg::this_cluster();
   const int cs = (int)cluster.num_blocks();
   const int crank = (int)cluster.block_rank();
-  const int tid = threadIdx.x, nth = blockDim.x;
-  const int lane = tid & 31, warp = tid >> 5, nwarp = nth >> 5;
-  const int rpc = (nrows + cs - 1) / cs;
-  const int ws = w + 1;  // padded row stride in shared memory
-  const int my0 = crank * rpc;
-  const int myn = max(0, min(rpc, nrows - my0));
-  extern __shared__ __align__(16) unsigned char smraw[];
-  E *tile = (E *)smraw;
-  E *prow = tile + (size_t)rpc * ws;
-  E *oldj = prow + 32;
-  double *candv = (double *)(oldj + 32);
-  int *candi = (int *)(candv + 2);
-  int *pivs = candi + 2;       // 32
-  double *redv = (double *)(pivs + 32);
-  int *redi = (int *)(redv + 32);
-  int *bcast = redi + 32;      // [0] = p, [1] = singular
-
-  for (int r = warp; r < myn; r += nwarp)
-    for (int c = lane; c < w; c += 32) tile[r * ws + c] = M.get(row0 + my0 + r, col0 + c);
-  __syncthreads();
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int NW = kPanelThreads / 32;
+  __shared__ E srow[2][kMaxCluster][W];   // candidate rows pushed by every CTA (double-buffered)
+  __shared__ double sval[2][kMaxCluster];
+  __shared__ int sidx[2][kMaxCluster];
+  __shared__ E own[W];                    // this CTA's candidate row, staged for the push
+  __shared__ double redv[NW];
+  __shared__ int redi[NW];
+  __shared__ int chosen[kMaxW];
+  const int gr = crank * kPanelThreads + tid;  // panel-relative row of this thread
+  const bool have = gr < nrows;
+  bool active = have;
+  E row[W];
+#pragma unroll
+  for (int c = 0; c < W; ++c) row[c] = (have && c < w) ? M.get(row0 + gr, col0 + c) : E{0, 0};
 
   for (int j = 0; j < w; ++j) {
-    // CTA-local argmax of |re|+|im| over panel rows >= j
-    double best = -1.0;
-    int bidx = 0x7fffffff;
-    for (int r = tid; r < myn; r += nth) {
-      int pr = my0 + r;
-      if (pr < j) continue;
-      E v = tile[r * ws + j];
-      double a = fabs((double)v.x) + fabs((double)v.y);
-      if (a > best || (a == best && pr < bidx)) { best = a; bidx = pr; }
-    }
+    const int par = j & 1;
+    E vj = E{0, 0};
+#pragma unroll
+    for (int c = 0; c < W; ++c)
+      if (c == j) vj = row[c];
+    double best = active ? fabs((double)vj.x) + fabs((double)vj.y) : -1.0;
+    int bidx = active ? gr : 0x7fffffff;
     for (int o = 16; o > 0; o >>= 1) {
       double ob = __shfl_xor_sync(0xffffffff, best, o);
       int oi = __shfl_xor_sync(0xffffffff, bidx, o);
@@ -105,53 +104,41 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(Mat<F32> M, int row0, i
     }
     if (lane == 0) { redv[warp] = best; redi[warp] = bidx; }
     __syncthreads();
-    if (tid == 0) {
-      for (int k = 1; k < nwarp; ++k)
-        if (redv[k] > best || (redv[k] == best && redi[k] < bidx)) { best = redv[k]; bidx = redi[k]; }
-      candv[j & 1] = best;
-      candi[j & 1] = bidx;
-    }
-    cluster.sync();  // candidates visible cluster-wide
-    if (tid == 0) {
-      double gb = -1.0;
-      int gi = 0x7fffffff;
-      for (int c = 0; c < cs; ++c) {
-        double *rv = cluster.map_shared_rank(candv, c);
-        int *ri = cluster.map_shared_rank(candi, c);
-        double v = rv[j & 1];
-        int i = ri[j & 1];
-        if (v > gb || (v == gb && i < gi)) { gb = v; gi = i; }
-      }
-      int sing = !(gb > 0.0);
-      bcast[0] = sing ? j : gi;
-      bcast[1] = sing;
-      if (crank == 0) pivs[j] = bcast[0];
+    double cb = redv[0];
+    int ci = redi[0];
+#pragma unroll
+    for (int k = 1; k < NW; ++k)
+      if (redv[k] > cb || (redv[k] == cb && redi[k] < ci)) { cb = redv[k]; ci = redi[k]; }
+    if (cb >= 0.0 && gr == ci) {
+#pragma unroll
+      for (int c = 0; c < W; ++c) own[c] = row[c];
     }
     __syncthreads();
-    const int p = bcast[0];
-    const int sing = bcast[1];
-    const int op = p / rpc, rp = p % rpc, oj = j / rpc, rj = j % rpc;
-    {
-      E *tp = cluster.map_shared_rank(tile, op);
-      for (int c = tid; c < w; c += nth) prow[c] = tp[rp * ws + c];
-      if (crank == op && p != j) {
-        E *tj = cluster.map_shared_rank(tile, oj);
-        for (int c = tid; c < w; c += nth) oldj[c] = tj[rj * ws + c];
+    if (warp == 0) {  // push (value, row, candidate row) to slot [par][crank] of every CTA
+      for (int dst = 0; dst < cs; ++dst) {
+        E *rr = &cluster.map_shared_rank(&srow[0][0][0], dst)[(par * kMaxCluster + crank) * W];
+        for (int c = lane; c < w; c += 32) rr[c] = cb >= 0.0 ? own[c] : E{0, 0};
+        if (lane == 0) {
+          cluster.map_shared_rank(&sval[0][0], dst)[par * kMaxCluster + crank] = cb;
+          cluster.map_shared_rank(&sidx[0][0], dst)[par * kMaxCluster + crank] = ci;
+        }
       }
     }
-    cluster.sync();  // all remote reads of rows j and p done
-    if (p != j) {
-      if (crank == oj)
-        for (int c = tid; c < w; c += nth) tile[rj * ws + c] = prow[c];
-      if (crank == op)
-        for (int c = tid; c < w; c += nth) tile[rp * ws + c] = oldj[c];
+    cluster.sync();
+    double gb = -1.0;
+    int gi = 0x7fffffff, gc = 0;
+    for (int q = 0; q < cs; ++q) {
+      const double v = sval[par][q];
+      const int i = sidx[par][q];
+      if (v > gb || (v == gb && i < gi)) { gb = v; gi = i; gc = q; }
     }
-    __syncthreads();
+    const bool sing = !(gb > 0.0);
+    if (tid == 0) chosen[j] = sing ? -1 : gi;
     if (!sing) {
+      if (gr == gi) active = false;
+      const E *prow = srow[par][gc];
       E piv = prow[j];
-      Rl den = piv.x * piv.x + piv.y * piv.y;
-      // reciprocal of the pivot (LAPACK zgetf2 scales by 1/pivot)
-      E inv;
+      E inv;  // 1/pivot (LAPACK zgetf2 scales the column by the reciprocal)
       if (fabs((double)piv.y) <= fabs((double)piv.x)) {
         Rl rr = piv.y / piv.x, d = piv.x + piv.y * rr;
         inv = E{(Rl)1 / d, -rr / d};
@@ -159,52 +146,104 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(Mat<F32> M, int row0, i
         Rl rr = piv.x / piv.y, d = piv.y + piv.x * rr;
         inv = E{rr / d, (Rl)-1 / d};
       }
-      (void)den;
-      for (int r = warp; r < myn; r += nwarp) {
-        int pr = my0 + r;
-        if (pr <= j) continue;
-        E l = cmulE(tile[r * ws + j], inv);
-        for (int c = j + 1 + lane; c < w; c += 32) tile[r * ws + c] = csubE(tile[r * ws + c], cmulE(l, prow[c]));
-        if (lane == 0) tile[r * ws + j] = l;
+      if (active) {
+        const E l = cmulE(vj, inv);
+#pragma unroll
+        for (int c = 0; c < W; ++c) {
+          if (c == j) row[c] = l;
+          else if (c > j) row[c] = csubE(row[c], cmulE(l, prow[c]));
+        }
+      }
+    } else if (tid == 0 && crank == 0) {
+      atomicCAS(info, 0, col0 + j + 1);
+    }
+  }
+  __syncthreads();
+  // Replay the interchanges (LAPACK semantics) to get ipiv and every row's final position.
+  int *row_at = scratch, *pos_of = scratch + nrows;
+  if (crank == 0) {
+    for (int i = tid; i < nrows; i += blockDim.x) { row_at[i] = i; pos_of[i] = i; }
+    __syncthreads();
+    if (tid == 0) {
+      for (int j = 0; j < w; ++j) {
+        const int r = chosen[j];
+        const int p = r < 0 ? j : pos_of[r];  // a zero column keeps its row (no interchange)
+        ipiv[col0 + j] = row0 + p;
+        const int a = row_at[j], b = row_at[p];
+        row_at[j] = b; row_at[p] = a;
+        pos_of[b] = j; pos_of[a] = p;
       }
     }
-    if (sing && tid == 0 && crank == 0) atomicCAS(info, 0, col0 + j + 1);
-    __syncthreads();
   }
-  for (int r = warp; r < myn; r += nwarp)
-    for (int c = lane; c < w; c += 32) M.put(row0 + my0 + r, col0 + c, tile[r * ws + c]);
-  if (crank == 0)
-    for (int j = tid; j < w; j += nth) ipiv[col0 + j] = row0 + pivs[j];
-}
-
-// Apply swaps k = k0..k0+cnt-1 (row k <-> ipiv[k]) to columns [c0, c1).
-template <bool F32>
-__global__ void k_laswp(Mat<F32> M, int k0, int cnt, const int *ipiv, int c0, int c1) {
-  int c = c0 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= c1) return;
-  for (int k = k0; k < k0 + cnt; ++k) {
-    int p = ipiv[k];
-    if (p != k) {
-      auto a = M.get(k, c), b = M.get(p, c);
-      M.put(k, c, b);
-      M.put(p, c, a);
-    }
+  cluster.sync();
+  if (have) {
+    const int dst = pos_of[gr];
+#pragma unroll
+    for (int c = 0; c < W; ++c)
+      if (c < w) M.put(row0 + dst, col0 + c, row[c]);
   }
 }
 
-// Rows k0..k0+kb-1, columns [c0, c1): X = L11^{-1} X with L11 unit lower (in A).
+// Apply the interchanges k = k0..k0+cnt-1 (row k <-> ipiv[k], in order) to columns
+// [c0, c1): the composed permutation of the <= 2*cnt rows involved is built once per CTA,
+// then every column gathers all its moved entries first and scatters them after, so no
+// load waits on a previous swap.  128 threads, one column each.
 template <bool F32>
-__global__ void __launch_bounds__(32) k_trsm(Mat<F32> M, int k0, int kb, int c0, int c1) {
+__global__ void __launch_bounds__(128) k_laswp(Mat<F32> M, int k0, int cnt, const int *ipiv, int c0, int c1) {
   using E = typename Prec<F32>::E;
+  __shared__ int rows[2 * kMaxW], from[2 * kMaxW];
+  __shared__ int nmov;
   extern __shared__ __align__(16) unsigned char smraw[];
-  E *xs = (E *)smraw;  // kb x 32
-  int c = c0 + blockIdx.x * 32 + threadIdx.x;
-  bool ok = c < c1;
-  for (int i = 0; i < kb; ++i) {
-    E v = ok ? M.get(k0 + i, c) : E{0, 0};
-    for (int t = 0; t < i; ++t) v = csubE(v, cmulE(M.get(k0 + i, k0 + t), xs[t * 32 + threadIdx.x]));
-    xs[i * 32 + threadIdx.x] = v;
-    if (ok) M.put(k0 + i, c, v);
+  E *stage = (E *)smraw;  // [2*kMaxW][128]
+  if (threadIdx.x == 0) {
+    int nr = 0;
+    for (int k = k0; k < k0 + cnt; ++k) {
+      const int p = ipiv[k];
+      int ik = -1, ip = -1;
+      for (int q = 0; q < nr; ++q) {
+        if (rows[q] == k) ik = q;
+        if (rows[q] == p) ip = q;
+      }
+      if (ik < 0) { rows[nr] = k; from[nr] = k; ik = nr++; }
+      if (ip < 0) { rows[nr] = p; from[nr] = p; ip = nr++; }
+      const int t = from[ik]; from[ik] = from[ip]; from[ip] = t;
+    }
+    int m = 0;  // keep only rows whose content changes
+    for (int q = 0; q < nr; ++q)
+      if (from[q] != rows[q]) { rows[m] = rows[q]; from[m] = from[q]; ++m; }
+    nmov = m;
+  }
+  __syncthreads();
+  const int c = c0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= c1) return;
+  const int m = nmov;
+  for (int q = 0; q < m; ++q) stage[q * 128 + threadIdx.x] = M.get(from[q], c);
+  for (int q = 0; q < m; ++q) M.put(rows[q], c, stage[q * 128 + threadIdx.x]);
+}
+
+// Rows k0..k0+w-1 of columns [c0, c1): X = L11^{-1} X, L11 the w x w unit-lower block at
+// (k0, k0) held in shared memory; one column per thread, the solution in registers.
+template <bool F32, int W>
+__global__ void __launch_bounds__(128) k_trsm_small(Mat<F32> M, int k0, int w, int c0, int c1) {
+  using E = typename Prec<F32>::E;
+  __shared__ E L[W][W];
+  for (int e = threadIdx.x; e < W * W; e += blockDim.x) {
+    const int i = e / W, t = e % W;
+    L[i][t] = (i < w && t < i) ? M.get(k0 + i, k0 + t) : E{0, 0};
+  }
+  __syncthreads();
+  const int c = c0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= c1) return;
+  E x[W];
+#pragma unroll
+  for (int i = 0; i < W; ++i) {
+    if (i < w) {
+      E v = M.get(k0 + i, c);
+#pragma unroll
+      for (int t = 0; t < i; ++t) v = csubE(v, cmulE(L[i][t], x[t]));
+      x[i] = v;
+      M.put(k0 + i, c, v);
+    }
   }
 }
 
@@ -302,242 +341,107 @@ __global__ void __launch_bounds__(256) k_gemm32(float *Ar, float *Ai, long long 
   }
 }
 
-// ---- solves (one CTA of 1024 threads per call) ----
-template <bool F32>
-__device__ __forceinline__ cd lu_at(const Mat<F32> &M, long long r, long long c) {
-  auto v = M.get(r, c);
-  return mkcd((double)v.x, (double)v.y);
-}
-
-template <bool F32>
-__global__ void __launch_bounds__(1024) k_solve(Mat<F32> M, int n, const int *ipiv, int nrhs, cd *B,
-                                                const int *done) {
-  if (done && *done) return;
-  __shared__ cd part[32][8];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  // row interchanges (sequential, one thread per rhs)
-  if (tid < nrhs) {
-    cd *b = B + (size_t)tid * n;
-    for (int k = 0; k < n; ++k) {
-      int p = ipiv[k];
-      if (p != k) { cd t = b[k]; b[k] = b[p]; b[p] = t; }
-    }
-  }
-  __syncthreads();
-  for (int j0 = 0; j0 < nrhs; j0 += 8) {
-    const int nj = min(8, nrhs - j0);
-    // forward: unit lower
-    for (int blk = 0; blk < n; blk += 32) {
-      const int nr = min(32, n - blk);
-      if (warp < nr) {
-        const int row = blk + warp;
-        cd acc[8];
-        for (int j = 0; j < 8; ++j) acc[j] = mkcd(0, 0);
-        for (int t = lane; t < blk; t += 32) {
-          cd l = lu_at<F32>(M, row, t);
-          for (int j = 0; j < nj; ++j) acc[j] = acc[j] + l * B[(size_t)(j0 + j) * n + t];
-        }
-        for (int j = 0; j < nj; ++j)
-          for (int o = 16; o > 0; o >>= 1) {
-            acc[j].x += __shfl_xor_sync(0xffffffff, acc[j].x, o);
-            acc[j].y += __shfl_xor_sync(0xffffffff, acc[j].y, o);
-          }
-        if (lane == 0)
-          for (int j = 0; j < nj; ++j) part[warp][j] = B[(size_t)(j0 + j) * n + row] - acc[j];
-      }
-      __syncthreads();
-      if (warp == 0 && lane < nj) {
-        cd *b = B + (size_t)(j0 + lane) * n;
-        for (int i = 0; i < nr; ++i) {
-          cd v = part[i][lane];
-          for (int t = 0; t < i; ++t) v = v - lu_at<F32>(M, blk + i, blk + t) * b[blk + t];
-          b[blk + i] = v;
-        }
-      }
-      __syncthreads();
-    }
-    // backward: upper with diagonal
-    for (int top = n; top > 0; top -= 32) {
-      const int blk = max(0, top - 32);
-      const int nr = top - blk;
-      if (warp < nr) {
-        const int row = blk + warp;
-        cd acc[8];
-        for (int j = 0; j < 8; ++j) acc[j] = mkcd(0, 0);
-        for (int t = top + lane; t < n; t += 32) {
-          cd u = lu_at<F32>(M, row, t);
-          for (int j = 0; j < nj; ++j) acc[j] = acc[j] + u * B[(size_t)(j0 + j) * n + t];
-        }
-        for (int j = 0; j < nj; ++j)
-          for (int o = 16; o > 0; o >>= 1) {
-            acc[j].x += __shfl_xor_sync(0xffffffff, acc[j].x, o);
-            acc[j].y += __shfl_xor_sync(0xffffffff, acc[j].y, o);
-          }
-        if (lane == 0)
-          for (int j = 0; j < nj; ++j) part[warp][j] = B[(size_t)(j0 + j) * n + row] - acc[j];
-      }
-      __syncthreads();
-      if (warp == 0 && lane < nj) {
-        cd *b = B + (size_t)(j0 + lane) * n;
-        for (int i = nr - 1; i >= 0; --i) {
-          cd v = part[i][lane];
-          for (int t = i + 1; t < nr; ++t) v = v - lu_at<F32>(M, blk + i, blk + t) * b[blk + t];
-          b[blk + i] = v / lu_at<F32>(M, blk + i, blk + i);
-        }
-      }
-      __syncthreads();
-    }
-  }
-}
-
-// R = B - A X  (A row-major FP64), one warp per row.
-__global__ void __launch_bounds__(256) k_residual(int n, const cd *A, long long ld, int nrhs, const cd *X,
-                                                  const cd *B, cd *Rr, const int *done) {
-  if (done && *done) return;
-  const int lane = threadIdx.x & 31;
-  const int row = blockIdx.x * 8 + (threadIdx.x >> 5);
-  if (row >= n) return;
-  for (int j0 = 0; j0 < nrhs; j0 += 8) {
-    const int nj = min(8, nrhs - j0);
-    cd acc[8];
-    for (int j = 0; j < 8; ++j) acc[j] = mkcd(0, 0);
-    const cd *a = A + (long long)row * ld;
-    for (int t = lane; t < n; t += 32) {
-      cd av = a[t];
-      for (int j = 0; j < nj; ++j) acc[j] = acc[j] + av * X[(size_t)(j0 + j) * n + t];
-    }
-    for (int j = 0; j < nj; ++j)
-      for (int o = 16; o > 0; o >>= 1) {
-        acc[j].x += __shfl_xor_sync(0xffffffff, acc[j].x, o);
-        acc[j].y += __shfl_xor_sync(0xffffffff, acc[j].y, o);
-      }
-    if (lane == 0)
-      for (int j = 0; j < nj; ++j) Rr[(size_t)(j0 + j) * n + row] = B[(size_t)(j0 + j) * n + row] - acc[j];
-  }
-}
-
-__device__ __forceinline__ void atomic_max_pos(double *addr, double v) {
-  atomicMax((unsigned long long *)addr, (unsigned long long)__double_as_longlong(v));
-}
-
-// X += D; norms[0] = max|D|, norms[1] = max|X| (over all entries).
-__global__ void k_axpy_norms(long long total, cd *X, const cd *D, double *norms, const int *done) {
-  if (done && *done) return;
-  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  double md = 0, mx = 0;
-  if (i < total) {
-    cd x = X[i] + D[i];
-    X[i] = x;
-    md = fmax(fabs(D[i].x), fabs(D[i].y));
-    mx = fmax(fabs(x.x), fabs(x.y));
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    md = fmax(md, __shfl_xor_sync(0xffffffff, md, o));
-    mx = fmax(mx, __shfl_xor_sync(0xffffffff, mx, o));
-  }
-  if ((threadIdx.x & 31) == 0) {
-    atomic_max_pos(&norms[0], md);
-    atomic_max_pos(&norms[1], mx);
-  }
-}
-
-}  // namespace
-
 // ------------------------------- host side -------------------------------
-
-namespace {
-constexpr int kClusterCTAs = 8;
-constexpr size_t kPanelSmemCap = 220 * 1024;
-
 template <bool F32>
-size_t panel_smem(int nrows, int w) {
-  using E = typename Prec<F32>::E;
-  int rpc = (nrows + kClusterCTAs - 1) / kClusterCTAs;
-  return (size_t)rpc * (w + 1) * sizeof(E) + 64 * sizeof(E) + 2 * sizeof(double) + 2 * sizeof(int) +
-         32 * sizeof(int) + 32 * sizeof(double) + 32 * sizeof(int) + 2 * sizeof(int) + 64;
-}
-
-template <bool F32>
-int launch_panel(Mat<F32> M, int row0, int nrows, int col0, int w, int *ipiv, int *info, cudaStream_t st) {
-  size_t smem = panel_smem<F32>(nrows, w);
-  if (smem > kPanelSmemCap) {
-    pss_set_error("panel %d x %d does not fit a %d-CTA cluster", nrows, w, kClusterCTAs);
+int launch_panel(Mat<F32> M, int row0, int nrows, int col0, int w, int *ipiv, int *info, int *scratch,
+                 cudaStream_t st) {
+  const int cs = (nrows + kPanelThreads - 1) / kPanelThreads;
+  const int Wt = F32 ? 32 : 16;
+  if (cs > kMaxCluster || w > Wt) {
+    pss_set_error("panel %d x %d exceeds a %d-CTA cluster", nrows, w, kMaxCluster);
     return -6;
   }
+  auto kern = k_panel<F32, (F32 ? 32 : 16)>;
   static bool attr[2] = {false, false};
   if (!attr[F32]) {
-    cudaFuncSetAttribute(k_panel<F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmemCap);
+    cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
     attr[F32] = true;
   }
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(kClusterCTAs);
+  cfg.gridDim = dim3(cs);
   cfg.blockDim = dim3(kPanelThreads);
-  cfg.dynamicSmemBytes = smem;
+  cfg.dynamicSmemBytes = 0;
   cfg.stream = st;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeClusterDimension;
-  at[0].val.clusterDim.x = kClusterCTAs;
+  at[0].val.clusterDim.x = cs;
   at[0].val.clusterDim.y = 1;
   at[0].val.clusterDim.z = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
   pss_count_launch();
-  PSS_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_panel<F32>, M, row0, nrows, col0, w, ipiv, info));
+  PSS_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, M, row0, nrows, col0, w, ipiv, info, scratch));
   return 0;
 }
 
 template <bool F32>
 void launch_laswp(Mat<F32> M, int k0, int cnt, const int *ipiv, int c0, int c1, cudaStream_t st) {
-  if (c1 <= c0) return;
-  pss_count_launch();
-  k_laswp<F32><<<cdiv_u(c1 - c0, 256), 256, 0, st>>>(M, k0, cnt, ipiv, c0, c1);
-}
-
-template <bool F32>
-void launch_trsm(Mat<F32> M, int k0, int kb, int c0, int c1, cudaStream_t st) {
-  if (c1 <= c0) return;
-  size_t smem = (size_t)kb * 32 * sizeof(typename Prec<F32>::E);
+  if (c1 <= c0 || cnt <= 0) return;
+  using E = typename Prec<F32>::E;
   static bool attr[2] = {false, false};
   if (!attr[F32]) {
-    cudaFuncSetAttribute(k_trsm<F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_laswp<F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kMaxW * 128 * (int)sizeof(E));
     attr[F32] = true;
   }
   pss_count_launch();
-  k_trsm<F32><<<cdiv_u(c1 - c0, 32), 32, smem, st>>>(M, k0, kb, c0, c1);
+  k_laswp<F32><<<cdiv_u(c1 - c0, 128), 128, 2 * (size_t)cnt * 128 * sizeof(E), st>>>(M, k0, cnt, ipiv, c0, c1);
+}
+
+template <bool F32>
+void launch_trsm(Mat<F32> M, int k0, int w, int c0, int c1, cudaStream_t st) {
+  if (c1 <= c0) return;
+  pss_count_launch();
+  if (w <= 16)
+    k_trsm_small<F32, 16><<<cdiv_u(c1 - c0, 128), 128, 0, st>>>(M, k0, w, c0, c1);
+  else
+    k_trsm_small<F32, 32><<<cdiv_u(c1 - c0, 128), 128, 0, st>>>(M, k0, w, c0, c1);
 }
 
 void launch_gemm(Mat<false> M, int r0, int r1, int c0, int c1, int k0, int kb, cudaStream_t st) {
   if (r1 <= r0 || c1 <= c0) return;
+  int tok = pss_prof_begin(st);
   pss_count_launch();
   k_gemm64<<<dim3(cdiv_u(c1 - c0, 64), cdiv_u(r1 - r0, 64)), 256, 0, st>>>((cd *)M.a, M.ld, r0, r1, c0, c1, k0, kb);
+  pss_prof_end(tok, st, 8.0 * (r1 - r0) * (double)(c1 - c0) * kb);
 }
 void launch_gemm(Mat<true> M, int r0, int r1, int c0, int c1, int k0, int kb, cudaStream_t st) {
   if (r1 <= r0 || c1 <= c0) return;
+  int tok = pss_prof_begin(st);
   pss_count_launch();
   k_gemm32<<<dim3(cdiv_u(c1 - c0, 128), cdiv_u(r1 - r0, 128)), 256, 0, st>>>((float *)M.a, M.ai, M.ld, r0, r1, c0,
                                                                              c1, k0, kb);
+  pss_prof_end(tok, st, 8.0 * (r1 - r0) * (double)(c1 - c0) * kb);
 }
 
+// Outer blocks of NB columns, inner panels of W columns (LAPACK dgetrf order):
+//   1. each inner panel: factor, its interchanges on every other column, the W-row
+//      triangular solve and Schur update restricted to the outer block's own columns;
+//   2. once all interchanges of the outer block are applied, the block row of the
+//      trailing columns, U12 = L11^{-1} A12, as W-row solves plus block-row updates;
+//   3. the trailing matrix A22 -= L21 U12, one GEMM with K = NB.
 template <bool F32>
-int lu_blocked(int n, Mat<F32> M, int *ipiv, int *info, int NB, int W, cudaStream_t st) {
+int lu_blocked(int n, Mat<F32> M, int *ipiv, int *info, int NB, int W, int *pscratch, cudaStream_t st) {
   for (int K0 = 0; K0 < n; K0 += NB) {
     const int JB = min(NB, n - K0);
-    for (int k0 = K0; k0 < K0 + JB; k0 += W) {
-      const int w = min(W, K0 + JB - k0);
-      int rc = launch_panel<F32>(M, k0, n - k0, k0, w, ipiv, info, st);
+    const int E = K0 + JB;
+    for (int k0 = K0; k0 < E; k0 += W) {
+      const int w = min(W, E - k0);
+      int rc = launch_panel<F32>(M, k0, n - k0, k0, w, ipiv, info, pscratch, st);
       if (rc) return rc;
-      launch_laswp<F32>(M, k0, w, ipiv, K0, k0, st);
-      launch_laswp<F32>(M, k0, w, ipiv, k0 + w, K0 + JB, st);
-      if (k0 + w < K0 + JB) {
-        launch_trsm<F32>(M, k0, w, k0 + w, K0 + JB, st);
-        launch_gemm(M, k0 + w, n, k0 + w, K0 + JB, k0, w, st);
+      launch_laswp<F32>(M, k0, w, ipiv, 0, k0, st);
+      launch_laswp<F32>(M, k0, w, ipiv, k0 + w, n, st);
+      if (k0 + w < E) {
+        launch_trsm<F32>(M, k0, w, k0 + w, E, st);
+        launch_gemm(M, k0 + w, n, k0 + w, E, k0, w, st);
       }
     }
-    launch_laswp<F32>(M, K0, JB, ipiv, 0, K0, st);
-    launch_laswp<F32>(M, K0, JB, ipiv, K0 + JB, n, st);
-    if (K0 + JB < n) {
-      launch_trsm<F32>(M, K0, JB, K0 + JB, n, st);
-      launch_gemm(M, K0 + JB, n, K0 + JB, n, K0, JB, st);
+    if (E < n) {
+      for (int k0 = K0; k0 < E; k0 += W) {
+        const int w = min(W, E - k0);
+        launch_trsm<F32>(M, k0, w, E, n, st);
+        if (k0 + w < E) launch_gemm(M, k0 + w, E, E, n, k0, w, st);
+      }
+      launch_gemm(M, E, n, E, n, K0, JB, st);
     }
   }
   PSS_CUDA_TRY(cudaGetLastError());
@@ -546,74 +450,31 @@ int lu_blocked(int n, Mat<F32> M, int *ipiv, int *info, int NB, int W, cudaStrea
 
 template <bool F32>
 int pick_panel_width(int n, int want) {
-  int w = want;
-  while (w > 4 && panel_smem<F32>(n, w) > kPanelSmemCap) w /= 2;
-  if (panel_smem<F32>(n, w) > kPanelSmemCap) return -1;
-  return w;
+  if ((n + kPanelThreads - 1) / kPanelThreads > kMaxCluster) return -1;
+  return want;
 }
+
+constexpr int kNB64 = 64, kNB32 = 128;
 }  // namespace
 
-size_t pss_lu_ws_bytes(int n, int precision) { (void)n; (void)precision; return 0; }
+size_t pss_lu_ws_bytes(int n, int precision) {
+  (void)precision;
+  return 2 * (size_t)n * sizeof(int) + 256;  // panel row bookkeeping
+}
 
 int pss_lu64(int n, cd *A, long long ld, int *ipiv, int *info, void *ws, size_t ws_bytes, cudaStream_t st) {
-  (void)ws; (void)ws_bytes;
+  if (ws_bytes < pss_lu_ws_bytes(n, 0)) { pss_set_error("LU workspace too small"); return -4; }
   Mat<false> M{A, nullptr, ld};
   int W = pick_panel_width<false>(n, 16);
   if (W < 0) { pss_set_error("matrix order %d too large for the cluster panel", n); return -6; }
-  return lu_blocked<false>(n, M, ipiv, info, 64, W, st);
+  return lu_blocked<false>(n, M, ipiv, info, kNB64, W, (int *)ws, st);
 }
 
 int pss_lu32(int n, float *Ar, float *Ai, long long ld, int *ipiv, int *info, void *ws, size_t ws_bytes,
              cudaStream_t st) {
-  (void)ws; (void)ws_bytes;
+  if (ws_bytes < pss_lu_ws_bytes(n, 1)) { pss_set_error("LU workspace too small"); return -4; }
   Mat<true> M{Ar, Ai, ld};
   int W = pick_panel_width<true>(n, 32);
   if (W < 0) { pss_set_error("matrix order %d too large for the cluster panel", n); return -6; }
-  return lu_blocked<true>(n, M, ipiv, info, 128, W, st);
-}
-
-void pss_solve64(int n, const cd *LU, long long ld, const int *ipiv, int nrhs, cd *B, const int *done,
-                 cudaStream_t st) {
-  Mat<false> M{(void *)LU, nullptr, ld};
-  pss_count_launch();
-  k_solve<false><<<1, 1024, 0, st>>>(M, n, ipiv, nrhs, B, done);
-}
-
-void pss_solve32(int n, const float *Lr, const float *Li, long long ld, const int *ipiv, int nrhs, cd *B,
-                 const int *done, cudaStream_t st) {
-  Mat<true> M{(void *)Lr, (float *)Li, ld};
-  pss_count_launch();
-  k_solve<true><<<1, 1024, 0, st>>>(M, n, ipiv, nrhs, B, done);
-}
-
-void pss_residual64(int n, const cd *A, long long ld, int nrhs, const cd *X, const cd *B, cd *Rout,
-                    const int *done, cudaStream_t st) {
-  pss_count_launch();
-  k_residual<<<cdiv_u(n, 8), 256, 0, st>>>(n, A, ld, nrhs, X, B, Rout, done);
-}
-
-void pss_axpy_norms(int n, int nrhs, cd *X, const cd *D, double *norms, const int *done, cudaStream_t st) {
-  long long total = (long long)n * nrhs;
-  pss_count_launch();
-  k_axpy_norms<<<cdiv_u(total, 256), 256, 0, st>>>(total, X, D, norms, done);
-}
-
-namespace {
-// After a refinement step: converged when max|dx| <= tol * max|x|.  Resets the norm
-// accumulators for the next step; on the last step records non-convergence.
-__global__ void k_refine_check(double *norms, double tol, int *done, int *status, int last) {
-  if (*done) return;
-  double dn = norms[0], xn = norms[1];
-  bool finite = isfinite(dn) && isfinite(xn);
-  if (!finite) { *status |= PSS_ST_NONFINITE; *done = 1; }
-  else if (dn <= tol * xn) *done = 1;
-  else if (last) *status |= PSS_ST_REFINE_NOCONV;
-  norms[0] = 0.0;
-  norms[1] = 0.0;
-}
-}  // namespace
-
-void pss_refine_check(double *norms, double tol, int *done, int *status, int last, cudaStream_t st) {
-  pss_count_launch();
-  k_refine_check<<<1, 1, 0, st>>>(norms, tol, done, status, last);
+  return lu_blocked<true>(n, M, ipiv, info, kNB32, W, (int *)ws, st);
 }

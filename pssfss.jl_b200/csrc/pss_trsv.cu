@@ -1,0 +1,341 @@
+// K5: triangular solves with the LU factors, FP64 residuals and iterative refinement.
+//
+// Replaces LAPACK zgetrs (ldiv!, PSSFSS.jl:439,566) for the small right-hand-side sets
+// of a sweep point (n_rhs = number of incident modes, 4 at normal incidence).
+//
+// Chained block substitution: the factor is cut into 64-row blocks; CTA tickets are
+// taken in start order (atomicAdd), CTA b solves block b and only waits (bounded spin on
+// a per-block epoch flag) for blocks that started before it, so it never waits on a CTA
+// that is not resident.  Every CTA streams its share of the triangle (the bulk of the
+// bytes) concurrently; the serial chain per block is one 64x64 product with the
+// precomputed inverse of the diagonal block.  FP64 arithmetic for FP32 or FP64 factors.
+//
+// Refinement (LAPACK zcgesv's scheme): r = b - A x with the FP64 matrix, stop when
+// max|r_j| <= max|x_j| * ||A||_inf * eps * sqrt(n) for every rhs j (cabs1 norms).
+#include <cuda/atomic>
+#include "pss_internal.cuh"
+
+namespace {
+
+constexpr int BS = 64;        // block rows
+constexpr int kMaxRhs = 8;    // right-hand sides per pass
+constexpr int kMaxRefRhs = 1024;          // right-hand sides of one refinement
+constexpr int kNX = kMaxRefRhs;           // norms layout: [max|r_j|] [max|x_j|] [||A||]
+constexpr int kNA = 2 * kMaxRefRhs;
+constexpr int kNormCount = 2 * kMaxRefRhs + 1;
+constexpr long long kSpinCap = 1LL << 24;
+
+struct Fac {  // row-major factor access: FP64 interleaved or FP32 planes
+  const cd *a64;
+  const float *ar, *ai;
+  long long ld;
+  __device__ __forceinline__ cd at(long long r, long long c) const {
+    if (a64) return a64[r * ld + c];
+    return mkcd((double)ar[r * ld + c], (double)ai[r * ld + c]);
+  }
+};
+
+__device__ __forceinline__ double cabs1(cd z) { return fabs(z.x) + fabs(z.y); }
+
+// Spin until flags[c] >= epoch (acquire).  Returns false (and records an error) at the cap.
+__device__ __forceinline__ bool wait_flag(int *flags, int c, int epoch, int *err) {
+  cuda::atomic_ref<int, cuda::thread_scope_device> f(flags[c]);
+  long long it = 0;
+  while (f.load(cuda::memory_order_acquire) < epoch) {
+    if (++it > kSpinCap) {
+      atomicExch(err, 1);
+      return false;
+    }
+    __nanosleep(100);
+  }
+  return true;
+}
+
+__device__ __forceinline__ void post_flag(int *flags, int b, int epoch) {
+  cuda::atomic_ref<int, cuda::thread_scope_device> f(flags[b]);
+  f.store(epoch, cuda::memory_order_release);
+}
+
+// Inverses of the 64x64 diagonal blocks: Dinv[(2*blk + 0)] = L_bb^{-1} (unit lower),
+// Dinv[(2*blk + 1)] = U_bb^{-1}; each 64x64 row-major FP64.
+__global__ void __launch_bounds__(64) k_diag_inv(Fac F, int n, cd *Dinv) {
+  const int blk = blockIdx.x, upper = blockIdx.y;
+  const int r0 = blk * BS, nb = min(BS, n - r0);
+  extern __shared__ cd sm[];
+  cd *T = sm;            // 64 x 64 block
+  cd *X = sm + BS * BS;  // 64 x 64 inverse, column k owned by thread k
+  const int k = threadIdx.x;
+  for (int i = 0; i < BS; ++i) T[i * BS + k] = (i < nb && k < nb) ? F.at(r0 + i, r0 + k) : mkcd(i == k, 0);
+  __syncthreads();
+  if (!upper) {
+    for (int i = 0; i < BS; ++i) {
+      cd v = mkcd(i == k, 0);
+      for (int t = k; t < i; ++t) v = v - T[i * BS + t] * X[t * BS + k];
+      X[i * BS + k] = (i < k) ? mkcd(0, 0) : v;
+    }
+  } else {
+    for (int i = BS - 1; i >= 0; --i) {
+      cd v = mkcd(i == k, 0);
+      for (int t = i + 1; t <= k; ++t) v = v - T[i * BS + t] * X[t * BS + k];
+      X[i * BS + k] = (i > k) ? mkcd(0, 0) : v / T[i * BS + i];
+    }
+  }
+  __syncthreads();
+  cd *D = Dinv + (size_t)(2 * blk + upper) * BS * BS;
+  for (int i = 0; i < BS; ++i) D[i * BS + k] = X[i * BS + k];
+}
+
+// perm[i] = original row that ends in position i after the LAPACK swap sequence ipiv.
+__global__ void __launch_bounds__(1024) k_ipiv_to_perm(int n, const int *ipiv, int *perm) {
+  extern __shared__ int sp[];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) sp[i] = i;
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int k = 0; k < n; ++k) {
+      int p = ipiv[k];
+      int t = sp[k]; sp[k] = sp[p]; sp[p] = t;
+    }
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = sp[i];
+}
+
+// One chained substitution pass.  lower: X[rows] = Linv_b (B[perm[rows]] - L[rows, :b] X[:b]);
+// upper: X[rows] = Uinv_b (X[rows] - U[rows, b+1:] X[b+1:]) (in place).  256 threads.
+// 256 threads: row i of the block = tid / 4, quarter p = tid % 4 covers 16 columns of
+// each 64-column block; the block of X it multiplies is staged in shared memory.
+template <bool LOWER>
+__global__ void __launch_bounds__(256) k_trsv(Fac F, int n, const int *__restrict__ perm, const cd *__restrict__ B,
+                                              cd *__restrict__ X, int nrhs, const cd *__restrict__ Dinv,
+                                              int *ticket, int *flags, int epoch, int *err,
+                                              const int *__restrict__ done) {
+  if (done && *done) return;
+  __shared__ int s_b;
+  __shared__ cd y[BS][kMaxRhs];
+  __shared__ cd xs[BS][kMaxRhs];
+  const int tid = threadIdx.x;
+  const int i = tid >> 2, p = tid & 3;
+  const int nblk = (n + BS - 1) / BS;
+  if (tid == 0) s_b = atomicAdd(ticket, 1);
+  __syncthreads();
+  const int tk = s_b;
+  const int b = LOWER ? tk : nblk - 1 - tk;
+  const int r0 = b * BS, nr = min(BS, n - r0);
+  for (int j0 = 0; j0 < nrhs; j0 += kMaxRhs) {
+    const int nj = min(kMaxRhs, nrhs - j0);
+    cd acc[kMaxRhs];
+#pragma unroll
+    for (int j = 0; j < kMaxRhs; ++j) acc[j] = mkcd(0, 0);
+    const int c_lo = LOWER ? 0 : b + 1, c_hi = LOWER ? b : nblk;
+    for (int cc = c_lo; cc < c_hi; ++cc) {
+      const int c = LOWER ? cc : c_hi - 1 - (cc - c_lo);  // upper: nearest (earliest-ready) block first
+      if (j0 == 0 && tid == 0) wait_flag(flags, c, epoch, err);
+      __syncthreads();
+      // every thread acquires the producer's release before reading its block of X
+      if (j0 == 0) cuda::atomic_ref<int, cuda::thread_scope_device>(flags[c]).load(cuda::memory_order_acquire);
+      const int t0 = c * BS, nt = min(BS, n - t0);
+      for (int e = tid; e < BS * kMaxRhs; e += 256) {
+        const int t = e / kMaxRhs, j = e % kMaxRhs;
+        xs[t][j] = (t < nt && j < nj) ? X[(size_t)(j0 + j) * n + t0 + t] : mkcd(0, 0);
+      }
+      __syncthreads();
+      if (i < nr) {
+#pragma unroll 4
+        for (int q = 0; q < 16; ++q) {
+          const int t = p * 16 + q;
+          if (t >= nt) break;
+          cd l = F.at(r0 + i, t0 + t);
+#pragma unroll
+          for (int j = 0; j < kMaxRhs; ++j) acc[j] = acc[j] + l * xs[t][j];
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kMaxRhs; ++j)
+      for (int o = 1; o < 4; o <<= 1) {
+        acc[j].x += __shfl_xor_sync(0xffffffff, acc[j].x, o);
+        acc[j].y += __shfl_xor_sync(0xffffffff, acc[j].y, o);
+      }
+    if (p == 0 && i < nr) {
+#pragma unroll
+      for (int j = 0; j < kMaxRhs; ++j) {
+        if (j >= nj) break;
+        cd rhs = LOWER ? B[(size_t)(j0 + j) * n + perm[r0 + i]] : X[(size_t)(j0 + j) * n + r0 + i];
+        y[i][j] = rhs - acc[j];
+      }
+    }
+    __syncthreads();
+    // X[rows] = Dinv_b * y
+    const cd *D = Dinv + (size_t)(2 * b + (LOWER ? 0 : 1)) * BS * BS;
+    for (int e = tid; e < nr * nj; e += blockDim.x) {
+      const int i = e / nj, j = e % nj;
+      cd s = mkcd(0, 0);
+      for (int k = 0; k < nr; ++k) s = s + D[i * BS + k] * y[k][j];
+      X[(size_t)(j0 + j) * n + r0 + i] = s;
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    __threadfence();
+    post_flag(flags, b, epoch);
+  }
+}
+
+// R = B - A X with max|r_j| (norms[j]), max|x_j| (norms[kNX + j]) and ||A||_inf (norms[kNA]).
+__global__ void __launch_bounds__(256) k_resid(int n, const cd *__restrict__ A, long long ld, int nrhs,
+                                               const cd *__restrict__ X, const cd *__restrict__ B,
+                                               cd *__restrict__ R, double *norms, const int *__restrict__ done) {
+  if (done && *done) return;
+  const int lane = threadIdx.x & 31;
+  const int row = blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (row < n) {
+    const cd *a = A + (long long)row * ld;
+    for (int j0 = 0; j0 < nrhs; j0 += kMaxRhs) {
+      const int nj = min(kMaxRhs, nrhs - j0);
+      cd acc[kMaxRhs];
+      for (int j = 0; j < kMaxRhs; ++j) acc[j] = mkcd(0, 0);
+      double rs = 0;
+      for (int t = lane; t < n; t += 32) {
+        cd av = a[t];
+        if (j0 == 0) rs += cabs1(av);
+        for (int j = 0; j < nj; ++j) acc[j] = acc[j] + av * X[(size_t)(j0 + j) * n + t];
+      }
+      for (int j = 0; j < nj; ++j)
+        for (int o = 16; o > 0; o >>= 1) {
+          acc[j].x += __shfl_xor_sync(0xffffffff, acc[j].x, o);
+          acc[j].y += __shfl_xor_sync(0xffffffff, acc[j].y, o);
+        }
+      if (j0 == 0) {
+        for (int o = 16; o > 0; o >>= 1) rs += __shfl_xor_sync(0xffffffff, rs, o);
+        if (lane == 0) atomicMax((unsigned long long *)&norms[kNA], (unsigned long long)__double_as_longlong(rs));
+      }
+#pragma unroll
+      for (int j = 0; j < kMaxRhs; ++j) {
+        if (j < nj && lane == j) {
+          cd r = B[(size_t)(j0 + j) * n + row] - acc[j];
+          R[(size_t)(j0 + j) * n + row] = r;
+          atomicMax((unsigned long long *)&norms[j0 + j], (unsigned long long)__double_as_longlong(cabs1(r)));
+          double xv = cabs1(X[(size_t)(j0 + j) * n + row]);
+          atomicMax((unsigned long long *)&norms[kNX + j0 + j], (unsigned long long)__double_as_longlong(xv));
+        }
+      }
+    }
+  }
+}
+
+__global__ void k_ir_check(int n, int nrhs, double *norms, int *done, int *status, int last, int *err) {
+  if (*done) return;
+  const double cte = 1.1102230246251565e-16 * sqrt((double)n) * norms[kNA];
+  int ok = 1, bad = 0;
+  for (int j = 0; j < nrhs; ++j) {
+    double rn = norms[j], xn = norms[kNX + j];
+    if (!(isfinite(rn) && isfinite(xn))) bad = 1;
+    else if (rn > xn * cte) ok = 0;
+  }
+  if (*err) { bad = 1; *status |= PSS_ST_REFINE_NOCONV; }
+  if (bad) { *status |= PSS_ST_NONFINITE; *done = 1; }
+  else if (ok) *done = 1;
+  else if (last) { *status |= PSS_ST_REFINE_NOCONV; *done = 1; }
+  for (int j = 0; j < nrhs; ++j) norms[j] = norms[kNX + j] = 0.0;
+  norms[kNA] = 0.0;
+}
+
+__global__ void k_err_status(int *err, int *status) {
+  if (*err) *status |= PSS_ST_NONFINITE;
+  *err = 0;
+}
+
+__global__ void k_axpy(long long total, cd *X, const cd *D, const int *done) {
+  if (done && *done) return;
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < total) X[i] = X[i] + D[i];
+}
+
+}  // namespace
+
+// ------------------------------- host side -------------------------------
+
+size_t pss_solve_ws_bytes(int n) {
+  int nblk = (n + BS - 1) / BS;
+  return (size_t)nblk * 2 * BS * BS * sizeof(cd) + (size_t)n * sizeof(int) + (size_t)(nblk + 64) * sizeof(int) +
+         kNormCount * sizeof(double) + 256;
+}
+
+void SolveWS::bind(void *base, int n_) {
+  n = n_;
+  nblk = (n + BS - 1) / BS;
+  char *p = (char *)base;
+  Dinv = (cd *)p;
+  p += (size_t)nblk * 2 * BS * BS * sizeof(cd);
+  perm = (int *)p;
+  p += (size_t)n * sizeof(int);
+  ctrl = (int *)p;  // [0] ticket, [1] err, [2] done, [8..8+nblk) flags
+  p += (size_t)(nblk + 64) * sizeof(int);
+  p = (char *)(((uintptr_t)p + 15) & ~(uintptr_t)15);
+  norms = (double *)p;
+}
+
+// After the LU: pivot permutation and diagonal-block inverses.  flags/epoch reset.
+int pss_solve_prepare(SolveWS &ws, const cd *LU64, const float *Lr, const float *Li, long long ld, const int *ipiv,
+                      cudaStream_t st) {
+  Fac F{LU64, Lr, Li, ld};
+  pss_count_launch();
+  k_ipiv_to_perm<<<1, 1024, ws.n * sizeof(int), st>>>(ws.n, ipiv, ws.perm);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_diag_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * BS * BS * (int)sizeof(cd));
+    attr = true;
+  }
+  pss_count_launch();
+  k_diag_inv<<<dim3(ws.nblk, 2), BS, 2 * BS * BS * sizeof(cd), st>>>(F, ws.n, ws.Dinv);
+  PSS_CUDA_TRY(cudaMemsetAsync(ws.ctrl, 0, (size_t)(ws.nblk + 64) * sizeof(int), st));
+  PSS_CUDA_TRY(cudaMemsetAsync(ws.norms, 0, kNormCount * sizeof(double), st));
+  ws.epoch = 0;
+  return 0;
+}
+
+// X = (LU)^{-1} P B (B and X distinct, n x nrhs column-major).
+int pss_solve_lu(SolveWS &ws, const cd *LU64, const float *Lr, const float *Li, long long ld, int nrhs, const cd *B,
+                 cd *X, const int *done, cudaStream_t st) {
+  Fac F{LU64, Lr, Li, ld};
+  int *ticket = ws.ctrl, *err = ws.ctrl + 1, *flags = ws.ctrl + 8;
+  for (int pass = 0; pass < 2; ++pass) {
+    ++ws.epoch;
+    PSS_CUDA_TRY(cudaMemsetAsync(ticket, 0, sizeof(int), st));
+    pss_count_launch();
+    if (pass == 0)
+      k_trsv<true><<<ws.nblk, 256, 0, st>>>(F, ws.n, ws.perm, B, X, nrhs, ws.Dinv, ticket, flags, ws.epoch, err, done);
+    else
+      k_trsv<false><<<ws.nblk, 256, 0, st>>>(F, ws.n, ws.perm, B, X, nrhs, ws.Dinv, ticket, flags, ws.epoch, err,
+                                             done);
+  }
+  PSS_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+// A timed-out wait in a solve (never expected) marks the point non-finite.
+void pss_solve_status(SolveWS &ws, int *status, cudaStream_t st) {
+  pss_count_launch();
+  k_err_status<<<1, 1, 0, st>>>(ws.ctrl + 1, status);
+}
+
+// Iterative refinement of X against the FP64 matrix A (FP32 factors), up to maxit steps.
+int pss_refine(SolveWS &ws, const cd *A, long long ld, const float *Lr, const float *Li, int nrhs, const cd *B,
+               cd *X, cd *R, cd *D, int maxit, int *status, cudaStream_t st) {
+  int *done = ws.ctrl + 2, *err = ws.ctrl + 1;
+  if (nrhs > kMaxRefRhs) { pss_set_error("refinement supports at most %d right-hand sides", kMaxRefRhs); return -1; }
+  PSS_CUDA_TRY(cudaMemsetAsync(done, 0, sizeof(int), st));
+  const long long total = (long long)ws.n * nrhs;
+  for (int it = 0; it <= maxit; ++it) {
+    pss_count_launch();
+    k_resid<<<cdiv_u(ws.n, 8), 256, 0, st>>>(ws.n, A, ld, nrhs, X, B, R, ws.norms, done);
+    pss_count_launch();
+    k_ir_check<<<1, 1, 0, st>>>(ws.n, nrhs, ws.norms, done, status, it == maxit, err);
+    if (it == maxit) break;
+    int rc = pss_solve_lu(ws, nullptr, Lr, Li, ld, nrhs, R, D, done, st);
+    if (rc) return rc;
+    pss_count_launch();
+    k_axpy<<<cdiv_u(total, 256), 256, 0, st>>>(total, X, D, done);
+  }
+  PSS_CUDA_TRY(cudaGetLastError());
+  return 0;
+}

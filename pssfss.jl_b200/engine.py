@@ -47,7 +47,19 @@ SIGNATURES = {
     "pss_basis_transforms": (_I, [_P, _I, _P, _D, _D, _P]),
     "pss_lu_solve": (_I, [_P, _I, _P, _I, _P, _I, _P, _P]),
     "pss_last_timings": (_I, [_P, _P]),
+    "pss_profile": (_I, [_P, _I]),
+    "pss_profile_result": (_I, [_P, _P]),
 }
+
+
+def set_profiling(on, device=0, nworkers=None):
+    _check(lib().pss_profile(context(device, nworkers), int(on)), "pss_profile")
+
+
+def profile_result(device=0, nworkers=None):
+    out = np.zeros(3)
+    _check(lib().pss_profile_result(context(device, nworkers), _p(out)), "pss_profile_result")
+    return {"launches": int(out[0]), "ms": float(out[1]), "flops": float(out[2])}
 
 
 def lib():
@@ -177,8 +189,9 @@ def partial_gsms(sheet, rwg, points, region_rng, s, u, ios, precision="fp64", de
         t = np.zeros(8)
         lib().pss_last_timings(context(device, nworkers), _p(t))
         stats.setdefault("status", []).extend(status.tolist())
-        stats["timings_ms"] = dict(zip(["tables", "face_integrals", "fill", "factor", "transforms", "solve",
-                                        "project", "total"], t.tolist()))
+        stats["timings_ms"] = dict(zip(["tables", "face_integrals", "fill", "transforms", "unused",
+                                        "factor_solve", "project", "total"], t.tolist()))
+        stats["timings_ms"].pop("unused")
     bad = status & (4 | 16)
     if bad.any():
         raise RuntimeError(f"solver status {status.tolist()} (singular or non-finite)")
