@@ -47,6 +47,8 @@ typedef struct pss_sheet pss_sheet;
 #define PSS_STATUS_NONFINITE 16     /* NaN or Inf in the solution */
 #define PSS_STATUS_FP64_FALLBACK 32 /* PSS_FP32_REFINE only: refinement stalled (cond(Z) too
                                        large for FP32 factors), point recomputed in FP64 */
+#define PSS_STATUS_DEVICE_TIMEOUT 64 /* a bounded wait inside a kernel gave up (a pipeline or
+                                        solve-chain stall); the point's results are invalid */
 
 const char *pss_last_error(void);
 int pss_version(void);
@@ -117,6 +119,15 @@ int pss_last_timings(pss_ctx *ctx, double *ms8);
  * flops (8*M*N*K per complex update)] of the last call. */
 int pss_profile(pss_ctx *ctx, int enable);
 int pss_profile_result(pss_ctx *ctx, double *out3);
+
+/* Schur-complement update C -= L * U in complex FP32 on the tensor cores (tcgen05, 3xTF32
+ * products: FP32-level accuracy), the kernel the PSS_FP32_REFINE factorisation uses for its
+ * trailing updates.  Host arrays, row-major, real and imaginary parts separate: L m x k,
+ * U k x n, C m x n (updated in place).  status: 0, or PSS_STATUS_DEVICE_TIMEOUT.
+ * No counterpart in the reference, whose LU is LAPACK zgetrf behind `Z \ rhs`
+ * (src/PSSFSS.jl:473); exposed so the kernel can be checked on its own. */
+int pss_schur_update(pss_ctx *ctx, int m, int n, int k, const float *Lr, const float *Li, const float *Ur,
+                     const float *Ui, float *Cr, float *Ci, int *status);
 
 #ifdef __cplusplus
 }

@@ -148,7 +148,8 @@ struct Worker {
 };
 
 __global__ void k_info_to_status(int *info, int *status) {
-  if (*info) *status |= PSS_ST_SINGULAR;
+  if (*info > 0) *status |= PSS_ST_SINGULAR;
+  if (*info < 0) *status |= PSS_ST_DEVICE_TIMEOUT;
   *info = 0;
 }
 __global__ void k_nonconv_to_status(int *nonconv, int *status) {
@@ -893,6 +894,52 @@ int pss_lu_solve(pss_ctx *c, int n, const double *Z, int nrhs, const double *B, 
   PSS_CUDA_TRY(cudaMemcpy(X, w.X.p, (size_t)n * nrhs * sizeof(cd), cudaMemcpyDeviceToHost));
   if (status) *status = hs;
   st_buf.release();
+  return 0;
+}
+
+int pss_schur_update(pss_ctx *c, int m, int n, int k, const float *Lr, const float *Li, const float *Ur,
+                     const float *Ui, float *Cr, float *Ci, int *status) {
+  if (!c || !Lr || !Li || !Ur || !Ui || !Cr || !Ci || m <= 0 || n <= 0 || k <= 0) {
+    pss_set_error("invalid argument");
+    return -1;
+  }
+  if (set_device(c)) return -3;
+  Worker &w = c->w[0];
+  cudaStream_t st = w.st;
+  // One (k + m) x (k + n) row-major matrix: U top right, L bottom left, C bottom right.
+  const long long ld = k + n, rows = k + m;
+  const size_t total = (size_t)rows * ld;
+  std::vector<float> hr(total, 0.f), hi(total, 0.f);
+  for (long long r = 0; r < k; ++r)
+    for (long long q = 0; q < n; ++q) { hr[r * ld + k + q] = Ur[r * n + q]; hi[r * ld + k + q] = Ui[r * n + q]; }
+  for (long long r = 0; r < m; ++r) {
+    for (long long q = 0; q < k; ++q) { hr[(k + r) * ld + q] = Lr[r * k + q]; hi[(k + r) * ld + q] = Li[r * k + q]; }
+    for (long long q = 0; q < n; ++q) {
+      hr[(k + r) * ld + k + q] = Cr[r * n + q];
+      hi[(k + r) * ld + k + q] = Ci[r * n + q];
+    }
+  }
+  const size_t tcb = pss_tc_ws_bytes(m, n, (k + 15) / 16 * 16);
+  DevBuf ar, ai, ws, err;
+  if (ar.ensure(total * sizeof(float)) || ai.ensure(total * sizeof(float)) || ws.ensure(tcb) ||
+      err.ensure(sizeof(int)))
+    return -3;
+  PSS_CUDA_TRY(cudaMemcpyAsync(ar.p, hr.data(), total * sizeof(float), cudaMemcpyHostToDevice, st));
+  PSS_CUDA_TRY(cudaMemcpyAsync(ai.p, hi.data(), total * sizeof(float), cudaMemcpyHostToDevice, st));
+  PSS_CUDA_TRY(cudaMemsetAsync(err.p, 0, sizeof(int), st));
+  int rc = pss_cgemm_tc(ar.as<float>(), ai.as<float>(), ld, k, m, k, n, 0, k, ws.p, ws.n, err.as<int>(), st);
+  if (rc) return rc;
+  PSS_CUDA_TRY(cudaMemcpyAsync(hr.data(), ar.p, total * sizeof(float), cudaMemcpyDeviceToHost, st));
+  PSS_CUDA_TRY(cudaMemcpyAsync(hi.data(), ai.p, total * sizeof(float), cudaMemcpyDeviceToHost, st));
+  int herr = 0;
+  PSS_CUDA_TRY(cudaMemcpyAsync(&herr, err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  PSS_CUDA_TRY(cudaStreamSynchronize(st));
+  for (long long r = 0; r < m; ++r)
+    for (long long q = 0; q < n; ++q) {
+      Cr[r * n + q] = hr[(k + r) * ld + k + q];
+      Ci[r * n + q] = hi[(k + r) * ld + k + q];
+    }
+  if (status) *status = herr ? PSS_ST_DEVICE_TIMEOUT : 0;
   return 0;
 }
 

@@ -22,6 +22,7 @@ enum {
   PSS_ST_REFINE_NOCONV = 8,  // iterative refinement did not reach its tolerance
   PSS_ST_NONFINITE = 16,     // NaN/Inf in the solution
   PSS_ST_FP64_FALLBACK = 32, // FP32 refinement stalled; the point was recomputed in FP64
+  PSS_ST_DEVICE_TIMEOUT = 64, // a bounded device-side wait gave up; results are invalid
 };
 
 struct cd {

@@ -29,7 +29,10 @@ constexpr int TILE_BYTES = BM * BK * 4;          // 8 KB per plane tile
 constexpr int STAGE_BYTES = 8 * TILE_BYTES;      // 4 A + 4 B planes
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
 constexpr uint32_t TMEM_COLS = 512;
-constexpr long long kWaitCap = 1LL << 26;
+constexpr long long kWaitCap = 1LL << 24;
+// Written to *err when a bounded wait gives up: negative, like LAPACK's argument errors, so an
+// LU's info keeps its positive values for zero pivots.
+constexpr int kErrTimeout = -1;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -135,7 +138,8 @@ __global__ void __launch_bounds__(192, 1) k_cgemm_tf32x3(const __grid_constant__
   uint64_t *empty = full + STAGES;
   uint64_t *accf = empty + STAGES;  // [2]
   uint64_t *acce = accf + 2;        // [2]
-  uint32_t *tmem_slot = (uint32_t *)(acce + 2);
+  uint64_t *drain = acce + 2;       // MMA issuer's final commit
+  uint32_t *tmem_slot = (uint32_t *)(drain + 1);
   int *abort_flag = (int *)(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -145,6 +149,7 @@ __global__ void __launch_bounds__(192, 1) k_cgemm_tf32x3(const __grid_constant__
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
     for (int a = 0; a < 2; ++a) { mbar_init(&accf[a], 1); mbar_init(&acce[a], 4); }
+    mbar_init(drain, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -162,17 +167,23 @@ __global__ void __launch_bounds__(192, 1) k_cgemm_tf32x3(const __grid_constant__
     if (lane == 0) {  // ---------------- TMA producer ----------------
       int s = 0;
       uint32_t ph = 0;
+      int last_ph[STAGES];  // parity of the last phase each stage was loaded for (-1: never)
+      for (int q = 0; q < STAGES; ++q) last_ph[q] = -1;
       for (int t = blockIdx.x; t < ntiles && !*(volatile int *)abort_flag; t += gridDim.x) {
         const int mt = t / tiles_n, nt = t % tiles_n;
         for (int kb = 0; kb < g.nk; ++kb) {
-          if (!mbar_wait(&empty[s], ph ^ 1)) { atomicExch(g.err, 1); *(volatile int *)abort_flag = 1; break; }
+          if (!mbar_wait(&empty[s], ph ^ 1)) { atomicExch(g.err, kErrTimeout); *(volatile int *)abort_flag = 1; break; }
           mbar_expect_tx(&full[s], STAGE_BYTES);
           unsigned char *st = base + s * STAGE_BYTES;
           for (int p = 0; p < 4; ++p) tma_load_3d(st + p * TILE_BYTES, &mapA, &full[s], kb * BK, mt * BM, p);
           for (int p = 0; p < 4; ++p) tma_load_3d(st + (4 + p) * TILE_BYTES, &mapB, &full[s], kb * BK, nt * BN, p);
+          last_ph[s] = (int)ph;
           if (++s == STAGES) { s = 0; ph ^= 1; }
         }
       }
+      // Copies still in flight land before the shared memory is released (bounded).
+      for (int q = 0; q < STAGES; ++q)
+        if (last_ph[q] >= 0 && !mbar_wait(&full[q], (uint32_t)last_ph[q])) atomicExch(g.err, kErrTimeout);
     }
   } else if (warp == 1) {
     if (lane == 0) {  // ---------------- MMA issuer ----------------
@@ -183,7 +194,7 @@ __global__ void __launch_bounds__(192, 1) k_cgemm_tf32x3(const __grid_constant__
       for (int t = blockIdx.x; t < ntiles && !*(volatile int *)abort_flag; t += gridDim.x, ++local) {
         const int ab = local & 1;
         const uint32_t aph = (local >> 1) & 1;
-        if (!mbar_wait(&acce[ab], aph ^ 1)) { atomicExch(g.err, 1); *(volatile int *)abort_flag = 1; break; }
+        if (!mbar_wait(&acce[ab], aph ^ 1)) { atomicExch(g.err, kErrTimeout); *(volatile int *)abort_flag = 1; break; }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t dr = tmem + ab * 256, di = dr + 128;
         bool ok = true;
@@ -214,9 +225,12 @@ __global__ void __launch_bounds__(192, 1) k_cgemm_tf32x3(const __grid_constant__
           mma_commit(&empty[s]);  // stage s free once these MMAs have read it
           if (++s == STAGES) { s = 0; ph ^= 1; }
         }
-        if (!ok) { atomicExch(g.err, 1); *(volatile int *)abort_flag = 1; break; }
+        if (!ok) { atomicExch(g.err, kErrTimeout); *(volatile int *)abort_flag = 1; break; }
         mma_commit(&accf[ab]);    // accumulators ready for the epilogue
       }
+      // Every MMA this thread issued completes before the accumulators are freed (bounded).
+      mma_commit(drain);
+      if (!mbar_wait(drain, 0)) atomicExch(g.err, kErrTimeout);
     }
   } else {  // ---------------- epilogue: warps 2..5 ----------------
     const int lg = warp & 3;             // TMEM lane group this warp may access
@@ -225,9 +239,14 @@ __global__ void __launch_bounds__(192, 1) k_cgemm_tf32x3(const __grid_constant__
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++local) {
       const int ab = local & 1;
       const uint32_t aph = (local >> 1) & 1;
-      if (*(volatile int *)abort_flag) break;
-      bool ok = mbar_wait(&accf[ab], aph);
-      if (!ok) { atomicExch(g.err, 1); *(volatile int *)abort_flag = 1; break; }
+      // warp-uniform decisions: tcgen05.ld below needs the whole warp converged
+      const bool stop = __shfl_sync(0xffffffffu, *(volatile int *)abort_flag, 0) != 0;
+      if (stop) break;
+      const bool ok = __all_sync(0xffffffffu, mbar_wait(&accf[ab], aph));
+      if (!ok) {
+        if (lane == 0) { atomicExch(g.err, kErrTimeout); *(volatile int *)abort_flag = 1; }
+        break;
+      }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const int mt = t / tiles_n, nt = t % tiles_n;
       const int r = mt * BM + row_in_tile;
@@ -350,7 +369,8 @@ int make_map(CUtensorMap *m, const float *planes, int rows, int KP) {
   return 0;
 }
 
-int g_num_sms = 0;
+constexpr int kMaxDevices = 64;
+int g_num_sms[kMaxDevices] = {};  // per device, set with the kernel's shared-memory attribute
 
 }  // namespace
 
@@ -366,11 +386,14 @@ int pss_cgemm_tc(float *Ar, float *Ai, long long ld, int m0, int M, int n0, int 
   const int KP = ((K + BK - 1) / BK) * BK;
   if (ws_bytes < pss_tc_ws_bytes(M, N, KP)) { pss_set_error("tensor-core GEMM workspace too small"); return -4; }
   if (get_encoder()) return -3;
-  if (!g_num_sms) {
-    int dev;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaFuncSetAttribute(k_cgemm_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+  int dev = 0;
+  PSS_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) { pss_set_error("device %d out of range", dev); return -3; }
+  if (!g_num_sms[dev]) {
+    int nsm = 0;
+    PSS_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    PSS_CUDA_TRY(cudaFuncSetAttribute(k_cgemm_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+    g_num_sms[dev] = nsm;
   }
   float *pa = (float *)(((uintptr_t)ws + 255) & ~(uintptr_t)255);
   float *pb = pa + 4 * (size_t)M * KP;
@@ -383,7 +406,7 @@ int pss_cgemm_tc(float *Ar, float *Ai, long long ld, int m0, int M, int n0, int 
   if (make_map(&ma, pa, M, KP) || make_map(&mb, pb, N, KP)) return -3;
   GemmArgs g{Ar, Ai, ld, m0, n0, M, N, KP / BK, err};
   const int tiles = ((M + BM - 1) / BM) * ((N + BN - 1) / BN);
-  const int grid = std::min(tiles, g_num_sms);
+  const int grid = std::min(tiles, g_num_sms[dev]);
   const int tok = pss_prof_begin(st);
   pss_count_launch();
   k_cgemm_tf32x3<<<grid, 192, SMEM_BYTES, st>>>(ma, mb, g);

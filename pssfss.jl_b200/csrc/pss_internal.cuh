@@ -126,6 +126,14 @@ int pss_lu32(int n, float *Ar, float *Ai, long long ld, int *ipiv, int *info, vo
              cudaStream_t st);
 size_t pss_lu_ws_bytes(int n, int precision);
 
+// Tensor-core (tcgen05, 3xTF32) complex Schur update on FP32 planes (pss_gemm_tc.cu):
+// A[m0:m0+M, n0:n0+N] -= A[m0:m0+M, k0:k0+K] * A[k0:k0+K, n0:n0+N], row-major, leading
+// dimension ld; ws holds the split operands (pss_tc_ws_bytes(M, N, K rounded up to 16)).
+// A bounded pipeline wait that gives up writes -1 to *err.
+size_t pss_tc_ws_bytes(int Mmax, int Nmax, int KP);
+int pss_cgemm_tc(float *Ar, float *Ai, long long ld, int m0, int M, int n0, int N, int k0, int K, void *ws,
+                 size_t ws_bytes, int *err, cudaStream_t st);
+
 // Triangular solves and refinement (pss_trsv.cu).  The factor is either FP64 (LU64) or
 // FP32 planes (Lr, Li); pass the other as null.
 struct SolveWS {

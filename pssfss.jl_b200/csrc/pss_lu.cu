@@ -62,6 +62,7 @@ struct Mat {
 constexpr int kPanelThreads = 512;  // one panel row per thread
 constexpr int kMaxCluster = 16;
 constexpr int kMaxW = 32;
+constexpr int kTcMin = 128;  // smallest trailing update sent to the tensor cores
 
 // Panel of W columns (w <= W used), rows row0..row0+nrows-1, factored by a cluster of
 // cs = gridDim.x CTAs; thread t of CTA q holds row q*512 + t in registers.
@@ -419,8 +420,24 @@ void launch_gemm(Mat<true> M, int r0, int r1, int c0, int c1, int k0, int kb, cu
 //   2. once all interchanges of the outer block are applied, the block row of the
 //      trailing columns, U12 = L11^{-1} A12, as W-row solves plus block-row updates;
 //   3. the trailing matrix A22 -= L21 U12, one GEMM with K = NB.
+// Trailing update A22 -= L21 U12 of an outer block: tensor cores (3xTF32) for the FP32
+// factorisation once the update is at least one 128 x 128 tile, SIMT otherwise.
+int launch_trailing(Mat<false> M, int E, int n, int K0, int JB, void *, size_t, int *, cudaStream_t st) {
+  launch_gemm(M, E, n, E, n, K0, JB, st);
+  return 0;
+}
+int launch_trailing(Mat<true> M, int E, int n, int K0, int JB, void *tcws, size_t tcws_bytes, int *info,
+                    cudaStream_t st) {
+  if (n - E < kTcMin) {
+    launch_gemm(M, E, n, E, n, K0, JB, st);
+    return 0;
+  }
+  return pss_cgemm_tc((float *)M.a, M.ai, M.ld, E, n - E, E, n - E, K0, JB, tcws, tcws_bytes, info, st);
+}
+
 template <bool F32>
-int lu_blocked(int n, Mat<F32> M, int *ipiv, int *info, int NB, int W, int *pscratch, cudaStream_t st) {
+int lu_blocked(int n, Mat<F32> M, int *ipiv, int *info, int NB, int W, int *pscratch, void *tcws,
+               size_t tcws_bytes, cudaStream_t st) {
   for (int K0 = 0; K0 < n; K0 += NB) {
     const int JB = min(NB, n - K0);
     const int E = K0 + JB;
@@ -441,7 +458,8 @@ int lu_blocked(int n, Mat<F32> M, int *ipiv, int *info, int NB, int W, int *pscr
         launch_trsm<F32>(M, k0, w, E, n, st);
         if (k0 + w < E) launch_gemm(M, k0 + w, E, E, n, k0, w, st);
       }
-      launch_gemm(M, E, n, E, n, K0, JB, st);
+      int rc = launch_trailing(M, E, n, K0, JB, tcws, tcws_bytes, info, st);
+      if (rc) return rc;
     }
   }
   PSS_CUDA_TRY(cudaGetLastError());
@@ -455,11 +473,13 @@ int pick_panel_width(int n, int want) {
 }
 
 constexpr int kNB64 = 64, kNB32 = 128;
+size_t scratch_bytes(int n) { return (2 * (size_t)n * sizeof(int) + 256 + 255) & ~(size_t)255; }
 }  // namespace
 
+// Workspace: panel row bookkeeping (2n ints), then for the FP32 factorisation the split
+// operand planes of the tensor-core trailing update.
 size_t pss_lu_ws_bytes(int n, int precision) {
-  (void)precision;
-  return 2 * (size_t)n * sizeof(int) + 256;  // panel row bookkeeping
+  return scratch_bytes(n) + (precision == 0 ? 0 : pss_tc_ws_bytes(n, n, kNB32));
 }
 
 int pss_lu64(int n, cd *A, long long ld, int *ipiv, int *info, void *ws, size_t ws_bytes, cudaStream_t st) {
@@ -467,7 +487,7 @@ int pss_lu64(int n, cd *A, long long ld, int *ipiv, int *info, void *ws, size_t 
   Mat<false> M{A, nullptr, ld};
   int W = pick_panel_width<false>(n, 16);
   if (W < 0) { pss_set_error("matrix order %d too large for the cluster panel", n); return -6; }
-  return lu_blocked<false>(n, M, ipiv, info, kNB64, W, (int *)ws, st);
+  return lu_blocked<false>(n, M, ipiv, info, kNB64, W, (int *)ws, nullptr, 0, st);
 }
 
 int pss_lu32(int n, float *Ar, float *Ai, long long ld, int *ipiv, int *info, void *ws, size_t ws_bytes,
@@ -476,5 +496,6 @@ int pss_lu32(int n, float *Ar, float *Ai, long long ld, int *ipiv, int *info, vo
   Mat<true> M{Ar, Ai, ld};
   int W = pick_panel_width<true>(n, 32);
   if (W < 0) { pss_set_error("matrix order %d too large for the cluster panel", n); return -6; }
-  return lu_blocked<true>(n, M, ipiv, info, kNB32, W, (int *)ws, st);
+  const size_t sb = scratch_bytes(n);
+  return lu_blocked<true>(n, M, ipiv, info, kNB32, W, (int *)ws, (char *)ws + sb, ws_bytes - sb, st);
 }

@@ -231,7 +231,7 @@ __global__ void k_ir_check(int n, int nrhs, double *norms, int *done, int *statu
     if (!(isfinite(rn) && isfinite(xn))) bad = 1;
     else if (rn > xn * cte) ok = 0;
   }
-  if (*err) { bad = 1; *status |= PSS_ST_REFINE_NOCONV; }
+  if (*err) { bad = 1; *status |= PSS_ST_DEVICE_TIMEOUT; }
   if (bad) { *status |= PSS_ST_NONFINITE; *done = 1; }
   else if (ok) *done = 1;
   else if (last) { *status |= PSS_ST_REFINE_NOCONV; *done = 1; }
@@ -240,7 +240,7 @@ __global__ void k_ir_check(int n, int nrhs, double *norms, int *done, int *statu
 }
 
 __global__ void k_err_status(int *err, int *status) {
-  if (*err) *status |= PSS_ST_NONFINITE;
+  if (*err) *status |= PSS_ST_DEVICE_TIMEOUT;
   *err = 0;
 }
 

@@ -17,7 +17,8 @@ PSS_FP32_REFINE = 1
 PRECISIONS = {"fp64": PSS_FP64, "fp32r": PSS_FP32_REFINE}
 
 STATUS_BITS = {1: "table_noconv", 2: "jk_noconv", 4: "singular", 8: "refine_noconv", 16: "nonfinite",
-               32: "fp64_fallback"}
+               32: "fp64_fallback", 64: "device_timeout"}
+FATAL_STATUS = 4 | 16 | 64
 
 _lib = None
 _lock = threading.Lock()
@@ -49,6 +50,7 @@ SIGNATURES = {
     "pss_last_timings": (_I, [_P, _P]),
     "pss_profile": (_I, [_P, _I]),
     "pss_profile_result": (_I, [_P, _P]),
+    "pss_schur_update": (_I, [_P, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P]),
 }
 
 
@@ -192,9 +194,9 @@ def partial_gsms(sheet, rwg, points, region_rng, s, u, ios, precision="fp64", de
         stats["timings_ms"] = dict(zip(["tables", "face_integrals", "fill", "transforms", "unused",
                                         "factor_solve", "project", "total"], t.tolist()))
         stats["timings_ms"].pop("unused")
-    bad = status & (4 | 16)
+    bad = status & FATAL_STATUS
     if bad.any():
-        raise RuntimeError(f"solver status {status.tolist()} (singular or non-finite)")
+        raise RuntimeError(f"solver status {status.tolist()} (singular, non-finite or device timeout)")
     return [d.T.copy() for d in dS]
 
 
@@ -259,3 +261,19 @@ def lu_solve(Z, B, precision="fp64", device=0):
                               PRECISIONS[precision], X.ctypes.data_as(ctypes.c_void_p), ctypes.byref(st)),
            "pss_lu_solve")
     return X, st.value
+
+
+def schur_update(L, U, C, device=0):
+    """C - L @ U in complex FP32 on the tensor cores (``pss_schur_update``); returns (C', status)."""
+    L = np.asarray(L, np.complex64)
+    U = np.asarray(U, np.complex64)
+    C = np.asarray(C, np.complex64)
+    m, k = L.shape
+    k2, n = U.shape
+    if k2 != k or C.shape != (m, n):
+        raise ValueError("shape mismatch")
+    parts = [np.ascontiguousarray(x, np.float32) for x in (L.real, L.imag, U.real, U.imag, C.real, C.imag)]
+    st = ctypes.c_int()
+    _check(lib().pss_schur_update(context(device), m, n, k, *[_p(x) for x in parts], ctypes.byref(st)),
+           "pss_schur_update")
+    return parts[4] + 1j * parts[5], st.value
