@@ -129,6 +129,28 @@ int pss_profile_result(pss_ctx *ctx, double *out3);
 int pss_schur_update(pss_ctx *ctx, int m, int n, int k, const float *Lr, const float *Li, const float *Ur,
                      const float *Ui, float *Cr, float *Ci, int *status);
 
+/* FP64 complex LU factorisation, in place, on caller-owned device memory, allocating no
+ * device memory at all (no cudaMalloc, cudaFree or allocating library routine).  No
+ * counterpart in the reference (its factorisation is LAPACK zgetrf behind `Z \ rhs`,
+ * src/PSSFSS.jl:473); it serves callers that cannot let a library allocate per call - a
+ * host whose device memory is held by its own pool (Julia CUDA.jl, PyTorch), or a
+ * latency-sensitive loop in which cudaFree's device-wide synchronisation would stall
+ * every other stream.
+ *   A     device, n x n interleaved complex128, ROW-major, leading dimension ld >= n
+ *         (elements), 16-byte aligned; overwritten by U (upper) and the unit-lower L.
+ *   ipiv  device, n ints, 0-based: row k was interchanged with row ipiv[k], k = 0..n-1
+ *         applied in order (LAPACK's convention minus one).
+ *   info  device int: set to 0 by this call (on `stream`, before the first kernel), then
+ *         to j+1 if column j held the first exactly-zero pivot.
+ *   stream  a cudaStream_t of the current device (NULL: the legacy default stream).
+ * Runs on the current device and is asynchronous with respect to the host.
+ * Limit: n <= 8192; larger n returns -1 with a message in pss_last_error().  Its scratch is
+ * a fixed 64 KB file-scope device array, one per device: nothing in it has to start at
+ * zero, but calls that overlap in time on the same device race on it - serialise them.
+ * The first call on each device resolves that array's address (cudaGetSymbolAddress);
+ * make that first call before any stream capture on the device. */
+int pss_lu_factor_noalloc(int n, double *A, int64_t ld, int *ipiv, int *info, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
