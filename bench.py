@@ -30,6 +30,10 @@ import time
 
 import numpy as np
 
+# Worker streams beyond the default 8 hardware work queues would share queues (false
+# dependencies); this process-local setting must precede CUDA context creation.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 NFREQ = 101
 WORKLOAD = ("meanderline a=5 b=10 h=6 w1=w2=0.3 mm ntri=3000 (2840 faces, N=3976) on 1 mm eps_r=2.2, "

@@ -144,11 +144,12 @@ int pss_schur_update(pss_ctx *ctx, int m, int n, int k, const float *Lr, const f
  *         to j+1 if column j held the first exactly-zero pivot.
  *   stream  a cudaStream_t of the current device (NULL: the legacy default stream).
  * Runs on the current device and is asynchronous with respect to the host.
- * Limit: n <= 8192; larger n returns -1 with a message in pss_last_error().  Its scratch is
- * a fixed 64 KB file-scope device array, one per device: nothing in it has to start at
- * zero, but calls that overlap in time on the same device race on it - serialise them.
- * The first call on each device resolves that array's address (cudaGetSymbolAddress);
- * make that first call before any stream capture on the device. */
+ * Limit: n <= 8192; larger n returns -1 with a message in pss_last_error().  Its scratch
+ * is a fixed 1 KB file-scope device array (the panels' interchange list), one per device:
+ * nothing in it has to start at zero, but calls that overlap in time on the same device
+ * race on it - serialise them.  The first call on each device resolves that array's
+ * address (cudaGetSymbolAddress); make that first call before any stream capture on the
+ * device. */
 int pss_lu_factor_noalloc(int n, double *A, int64_t ld, int *ipiv, int *info, void *stream);
 
 #ifdef __cplusplus

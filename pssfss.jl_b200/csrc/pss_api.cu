@@ -15,6 +15,8 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstring>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include "pss_internal.cuh"
@@ -632,9 +634,8 @@ int pss_partial_gsms(pss_sheet *sh, int nl, const double *eps, const double *mu,
 
   const int n = sh->nbf;
   const long long ld = n;
-  std::vector<cudaEvent_t> ev;
-  KProf kprof;
-  g_kprof = c->prof_on ? &kprof : nullptr;
+  std::vector<cudaEvent_t> ev;  // phase events of worker 0's points (pushed by its thread only)
+  std::vector<KProf> kprofs(nw);
   // One point through fill, LU, transforms, solve(s) and projection on worker w's stream.
   auto run_point = [&](int i, int prec, Worker &w, bool rec) -> int {
     cudaStream_t st = w.st;
@@ -675,8 +676,31 @@ int pss_partial_gsms(pss_sheet *sh, int nl, const double *eps, const double *mu,
     PSS_CUDA_TRY(cudaGetLastError());
     return 0;
   };
-  for (int i = 0; i < npts; ++i) {
-    if ((rc = run_point(i, precision, c->w[i % nw], (i % nw) == 0))) return rc;
+  // One host thread per worker stream: each enqueues its own points (i = k, k + nw, ...), so
+  // a stream whose launch queue is full blocks only its own thread, not the other streams.
+  {
+    std::vector<int> wrc(nw, 0);
+    std::vector<std::string> werr(nw);
+    auto feed = [&](int k) {
+      if (cudaSetDevice(c->device) != cudaSuccess) {
+        wrc[k] = -3;
+        werr[k] = "cudaSetDevice failed in a worker thread";
+        return;
+      }
+      g_kprof = c->prof_on ? &kprofs[k] : nullptr;
+      for (int i = k; i < npts && !wrc[k]; i += nw) wrc[k] = run_point(i, precision, c->w[k], k == 0);
+      g_kprof = nullptr;
+      if (wrc[k]) werr[k] = pss_last_error();
+    };
+    std::vector<std::thread> th;
+    for (int k = 1; k < nw; ++k) th.emplace_back(feed, k);
+    feed(0);
+    for (auto &t : th) t.join();
+    for (int k = 0; k < nw; ++k)
+      if (wrc[k]) {
+        pss_set_error("%s", werr[k].c_str());
+        return wrc[k];
+      }
   }
   for (auto &w : c->w) PSS_CUDA_TRY(cudaStreamSynchronize(w.st));
   PSS_CUDA_TRY(cudaMemcpy(status, c->status.p, (size_t)npts * sizeof(int), cudaMemcpyDeviceToHost));
@@ -721,17 +745,18 @@ int pss_partial_gsms(pss_sheet *sh, int nl, const double *eps, const double *mu,
       c->last_ms[q + 1] += ms;
     }
   }
-  g_kprof = nullptr;
   c->prof[0] = c->prof[1] = c->prof[2] = 0;
-  for (size_t q = 0; q < kprof.e1.size(); ++q) {
-    float ms = 0;
-    cudaEventElapsedTime(&ms, kprof.e0[q], kprof.e1[q]);
-    c->prof[0] += 1;
-    c->prof[1] += ms;
-    c->prof[2] += kprof.flops[q];
+  for (auto &kprof : kprofs) {
+    for (size_t q = 0; q < kprof.e1.size(); ++q) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, kprof.e0[q], kprof.e1[q]);
+      c->prof[0] += 1;
+      c->prof[1] += ms;
+      c->prof[2] += kprof.flops[q];
+    }
+    for (auto e : kprof.e0) cudaEventDestroy(e);
+    for (auto e : kprof.e1) cudaEventDestroy(e);
   }
-  for (auto e : kprof.e0) cudaEventDestroy(e);
-  for (auto e : kprof.e1) cudaEventDestroy(e);
   c->last_ms[0] = tables_ms;
   c->last_ms[7] = span_ms;
   for (auto e : ev) cudaEventDestroy(e);

@@ -339,10 +339,10 @@ __global__ void k_split_b(const float *__restrict__ Ar, const float *__restrict_
   }
 }
 
-PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+std::atomic<PFN_cuTensorMapEncodeTiled_v12000> g_encode{nullptr};
 
 int get_encoder() {
-  if (g_encode) return 0;
+  if (g_encode.load(std::memory_order_acquire)) return 0;
   cudaDriverEntryPointQueryResult q;
   void *fn = nullptr;
   if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
@@ -350,7 +350,7 @@ int get_encoder() {
     pss_set_error("cuTensorMapEncodeTiled unavailable");
     return -3;
   }
-  g_encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+  g_encode.store((PFN_cuTensorMapEncodeTiled_v12000)fn, std::memory_order_release);
   return 0;
 }
 
@@ -359,7 +359,7 @@ int make_map(CUtensorMap *m, const float *planes, int rows, int KP) {
   cuuint64_t strides[2] = {(cuuint64_t)KP * 4, (cuuint64_t)rows * KP * 4};
   cuuint32_t box[3] = {BK, BM, 1};
   cuuint32_t es[3] = {1, 1, 1};
-  CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)planes, dims, strides, box, es,
+  CUresult r = g_encode.load(std::memory_order_acquire)(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)planes, dims, strides, box, es,
                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
@@ -370,7 +370,8 @@ int make_map(CUtensorMap *m, const float *planes, int rows, int KP) {
 }
 
 constexpr int kMaxDevices = 64;
-int g_num_sms[kMaxDevices] = {};  // per device, set with the kernel's shared-memory attribute
+int g_num_sms[kMaxDevices] = {};  // per device, written once under g_setup
+DeviceOnce g_setup;
 
 }  // namespace
 
@@ -389,12 +390,14 @@ int pss_cgemm_tc(float *Ar, float *Ai, long long ld, int m0, int M, int n0, int 
   int dev = 0;
   PSS_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices) { pss_set_error("device %d out of range", dev); return -3; }
-  if (!g_num_sms[dev]) {
-    int nsm = 0;
-    PSS_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    PSS_CUDA_TRY(cudaFuncSetAttribute(k_cgemm_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
-    g_num_sms[dev] = nsm;
-  }
+  if (int rc = device_once(g_setup, [dev] {
+        int nsm = 0;
+        PSS_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        PSS_CUDA_TRY(cudaFuncSetAttribute(k_cgemm_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+        g_num_sms[dev] = nsm;
+        return 0;
+      }))
+    return rc;
   float *pa = (float *)(((uintptr_t)ws + 255) & ~(uintptr_t)255);
   float *pb = pa + 4 * (size_t)M * KP;
   pb = (float *)(((uintptr_t)pb + 255) & ~(uintptr_t)255);

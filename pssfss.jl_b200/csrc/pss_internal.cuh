@@ -1,6 +1,31 @@
 // Internal declarations shared by the library's translation units.
 #pragma once
+#include <atomic>
+#include <mutex>
+
 #include "pss_common.cuh"
+
+// Per-device one-time set-up (kernel attributes and the like), safe to reach from several
+// host threads: f() runs once for each device it is first called on (that device current).
+struct DeviceOnce {
+  std::atomic<unsigned long long> done{0};
+  std::mutex mu;
+};
+template <class F>
+int device_once(DeviceOnce &o, F &&f) {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    pss_set_error("no usable current device (%d) for kernel set-up", dev);
+    return -3;
+  }
+  const unsigned long long bit = 1ull << dev;
+  if (o.done.load(std::memory_order_acquire) & bit) return 0;
+  std::lock_guard<std::mutex> lk(o.mu);
+  if (o.done.load(std::memory_order_relaxed) & bit) return 0;
+  const int rc = f();
+  if (!rc) o.done.fetch_or(bit, std::memory_order_release);
+  return rc;
+}
 
 // Layer stack of one Gblock region (same for every frequency point of a batch).
 struct StackParams {

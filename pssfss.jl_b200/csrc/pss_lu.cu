@@ -1,20 +1,21 @@
 // K4: dense complex LU with partial pivoting (replaces LAPACK zgetrf behind lu!,
 // PSSFSS.jl:401, 526).
 //
-// Matrices are row-major (row interchanges are contiguous).  Blocked right-looking LU,
-// two-level: an outer block of NB columns is factored as panels of W columns.
-//   * k_panel: one thread-block cluster (8 CTAs) owns a W-column panel; its rows are
-//     spread over the CTAs' shared memory and never move during the factorisation.  For
-//     each column every CTA pushes its local pivot candidate (|re|+|im| as LAPACK izamax,
-//     the row index, and the candidate row itself) into every CTA's shared memory, one
-//     cluster barrier makes them visible, and every CTA picks the same winner and applies
-//     the rank-1 update to its own active rows - one barrier and no remote round trip per
-//     column.  At the end the LAPACK swap sequence (ipiv) is replayed once and each CTA
-//     writes its rows to their final positions.
-//   * k_laswp applies the panel's interchanges to the other columns.
-//   * the block-row triangular solve U12 = L11^{-1} A12 uses the explicit inverse of the
-//     unit-lower diagonal block (k_tri_inv, then k_trsm_apply, a small dense product).
-//   * the Schur complement A22 -= L21 U12 is the GEMM (k_gemm64 / k_gemm32).
+// Matrices are row-major (row interchanges are contiguous).  Blocked right-looking LU in
+// LAPACK zgetrf order, two-level: an outer block of NB columns is factored as panels of W.
+//   * k_panel: a thread-block cluster of ceil(rows / 512) CTAs (<= 16) owns a W-column
+//     panel, one row per thread held in registers for the whole factorisation.  For each
+//     column every CTA pushes its local pivot candidate (|re|+|im| as LAPACK izamax, the
+//     row index and the candidate row) into every CTA's shared memory, one cluster barrier
+//     makes them visible, and every CTA picks the same winner and applies the rank-1
+//     update to its own rows.  At the end every CTA replays the interchange sequence in
+//     shared memory (a sparse map of the <= 2W moved positions), CTA 0 writes ipiv and a
+//     compact interchange list, and each thread writes its row to its final position.
+//   * k_laswp applies that list to all other columns in one launch.
+//   * k_trsm_small: the W-row block-row solve L11^{-1} X, one column per thread.
+//   * the Schur complement A22 -= L21 U12: k_gemm64 (FP64, SIMT), and in FP32 mode
+//     k_gemm32 for the skinny updates inside an outer block and the tcgen05 3xTF32 kernel
+//     (pss_gemm_tc.cu) for the trailing update of each outer block.
 // In FP32 mode the matrix is two float planes (real, imaginary).
 #include <cooperative_groups.h>
 #include "pss_internal.cuh"
@@ -62,13 +63,16 @@ struct Mat {
 constexpr int kPanelThreads = 512;  // one panel row per thread
 constexpr int kMaxCluster = 16;
 constexpr int kMaxW = 32;
+constexpr int kMaxMov = 2 * kMaxW;  // rows one panel's interchanges can move
+constexpr int kSwpThreads = 64;
+constexpr int kListInts = 1 + 2 * kMaxMov;  // interchange list: count, destinations, sources
 constexpr int kTcMin = 128;  // smallest trailing update sent to the tensor cores
 
 // Panel of W columns (w <= W used), rows row0..row0+nrows-1, factored by a cluster of
 // cs = gridDim.x CTAs; thread t of CTA q holds row q*512 + t in registers.
 template <bool F32, int W>
 __global__ void __launch_bounds__(kPanelThreads) k_panel(Mat<F32> M, int row0, int nrows, int col0, int w,
-                                                         int *ipiv, int *info, int *scratch) {
+                                                         int *ipiv, int *info, int *xlist) {
   using E = typename Prec<F32>::E;
   using Rl = typename Prec<F32>::R;
   cg::cluster_group cluster = cg::this_cluster();
@@ -83,6 +87,8 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(Mat<F32> M, int row0, i
   __shared__ double redv[NW];
   __shared__ int redi[NW];
   __shared__ int chosen[kMaxW];
+  __shared__ int mpos[2 * kMaxW], morig[2 * kMaxW];  // moved positions and the row each now holds
+  __shared__ int nmoved;
   const int gr = crank * kPanelThreads + tid;  // panel-relative row of this thread
   const bool have = gr < nrows;
   bool active = have;
@@ -160,66 +166,83 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(Mat<F32> M, int row0, i
     }
   }
   __syncthreads();
-  // Replay the interchanges (LAPACK semantics) to get ipiv and every row's final position.
-  int *row_at = scratch, *pos_of = scratch + nrows;
-  if (crank == 0) {
-    for (int i = tid; i < nrows; i += blockDim.x) { row_at[i] = i; pos_of[i] = i; }
-    __syncthreads();
-    if (tid == 0) {
-      for (int j = 0; j < w; ++j) {
-        const int r = chosen[j];
-        const int p = r < 0 ? j : pos_of[r];  // a zero column keeps its row (no interchange)
-        ipiv[col0 + j] = row0 + p;
-        const int a = row_at[j], b = row_at[p];
-        row_at[j] = b; row_at[p] = a;
-        pos_of[b] = j; pos_of[a] = p;
+  // Replay the interchanges (LAPACK semantics) in shared memory, by warp 0 of every CTA
+  // (each holds the same chosen[]): a sparse map of the <= 2w positions whose row changed.
+  if (warp == 0) {
+    int cnt = 0;  // warp-uniform
+    auto find = [&](const int *keys, int key) -> int {  // index of key in keys[0..cnt), or -1
+      const bool h0 = lane < cnt && keys[lane] == key;
+      const bool h1 = lane + 32 < cnt && keys[lane + 32] == key;
+      const unsigned b0 = __ballot_sync(0xffffffffu, h0), b1 = __ballot_sync(0xffffffffu, h1);
+      return b0 ? __ffs(b0) - 1 : (b1 ? 32 + __ffs(b1) - 1 : -1);
+    };
+    for (int j = 0; j < w; ++j) {
+      const int r = chosen[j];
+      int p = j;
+      if (r >= 0) {  // current position of original row r
+        const int e = find(morig, r);
+        p = e >= 0 ? mpos[e] : r;
+      }
+      if (crank == 0 && lane == 0) ipiv[col0 + j] = row0 + p;
+      if (p != j) {
+        const int ej = find(mpos, j), ep = find(mpos, p);
+        const int a = ej >= 0 ? morig[ej] : j;  // row now at position j
+        const int b = ep >= 0 ? morig[ep] : p;  // row now at position p
+        __syncwarp();
+        if (lane == 0) {
+          if (ej >= 0) morig[ej] = b; else { mpos[cnt] = j; morig[cnt] = b; }
+          if (ep >= 0) morig[ep] = a; else { mpos[cnt + (ej < 0)] = p; morig[cnt + (ej < 0)] = a; }
+        }
+        cnt += (ej < 0) + (ep < 0);
+        __syncwarp();
       }
     }
+    if (lane == 0) nmoved = cnt;
+    // Interchange list for the other columns: dst = row0 + position, src = row0 + original row.
+    if (crank == 0) {
+      int m = 0;
+      for (int e = 0; e < cnt; ++e)
+        if (mpos[e] != morig[e]) {
+          if (lane == 0) { xlist[1 + m] = row0 + mpos[e]; xlist[1 + kMaxMov + m] = row0 + morig[e]; }
+          ++m;
+        }
+      if (lane == 0) xlist[0] = m;
+    }
   }
-  cluster.sync();
+  __syncthreads();
   if (have) {
-    const int dst = pos_of[gr];
+    int dst = gr;
+    for (int e = 0; e < nmoved; ++e)
+      if (morig[e] == gr) dst = mpos[e];
 #pragma unroll
     for (int c = 0; c < W; ++c)
       if (c < w) M.put(row0 + dst, col0 + c, row[c]);
   }
 }
 
-// Apply the interchanges k = k0..k0+cnt-1 (row k <-> ipiv[k], in order) to columns
-// [c0, c1): the composed permutation of the <= 2*cnt rows involved is built once per CTA,
-// then every column gathers all its moved entries first and scatters them after, so no
-// load waits on a previous swap.  128 threads, one column each.
+// Apply a panel's interchanges (its list: xlist[0] = m moves, dst rows xlist[1..m], source
+// rows xlist[1+kMaxMov..]) to columns [0, ncol) except the panel's own [skip0, skip0 + w):
+// every thread gathers its column's moved entries first and scatters them after.
 template <bool F32>
-__global__ void __launch_bounds__(128) k_laswp(Mat<F32> M, int k0, int cnt, const int *ipiv, int c0, int c1) {
+__global__ void __launch_bounds__(kSwpThreads) k_laswp(Mat<F32> M, const int *__restrict__ xlist, int ncol,
+                                                       int skip0, int w) {
   using E = typename Prec<F32>::E;
-  __shared__ int rows[2 * kMaxW], from[2 * kMaxW];
-  __shared__ int nmov;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  E *stage = (E *)smraw;  // [2*kMaxW][128]
-  if (threadIdx.x == 0) {
-    int nr = 0;
-    for (int k = k0; k < k0 + cnt; ++k) {
-      const int p = ipiv[k];
-      int ik = -1, ip = -1;
-      for (int q = 0; q < nr; ++q) {
-        if (rows[q] == k) ik = q;
-        if (rows[q] == p) ip = q;
-      }
-      if (ik < 0) { rows[nr] = k; from[nr] = k; ik = nr++; }
-      if (ip < 0) { rows[nr] = p; from[nr] = p; ip = nr++; }
-      const int t = from[ik]; from[ik] = from[ip]; from[ip] = t;
-    }
-    int m = 0;  // keep only rows whose content changes
-    for (int q = 0; q < nr; ++q)
-      if (from[q] != rows[q]) { rows[m] = rows[q]; from[m] = from[q]; ++m; }
-    nmov = m;
+  constexpr int MOV = F32 ? 2 * 32 : 2 * 16;  // 2 x panel width
+  __shared__ int dst[MOV], src[MOV];
+  __shared__ E stage[MOV][kSwpThreads];
+  __shared__ int nm;
+  if (threadIdx.x == 0) nm = min(xlist[0], MOV);
+  for (int q = threadIdx.x; q < MOV; q += blockDim.x) {
+    dst[q] = xlist[1 + q];
+    src[q] = xlist[1 + kMaxMov + q];
   }
   __syncthreads();
-  const int c = c0 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= c1) return;
-  const int m = nmov;
-  for (int q = 0; q < m; ++q) stage[q * 128 + threadIdx.x] = M.get(from[q], c);
-  for (int q = 0; q < m; ++q) M.put(rows[q], c, stage[q * 128 + threadIdx.x]);
+  const int m = nm;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ncol - w) return;
+  const int c = t < skip0 ? t : t + w;
+  for (int q = 0; q < m; ++q) stage[q][threadIdx.x] = M.get(src[q], c);
+  for (int q = 0; q < m; ++q) M.put(dst[q], c, stage[q][threadIdx.x]);
 }
 
 // Rows k0..k0+w-1 of columns [c0, c1): X = L11^{-1} X, L11 the w x w unit-lower block at
@@ -237,15 +260,17 @@ __global__ void __launch_bounds__(128) k_trsm_small(Mat<F32> M, int k0, int w, i
   if (c >= c1) return;
   E x[W];
 #pragma unroll
-  for (int i = 0; i < W; ++i) {
-    if (i < w) {
-      E v = M.get(k0 + i, c);
+  for (int i = 0; i < W; ++i) x[i] = i < w ? M.get(k0 + i, c) : E{0, 0};  // all loads in flight at once
 #pragma unroll
-      for (int t = 0; t < i; ++t) v = csubE(v, cmulE(L[i][t], x[t]));
-      x[i] = v;
-      M.put(k0 + i, c, v);
-    }
+  for (int i = 1; i < W; ++i) {
+    E v = x[i];
+#pragma unroll
+    for (int t = 0; t < i; ++t) v = csubE(v, cmulE(L[i][t], x[t]));
+    x[i] = v;
   }
+#pragma unroll
+  for (int i = 0; i < W; ++i)
+    if (i < w) M.put(k0 + i, c, x[i]);
 }
 
 // C[r0:r1, c0:c1] -= A[r0:r1, k0:k0+kb] * A[k0:k0+kb, c0:c1]  (FP64 complex, SIMT, 64x64 tiles)
@@ -344,7 +369,7 @@ __global__ void __launch_bounds__(256) k_gemm32(float *Ar, float *Ai, long long 
 
 // ------------------------------- host side -------------------------------
 template <bool F32>
-int launch_panel(Mat<F32> M, int row0, int nrows, int col0, int w, int *ipiv, int *info, int *scratch,
+int launch_panel(Mat<F32> M, int row0, int nrows, int col0, int w, int *ipiv, int *info, int *xlist,
                  cudaStream_t st) {
   const int cs = (nrows + kPanelThreads - 1) / kPanelThreads;
   const int Wt = F32 ? 32 : 16;
@@ -353,11 +378,12 @@ int launch_panel(Mat<F32> M, int row0, int nrows, int col0, int w, int *ipiv, in
     return -6;
   }
   auto kern = k_panel<F32, (F32 ? 32 : 16)>;
-  static bool attr[2] = {false, false};
-  if (!attr[F32]) {
-    cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-    attr[F32] = true;
-  }
+  static DeviceOnce once;
+  if (int rc = device_once(once, [&] {
+        PSS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        return 0;
+      }))
+    return rc;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(cs);
   cfg.blockDim = dim3(kPanelThreads);
@@ -371,21 +397,15 @@ int launch_panel(Mat<F32> M, int row0, int nrows, int col0, int w, int *ipiv, in
   cfg.attrs = at;
   cfg.numAttrs = 1;
   pss_count_launch();
-  PSS_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, M, row0, nrows, col0, w, ipiv, info, scratch));
+  PSS_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, M, row0, nrows, col0, w, ipiv, info, xlist));
   return 0;
 }
 
 template <bool F32>
-void launch_laswp(Mat<F32> M, int k0, int cnt, const int *ipiv, int c0, int c1, cudaStream_t st) {
-  if (c1 <= c0 || cnt <= 0) return;
-  using E = typename Prec<F32>::E;
-  static bool attr[2] = {false, false};
-  if (!attr[F32]) {
-    cudaFuncSetAttribute(k_laswp<F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * kMaxW * 128 * (int)sizeof(E));
-    attr[F32] = true;
-  }
+void launch_laswp(Mat<F32> M, const int *xlist, int n, int k0, int w, cudaStream_t st) {
+  if (n - w <= 0) return;
   pss_count_launch();
-  k_laswp<F32><<<cdiv_u(c1 - c0, 128), 128, 2 * (size_t)cnt * 128 * sizeof(E), st>>>(M, k0, cnt, ipiv, c0, c1);
+  k_laswp<F32><<<cdiv_u(n - w, kSwpThreads), kSwpThreads, 0, st>>>(M, xlist, n, k0, w);
 }
 
 template <bool F32>
@@ -445,8 +465,7 @@ int lu_blocked(int n, Mat<F32> M, int *ipiv, int *info, int NB, int W, int *pscr
       const int w = min(W, E - k0);
       int rc = launch_panel<F32>(M, k0, n - k0, k0, w, ipiv, info, pscratch, st);
       if (rc) return rc;
-      launch_laswp<F32>(M, k0, w, ipiv, 0, k0, st);
-      launch_laswp<F32>(M, k0, w, ipiv, k0 + w, n, st);
+      launch_laswp<F32>(M, pscratch, n, k0, w, st);
       if (k0 + w < E) {
         launch_trsm<F32>(M, k0, w, k0 + w, E, st);
         launch_gemm(M, k0 + w, n, k0 + w, E, k0, w, st);
@@ -473,11 +492,11 @@ int pick_panel_width(int n, int want) {
 }
 
 constexpr int kNB64 = 64, kNB32 = 128;
-size_t scratch_bytes(int n) { return (2 * (size_t)n * sizeof(int) + 256 + 255) & ~(size_t)255; }
+size_t scratch_bytes(int) { return (kListInts * sizeof(int) + 255) & ~(size_t)255; }
 }  // namespace
 
-// Workspace: panel row bookkeeping (2n ints), then for the FP32 factorisation the split
-// operand planes of the tensor-core trailing update.
+// Workspace: the panel's interchange list (kListInts ints), then for the FP32 factorisation
+// the split operand planes of the tensor-core trailing update.
 size_t pss_lu_ws_bytes(int n, int precision) {
   return scratch_bytes(n) + (precision == 0 ? 0 : pss_tc_ws_bytes(n, n, kNB32));
 }

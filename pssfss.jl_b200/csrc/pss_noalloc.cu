@@ -7,17 +7,20 @@
 // call cudaMalloc/cudaFree per call: cudaMalloc can fail against the pool's reservation,
 // and cudaFree synchronises the whole device, stalling every other stream.  The regular
 // entry points (pss_lu_solve and the context workers) own their workspaces; this one keeps
-// its only scratch, the panel's row bookkeeping, in a fixed file-scope device array.
+// its only scratch, the panels' interchange list, in a fixed file-scope device array.
 //
 // Limits and rules (also stated in include/pssfss_b200.h):
 //   * order n <= kNoAllocMaxOrder (8192, the cluster panel's own limit of 16 CTAs x 512
 //     rows); larger n is rejected with an error message before anything is launched;
+//   * the scratch is kScratchBytes (1 KB): one panel's interchange list (count, 64
+//     destination rows, 64 source rows), rewritten by every panel;
 //   * the scratch array is one per device and is shared by every call on that device:
 //     calls that overlap in time on one device (different streams or host threads) race
 //     on it and produce wrong factors - serialise them (one stream, or synchronise);
-//   * nothing in the scratch has to start at zero (each panel initialises the bookkeeping
-//     it reads); *info must be zero when the factorisation starts, and this function
-//     writes that zero itself, on the caller's stream, before the first kernel;
+//   * nothing in the scratch has to start at zero (each panel writes the list before the
+//     interchange kernel reads it); *info must be zero when the factorisation starts,
+//     and this function writes that zero itself, on the caller's stream, before the first
+//     kernel;
 //   * the first call on each device resolves the scratch array's address with
 //     cudaGetSymbolAddress (a one-time set-up, done with that device current); make that
 //     first call before any stream capture on the device.
@@ -29,8 +32,8 @@
 namespace {
 
 constexpr int kNoAllocMaxOrder = 8192;
-// 2 ints per row plus alignment slack: at least pss_lu_ws_bytes(kNoAllocMaxOrder, PSS_FP64).
-constexpr size_t kScratchBytes = 2 * sizeof(int) * (size_t)kNoAllocMaxOrder + 512;
+// One panel's interchange list (129 ints) rounded up: pss_lu_ws_bytes(n, PSS_FP64) for every n.
+constexpr size_t kScratchBytes = 1024;
 
 static __device__ __align__(256) unsigned char g_lu_scratch[kScratchBytes];
 

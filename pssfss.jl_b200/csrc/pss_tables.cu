@@ -346,12 +346,13 @@ void pss_tables_find_mmax(int npts, int R, const unsigned char *conv, int *mmax,
 // dense: this point's (2R+1)^2 x 2 tables; stage: >= 2*mmax^2 entries; t1/t2: (mmax+2)^2 each.
 int pss_tables_finish(const cd *dense, int R, int mmax, const PointParams *dP1, cd *stage, cd *t1, cd *t2,
                       cudaStream_t st) {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_fft_lines, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         2 * PSS_MMAX_CAP * (int)sizeof(cd));
-    attr = true;
-  }
+  static DeviceOnce once;
+  if (int rc = device_once(once, [] {
+        PSS_CUDA_TRY(cudaFuncSetAttribute(k_fft_lines, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          2 * PSS_MMAX_CAP * (int)sizeof(cd)));
+        return 0;
+      }))
+    return rc;
   long long nn = (long long)mmax * mmax;
   cd *a1 = stage, *a2 = stage + nn;
   if (nn > 0) {

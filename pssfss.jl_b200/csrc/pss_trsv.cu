@@ -24,6 +24,7 @@ constexpr int kNX = kMaxRefRhs;           // norms layout: [max|r_j|] [max|x_j|]
 constexpr int kNA = 2 * kMaxRefRhs;
 constexpr int kNormCount = 2 * kMaxRefRhs + 1;
 constexpr long long kSpinCap = 1LL << 24;
+constexpr int kTrsvSmem = BS * BS * (int)sizeof(cd);  // Dinv_b staged by each chained-solve CTA
 
 struct Fac {  // row-major factor access: FP64 interleaved or FP32 planes
   const cd *a64;
@@ -37,6 +38,13 @@ struct Fac {  // row-major factor access: FP64 interleaved or FP32 planes
 
 __device__ __forceinline__ double cabs1(cd z) { return fabs(z.x) + fabs(z.y); }
 
+// L2-only (L1-bypassing) access to blocks of X that other CTAs produce or consume.
+__device__ __forceinline__ cd ldcg(const cd *p) {
+  const double2 v = __ldcg(reinterpret_cast<const double2 *>(p));
+  return mkcd(v.x, v.y);
+}
+__device__ __forceinline__ void stcg(cd *p, cd v) { __stcg(reinterpret_cast<double2 *>(p), make_double2(v.x, v.y)); }
+
 // Spin until flags[c] >= epoch (acquire).  Returns false (and records an error) at the cap.
 __device__ __forceinline__ bool wait_flag(int *flags, int c, int epoch, int *err) {
   cuda::atomic_ref<int, cuda::thread_scope_device> f(flags[c]);
@@ -46,7 +54,7 @@ __device__ __forceinline__ bool wait_flag(int *flags, int c, int epoch, int *err
       atomicExch(err, 1);
       return false;
     }
-    __nanosleep(100);
+    if (it > 512) __nanosleep(64);  // hot spin first: the chain's step time is a few microseconds
   }
   return true;
 }
@@ -99,81 +107,92 @@ __global__ void __launch_bounds__(1024) k_ipiv_to_perm(int n, const int *ipiv, i
   for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = sp[i];
 }
 
-// One chained substitution pass.  lower: X[rows] = Linv_b (B[perm[rows]] - L[rows, :b] X[:b]);
-// upper: X[rows] = Uinv_b (X[rows] - U[rows, b+1:] X[b+1:]) (in place).  256 threads.
-// 256 threads: row i of the block = tid / 4, quarter p = tid % 4 covers 16 columns of
-// each 64-column block; the block of X it multiplies is staged in shared memory.
+// One chained substitution pass over right-hand sides j0 .. j0+nj-1 (nj <= kMaxRhs):
+//   lower: X[rows_b] = Linv_b (B[perm[rows_b]] - sum_{c<b} L[b,c] X[c])
+//   upper: X[rows_b] = Uinv_b (X[rows_b] - sum_{c>b} U[b,c] X[c])   (in place)
+// One CTA per 64-row block b (ticket order), 256 threads: row i = tid/4 of the block,
+// quarter p = tid%4 covers 16 columns of each 64-column tile.  Each tile of the factor is
+// loaded into registers BEFORE the wait for the CTA that produces x_c, so the wait hides
+// the load; Dinv_b (64 KB, dynamic shared memory) and the block's right-hand side are
+// staged at the start.  Blocks of X written by other CTAs are read with L1-bypassing loads.
 template <bool LOWER>
 __global__ void __launch_bounds__(256) k_trsv(Fac F, int n, const int *__restrict__ perm, const cd *__restrict__ B,
-                                              cd *__restrict__ X, int nrhs, const cd *__restrict__ Dinv,
+                                              cd *__restrict__ X, int nrhs, int j0, const cd *__restrict__ Dinv,
                                               int *ticket, int *flags, int epoch, int *err,
                                               const int *__restrict__ done) {
   if (done && *done) return;
-  __shared__ int s_b;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  cd *Ds = (cd *)smraw;  // BS x BS, row-major
   __shared__ cd y[BS][kMaxRhs];
   __shared__ cd xs[BS][kMaxRhs];
+  __shared__ int s_b;
   const int tid = threadIdx.x;
   const int i = tid >> 2, p = tid & 3;
   const int nblk = (n + BS - 1) / BS;
+  const int nj = min(kMaxRhs, nrhs - j0);
   if (tid == 0) s_b = atomicAdd(ticket, 1);
   __syncthreads();
   const int tk = s_b;
   const int b = LOWER ? tk : nblk - 1 - tk;
   const int r0 = b * BS, nr = min(BS, n - r0);
-  for (int j0 = 0; j0 < nrhs; j0 += kMaxRhs) {
-    const int nj = min(kMaxRhs, nrhs - j0);
-    cd acc[kMaxRhs];
-#pragma unroll
-    for (int j = 0; j < kMaxRhs; ++j) acc[j] = mkcd(0, 0);
-    const int c_lo = LOWER ? 0 : b + 1, c_hi = LOWER ? b : nblk;
-    for (int cc = c_lo; cc < c_hi; ++cc) {
-      const int c = LOWER ? cc : c_hi - 1 - (cc - c_lo);  // upper: nearest (earliest-ready) block first
-      if (j0 == 0 && tid == 0) wait_flag(flags, c, epoch, err);
-      __syncthreads();
-      // every thread acquires the producer's release before reading its block of X
-      if (j0 == 0) cuda::atomic_ref<int, cuda::thread_scope_device>(flags[c]).load(cuda::memory_order_acquire);
-      const int t0 = c * BS, nt = min(BS, n - t0);
-      for (int e = tid; e < BS * kMaxRhs; e += 256) {
-        const int t = e / kMaxRhs, j = e % kMaxRhs;
-        xs[t][j] = (t < nt && j < nj) ? X[(size_t)(j0 + j) * n + t0 + t] : mkcd(0, 0);
-      }
-      __syncthreads();
-      if (i < nr) {
-#pragma unroll 4
-        for (int q = 0; q < 16; ++q) {
-          const int t = p * 16 + q;
-          if (t >= nt) break;
-          cd l = F.at(r0 + i, t0 + t);
-#pragma unroll
-          for (int j = 0; j < kMaxRhs; ++j) acc[j] = acc[j] + l * xs[t][j];
-        }
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < kMaxRhs; ++j)
-      for (int o = 1; o < 4; o <<= 1) {
-        acc[j].x += __shfl_xor_sync(0xffffffff, acc[j].x, o);
-        acc[j].y += __shfl_xor_sync(0xffffffff, acc[j].y, o);
-      }
-    if (p == 0 && i < nr) {
-#pragma unroll
-      for (int j = 0; j < kMaxRhs; ++j) {
-        if (j >= nj) break;
-        cd rhs = LOWER ? B[(size_t)(j0 + j) * n + perm[r0 + i]] : X[(size_t)(j0 + j) * n + r0 + i];
-        y[i][j] = rhs - acc[j];
-      }
-    }
-    __syncthreads();
-    // X[rows] = Dinv_b * y
-    const cd *D = Dinv + (size_t)(2 * b + (LOWER ? 0 : 1)) * BS * BS;
-    for (int e = tid; e < nr * nj; e += blockDim.x) {
-      const int i = e / nj, j = e % nj;
-      cd s = mkcd(0, 0);
-      for (int k = 0; k < nr; ++k) s = s + D[i * BS + k] * y[k][j];
-      X[(size_t)(j0 + j) * n + r0 + i] = s;
-    }
-    __syncthreads();
+  const cd *D = Dinv + (size_t)(2 * b + (LOWER ? 0 : 1)) * BS * BS;
+  for (int e = tid; e < BS * BS; e += 256) Ds[e] = D[e];
+  for (int e = tid; e < BS * kMaxRhs; e += 256) {
+    const int r = e / kMaxRhs, j = e % kMaxRhs;
+    cd v = mkcd(0, 0);
+    if (r < nr && j < nj)
+      v = LOWER ? B[(size_t)(j0 + j) * n + perm[r0 + r]] : ldcg(&X[(size_t)(j0 + j) * n + r0 + r]);
+    y[r][j] = v;
   }
+  cd acc[kMaxRhs];
+#pragma unroll
+  for (int j = 0; j < kMaxRhs; ++j) acc[j] = mkcd(0, 0);
+  const int c_lo = LOWER ? 0 : b + 1, c_hi = LOWER ? b : nblk;
+  for (int cc = c_lo; cc < c_hi; ++cc) {
+    const int c = LOWER ? cc : c_hi - 1 - (cc - c_lo);  // upper: the last block is ready first
+    const int t0 = c * BS, nt = min(BS, n - t0);
+    cd lv[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int t = p * 16 + q;
+      lv[q] = (i < nr && t < nt) ? F.at(r0 + i, t0 + t) : mkcd(0, 0);
+    }
+    if (tid == 0) {
+      wait_flag(flags, c, epoch, err);
+      __threadfence();
+    }
+    __syncthreads();
+    for (int e = tid; e < BS * kMaxRhs; e += 256) {
+      const int t = e / kMaxRhs, j = e % kMaxRhs;
+      xs[t][j] = (t < nt && j < nj) ? ldcg(&X[(size_t)(j0 + j) * n + t0 + t]) : mkcd(0, 0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+#pragma unroll
+      for (int j = 0; j < kMaxRhs; ++j) acc[j] = acc[j] + lv[q] * xs[p * 16 + q][j];
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < kMaxRhs; ++j)
+    for (int o = 1; o < 4; o <<= 1) {
+      acc[j].x += __shfl_xor_sync(0xffffffff, acc[j].x, o);
+      acc[j].y += __shfl_xor_sync(0xffffffff, acc[j].y, o);
+    }
+  __syncthreads();
+  if (p == 0 && i < nr) {
+#pragma unroll
+    for (int j = 0; j < kMaxRhs; ++j) y[i][j] = y[i][j] - acc[j];
+  }
+  __syncthreads();
+  // X[rows] = Dinv_b * y
+  for (int e = tid; e < nr * nj; e += blockDim.x) {
+    const int r = e / nj, j = e % nj;
+    cd s = mkcd(0, 0);
+    for (int k = 0; k < nr; ++k) s = s + Ds[r * BS + k] * y[k][j];
+    stcg(&X[(size_t)(j0 + j) * n + r0 + r], s);
+  }
+  __syncthreads();
   if (tid == 0) {
     __threadfence();
     post_flag(flags, b, epoch);
@@ -280,11 +299,13 @@ int pss_solve_prepare(SolveWS &ws, const cd *LU64, const float *Lr, const float 
   Fac F{LU64, Lr, Li, ld};
   pss_count_launch();
   k_ipiv_to_perm<<<1, 1024, ws.n * sizeof(int), st>>>(ws.n, ipiv, ws.perm);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_diag_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * BS * BS * (int)sizeof(cd));
-    attr = true;
-  }
+  static DeviceOnce once;
+  if (int rc = device_once(once, [] {
+        PSS_CUDA_TRY(
+            cudaFuncSetAttribute(k_diag_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * BS * BS * (int)sizeof(cd)));
+        return 0;
+      }))
+    return rc;
   pss_count_launch();
   k_diag_inv<<<dim3(ws.nblk, 2), BS, 2 * BS * BS * sizeof(cd), st>>>(F, ws.n, ws.Dinv);
   PSS_CUDA_TRY(cudaMemsetAsync(ws.ctrl, 0, (size_t)(ws.nblk + 64) * sizeof(int), st));
@@ -298,16 +319,25 @@ int pss_solve_lu(SolveWS &ws, const cd *LU64, const float *Lr, const float *Li, 
                  cd *X, const int *done, cudaStream_t st) {
   Fac F{LU64, Lr, Li, ld};
   int *ticket = ws.ctrl, *err = ws.ctrl + 1, *flags = ws.ctrl + 8;
-  for (int pass = 0; pass < 2; ++pass) {
-    ++ws.epoch;
-    PSS_CUDA_TRY(cudaMemsetAsync(ticket, 0, sizeof(int), st));
-    pss_count_launch();
-    if (pass == 0)
-      k_trsv<true><<<ws.nblk, 256, 0, st>>>(F, ws.n, ws.perm, B, X, nrhs, ws.Dinv, ticket, flags, ws.epoch, err, done);
-    else
-      k_trsv<false><<<ws.nblk, 256, 0, st>>>(F, ws.n, ws.perm, B, X, nrhs, ws.Dinv, ticket, flags, ws.epoch, err,
-                                             done);
-  }
+  static DeviceOnce once;
+  if (int rc = device_once(once, [] {
+        PSS_CUDA_TRY(cudaFuncSetAttribute(k_trsv<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrsvSmem));
+        PSS_CUDA_TRY(cudaFuncSetAttribute(k_trsv<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrsvSmem));
+        return 0;
+      }))
+    return rc;
+  for (int pass = 0; pass < 2; ++pass)
+    for (int j0 = 0; j0 < nrhs; j0 += kMaxRhs) {
+      ++ws.epoch;
+      PSS_CUDA_TRY(cudaMemsetAsync(ticket, 0, sizeof(int), st));
+      pss_count_launch();
+      if (pass == 0)
+        k_trsv<true><<<ws.nblk, 256, kTrsvSmem, st>>>(F, ws.n, ws.perm, B, X, nrhs, j0, ws.Dinv, ticket, flags,
+                                                      ws.epoch, err, done);
+      else
+        k_trsv<false><<<ws.nblk, 256, kTrsvSmem, st>>>(F, ws.n, ws.perm, B, X, nrhs, j0, ws.Dinv, ticket, flags,
+                                                       ws.epoch, err, done);
+    }
   PSS_CUDA_TRY(cudaGetLastError());
   return 0;
 }

@@ -108,7 +108,7 @@ def _i64(x):
 def context(device=0, nworkers=None):
     """Per-device ``pss_ctx`` (created once)."""
     if nworkers is None:
-        nworkers = int(os.environ.get("PSS_WORKERS", "4"))
+        nworkers = int(os.environ.get("PSS_WORKERS", "8"))
     key = (device, nworkers)
     with _lock:
         c = _ctx.get(key)
