@@ -114,11 +114,19 @@ int pss_lu_solve(pss_ctx *ctx, int n, const double *Z, int nrhs, const double *B
  * [tables, face_integrals, fill, factor, transforms+rhs, solve+refine, projection, total]. */
 int pss_last_timings(pss_ctx *ctx, double *ms8);
 
-/* Per-launch CUDA-event timing of the Schur-complement GEMM (the dominant kernel) during
- * pss_partial_gsms calls while enabled.  out3 = [launches, summed ms, summed algorithmic
- * flops (8*M*N*K per complex update)] of the last call. */
+/* Per-launch CUDA-event timing (on each launch's own stream) of the factorisation's main
+ * kernels during pss_partial_gsms calls while enabled.  out receives 3 doubles per kind -
+ * launches, summed milliseconds, summed algorithmic work - for the last call:
+ *   PSS_PROF_TC_UPDATE   tensor-core Schur update, work = 8*M*N*K flops per complex update
+ *   PSS_PROF_PANEL       cluster panel factorisation, work = bytes of the panel read + written
+ *   PSS_PROF_SIMT_UPDATE SIMT Schur update (FP64, and FP32 updates below the tensor-core size),
+ *                        work = 8*M*N*K flops */
+#define PSS_PROF_TC_UPDATE 0
+#define PSS_PROF_PANEL 1
+#define PSS_PROF_SIMT_UPDATE 2
+#define PSS_PROF_KINDS 3
 int pss_profile(pss_ctx *ctx, int enable);
-int pss_profile_result(pss_ctx *ctx, double *out3);
+int pss_profile_result(pss_ctx *ctx, double *out);
 
 /* Schur-complement update C -= L * U in complex FP32 on the tensor cores (tcgen05, 3xTF32
  * products: FP32-level accuracy), the kernel the PSS_FP32_REFINE factorisation uses for its

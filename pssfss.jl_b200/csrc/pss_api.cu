@@ -32,7 +32,8 @@ void pss_count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 namespace {
 struct KProf {
   std::vector<cudaEvent_t> e0, e1;
-  std::vector<double> flops;
+  std::vector<double> work;
+  std::vector<int> kind;
 };
 thread_local KProf *g_kprof = nullptr;
 }  // namespace
@@ -46,13 +47,14 @@ int pss_prof_begin(cudaStream_t st) {
   return (int)g_kprof->e0.size() - 1;
 }
 
-void pss_prof_end(int token, cudaStream_t st, double flops) {
+void pss_prof_end(int token, cudaStream_t st, int kind, double work) {
   if (token < 0 || !g_kprof) return;
   cudaEvent_t b;
   cudaEventCreate(&b);
   cudaEventRecord(b, st);
   g_kprof->e1.push_back(b);
-  g_kprof->flops.push_back(flops);
+  g_kprof->work.push_back(work);
+  g_kprof->kind.push_back(kind);
 }
 
 void pss_set_error(const char *fmt, ...) {
@@ -183,7 +185,7 @@ struct pss_ctx {
   std::vector<DevBuf> bigtables;
   double last_ms[8] = {0};
   bool prof_on = false;
-  double prof[3] = {0, 0, 0};  // GEMM launches, summed ms, summed algorithmic flops
+  double prof[3 * PSS_PROF_KINDS] = {};  // per kind: launches, summed ms, summed algorithmic work
 };
 
 struct pss_sheet {
@@ -745,14 +747,16 @@ int pss_partial_gsms(pss_sheet *sh, int nl, const double *eps, const double *mu,
       c->last_ms[q + 1] += ms;
     }
   }
-  c->prof[0] = c->prof[1] = c->prof[2] = 0;
+  for (double &v : c->prof) v = 0;
   for (auto &kprof : kprofs) {
     for (size_t q = 0; q < kprof.e1.size(); ++q) {
       float ms = 0;
       cudaEventElapsedTime(&ms, kprof.e0[q], kprof.e1[q]);
-      c->prof[0] += 1;
-      c->prof[1] += ms;
-      c->prof[2] += kprof.flops[q];
+      const int k = kprof.kind[q];
+      if (k < 0 || k >= PSS_PROF_KINDS) continue;
+      c->prof[3 * k] += 1;
+      c->prof[3 * k + 1] += ms;
+      c->prof[3 * k + 2] += kprof.work[q];
     }
     for (auto e : kprof.e0) cudaEventDestroy(e);
     for (auto e : kprof.e1) cudaEventDestroy(e);
@@ -775,9 +779,9 @@ int pss_profile(pss_ctx *c, int enable) {
   return 0;
 }
 
-int pss_profile_result(pss_ctx *c, double *out3) {
-  if (!c || !out3) { pss_set_error("null argument"); return -1; }
-  for (int q = 0; q < 3; ++q) out3[q] = c->prof[q];
+int pss_profile_result(pss_ctx *c, double *out) {
+  if (!c || !out) { pss_set_error("null argument"); return -1; }
+  for (int q = 0; q < 3 * PSS_PROF_KINDS; ++q) out[q] = c->prof[q];
   return 0;
 }
 

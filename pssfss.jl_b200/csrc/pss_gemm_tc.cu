@@ -413,7 +413,7 @@ int pss_cgemm_tc(float *Ar, float *Ai, long long ld, int m0, int M, int n0, int 
   const int tok = pss_prof_begin(st);
   pss_count_launch();
   k_cgemm_tf32x3<<<grid, 192, SMEM_BYTES, st>>>(ma, mb, g);
-  pss_prof_end(tok, st, 8.0 * M * (double)N * K);
+  pss_prof_end(tok, st, PSS_PROF_TC_UPDATE, 8.0 * M * (double)N * K);
   PSS_CUDA_TRY(cudaGetLastError());
   return 0;
 }

@@ -4,6 +4,7 @@
 #include <mutex>
 
 #include "pss_common.cuh"
+#include "pssfss_b200.h"
 
 // Per-device one-time set-up (kernel attributes and the like), safe to reach from several
 // host threads: f() runs once for each device it is first called on (that device current).
@@ -116,7 +117,7 @@ void pss_count_launch();
 // Optional CUDA-event timing of the Schur-complement GEMM launches (pss_profile): returns
 // a token (-1 when profiling is off) to pass to pss_prof_end with the launch's flops.
 int pss_prof_begin(cudaStream_t st);
-void pss_prof_end(int token, cudaStream_t st, double flops);
+void pss_prof_end(int token, cudaStream_t st, int kind, double work);
 
 // ---- host launchers (return 0 or a negative error code; errors via pss_set_error) ----
 // Modal tables (pss_tables.cu)

@@ -66,26 +66,60 @@ constexpr int kMaxW = 32;
 constexpr int kMaxMov = 2 * kMaxW;  // rows one panel's interchanges can move
 constexpr int kSwpThreads = 64;
 constexpr int kListInts = 1 + 2 * kMaxMov;  // interchange list: count, destinations, sources
-constexpr int kTcMin = 128;  // smallest trailing update sent to the tensor cores
+constexpr int kTcMinRows = 64, kTcMinCols = 32;  // smallest FP32 update sent to the tensor cores
+
+// Pivot candidate of one column: LAPACK's izamax order (largest |re|+|im|, then the lowest
+// row).  FP32: value and row packed in one 64-bit key (non-negative float bits are
+// monotonic), so a comparison is one integer compare and a shuffle is one 64-bit shuffle.
+template <bool F32>
+struct PivKey;
+template <>
+struct PivKey<true> {
+  unsigned long long k;  // 0 = no candidate
+  __device__ static PivKey make(float re, float im, int row, bool act) {
+    const float v = fabsf(re) + fabsf(im);
+    return {act ? ((unsigned long long)__float_as_uint(v) << 32) | (0xffffffffu - (unsigned)row) : 0ull};
+  }
+  __device__ static PivKey none() { return {0ull}; }
+  __device__ bool worse_than(const PivKey &o) const { return o.k > k; }
+  __device__ PivKey shfl_xor(int o) const { return {__shfl_xor_sync(0xffffffffu, k, o)}; }
+  __device__ int row() const { return (int)(0xffffffffu - (unsigned)(k & 0xffffffffu)); }
+  __device__ bool nonzero() const { return (k >> 32) != 0ull; }  // a candidate with |re|+|im| > 0
+};
+template <>
+struct PivKey<false> {
+  double v;  // -1: no candidate
+  int r;
+  __device__ static PivKey make(double re, double im, int row, bool act) {
+    return act ? PivKey{fabs(re) + fabs(im), row} : none();
+  }
+  __device__ static PivKey none() { return {-1.0, 0x7fffffff}; }
+  __device__ bool worse_than(const PivKey &o) const { return o.v > v || (o.v == v && o.r < r); }
+  __device__ PivKey shfl_xor(int o) const {
+    return {__shfl_xor_sync(0xffffffffu, v, o), __shfl_xor_sync(0xffffffffu, r, o)};
+  }
+  __device__ int row() const { return r; }
+  __device__ bool nonzero() const { return v > 0.0; }
+};
 
 // Panel of W columns (w <= W used), rows row0..row0+nrows-1, factored by a cluster of
-// cs = gridDim.x CTAs; thread t of CTA q holds row q*512 + t in registers.
+// cs = gridDim.x CTAs; thread t of CTA q holds row q*512 + t in registers.  The column
+// loop is fully unrolled so every register index is a compile-time constant.
 template <bool F32, int W>
 __global__ void __launch_bounds__(kPanelThreads) k_panel(Mat<F32> M, int row0, int nrows, int col0, int w,
                                                          int *ipiv, int *info, int *xlist) {
   using E = typename Prec<F32>::E;
   using Rl = typename Prec<F32>::R;
+  using K = PivKey<F32>;
   cg::cluster_group cluster = cg::this_cluster();
   const int cs = (int)cluster.num_blocks();
   const int crank = (int)cluster.block_rank();
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   constexpr int NW = kPanelThreads / 32;
   __shared__ E srow[2][kMaxCluster][W];   // candidate rows pushed by every CTA (double-buffered)
-  __shared__ double sval[2][kMaxCluster];
-  __shared__ int sidx[2][kMaxCluster];
+  __shared__ K skey[2][kMaxCluster];      // their keys
   __shared__ E own[W];                    // this CTA's candidate row, staged for the push
-  __shared__ double redv[NW];
-  __shared__ int redi[NW];
+  __shared__ K redk[NW];                  // per-warp winners
   __shared__ int chosen[kMaxW];
   __shared__ int mpos[2 * kMaxW], morig[2 * kMaxW];  // moved positions and the row each now holds
   __shared__ int nmoved;
@@ -96,73 +130,71 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(Mat<F32> M, int row0, i
 #pragma unroll
   for (int c = 0; c < W; ++c) row[c] = (have && c < w) ? M.get(row0 + gr, col0 + c) : E{0, 0};
 
-  for (int j = 0; j < w; ++j) {
-    const int par = j & 1;
-    E vj = E{0, 0};
 #pragma unroll
-    for (int c = 0; c < W; ++c)
-      if (c == j) vj = row[c];
-    double best = active ? fabs((double)vj.x) + fabs((double)vj.y) : -1.0;
-    int bidx = active ? gr : 0x7fffffff;
-    for (int o = 16; o > 0; o >>= 1) {
-      double ob = __shfl_xor_sync(0xffffffff, best, o);
-      int oi = __shfl_xor_sync(0xffffffff, bidx, o);
-      if (ob > best || (ob == best && oi < bidx)) { best = ob; bidx = oi; }
-    }
-    if (lane == 0) { redv[warp] = best; redi[warp] = bidx; }
-    __syncthreads();
-    double cb = redv[0];
-    int ci = redi[0];
+  for (int j = 0; j < W; ++j) {
+    if (j < w) {  // uniform over the cluster
+      const int par = j & 1;
+      const E vj = row[j];
+      K key = K::make(vj.x, vj.y, gr, active);
 #pragma unroll
-    for (int k = 1; k < NW; ++k)
-      if (redv[k] > cb || (redv[k] == cb && redi[k] < ci)) { cb = redv[k]; ci = redi[k]; }
-    if (cb >= 0.0 && gr == ci) {
+      for (int o = 16; o > 0; o >>= 1) {
+        const K ok = key.shfl_xor(o);
+        if (key.worse_than(ok)) key = ok;
+      }
+      if (lane == 0) redk[warp] = key;
+      __syncthreads();
+      K cb = lane < NW ? redk[lane] : K::none();  // every warp reduces the NW warp winners
 #pragma unroll
-      for (int c = 0; c < W; ++c) own[c] = row[c];
-    }
-    __syncthreads();
-    if (warp == 0) {  // push (value, row, candidate row) to slot [par][crank] of every CTA
-      for (int dst = 0; dst < cs; ++dst) {
-        E *rr = &cluster.map_shared_rank(&srow[0][0][0], dst)[(par * kMaxCluster + crank) * W];
-        for (int c = lane; c < w; c += 32) rr[c] = cb >= 0.0 ? own[c] : E{0, 0};
-        if (lane == 0) {
-          cluster.map_shared_rank(&sval[0][0], dst)[par * kMaxCluster + crank] = cb;
-          cluster.map_shared_rank(&sidx[0][0], dst)[par * kMaxCluster + crank] = ci;
+      for (int o = NW / 2; o > 0; o >>= 1) {
+        const K ok = cb.shfl_xor(o);
+        if (cb.worse_than(ok)) cb = ok;
+      }
+      if (active && gr == cb.row()) {
+#pragma unroll
+        for (int c = j; c < W; ++c) own[c] = row[c];
+      }
+      __syncthreads();
+      if (warp == 0) {  // push (key, candidate row) to slot [par][crank] of every CTA
+        for (int e = lane; e < cs * W; e += 32) {
+          const int dst = e / W, c = e % W;
+          if (c >= j && c < w)
+            cluster.map_shared_rank(&srow[0][0][0], dst)[(par * kMaxCluster + crank) * W + c] = own[c];
         }
+        if (lane < cs) cluster.map_shared_rank(&skey[0][0], lane)[par * kMaxCluster + crank] = cb;
       }
-    }
-    cluster.sync();
-    double gb = -1.0;
-    int gi = 0x7fffffff, gc = 0;
-    for (int q = 0; q < cs; ++q) {
-      const double v = sval[par][q];
-      const int i = sidx[par][q];
-      if (v > gb || (v == gb && i < gi)) { gb = v; gi = i; gc = q; }
-    }
-    const bool sing = !(gb > 0.0);
-    if (tid == 0) chosen[j] = sing ? -1 : gi;
-    if (!sing) {
-      if (gr == gi) active = false;
-      const E *prow = srow[par][gc];
-      E piv = prow[j];
-      E inv;  // 1/pivot (LAPACK zgetf2 scales the column by the reciprocal)
-      if (fabs((double)piv.y) <= fabs((double)piv.x)) {
-        Rl rr = piv.y / piv.x, d = piv.x + piv.y * rr;
-        inv = E{(Rl)1 / d, -rr / d};
-      } else {
-        Rl rr = piv.x / piv.y, d = piv.y + piv.x * rr;
-        inv = E{rr / d, (Rl)-1 / d};
-      }
-      if (active) {
-        const E l = cmulE(vj, inv);
+      cluster.sync();
+      K gk = lane < cs ? skey[par][lane] : K::none();
 #pragma unroll
-        for (int c = 0; c < W; ++c) {
-          if (c == j) row[c] = l;
-          else if (c > j) row[c] = csubE(row[c], cmulE(l, prow[c]));
-        }
+      for (int o = kMaxCluster / 2; o > 0; o >>= 1) {
+        const K ok = gk.shfl_xor(o);
+        if (gk.worse_than(ok)) gk = ok;
       }
-    } else if (tid == 0 && crank == 0) {
-      atomicCAS(info, 0, col0 + j + 1);
+      const bool sing = !gk.nonzero();
+      if (tid == 0) chosen[j] = sing ? -1 : gk.row();
+      if (!sing) {
+        const K mine = lane < cs ? skey[par][lane] : K::none();
+        const unsigned hit = __ballot_sync(0xffffffffu, lane < cs && !mine.worse_than(gk) && !gk.worse_than(mine));
+        const int gc = __ffs(hit) - 1;
+        if (gr == gk.row()) active = false;
+        const E *prow = srow[par][gc];
+        const E piv = prow[j];
+        E inv;  // 1/pivot (LAPACK zgetf2 scales the column by the reciprocal)
+        if (fabs((double)piv.y) <= fabs((double)piv.x)) {
+          const Rl rr = piv.y / piv.x, d = piv.x + piv.y * rr;
+          inv = E{(Rl)1 / d, -rr / d};
+        } else {
+          const Rl rr = piv.x / piv.y, d = piv.y + piv.x * rr;
+          inv = E{rr / d, (Rl)-1 / d};
+        }
+        if (active) {
+          const E l = cmulE(vj, inv);
+          row[j] = l;
+#pragma unroll
+          for (int c = j + 1; c < W; ++c) row[c] = csubE(row[c], cmulE(l, prow[c]));
+        }
+      } else if (tid == 0 && crank == 0) {
+        atomicCAS(info, 0, col0 + j + 1);
+      }
     }
   }
   __syncthreads();
@@ -397,7 +429,10 @@ int launch_panel(Mat<F32> M, int row0, int nrows, int col0, int w, int *ipiv, in
   cfg.attrs = at;
   cfg.numAttrs = 1;
   pss_count_launch();
+  const int tok = pss_prof_begin(st);
   PSS_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, M, row0, nrows, col0, w, ipiv, info, xlist));
+  // algorithmic bytes: the panel read once and written once
+  pss_prof_end(tok, st, PSS_PROF_PANEL, 2.0 * nrows * w * (F32 ? 8.0 : 16.0));
   return 0;
 }
 
@@ -423,7 +458,7 @@ void launch_gemm(Mat<false> M, int r0, int r1, int c0, int c1, int k0, int kb, c
   int tok = pss_prof_begin(st);
   pss_count_launch();
   k_gemm64<<<dim3(cdiv_u(c1 - c0, 64), cdiv_u(r1 - r0, 64)), 256, 0, st>>>((cd *)M.a, M.ld, r0, r1, c0, c1, k0, kb);
-  pss_prof_end(tok, st, 8.0 * (r1 - r0) * (double)(c1 - c0) * kb);
+  pss_prof_end(tok, st, PSS_PROF_SIMT_UPDATE, 8.0 * (r1 - r0) * (double)(c1 - c0) * kb);
 }
 void launch_gemm(Mat<true> M, int r0, int r1, int c0, int c1, int k0, int kb, cudaStream_t st) {
   if (r1 <= r0 || c1 <= c0) return;
@@ -431,7 +466,30 @@ void launch_gemm(Mat<true> M, int r0, int r1, int c0, int c1, int k0, int kb, cu
   pss_count_launch();
   k_gemm32<<<dim3(cdiv_u(c1 - c0, 128), cdiv_u(r1 - r0, 128)), 256, 0, st>>>((float *)M.a, M.ai, M.ld, r0, r1, c0,
                                                                              c1, k0, kb);
-  pss_prof_end(tok, st, 8.0 * (r1 - r0) * (double)(c1 - c0) * kb);
+  pss_prof_end(tok, st, PSS_PROF_SIMT_UPDATE, 8.0 * (r1 - r0) * (double)(c1 - c0) * kb);
+}
+
+// Tensor-core workspace of an FP32 factorisation (split operand planes) and its error word.
+struct TcWs {
+  void *ws = nullptr;
+  size_t bytes = 0;
+  int *err = nullptr;
+};
+
+void launch_gemm(Mat<false> M, int r0, int r1, int c0, int c1, int k0, int kb, const TcWs &, cudaStream_t st,
+                 int *rc) {
+  *rc = 0;
+  launch_gemm(M, r0, r1, c0, c1, k0, kb, st);
+}
+// FP32: updates of at least kTcMinRows x kTcMinCols go to the tcgen05 kernel, smaller ones SIMT.
+void launch_gemm(Mat<true> M, int r0, int r1, int c0, int c1, int k0, int kb, const TcWs &tc, cudaStream_t st,
+                 int *rc) {
+  *rc = 0;
+  if (r1 - r0 >= kTcMinRows && c1 - c0 >= kTcMinCols && tc.ws) {
+    *rc = pss_cgemm_tc((float *)M.a, M.ai, M.ld, r0, r1 - r0, c0, c1 - c0, k0, kb, tc.ws, tc.bytes, tc.err, st);
+    return;
+  }
+  launch_gemm(M, r0, r1, c0, c1, k0, kb, st);
 }
 
 // Outer blocks of NB columns, inner panels of W columns (LAPACK dgetrf order):
@@ -440,44 +498,34 @@ void launch_gemm(Mat<true> M, int r0, int r1, int c0, int c1, int k0, int kb, cu
 //   2. once all interchanges of the outer block are applied, the block row of the
 //      trailing columns, U12 = L11^{-1} A12, as W-row solves plus block-row updates;
 //   3. the trailing matrix A22 -= L21 U12, one GEMM with K = NB.
-// Trailing update A22 -= L21 U12 of an outer block: tensor cores (3xTF32) for the FP32
-// factorisation once the update is at least one 128 x 128 tile, SIMT otherwise.
-int launch_trailing(Mat<false> M, int E, int n, int K0, int JB, void *, size_t, int *, cudaStream_t st) {
-  launch_gemm(M, E, n, E, n, K0, JB, st);
-  return 0;
-}
-int launch_trailing(Mat<true> M, int E, int n, int K0, int JB, void *tcws, size_t tcws_bytes, int *info,
-                    cudaStream_t st) {
-  if (n - E < kTcMin) {
-    launch_gemm(M, E, n, E, n, K0, JB, st);
-    return 0;
-  }
-  return pss_cgemm_tc((float *)M.a, M.ai, M.ld, E, n - E, E, n - E, K0, JB, tcws, tcws_bytes, info, st);
-}
-
 template <bool F32>
 int lu_blocked(int n, Mat<F32> M, int *ipiv, int *info, int NB, int W, int *pscratch, void *tcws,
                size_t tcws_bytes, cudaStream_t st) {
+  const TcWs tc{tcws, tcws_bytes, info};  // a pipeline timeout writes -1 to info
+  int rc = 0;
   for (int K0 = 0; K0 < n; K0 += NB) {
     const int JB = min(NB, n - K0);
     const int E = K0 + JB;
     for (int k0 = K0; k0 < E; k0 += W) {
       const int w = min(W, E - k0);
-      int rc = launch_panel<F32>(M, k0, n - k0, k0, w, ipiv, info, pscratch, st);
-      if (rc) return rc;
+      if ((rc = launch_panel<F32>(M, k0, n - k0, k0, w, ipiv, info, pscratch, st))) return rc;
       launch_laswp<F32>(M, pscratch, n, k0, w, st);
       if (k0 + w < E) {
         launch_trsm<F32>(M, k0, w, k0 + w, E, st);
-        launch_gemm(M, k0 + w, n, k0 + w, E, k0, w, st);
+        launch_gemm(M, k0 + w, n, k0 + w, E, k0, w, tc, st, &rc);
+        if (rc) return rc;
       }
     }
     if (E < n) {
       for (int k0 = K0; k0 < E; k0 += W) {
         const int w = min(W, E - k0);
         launch_trsm<F32>(M, k0, w, E, n, st);
-        if (k0 + w < E) launch_gemm(M, k0 + w, E, E, n, k0, w, st);
+        if (k0 + w < E) {
+          launch_gemm(M, k0 + w, E, E, n, k0, w, tc, st, &rc);
+          if (rc) return rc;
+        }
       }
-      int rc = launch_trailing(M, E, n, K0, JB, tcws, tcws_bytes, info, st);
+      launch_gemm(M, E, n, E, n, K0, JB, tc, st, &rc);
       if (rc) return rc;
     }
   }

@@ -24,7 +24,6 @@ constexpr int kNX = kMaxRefRhs;           // norms layout: [max|r_j|] [max|x_j|]
 constexpr int kNA = 2 * kMaxRefRhs;
 constexpr int kNormCount = 2 * kMaxRefRhs + 1;
 constexpr long long kSpinCap = 1LL << 24;
-constexpr int kTrsvSmem = BS * BS * (int)sizeof(cd);  // Dinv_b staged by each chained-solve CTA
 
 struct Fac {  // row-major factor access: FP64 interleaved or FP32 planes
   const cd *a64;
@@ -107,74 +106,100 @@ __global__ void __launch_bounds__(1024) k_ipiv_to_perm(int n, const int *ipiv, i
   for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = sp[i];
 }
 
-// One chained substitution pass over right-hand sides j0 .. j0+nj-1 (nj <= kMaxRhs):
+// Arithmetic of a chained pass: FP64 for FP64 factors; FP32 for FP32 factors, as LAPACK
+// zcgesv solves its corrections in single precision (cgetrs) before the FP64 update.
+template <bool F32>
+struct SolveT;
+template <>
+struct SolveT<false> {
+  using C = cd;
+  __device__ static C fac(const Fac &F, long long r, long long c) { return F.a64[r * F.ld + c]; }
+  __device__ static C from(cd v) { return v; }
+  __device__ static cd to(C v) { return v; }
+};
+template <>
+struct SolveT<true> {
+  using C = cf;
+  __device__ static C fac(const Fac &F, long long r, long long c) { return cf{F.ar[r * F.ld + c], F.ai[r * F.ld + c]}; }
+  __device__ static C from(cd v) { return cf{(float)v.x, (float)v.y}; }
+  __device__ static cd to(C v) { return mkcd(v.x, v.y); }
+};
+__device__ __forceinline__ cf operator+(cf a, cf b) { return cf{a.x + b.x, a.y + b.y}; }
+__device__ __forceinline__ cf operator-(cf a, cf b) { return cf{a.x - b.x, a.y - b.y}; }
+__device__ __forceinline__ cf operator*(cf a, cf b) { return cf{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x}; }
+template <class C>
+__device__ __forceinline__ C czero() { return C{0, 0}; }
+
+// One chained substitution pass over right-hand sides j0 .. j0+nj-1 (nj <= NJ):
 //   lower: X[rows_b] = Linv_b (B[perm[rows_b]] - sum_{c<b} L[b,c] X[c])
 //   upper: X[rows_b] = Uinv_b (X[rows_b] - sum_{c>b} U[b,c] X[c])   (in place)
 // One CTA per 64-row block b (ticket order), 256 threads: row i = tid/4 of the block,
 // quarter p = tid%4 covers 16 columns of each 64-column tile.  Each tile of the factor is
 // loaded into registers BEFORE the wait for the CTA that produces x_c, so the wait hides
-// the load; Dinv_b (64 KB, dynamic shared memory) and the block's right-hand side are
-// staged at the start.  Blocks of X written by other CTAs are read with L1-bypassing loads.
-template <bool LOWER>
+// the load; Dinv_b (dynamic shared memory) and the block's right-hand side are staged at
+// the start.  Blocks of X written by other CTAs are read with L1-bypassing loads.
+template <bool LOWER, bool F32, int NJ>
 __global__ void __launch_bounds__(256) k_trsv(Fac F, int n, const int *__restrict__ perm, const cd *__restrict__ B,
                                               cd *__restrict__ X, int nrhs, int j0, const cd *__restrict__ Dinv,
                                               int *ticket, int *flags, int epoch, int *err,
                                               const int *__restrict__ done) {
+  using T = SolveT<F32>;
+  using C = typename T::C;
   if (done && *done) return;
   extern __shared__ __align__(16) unsigned char smraw[];
-  cd *Ds = (cd *)smraw;  // BS x BS, row-major
-  __shared__ cd y[BS][kMaxRhs];
-  __shared__ cd xs[BS][kMaxRhs];
+  C *Ds = (C *)smraw;  // BS x BS, row-major
+  __shared__ C y[BS][NJ];
+  __shared__ C xs[BS][NJ];
   __shared__ int s_b;
   const int tid = threadIdx.x;
   const int i = tid >> 2, p = tid & 3;
   const int nblk = (n + BS - 1) / BS;
-  const int nj = min(kMaxRhs, nrhs - j0);
+  const int nj = min(NJ, nrhs - j0);
   if (tid == 0) s_b = atomicAdd(ticket, 1);
   __syncthreads();
   const int tk = s_b;
   const int b = LOWER ? tk : nblk - 1 - tk;
   const int r0 = b * BS, nr = min(BS, n - r0);
   const cd *D = Dinv + (size_t)(2 * b + (LOWER ? 0 : 1)) * BS * BS;
-  for (int e = tid; e < BS * BS; e += 256) Ds[e] = D[e];
-  for (int e = tid; e < BS * kMaxRhs; e += 256) {
-    const int r = e / kMaxRhs, j = e % kMaxRhs;
+  for (int e = tid; e < BS * BS; e += 256) Ds[e] = T::from(D[e]);
+  for (int e = tid; e < BS * NJ; e += 256) {
+    const int r = e / NJ, j = e % NJ;
     cd v = mkcd(0, 0);
     if (r < nr && j < nj)
       v = LOWER ? B[(size_t)(j0 + j) * n + perm[r0 + r]] : ldcg(&X[(size_t)(j0 + j) * n + r0 + r]);
-    y[r][j] = v;
+    y[r][j] = T::from(v);
   }
-  cd acc[kMaxRhs];
+  C acc[NJ];
 #pragma unroll
-  for (int j = 0; j < kMaxRhs; ++j) acc[j] = mkcd(0, 0);
+  for (int j = 0; j < NJ; ++j) acc[j] = czero<C>();
   const int c_lo = LOWER ? 0 : b + 1, c_hi = LOWER ? b : nblk;
   for (int cc = c_lo; cc < c_hi; ++cc) {
     const int c = LOWER ? cc : c_hi - 1 - (cc - c_lo);  // upper: the last block is ready first
     const int t0 = c * BS, nt = min(BS, n - t0);
-    cd lv[16];
+    C lv[16];
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
       const int t = p * 16 + q;
-      lv[q] = (i < nr && t < nt) ? F.at(r0 + i, t0 + t) : mkcd(0, 0);
+      lv[q] = (i < nr && t < nt) ? T::fac(F, r0 + i, t0 + t) : czero<C>();
     }
     if (tid == 0) {
       wait_flag(flags, c, epoch, err);
       __threadfence();
     }
     __syncthreads();
-    for (int e = tid; e < BS * kMaxRhs; e += 256) {
-      const int t = e / kMaxRhs, j = e % kMaxRhs;
-      xs[t][j] = (t < nt && j < nj) ? ldcg(&X[(size_t)(j0 + j) * n + t0 + t]) : mkcd(0, 0);
+    for (int e = tid; e < BS * NJ; e += 256) {
+      const int t = e / NJ, j = e % NJ;
+      xs[t][j] = (t < nt && j < nj) ? T::from(ldcg(&X[(size_t)(j0 + j) * n + t0 + t])) : czero<C>();
     }
     __syncthreads();
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
 #pragma unroll
-      for (int j = 0; j < kMaxRhs; ++j) acc[j] = acc[j] + lv[q] * xs[p * 16 + q][j];
+      for (int j = 0; j < NJ; ++j) acc[j] = acc[j] + lv[q] * xs[p * 16 + q][j];
     }
   }
 #pragma unroll
-  for (int j = 0; j < kMaxRhs; ++j)
+  for (int j = 0; j < NJ; ++j)
     for (int o = 1; o < 4; o <<= 1) {
       acc[j].x += __shfl_xor_sync(0xffffffff, acc[j].x, o);
       acc[j].y += __shfl_xor_sync(0xffffffff, acc[j].y, o);
@@ -182,15 +207,24 @@ __global__ void __launch_bounds__(256) k_trsv(Fac F, int n, const int *__restric
   __syncthreads();
   if (p == 0 && i < nr) {
 #pragma unroll
-    for (int j = 0; j < kMaxRhs; ++j) y[i][j] = y[i][j] - acc[j];
+    for (int j = 0; j < NJ; ++j) y[i][j] = y[i][j] - acc[j];
   }
   __syncthreads();
-  // X[rows] = Dinv_b * y
-  for (int e = tid; e < nr * nj; e += blockDim.x) {
+  // X[rows] = Dinv_b * y: 4 threads per output, 16 terms each, combined by shuffles
+  for (int e0 = 0; e0 < nr * nj; e0 += 64) {
+    const int e = e0 + (tid >> 2), part = tid & 3;
     const int r = e / nj, j = e % nj;
-    cd s = mkcd(0, 0);
-    for (int k = 0; k < nr; ++k) s = s + Ds[r * BS + k] * y[k][j];
-    stcg(&X[(size_t)(j0 + j) * n + r0 + r], s);
+    C s = czero<C>();
+    if (e < nr * nj) {
+#pragma unroll 4
+      for (int k = part * 16; k < part * 16 + 16; ++k)
+        if (k < nr) s = s + Ds[r * BS + k] * y[k][j];
+    }
+    for (int o = 1; o < 4; o <<= 1) {
+      s.x += __shfl_xor_sync(0xffffffff, s.x, o);
+      s.y += __shfl_xor_sync(0xffffffff, s.y, o);
+    }
+    if (part == 0 && e < nr * nj) stcg(&X[(size_t)(j0 + j) * n + r0 + r], T::to(s));
   }
   __syncthreads();
   if (tid == 0) {
@@ -269,6 +303,15 @@ __global__ void k_axpy(long long total, cd *X, const cd *D, const int *done) {
   if (i < total) X[i] = X[i] + D[i];
 }
 
+template <bool LOWER>
+cudaError_t set_trsv_smem() {
+  const int s64 = BS * BS * (int)sizeof(cd);
+  cudaError_t e = cudaFuncSetAttribute(k_trsv<LOWER, false, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, s64);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_trsv<LOWER, false, kMaxRhs>, cudaFuncAttributeMaxDynamicSharedMemorySize, s64);
+  return e;  // the FP32 forms stage 32 KB, under the default limit
+}
+
 }  // namespace
 
 // ------------------------------- host side -------------------------------
@@ -321,22 +364,30 @@ int pss_solve_lu(SolveWS &ws, const cd *LU64, const float *Lr, const float *Li, 
   int *ticket = ws.ctrl, *err = ws.ctrl + 1, *flags = ws.ctrl + 8;
   static DeviceOnce once;
   if (int rc = device_once(once, [] {
-        PSS_CUDA_TRY(cudaFuncSetAttribute(k_trsv<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrsvSmem));
-        PSS_CUDA_TRY(cudaFuncSetAttribute(k_trsv<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrsvSmem));
+        PSS_CUDA_TRY(set_trsv_smem<true>());
+        PSS_CUDA_TRY(set_trsv_smem<false>());
         return 0;
       }))
     return rc;
+  const bool f32 = LU64 == nullptr;
   for (int pass = 0; pass < 2; ++pass)
     for (int j0 = 0; j0 < nrhs; j0 += kMaxRhs) {
       ++ws.epoch;
       PSS_CUDA_TRY(cudaMemsetAsync(ticket, 0, sizeof(int), st));
       pss_count_launch();
-      if (pass == 0)
-        k_trsv<true><<<ws.nblk, 256, kTrsvSmem, st>>>(F, ws.n, ws.perm, B, X, nrhs, j0, ws.Dinv, ticket, flags,
-                                                      ws.epoch, err, done);
-      else
-        k_trsv<false><<<ws.nblk, 256, kTrsvSmem, st>>>(F, ws.n, ws.perm, B, X, nrhs, j0, ws.Dinv, ticket, flags,
-                                                       ws.epoch, err, done);
+      const bool small = nrhs - j0 <= 4;
+      auto go = [&](auto kern, size_t smem) {
+        kern<<<ws.nblk, 256, smem, st>>>(F, ws.n, ws.perm, B, X, nrhs, j0, ws.Dinv, ticket, flags, ws.epoch, err,
+                                         done);
+      };
+      const size_t s64 = BS * BS * sizeof(cd), s32 = BS * BS * sizeof(cf);
+      if (pass == 0) {
+        if (f32) small ? go(k_trsv<true, true, 4>, s32) : go(k_trsv<true, true, kMaxRhs>, s32);
+        else small ? go(k_trsv<true, false, 4>, s64) : go(k_trsv<true, false, kMaxRhs>, s64);
+      } else {
+        if (f32) small ? go(k_trsv<false, true, 4>, s32) : go(k_trsv<false, true, kMaxRhs>, s32);
+        else small ? go(k_trsv<false, false, 4>, s64) : go(k_trsv<false, false, kMaxRhs>, s64);
+      }
     }
   PSS_CUDA_TRY(cudaGetLastError());
   return 0;

@@ -59,10 +59,16 @@ def set_profiling(on, device=0, nworkers=None):
     _check(lib().pss_profile(context(device, nworkers), int(on)), "pss_profile")
 
 
+PROFILE_KINDS = ("tc_update", "panel", "simt_update")  # PSS_PROF_* order
+
+
 def profile_result(device=0, nworkers=None):
-    out = np.zeros(3)
+    """Per kernel kind: launches, summed device ms and algorithmic work (flops, or bytes for
+    the panel) of the last ``partial_gsms`` call made while profiling was enabled."""
+    out = np.zeros(3 * len(PROFILE_KINDS))
     _check(lib().pss_profile_result(context(device, nworkers), _p(out)), "pss_profile_result")
-    return {"launches": int(out[0]), "ms": float(out[1]), "flops": float(out[2])}
+    return {k: {"launches": int(out[3 * i]), "ms": float(out[3 * i + 1]), "work": float(out[3 * i + 2])}
+            for i, k in enumerate(PROFILE_KINDS)}
 
 
 def lib():
@@ -108,7 +114,10 @@ def _i64(x):
 def context(device=0, nworkers=None):
     """Per-device ``pss_ctx`` (created once)."""
     if nworkers is None:
-        nworkers = int(os.environ.get("PSS_WORKERS", "8"))
+        # one stream per worker; more streams than the process's hardware work queues
+        # (CUDA_DEVICE_MAX_CONNECTIONS, default 8) would share queues
+        queues = int(os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS", "8"))
+        nworkers = int(os.environ.get("PSS_WORKERS", str(max(1, min(16, queues)))))
     key = (device, nworkers)
     with _lock:
         c = _ctx.get(key)
