@@ -6,7 +6,9 @@ and the modal projection of ``PSSFSS.jl:362-587``.  Only tests, ``__graft_entry_
 and the CPU-baseline leg of ``bench.py`` import this package; the product never does.
 
 Parity is pinned against the golden values hard-coded in the reference's own tests
-(test/FillZY_test.jl, test/PGF_test.jl, test/RWGData_test.jl, test/full_test.jl).
+(test/FillZY_test.jl:45-46,77-78, test/PGF_test.jl:40-44,56-60, test/RWGData_test.jl:46-48,56-58,
+collected in tests/golden/reference_golden.json) and the analytic grating of
+test/full_test.jl:65-91.
 """
 import ctypes
 import math

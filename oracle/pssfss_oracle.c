@@ -13,7 +13,8 @@
  * zgetrf/zgetrs in the Python wrapper.
  *
  * Parity pins: reference test golden values in test/FillZY_test.jl:45-46,77-78,
- * test/PGF_test.jl:126-146, test/RWGData_test.jl:46-58 (see tests/).
+ * test/PGF_test.jl:40-44,56-60 (checked as in :71-83), test/RWGData_test.jl:46-48,56-58
+ * (tests/golden/reference_golden.json).
  */
 #include <complex.h>
 #include <math.h>

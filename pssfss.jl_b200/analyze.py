@@ -119,8 +119,11 @@ def get_gbldup(gbls, layers, sheets, junc):
     return gd
 
 
-def make_plan(strata, flist, steering):
-    """Everything of ``_analyze`` (PSSFSS.jl:199-255) before the per-Gblock GSMs."""
+def make_plan(strata, flist, steering, plan_flist=None):
+    """Everything of ``_analyze`` (PSSFSS.jl:199-255) before the per-Gblock GSMs.
+
+    ``plan_flist`` (default ``flist``): the frequencies whose extremes choose the Gblocks
+    and layer modes (PSSFSS.jl:215-221) - the whole sweep when ``flist`` is one shard."""
     layers = [copy.deepcopy(s) for s in strata if isinstance(s, Layer)]
     sheets = [s for s in strata if isinstance(s, RWGSheet)]
     nl = len(layers)
@@ -137,8 +140,9 @@ def make_plan(strata, flist, steering):
     stkeys = tuple(steering.keys())
     stvalues = [[float(v) for v in np.atleast_1d(np.asarray(steering[k], float))] for k in stkeys]
     check_inputs(layers)
-    k0min = TWOPI * 1e9 / C0 * min(freqs)
-    k0max = TWOPI * 1e9 / C0 * max(freqs)
+    pfreqs = freqs if plan_flist is None else [float(f) for f in np.atleast_1d(np.asarray(plan_flist, float))]
+    k0min = TWOPI * 1e9 / C0 * min(pfreqs)
+    k0max = TWOPI * 1e9 / C0 * max(pfreqs)
     gbls = choose_gblocks(layers, sheets, junc, k0min)
     choose_layer_modes(layers, sheets, junc, gbls, k0max, DBMIN)
     gbldup = get_gbldup(gbls, layers, sheets, junc)
@@ -309,7 +313,7 @@ def assemble(plan, partial):
 
 
 def analyze(strata, flist, steering, *, precision="fp64", device=0, outlist=(),
-            logfile=None, resultfile=None, showprogress=False, stats=None):
+            logfile=None, resultfile=None, showprogress=False, stats=None, plan_flist=None):
     """Analyze a layered FSS/PSS over frequencies and steering (PSSFSS.jl:114).
 
     ``strata``: list of ``Layer`` and ``RWGSheet`` (first and last must be layers).
@@ -319,7 +323,7 @@ def analyze(strata, flist, steering, *, precision="fp64", device=0, outlist=(),
     Returns a list of ``Result``.
     """
     from . import engine
-    plan = make_plan(strata, flist, steering)
+    plan = make_plan(strata, flist, steering, plan_flist)
     partial = {}
     for ig, (i1, i2), isht, s in sheet_gblocks(plan):
         sheet = plan.sheets[isht - 1]

@@ -1,4 +1,5 @@
 import importlib.util
+import json
 import os
 import sys
 
@@ -31,3 +32,17 @@ def pytest_configure(config):
 @pytest.fixture(scope="session")
 def pkg():
     return _load_package()
+
+
+_GOLDEN = None
+
+
+def golden(key):
+    """Golden values from the reference's own tests (tests/golden/reference_golden.json,
+    made by tests/golden/extract_reference_golden.py): complex values and their record."""
+    global _GOLDEN
+    if _GOLDEN is None:
+        with open(os.path.join(ROOT, "tests", "golden", "reference_golden.json")) as f:
+            _GOLDEN = json.load(f)
+    g = _GOLDEN[key]
+    return [complex(re_, im) for re_, im in g["values"]], g

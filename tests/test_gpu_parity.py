@@ -13,6 +13,7 @@ import numpy as np
 import pytest
 
 import oracle
+from conftest import golden
 from pssfss_b200 import engine
 from pssfss_b200.analyze import make_plan, sheet_gblocks, sheet_io
 from pssfss_b200.elements import meander, rectstrip
@@ -75,11 +76,8 @@ def test_fill_matches_oracle_and_golden(cls):
     Zg, mmax = engine.fill_matrix(sheet, rwg, layers, 2, u, k0, 0.0, 0.0)
     assert mmax == info["mmax"]
     assert relerr(Zg, Zr) < 1e-10
-    gold = {"J": [((20, 30), 0.8990238712012797 - 354.1682770720877j),
-                  ((100, 100), 110.95156005861463 - 37529.820828933574j)],
-            "M": [((20, 30), 1.2168396602563192e-6 - 0.02476973884018213j),
-                  ((100, 100), 2.2127855040521283e-6 - 3.5131557304457406j)]}[cls]
-    for (i, j), v in gold:     # test/FillZY_test.jl:45-46, 77-78
+    vals, g = golden("fillz" if cls == "J" else "filly")  # test/FillZY_test.jl:45-46, 77-78
+    for (i, j), v in zip(g["index_1based"], vals):
         assert abs(Zg[i - 1, j - 1] - v) / abs(v) < 1e-10
 
 
@@ -98,14 +96,12 @@ def test_fill_oblique_periodic_strip_with_loss():
 
 
 def test_basis_transforms_golden():
-    # test/RWGData_test.jl:39-58
+    # test/RWGData_test.jl:56-58
     sheet = rectstrip(Lx=1, Ly=1, Px=1, Py=1, Nx=2, Ny=1, units=inch, fufp=False)
     rwg = setup_rwg(sheet)
     F = engine.basis_transforms(sheet, rwg, [[20.0, -30.3], [0.0, 0.0]], 0.8, -0.7)
-    gold = [[0.003986416685586114 - 0.0010511300702857503j, -0.008079847138694855 + 0.0021304773084817956j],
-            [0.008263557134402535 - 0.0010871639073400372j, 0.008284527320353664 - 0.0010899227712197804j],
-            [0.004122638196063312 - 1.5707327530113332e-5j, -0.008355946971820058 + 3.1836312009155855e-5j]]
-    assert np.allclose(F[0, :3], gold, rtol=1e-12, atol=0)
+    vals, _ = golden("rwgbfft_inch")
+    assert np.allclose(F[0, :3], np.reshape(vals, (3, 2)), rtol=1e-12, atol=0)
     assert relerr(F[1], oracle.rwgbfft(rwg, sheet, [0.0, 0.0], 0.8, -0.7)) < 1e-12
 
 

@@ -8,6 +8,7 @@ import math
 import numpy as np
 
 import oracle
+from conftest import golden
 from pssfss_b200.elements import meander, meander_counts, rectstrip
 from pssfss_b200.gsms import GSM, cascade, cascade_layer
 from pssfss_b200.layers import Layer
@@ -77,19 +78,15 @@ def test_rwgdata_fufp_true_false():
 
 
 def test_rwgbfft_golden():
-    # test/RWGData_test.jl:39-58
+    # test/RWGData_test.jl:46-48 and 56-58
     sh = rectstrip(Lx=1, Ly=1, Px=1, Py=1, Nx=2, Ny=1, units=mm, fufp=False)
     ft = oracle.rwgbfft(setup_rwg(sh), sh, [0., 0.], 0.0, 0.0)
-    gold = [[0.0001666666666666667, -0.0003333333333333334],
-            [0.0003333333333333334, 0.0003333333333333334],
-            [0.00016666666666666663, -0.0003333333333333334]]
-    assert np.allclose(ft[:3], gold, rtol=1e-12, atol=0)
+    vals, _ = golden("rwgbfft_mm")
+    assert np.allclose(ft[:3], np.reshape(vals, (3, 2)), rtol=1e-12, atol=0)
     sh = rectstrip(Lx=1, Ly=1, Px=1, Py=1, Nx=2, Ny=1, units=inch, fufp=False)
     ft = oracle.rwgbfft(setup_rwg(sh), sh, [20.0, -30.3], 0.8, -0.7)
-    gold = [[0.003986416685586114 - 0.0010511300702857503j, -0.008079847138694855 + 0.0021304773084817956j],
-            [0.008263557134402535 - 0.0010871639073400372j, 0.008284527320353664 - 0.0010899227712197804j],
-            [0.004122638196063312 - 1.5707327530113332e-5j, -0.008355946971820058 + 3.1836312009155855e-5j]]
-    assert np.allclose(ft[:3], gold, rtol=1e-12, atol=0)
+    vals, _ = golden("rwgbfft_inch")
+    assert np.allclose(ft[:3], np.reshape(vals, (3, 2)), rtol=1e-12, atol=0)
 
 
 def test_meander_counts_and_topology():

@@ -1,0 +1,102 @@
+"""Sharded sweeps across ranks (the multi-GPU path's host logic), on CPU with gloo.
+
+Each rank analyzes a contiguous block of the frequency list; the gathered result list
+must equal a single-process run in order and content, including points that ``analyze``
+skips (principal modes cut off), and every rank must plan with the whole band.  The
+per-point solver is replaced by a host function so no GPU is needed; under these ranks the
+GPU path is the same ``analyze`` that the parity tests cover.
+"""
+import os
+import socket
+import types
+
+import pytest
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+import conftest  # noqa: F401  (loads the package as pssfss_b200, also in spawned ranks)
+from pssfss_b200.sweep import merge_tagged, shard_range, steering_combos, tag_results
+
+
+def test_shard_range_covers_and_balances():
+    for n in (0, 1, 5, 101):
+        for world in (1, 2, 3, 8):
+            blocks = [shard_range(n, k, world) for k in range(world)]
+            assert blocks[0][0] == 0 and blocks[-1][1] == n
+            assert all(a[1] == b[0] for a, b in zip(blocks, blocks[1:]))
+            sizes = [hi - lo for lo, hi in blocks]
+            assert max(sizes) - min(sizes) <= 1
+    with pytest.raises(ValueError):
+        shard_range(4, 2, 2)
+
+
+def fake_analyze(strata, flist, steering, precision="fp64", device=0, plan_flist=None):
+    """Stand-in for analyze: one result per (steering, frequency); frequencies above 17 GHz
+    are skipped at the second steering point (a cut-off principal mode); echoes the band."""
+    out = []
+    band = (min(plan_flist or flist), max(plan_flist or flist))
+    for i, st in enumerate(steering_combos(steering)):
+        for f in flist:
+            if i == 1 and f > 17.0:
+                continue
+            out.append(types.SimpleNamespace(steering=st, FGHz=f, value=(i, f), band=band))
+    return out
+
+
+def _worker(rank, world, port, flist, steering, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), LOCAL_RANK=str(rank))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from pssfss_b200.sweep import analyze_sharded
+        res = analyze_sharded(None, flist, steering, analyze_fn=fake_analyze)
+        q.put((rank, [(r.value, r.band) for r in res]))
+    finally:
+        dist.destroy_process_group()
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def test_analyze_sharded_gloo_matches_single_process():
+    world = 2
+    flist = [10.0 + 0.5 * k for k in range(17)]
+    steering = {"θ": [0.0, 30.0], "ϕ": 45.0}
+    single = [(r.value, r.band) for r in fake_analyze(None, flist, steering, plan_flist=flist)]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(k, world, port, flist, steering, q)) for k in range(world)]
+    for p in procs:
+        p.start()
+    got = {}
+    try:
+        for _ in range(240):  # poll: a rank that died ends the wait at once
+            while not q.empty() and len(got) < world:
+                k, v = q.get()
+                got[k] = v
+            if len(got) == world or any(p.exitcode not in (None, 0) for p in procs):
+                break
+            procs[0].join(timeout=0.5)
+    finally:
+        for p in procs:
+            p.join(timeout=60)
+            if p.is_alive():
+                p.kill()
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    for k in range(world):
+        assert got[k] == single
+
+
+def test_merge_tagged_orders_by_steering_then_frequency():
+    flist = [1.0, 2.0, 3.0, 4.0]
+    steering = {"θ": [0.0, 10.0], "ϕ": 0.0}
+    combos = steering_combos(steering)
+    mk = lambda s, f: types.SimpleNamespace(steering=combos[s], FGHz=f)
+    part0 = tag_results([mk(0, 1.0), mk(0, 2.0), mk(1, 1.0)], combos, flist, 0, 2)
+    part1 = tag_results([mk(0, 3.0), mk(1, 3.0), mk(1, 4.0)], combos, flist, 2, 4)
+    merged = merge_tagged([part1, part0])
+    assert [(combos.index(r.steering), r.FGHz) for r in merged] == [(0, 1.0), (0, 2.0), (0, 3.0), (1, 1.0),
+                                                                    (1, 3.0), (1, 4.0)]

@@ -13,6 +13,7 @@ import numpy as np
 import pytest
 
 import oracle
+from conftest import golden
 from pssfss_b200.elements import rectstrip
 from pssfss_b200.layers import Layer
 from pssfss_b200.rwg import setup_rwg
@@ -38,25 +39,24 @@ def test_fillz_golden():
     # test/FillZY_test.jl:45-46 (reference tolerances 0.005 and 0.01 absolute)
     Z, info = _fillzy_case("J")
     assert info["converged"]
-    for (i, j), ref in (((20, 30), 0.8990238712012797 - 354.1682770720877j),
-                        ((100, 100), 110.95156005861463 - 37529.820828933574j)):
+    vals, g = golden("fillz")
+    for (i, j), ref in zip(g["index_1based"], vals):
         assert abs(Z[i - 1, j - 1] - ref) / abs(ref) < 1e-10
 
 
 def test_filly_golden():
     # test/FillZY_test.jl:77-78 (reference tolerance 1e-4 absolute)
     Y, info = _fillzy_case("M")
-    for (i, j), ref in (((20, 30), 1.2168396602563192e-6 - 0.02476973884018213j),
-                        ((100, 100), 2.2127855040521283e-6 - 3.5131557304457406j)):
+    vals, g = golden("filly")
+    for (i, j), ref in zip(g["index_1based"], vals):
         assert abs(Y[i - 1, j - 1] - ref) / abs(ref) < 1e-10
 
 
-PGF_GOLD = {  # test/PGF_test.jl:126-129, 142-146
-    0.1: ((-232.15311689927114 - 10.286495939161526j, -11.778556545589899 - 160.87504453495308j),
-          (-5905.287097073966 - 116.24899221632135j, -65.290894751642 - 115.6027231717079j)),
-    0.9: ((-86.47040978143367 - 9.887172408455307j, 133.51945406766538 - 160.47675058617088j),
-          (-2516.511258383936 - 111.36619289656556j, 138.66489521333057 - 115.0436702287188j)),
-}
+def _pgf_gold(ufact, magnetic):
+    # test/PGF_test.jl:40-44 (electric) and 56-60 (magnetic): [Σ1, Σ2] for u = ufact * max|β|
+    vals, g = golden("modal_series_magnetic" if magnetic else "modal_series_electric")
+    k = g["ufact"].index(ufact)
+    return vals[2 * k], vals[2 * k + 1]
 
 
 def _pgf_setup():
@@ -77,12 +77,12 @@ def _pgf_setup():
 
 @pytest.mark.parametrize("ufact", [0.1, 0.9])
 def test_modal_series_golden(ufact):
-    # test/PGF_test.jl:157-171, relative tolerance 2e-4
+    # test/PGF_test.jl:71-83 (modal series against the precomputed sums), relative tolerance 2e-4
     k0, layers, psi1, psi2, s1, s2, b1, b2, b00, rho = _pgf_setup()
     u = ufact * max(np.linalg.norm(b1), np.linalg.norm(b2))
     for mag in (0, 1):
         tb = oracle.modal_tables(mag, k0, u, psi1, psi2, layers, 2, b1, b2, b00)
-        g1, g2 = PGF_GOLD[ufact][mag]
+        g1, g2 = _pgf_gold(ufact, mag)
         assert abs(tb.sigma(1, rho) - g1) / abs(g1) < 2e-4
         assert abs(tb.sigma(2, rho) - g2) / abs(g2) < 2e-4
 
