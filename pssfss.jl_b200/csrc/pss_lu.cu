@@ -67,6 +67,7 @@ constexpr int kMaxMov = 2 * kMaxW;  // rows one panel's interchanges can move
 constexpr int kSwpThreads = 64;
 constexpr int kListInts = 1 + 2 * kMaxMov;  // interchange list: count, destinations, sources
 constexpr int kTcMinRows = 64, kTcMinCols = 32;  // smallest FP32 update sent to the tensor cores
+static_assert(kPanelThreads / 32 <= 32 && kMaxCluster <= 32, "panel reductions run over one warp's lanes");
 
 // Pivot candidate of one column: LAPACK's izamax order (largest |re|+|im|, then the lowest
 // row).  FP32: value and row packed in one 64-bit key (non-negative float bits are
@@ -143,9 +144,10 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(Mat<F32> M, int row0, i
       }
       if (lane == 0) redk[warp] = key;
       __syncthreads();
-      K cb = lane < NW ? redk[lane] : K::none();  // every warp reduces the NW warp winners
+      // every warp reduces the NW warp winners over all 32 lanes, so every lane agrees
+      K cb = lane < NW ? redk[lane] : K::none();
 #pragma unroll
-      for (int o = NW / 2; o > 0; o >>= 1) {
+      for (int o = 16; o > 0; o >>= 1) {
         const K ok = cb.shfl_xor(o);
         if (cb.worse_than(ok)) cb = ok;
       }
@@ -163,9 +165,9 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(Mat<F32> M, int row0, i
         if (lane < cs) cluster.map_shared_rank(&skey[0][0], lane)[par * kMaxCluster + crank] = cb;
       }
       cluster.sync();
-      K gk = lane < cs ? skey[par][lane] : K::none();
+      K gk = lane < cs ? skey[par][lane] : K::none();  // all 32 lanes: uniform result
 #pragma unroll
-      for (int o = kMaxCluster / 2; o > 0; o >>= 1) {
+      for (int o = 16; o > 0; o >>= 1) {
         const K ok = gk.shfl_xor(o);
         if (gk.worse_than(ok)) gk = ok;
       }

@@ -220,3 +220,42 @@ def test_status_flags_singular_matrix():
     Z[np.arange(7), np.arange(7)] = 1.0
     X, st = engine.lu_solve(Z, np.ones((8, 1)), "fp64")
     assert st & 4
+
+
+def _gsm_relerr(res, ref):
+    worst = 0.0
+    assert len(res) == len(ref)
+    for a, b in zip(res, ref):
+        assert a.FGHz == b.FGHz
+        for k in ((1, 1), (1, 2), (2, 1), (2, 2)):
+            worst = max(worst, float(np.max(np.abs(a.gsm[k] - b.gsm[k]))))
+    return worst
+
+
+def test_config1_square_patch_sweep():
+    """Plain FP64 config: 8 mm square patch in a 10 mm cell (structured, 512 triangles,
+    N = 736) in free space, normal incidence, 11 frequencies 10-20 GHz; the FP32 form is held
+    to |dS| <= 1e-6 of the FP64 oracle on the same sweep."""
+    from pssfss_b200 import analyze
+    sh = rectstrip(Lx=8, Ly=8, Px=10, Py=10, Nx=16, Ny=16, units=mm)
+    strata = [Layer(), sh, Layer()]
+    freqs = np.linspace(10, 20, 11)
+    ref = oracle.analyze(strata, freqs, {"θ": 0, "ϕ": 0})
+    assert _gsm_relerr(analyze(strata, freqs, {"θ": 0, "ϕ": 0}), ref) < 1e-9
+    assert _gsm_relerr(analyze(strata, freqs, {"θ": 0, "ϕ": 0}, precision="fp32r"), ref) <= 1e-6
+
+
+def test_two_sheet_cascade_oblique_scan():
+    """Two sheets cascaded through GSMs with a lossy substrate and an air gap: a conductor
+    strip sheet and an aperture (M-type) sheet, scan θ=30°, ϕ=45° (ψ changes with frequency,
+    so the face-pair integrals are recomputed per point), 3 frequencies 5-25 GHz."""
+    from pssfss_b200 import analyze
+    j = rectstrip(Lx=6, Ly=0.5, Px=8, Py=8, Nx=12, Ny=2, units=mm)
+    m = rectstrip(Lx=6, Ly=6, Px=8, Py=8, Nx=8, Ny=8, units=mm, **{"class": "M"})
+    strata = [Layer(), j, Layer(epsr=3.0, tandel=0.002, width=Length(0.5, mm)), Layer(width=Length(2, mm)), m,
+              Layer()]
+    freqs = [5.0, 15.0, 25.0]
+    steer = {"θ": 30, "ϕ": 45}
+    ref = oracle.analyze(strata, freqs, steer)
+    assert _gsm_relerr(analyze(strata, freqs, steer), ref) < 1e-9
+    assert _gsm_relerr(analyze(strata, freqs, steer, precision="fp32r"), ref) <= 1e-6
