@@ -86,6 +86,7 @@ struct PivKey<true> {
   __device__ PivKey shfl_xor(int o) const { return {__shfl_xor_sync(0xffffffffu, k, o)}; }
   __device__ int row() const { return (int)(0xffffffffu - (unsigned)(k & 0xffffffffu)); }
   __device__ bool nonzero() const { return (k >> 32) != 0ull; }  // a candidate with |re|+|im| > 0
+  __device__ bool valid() const { return k != 0ull; }
 };
 template <>
 struct PivKey<false> {
@@ -101,11 +102,19 @@ struct PivKey<false> {
   }
   __device__ int row() const { return r; }
   __device__ bool nonzero() const { return v > 0.0; }
+  __device__ bool valid() const { return v >= 0.0; }
 };
 
 // Panel of W columns (w <= W used), rows row0..row0+nrows-1, factored by a cluster of
-// cs = gridDim.x CTAs; thread t of CTA q holds row q*512 + t in registers.  The column
-// loop is fully unrolled so every register index is a compile-time constant.
+// cs = gridDim.x CTAs; thread t of CTA q holds row q*512 + t in registers.
+// The column loop is a runtime loop over a SHIFTING register array: at column j, row[c]
+// holds column j + c of the thread's row, so every register index is a compile-time
+// constant while the loop body stays small (an unrolled body per column would not fit the
+// instruction cache, and each column's code runs once per launch).  Multipliers go to
+// shared memory (lbuf[j][thread]); a row chosen as pivot at column j freezes (row[c] then
+// holds its U entries of columns j + c).  Per column: one CTA barrier (per-warp winners),
+// the warp holding the CTA's candidate pushes key and row into every CTA's shared memory,
+// one cluster barrier, and every CTA picks the same winner.
 template <bool F32, int W>
 __global__ void __launch_bounds__(kPanelThreads) k_panel(Mat<F32> M, int row0, int nrows, int col0, int w,
                                                          int *ipiv, int *info, int *xlist) {
@@ -117,9 +126,10 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(Mat<F32> M, int row0, i
   const int crank = (int)cluster.block_rank();
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   constexpr int NW = kPanelThreads / 32;
+  extern __shared__ __align__(16) unsigned char panel_smem[];
+  E *lbuf = (E *)panel_smem;              // [W][kPanelThreads] multipliers (dynamic shared memory)
   __shared__ E srow[2][kMaxCluster][W];   // candidate rows pushed by every CTA (double-buffered)
   __shared__ K skey[2][kMaxCluster];      // their keys
-  __shared__ E own[W];                    // this CTA's candidate row, staged for the push
   __shared__ K redk[NW];                  // per-warp winners
   __shared__ int chosen[kMaxW];
   __shared__ int mpos[2 * kMaxW], morig[2 * kMaxW];  // moved positions and the row each now holds
@@ -127,57 +137,63 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(Mat<F32> M, int row0, i
   const int gr = crank * kPanelThreads + tid;  // panel-relative row of this thread
   const bool have = gr < nrows;
   bool active = have;
+  int jp = -1;  // column at which this row became a pivot row
   E row[W];
 #pragma unroll
   for (int c = 0; c < W; ++c) row[c] = (have && c < w) ? M.get(row0 + gr, col0 + c) : E{0, 0};
 
+  for (int j = 0; j < w; ++j) {
+    const int par = j & 1;
+    const E vj = row[0];
+    K key = K::make(vj.x, vj.y, gr, active);
 #pragma unroll
-  for (int j = 0; j < W; ++j) {
-    if (j < w) {  // uniform over the cluster
-      const int par = j & 1;
-      const E vj = row[j];
-      K key = K::make(vj.x, vj.y, gr, active);
+    for (int o = 16; o > 0; o >>= 1) {
+      const K ok = key.shfl_xor(o);
+      if (key.worse_than(ok)) key = ok;
+    }
+    if (lane == 0) redk[warp] = key;
+    __syncthreads();
+    // every warp reduces the NW warp winners over all 32 lanes, so every lane agrees
+    K cb = lane < NW ? redk[lane] : K::none();
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const K ok = key.shfl_xor(o);
-        if (key.worse_than(ok)) key = ok;
-      }
-      if (lane == 0) redk[warp] = key;
-      __syncthreads();
-      // every warp reduces the NW warp winners over all 32 lanes, so every lane agrees
-      K cb = lane < NW ? redk[lane] : K::none();
+    for (int o = 16; o > 0; o >>= 1) {
+      const K ok = cb.shfl_xor(o);
+      if (cb.worse_than(ok)) cb = ok;
+    }
+    // the warp holding this CTA's candidate (warp 0 if the CTA has none left) pushes it
+    const bool has = cb.valid();
+    const int wt = has ? cb.row() - crank * kPanelThreads : 0;  // CTA-local thread of the candidate
+    if (warp == (wt >> 5)) {
+      const int wl = wt & 31;
+      E mine{0, 0};  // lane c: the candidate's column j + c
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const K ok = cb.shfl_xor(o);
-        if (cb.worse_than(ok)) cb = ok;
+      for (int c = 0; c < W; ++c) {
+        const E v{__shfl_sync(0xffffffffu, row[c].x, wl), __shfl_sync(0xffffffffu, row[c].y, wl)};
+        if (lane == c) mine = v;
       }
-      if (active && gr == cb.row()) {
+      if (lane < W && j + lane < w)
+        for (int dst = 0; dst < cs; ++dst)
+          cluster.map_shared_rank(&srow[0][0][0], dst)[(par * kMaxCluster + crank) * W + j + lane] = mine;
+      if (lane < cs) cluster.map_shared_rank(&skey[0][0], lane)[par * kMaxCluster + crank] = cb;
+    }
+    cluster.sync();
+    K gk = lane < cs ? skey[par][lane] : K::none();  // all 32 lanes: uniform result
 #pragma unroll
-        for (int c = j; c < W; ++c) own[c] = row[c];
+    for (int o = 16; o > 0; o >>= 1) {
+      const K ok = gk.shfl_xor(o);
+      if (gk.worse_than(ok)) gk = ok;
+    }
+    const bool sing = !gk.nonzero();
+    if (tid == 0) chosen[j] = sing ? -1 : gk.row();
+    if (!sing) {
+      const K mk = lane < cs ? skey[par][lane] : K::none();
+      const unsigned hit = __ballot_sync(0xffffffffu, lane < cs && !mk.worse_than(gk) && !gk.worse_than(mk));
+      const int gc = __ffs(hit) - 1;
+      if (active && gr == gk.row()) {
+        active = false;  // pivot row of column j: row[] keeps its U entries from here on
+        jp = j;
       }
-      __syncthreads();
-      if (warp == 0) {  // push (key, candidate row) to slot [par][crank] of every CTA
-        for (int e = lane; e < cs * W; e += 32) {
-          const int dst = e / W, c = e % W;
-          if (c >= j && c < w)
-            cluster.map_shared_rank(&srow[0][0][0], dst)[(par * kMaxCluster + crank) * W + c] = own[c];
-        }
-        if (lane < cs) cluster.map_shared_rank(&skey[0][0], lane)[par * kMaxCluster + crank] = cb;
-      }
-      cluster.sync();
-      K gk = lane < cs ? skey[par][lane] : K::none();  // all 32 lanes: uniform result
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const K ok = gk.shfl_xor(o);
-        if (gk.worse_than(ok)) gk = ok;
-      }
-      const bool sing = !gk.nonzero();
-      if (tid == 0) chosen[j] = sing ? -1 : gk.row();
-      if (!sing) {
-        const K mine = lane < cs ? skey[par][lane] : K::none();
-        const unsigned hit = __ballot_sync(0xffffffffu, lane < cs && !mine.worse_than(gk) && !gk.worse_than(mine));
-        const int gc = __ffs(hit) - 1;
-        if (gr == gk.row()) active = false;
+      if (active) {
         const E *prow = srow[par][gc];
         const E piv = prow[j];
         E inv;  // 1/pivot (LAPACK zgetf2 scales the column by the reciprocal)
@@ -188,14 +204,22 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(Mat<F32> M, int row0, i
           const Rl rr = piv.x / piv.y, d = piv.y + piv.x * rr;
           inv = E{rr / d, (Rl)-1 / d};
         }
-        if (active) {
-          const E l = cmulE(vj, inv);
-          row[j] = l;
+        const E l = cmulE(vj, inv);
+        lbuf[j * kPanelThreads + tid] = l;
 #pragma unroll
-          for (int c = j + 1; c < W; ++c) row[c] = csubE(row[c], cmulE(l, prow[c]));
+        for (int c = 1; c < W; ++c) {
+          const E pv = (j + c < W) ? prow[j + c] : E{0, 0};
+          row[c - 1] = csubE(row[c], cmulE(l, pv));
         }
-      } else if (tid == 0 && crank == 0) {
-        atomicCAS(info, 0, col0 + j + 1);
+        row[W - 1] = E{0, 0};
+      }
+    } else {
+      if (tid == 0 && crank == 0) atomicCAS(info, 0, col0 + j + 1);
+      if (active) {  // zero column: nothing to eliminate (LAPACK skips the scaling)
+        lbuf[j * kPanelThreads + tid] = vj;
+#pragma unroll
+        for (int c = 1; c < W; ++c) row[c - 1] = row[c];
+        row[W - 1] = E{0, 0};
       }
     }
   }
@@ -248,9 +272,13 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(Mat<F32> M, int row0, i
     int dst = gr;
     for (int e = 0; e < nmoved; ++e)
       if (morig[e] == gr) dst = mpos[e];
+    const int nl = jp < 0 ? w : jp;  // multipliers of columns [0, nl), then U entries
+    for (int c = 0; c < nl; ++c) M.put(row0 + dst, col0 + c, lbuf[c * kPanelThreads + tid]);
+    if (jp >= 0) {
 #pragma unroll
-    for (int c = 0; c < W; ++c)
-      if (c < w) M.put(row0 + dst, col0 + c, row[c]);
+      for (int c = 0; c < W; ++c)
+        if (jp + c < w) M.put(row0 + dst, col0 + jp + c, row[c]);
+    }
   }
 }
 
@@ -280,31 +308,38 @@ __global__ void __launch_bounds__(kSwpThreads) k_laswp(Mat<F32> M, const int *__
 }
 
 // Rows k0..k0+w-1 of columns [c0, c1): X = L11^{-1} X, L11 the w x w unit-lower block at
-// (k0, k0) held in shared memory; one column per thread, the solution in registers.
+// (k0, k0) in shared memory; one column per thread, its w entries in shared memory too.
+// Runtime loops keep the code small: each instruction of a fully unrolled triangle would
+// run once per launch and miss the instruction cache.
 template <bool F32, int W>
 __global__ void __launch_bounds__(128) k_trsm_small(Mat<F32> M, int k0, int w, int c0, int c1) {
   using E = typename Prec<F32>::E;
   __shared__ E L[W][W];
+  __shared__ E xs[W][128];
   for (int e = threadIdx.x; e < W * W; e += blockDim.x) {
     const int i = e / W, t = e % W;
     L[i][t] = (i < w && t < i) ? M.get(k0 + i, k0 + t) : E{0, 0};
   }
-  __syncthreads();
   const int c = c0 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= c1) return;
-  E x[W];
-#pragma unroll
-  for (int i = 0; i < W; ++i) x[i] = i < w ? M.get(k0 + i, c) : E{0, 0};  // all loads in flight at once
-#pragma unroll
-  for (int i = 1; i < W; ++i) {
-    E v = x[i];
-#pragma unroll
-    for (int t = 0; t < i; ++t) v = csubE(v, cmulE(L[i][t], x[t]));
-    x[i] = v;
+  const bool ok = c < c1;
+  const int tx = threadIdx.x;
+#pragma unroll 8
+  for (int i = 0; i < w; ++i) xs[i][tx] = ok ? M.get(k0 + i, c) : E{0, 0};
+  __syncthreads();
+  for (int i = 1; i < w; ++i) {
+    E v0 = xs[i][tx], v1{0, 0};  // two partial sums halve the dependency chain
+    int t = 0;
+    for (; t + 1 < i; t += 2) {
+      v0 = csubE(v0, cmulE(L[i][t], xs[t][tx]));
+      v1 = caddE(v1, cmulE(L[i][t + 1], xs[t + 1][tx]));
+    }
+    if (t < i) v0 = csubE(v0, cmulE(L[i][t], xs[t][tx]));
+    xs[i][tx] = csubE(v0, v1);
   }
-#pragma unroll
-  for (int i = 0; i < W; ++i)
-    if (i < w) M.put(k0 + i, c, x[i]);
+  if (ok) {
+#pragma unroll 8
+    for (int i = 0; i < w; ++i) M.put(k0 + i, c, xs[i][tx]);
+  }
 }
 
 // C[r0:r1, c0:c1] -= A[r0:r1, k0:k0+kb] * A[k0:k0+kb, c0:c1]  (FP64 complex, SIMT, 64x64 tiles)
@@ -412,16 +447,18 @@ int launch_panel(Mat<F32> M, int row0, int nrows, int col0, int w, int *ipiv, in
     return -6;
   }
   auto kern = k_panel<F32, (F32 ? 32 : 16)>;
+  constexpr int smem = kPanelThreads * (F32 ? 32 : 16) * (int)sizeof(typename Prec<F32>::E);  // multipliers
   static DeviceOnce once;
   if (int rc = device_once(once, [&] {
         PSS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        PSS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         return 0;
       }))
     return rc;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(cs);
   cfg.blockDim = dim3(kPanelThreads);
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeClusterDimension;
@@ -449,10 +486,12 @@ template <bool F32>
 void launch_trsm(Mat<F32> M, int k0, int w, int c0, int c1, cudaStream_t st) {
   if (c1 <= c0) return;
   pss_count_launch();
-  if (w <= 16)
-    k_trsm_small<F32, 16><<<cdiv_u(c1 - c0, 128), 128, 0, st>>>(M, k0, w, c0, c1);
-  else
-    k_trsm_small<F32, 32><<<cdiv_u(c1 - c0, 128), 128, 0, st>>>(M, k0, w, c0, c1);
+  if constexpr (F32) {
+    if (w <= 16) k_trsm_small<true, 16><<<cdiv_u(c1 - c0, 128), 128, 0, st>>>(M, k0, w, c0, c1);
+    else k_trsm_small<true, 32><<<cdiv_u(c1 - c0, 128), 128, 0, st>>>(M, k0, w, c0, c1);
+  } else {  // FP64 panels are at most 16 wide
+    k_trsm_small<false, 16><<<cdiv_u(c1 - c0, 128), 128, 0, st>>>(M, k0, w, c0, c1);
+  }
 }
 
 void launch_gemm(Mat<false> M, int r0, int r1, int c0, int c1, int k0, int kb, cudaStream_t st) {
