@@ -4,13 +4,13 @@
 // Matrices are row-major (row interchanges are contiguous).  Blocked right-looking LU in
 // LAPACK zgetrf order, two-level: an outer block of NB columns is factored as panels of W.
 //   * k_panel: a thread-block cluster of ceil(rows / 512) CTAs (<= 16) owns a W-column
-//     panel, one row per thread held in registers for the whole factorisation.  For each
-//     column every CTA pushes its local pivot candidate (|re|+|im| as LAPACK izamax, the
-//     row index and the candidate row) into every CTA's shared memory, one cluster barrier
-//     makes them visible, and every CTA picks the same winner and applies the rank-1
-//     update to its own rows.  At the end every CTA replays the interchange sequence in
-//     shared memory (a sparse map of the <= 2W moved positions), CTA 0 writes ipiv and a
-//     compact interchange list, and each thread writes its row to its final position.
+//     panel, 512 rows per CTA in shared memory.  For each column every CTA reduces its
+//     pivot candidates (|re|+|im| as LAPACK izamax, lowest row on ties) with redux.sync,
+//     pushes its candidate (key, row index, entries) into every CTA's shared memory, one
+//     cluster barrier makes them visible, and every CTA picks the same winner and updates
+//     its own rows.  At the end every CTA replays the interchange sequence in shared memory
+//     (a sparse map of the <= 2W moved positions), CTA 0 writes ipiv and a compact
+//     interchange list, and the rows are copied to their final positions.
 //   * k_laswp applies that list to all other columns in one launch.
 //   * k_trsm_small: the W-row block-row solve L11^{-1} X, one column per thread.
 //   * the Schur complement A22 -= L21 U12: k_gemm64 (FP64, SIMT), and in FP32 mode
@@ -18,6 +18,8 @@
 //     (pss_gemm_tc.cu) for the trailing update of each outer block.
 // In FP32 mode the matrix is two float planes (real, imaginary).
 #include <cooperative_groups.h>
+#include <type_traits>
+
 #include "pss_internal.cuh"
 
 namespace cg = cooperative_groups;
@@ -60,7 +62,8 @@ struct Mat {
   }
 };
 
-constexpr int kPanelThreads = 512;  // one panel row per thread
+constexpr int kPanelRows = 512;     // panel rows per CTA
+constexpr int kPanelThreads = 256;  // two panel rows per thread
 constexpr int kMaxCluster = 16;
 constexpr int kMaxW = 32;
 constexpr int kMaxMov = 2 * kMaxW;  // rows one panel's interchanges can move
@@ -68,159 +71,135 @@ constexpr int kSwpThreads = 64;
 constexpr int kListInts = 1 + 2 * kMaxMov;  // interchange list: count, destinations, sources
 constexpr int kTcMinRows = 64, kTcMinCols = 32;  // smallest FP32 update sent to the tensor cores
 static_assert(kPanelThreads / 32 <= 32 && kMaxCluster <= 32, "panel reductions run over one warp's lanes");
+static_assert(kPanelRows == 2 * kPanelThreads, "two rows per panel thread");
 
-// Pivot candidate of one column: LAPACK's izamax order (largest |re|+|im|, then the lowest
-// row).  FP32: value and row packed in one 64-bit key (non-negative float bits are
-// monotonic), so a comparison is one integer compare and a shuffle is one 64-bit shuffle.
+// Pivot keys: LAPACK's izamax order (largest |re|+|im|, then the lowest row) as one 64-bit
+// unsigned key per candidate, 0 = no candidate, 1 = an exactly zero candidate.  The bits
+// of a non-negative float or double are monotonic, so the largest key is the largest
+// value; among equal keys the lowest lane wins, and lanes, warps and cluster ranks are in
+// row order.  A warp reduces with redux.sync (one instruction per 32-bit half).
 template <bool F32>
-struct PivKey;
-template <>
-struct PivKey<true> {
-  unsigned long long k;  // 0 = no candidate
-  __device__ static PivKey make(float re, float im, int row, bool act) {
-    const float v = fabsf(re) + fabsf(im);
-    return {act ? ((unsigned long long)__float_as_uint(v) << 32) | (0xffffffffu - (unsigned)row) : 0ull};
+__device__ __forceinline__ unsigned long long piv_key(typename Prec<F32>::E v, bool act) {
+  if (!act) return 0ull;
+  if constexpr (F32) return (unsigned long long)__float_as_uint(fabsf(v.x) + fabsf(v.y)) + 1ull;
+  else return (unsigned long long)__double_as_longlong(fabs(v.x) + fabs(v.y)) + 1ull;
+}
+// Warp-wide maximum key and, among the lanes holding it, the lowest row (all lanes get both):
+// exactly izamax's choice whatever the lane order of the rows.
+template <bool F32>
+__device__ __forceinline__ unsigned long long warp_max_key(unsigned long long k, int r, int &win_row) {
+  const unsigned lo = (unsigned)k;
+  unsigned long long m;
+  bool mine;
+  if constexpr (F32) {  // keys fit in 32 bits
+    const unsigned ml = __reduce_max_sync(0xffffffffu, lo);
+    m = ml;
+    mine = lo == ml;
+  } else {
+    const unsigned hi = (unsigned)(k >> 32);
+    const unsigned mh = __reduce_max_sync(0xffffffffu, hi);
+    const unsigned ml = __reduce_max_sync(0xffffffffu, hi == mh ? lo : 0u);
+    m = ((unsigned long long)mh << 32) | ml;
+    mine = hi == mh && lo == ml;
   }
-  __device__ static PivKey none() { return {0ull}; }
-  __device__ bool worse_than(const PivKey &o) const { return o.k > k; }
-  __device__ PivKey shfl_xor(int o) const { return {__shfl_xor_sync(0xffffffffu, k, o)}; }
-  __device__ int row() const { return (int)(0xffffffffu - (unsigned)(k & 0xffffffffu)); }
-  __device__ bool nonzero() const { return (k >> 32) != 0ull; }  // a candidate with |re|+|im| > 0
-  __device__ bool valid() const { return k != 0ull; }
-};
-template <>
-struct PivKey<false> {
-  double v;  // -1: no candidate
-  int r;
-  __device__ static PivKey make(double re, double im, int row, bool act) {
-    return act ? PivKey{fabs(re) + fabs(im), row} : none();
-  }
-  __device__ static PivKey none() { return {-1.0, 0x7fffffff}; }
-  __device__ bool worse_than(const PivKey &o) const { return o.v > v || (o.v == v && o.r < r); }
-  __device__ PivKey shfl_xor(int o) const {
-    return {__shfl_xor_sync(0xffffffffu, v, o), __shfl_xor_sync(0xffffffffu, r, o)};
-  }
-  __device__ int row() const { return r; }
-  __device__ bool nonzero() const { return v > 0.0; }
-  __device__ bool valid() const { return v >= 0.0; }
-};
+  win_row = (int)__reduce_min_sync(0xffffffffu, mine ? (unsigned)r : 0x7fffffffu);
+  return m;
+}
 
 // Panel of W columns (w <= W used), rows row0..row0+nrows-1, factored by a cluster of
-// cs = gridDim.x CTAs; thread t of CTA q holds row q*512 + t in registers.
-// The column loop is a runtime loop over a SHIFTING register array: at column j, row[c]
-// holds column j + c of the thread's row, so every register index is a compile-time
-// constant while the loop body stays small (an unrolled body per column would not fit the
-// instruction cache, and each column's code runs once per launch).  Multipliers go to
-// shared memory (lbuf[j][thread]); a row chosen as pivot at column j freezes (row[c] then
-// holds its U entries of columns j + c).  Per column: one CTA barrier (per-warp winners),
-// the warp holding the CTA's candidate pushes key and row into every CTA's shared memory,
-// one cluster barrier, and every CTA picks the same winner.
+// cs = gridDim.x CTAs of 256 threads; CTA q owns panel rows q*512 .. q*512+511, held in its
+// shared memory column by column (R[c][local row], conflict-free for a warp), and thread t
+// works on local rows t and 256 + t.  Per column: the two rows' pivot keys are reduced per
+// warp (redux.sync), one CTA barrier, per CTA; warp 0 pushes the CTA's candidate (key, row
+// index and its entries j..w-1, read from shared memory) into every CTA's shared memory;
+// one cluster barrier; every CTA picks the same winner and updates its active rows over
+// the live columns only.  Multipliers overwrite the rows in place, pivot rows keep their U
+// entries, so the final write-back is a coalesced copy to the permuted positions.
 template <bool F32, int W>
 __global__ void __launch_bounds__(kPanelThreads) k_panel(Mat<F32> M, int row0, int nrows, int col0, int w,
                                                          int *ipiv, int *info, int *xlist) {
   using E = typename Prec<F32>::E;
   using Rl = typename Prec<F32>::R;
-  using K = PivKey<F32>;
   cg::cluster_group cluster = cg::this_cluster();
   const int cs = (int)cluster.num_blocks();
   const int crank = (int)cluster.block_rank();
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   constexpr int NW = kPanelThreads / 32;
   extern __shared__ __align__(16) unsigned char panel_smem[];
-  E *lbuf = (E *)panel_smem;              // [W][kPanelThreads] multipliers (dynamic shared memory)
-  __shared__ E srow[2][kMaxCluster][W];   // candidate rows pushed by every CTA (double-buffered)
-  __shared__ K skey[2][kMaxCluster];      // their keys
-  __shared__ K redk[NW];                  // per-warp winners
+  E *R = (E *)panel_smem;                      // [W][kPanelRows] the CTA's panel rows
+  __shared__ E srow[2][kMaxCluster][W];        // candidate rows pushed by every CTA (double-buffered)
+  __shared__ unsigned long long skey[2][kMaxCluster];
+  __shared__ int sidx[2][kMaxCluster];         // their panel rows
+  __shared__ unsigned long long wkey[NW];      // per-warp winners
+  __shared__ int wrow[NW];
   __shared__ int chosen[kMaxW];
   __shared__ int mpos[2 * kMaxW], morig[2 * kMaxW];  // moved positions and the row each now holds
   __shared__ int nmoved;
-  const int gr = crank * kPanelThreads + tid;  // panel-relative row of this thread
-  const bool have = gr < nrows;
-  bool active = have;
-  int jp = -1;  // column at which this row became a pivot row
-  E row[W];
-#pragma unroll
-  for (int c = 0; c < W; ++c) row[c] = (have && c < w) ? M.get(row0 + gr, col0 + c) : E{0, 0};
+  const int base = crank * kPanelRows;
+  const int nloc = max(0, min(kPanelRows, nrows - base));  // rows this CTA owns
+  // coalesced load: one row per warp step, one column per lane
+  for (int r = warp; r < kPanelRows; r += NW)
+    if (lane < W) R[lane * kPanelRows + r] = (r < nloc && lane < w) ? M.get(row0 + base + r, col0 + lane) : E{0, 0};
+  const int ta = tid, tb = kPanelThreads + tid;  // local rows of this thread
+  bool acta = ta < nloc, actb = tb < nloc;
+  __syncthreads();
 
   for (int j = 0; j < w; ++j) {
     const int par = j & 1;
-    const E vj = row[0];
-    K key = K::make(vj.x, vj.y, gr, active);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const K ok = key.shfl_xor(o);
-      if (key.worse_than(ok)) key = ok;
-    }
-    if (lane == 0) redk[warp] = key;
+    const E va = R[j * kPanelRows + ta], vb = R[j * kPanelRows + tb];
+    unsigned long long k = piv_key<F32>(va, acta);
+    int r = base + ta;
+    const unsigned long long kb = piv_key<F32>(vb, actb);
+    if (kb > k) { k = kb; r = base + tb; }  // equal keys keep the lower row
+    int wr;
+    k = warp_max_key<F32>(k, r, wr);
+    if (lane == 0) { wkey[warp] = k; wrow[warp] = wr; }
     __syncthreads();
-    // every warp reduces the NW warp winners over all 32 lanes, so every lane agrees
-    K cb = lane < NW ? redk[lane] : K::none();
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const K ok = cb.shfl_xor(o);
-      if (cb.worse_than(ok)) cb = ok;
-    }
-    // the warp holding this CTA's candidate (warp 0 if the CTA has none left) pushes it
-    const bool has = cb.valid();
-    const int wt = has ? cb.row() - crank * kPanelThreads : 0;  // CTA-local thread of the candidate
-    if (warp == (wt >> 5)) {
-      const int wl = wt & 31;
-      E mine{0, 0};  // lane c: the candidate's column j + c
-#pragma unroll
-      for (int c = 0; c < W; ++c) {
-        const E v{__shfl_sync(0xffffffffu, row[c].x, wl), __shfl_sync(0xffffffffu, row[c].y, wl)};
-        if (lane == c) mine = v;
-      }
+    if (warp == 0) {  // the CTA's candidate, pushed to slot [par][crank] of every CTA
+      int cr;
+      const unsigned long long kc =
+          warp_max_key<F32>(lane < NW ? wkey[lane] : 0ull, lane < NW ? wrow[lane] : 0x7fffffff, cr);
+      const int lr = kc ? cr - base : 0;
+      const E v = (lane < W && j + lane < w) ? R[(j + lane) * kPanelRows + lr] : E{0, 0};
       if (lane < W && j + lane < w)
         for (int dst = 0; dst < cs; ++dst)
-          cluster.map_shared_rank(&srow[0][0][0], dst)[(par * kMaxCluster + crank) * W + j + lane] = mine;
-      if (lane < cs) cluster.map_shared_rank(&skey[0][0], lane)[par * kMaxCluster + crank] = cb;
+          cluster.map_shared_rank(&srow[0][0][0], dst)[(par * kMaxCluster + crank) * W + j + lane] = v;
+      if (lane < cs) {
+        cluster.map_shared_rank(&skey[0][0], lane)[par * kMaxCluster + crank] = kc;
+        cluster.map_shared_rank(&sidx[0][0], lane)[par * kMaxCluster + crank] = cr;
+      }
     }
     cluster.sync();
-    K gk = lane < cs ? skey[par][lane] : K::none();  // all 32 lanes: uniform result
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const K ok = gk.shfl_xor(o);
-      if (gk.worse_than(ok)) gk = ok;
-    }
-    const bool sing = !gk.nonzero();
-    if (tid == 0) chosen[j] = sing ? -1 : gk.row();
-    if (!sing) {
-      const K mk = lane < cs ? skey[par][lane] : K::none();
-      const unsigned hit = __ballot_sync(0xffffffffu, lane < cs && !mk.worse_than(gk) && !gk.worse_than(mk));
-      const int gc = __ffs(hit) - 1;
-      if (active && gr == gk.row()) {
-        active = false;  // pivot row of column j: row[] keeps its U entries from here on
-        jp = j;
-      }
-      if (active) {
-        const E *prow = srow[par][gc];
-        const E piv = prow[j];
-        E inv;  // 1/pivot (LAPACK zgetf2 scales the column by the reciprocal)
-        if (fabs((double)piv.y) <= fabs((double)piv.x)) {
-          const Rl rr = piv.y / piv.x, d = piv.x + piv.y * rr;
-          inv = E{(Rl)1 / d, -rr / d};
-        } else {
-          const Rl rr = piv.x / piv.y, d = piv.y + piv.x * rr;
-          inv = E{rr / d, (Rl)-1 / d};
-        }
-        const E l = cmulE(vj, inv);
-        lbuf[j * kPanelThreads + tid] = l;
-#pragma unroll
-        for (int c = 1; c < W; ++c) {
-          const E pv = (j + c < W) ? prow[j + c] : E{0, 0};
-          row[c - 1] = csubE(row[c], cmulE(l, pv));
-        }
-        row[W - 1] = E{0, 0};
-      }
-    } else {
+    int grow;
+    const unsigned long long kg =
+        warp_max_key<F32>(lane < cs ? skey[par][lane] : 0ull, lane < cs ? sidx[par][lane] : 0x7fffffff, grow);
+    const bool sing = kg <= 1ull;  // no candidate, or an exactly zero one
+    if (tid == 0) chosen[j] = sing ? -1 : grow;
+    if (sing) {  // zero column: nothing to eliminate (LAPACK skips the scaling)
       if (tid == 0 && crank == 0) atomicCAS(info, 0, col0 + j + 1);
-      if (active) {  // zero column: nothing to eliminate (LAPACK skips the scaling)
-        lbuf[j * kPanelThreads + tid] = vj;
-#pragma unroll
-        for (int c = 1; c < W; ++c) row[c - 1] = row[c];
-        row[W - 1] = E{0, 0};
-      }
+      continue;
+    }
+    if (base + ta == grow) acta = false;  // the pivot row keeps its entries (row of U)
+    if (base + tb == grow) actb = false;
+    if (!(acta || actb)) continue;
+    const E *prow = srow[par][grow / kPanelRows];
+    const E piv = prow[j];
+    E inv;  // 1/pivot (LAPACK zgetf2 scales the column by the reciprocal)
+    if (fabs((double)piv.y) <= fabs((double)piv.x)) {
+      const Rl rr = piv.y / piv.x, d = piv.x + piv.y * rr;
+      inv = E{(Rl)1 / d, -rr / d};
+    } else {
+      const Rl rr = piv.x / piv.y, d = piv.y + piv.x * rr;
+      inv = E{rr / d, (Rl)-1 / d};
+    }
+    const E la = cmulE(va, inv), lb = cmulE(vb, inv);
+    if (acta) R[j * kPanelRows + ta] = la;
+    if (actb) R[j * kPanelRows + tb] = lb;
+#pragma unroll 4
+    for (int c = j + 1; c < w; ++c) {
+      const E p = prow[c];
+      if (acta) R[c * kPanelRows + ta] = csubE(R[c * kPanelRows + ta], cmulE(la, p));
+      if (actb) R[c * kPanelRows + tb] = csubE(R[c * kPanelRows + tb], cmulE(lb, p));
     }
   }
   __syncthreads();
@@ -244,12 +223,12 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(Mat<F32> M, int row0, i
       if (crank == 0 && lane == 0) ipiv[col0 + j] = row0 + p;
       if (p != j) {
         const int ej = find(mpos, j), ep = find(mpos, p);
-        const int a = ej >= 0 ? morig[ej] : j;  // row now at position j
-        const int b = ep >= 0 ? morig[ep] : p;  // row now at position p
+        const int x = ej >= 0 ? morig[ej] : j;  // row now at position j
+        const int y = ep >= 0 ? morig[ep] : p;  // row now at position p
         __syncwarp();
         if (lane == 0) {
-          if (ej >= 0) morig[ej] = b; else { mpos[cnt] = j; morig[cnt] = b; }
-          if (ep >= 0) morig[ep] = a; else { mpos[cnt + (ej < 0)] = p; morig[cnt + (ej < 0)] = a; }
+          if (ej >= 0) morig[ej] = y; else { mpos[cnt] = j; morig[cnt] = y; }
+          if (ep >= 0) morig[ep] = x; else { mpos[cnt + (ej < 0)] = p; morig[cnt + (ej < 0)] = x; }
         }
         cnt += (ej < 0) + (ep < 0);
         __syncwarp();
@@ -268,17 +247,13 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(Mat<F32> M, int row0, i
     }
   }
   __syncthreads();
-  if (have) {
-    int dst = gr;
-    for (int e = 0; e < nmoved; ++e)
-      if (morig[e] == gr) dst = mpos[e];
-    const int nl = jp < 0 ? w : jp;  // multipliers of columns [0, nl), then U entries
-    for (int c = 0; c < nl; ++c) M.put(row0 + dst, col0 + c, lbuf[c * kPanelThreads + tid]);
-    if (jp >= 0) {
-#pragma unroll
-      for (int c = 0; c < W; ++c)
-        if (jp + c < w) M.put(row0 + dst, col0 + jp + c, row[c]);
-    }
+  // coalesced write-back: one row per warp step, one column per lane, to its final position
+  for (int r = warp; r < nloc; r += NW) {
+    const int g = base + r;
+    const unsigned h0 = __ballot_sync(0xffffffffu, lane < nmoved && morig[lane] == g);
+    const unsigned h1 = __ballot_sync(0xffffffffu, lane + 32 < nmoved && morig[lane + 32] == g);
+    const int dst = h0 ? mpos[__ffs(h0) - 1] : (h1 ? mpos[32 + __ffs(h1) - 1] : g);
+    if (lane < w) M.put(row0 + dst, col0 + lane, R[lane * kPanelRows + r]);
   }
 }
 
@@ -440,14 +415,14 @@ __global__ void __launch_bounds__(256) k_gemm32(float *Ar, float *Ai, long long 
 template <bool F32>
 int launch_panel(Mat<F32> M, int row0, int nrows, int col0, int w, int *ipiv, int *info, int *xlist,
                  cudaStream_t st) {
-  const int cs = (nrows + kPanelThreads - 1) / kPanelThreads;
+  const int cs = (nrows + kPanelRows - 1) / kPanelRows;
   const int Wt = F32 ? 32 : 16;
   if (cs > kMaxCluster || w > Wt) {
     pss_set_error("panel %d x %d exceeds a %d-CTA cluster", nrows, w, kMaxCluster);
     return -6;
   }
   auto kern = k_panel<F32, (F32 ? 32 : 16)>;
-  constexpr int smem = kPanelThreads * (F32 ? 32 : 16) * (int)sizeof(typename Prec<F32>::E);  // multipliers
+  constexpr int smem = kPanelRows * (F32 ? 32 : 16) * (int)sizeof(typename Prec<F32>::E);  // multipliers
   static DeviceOnce once;
   if (int rc = device_once(once, [&] {
         PSS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
@@ -576,7 +551,7 @@ int lu_blocked(int n, Mat<F32> M, int *ipiv, int *info, int NB, int W, int *pscr
 
 template <bool F32>
 int pick_panel_width(int n, int want) {
-  if ((n + kPanelThreads - 1) / kPanelThreads > kMaxCluster) return -1;
+  if ((n + kPanelRows - 1) / kPanelRows > kMaxCluster) return -1;
   return want;
 }
 
