@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <thread>
@@ -112,49 +113,70 @@ struct JKBufs {
   }
 };
 
-__global__ void k_info_to_status(int *info, int *status);
+__global__ void k_info_to_status(int nb, int *info, int *status);
 
+// One CUDA stream with buffers for a batch of up to `cap` frequency points: their matrices,
+// pivots, right-hand sides and solutions side by side (matrix b at offset b*n*n, vectors
+// at b*n*nrhs), factored and solved together by the batched LU and solve kernels.
 struct Worker {
   cudaStream_t st = nullptr;
-  DevBuf zb, z64, zr, zi, ipiv, info, bf, rhs, X, R, D, nonconv, luws, solvews;
+  int cap = 1;  // batch capacity (points)
+  DevBuf zb, z64, zr, zi, ipiv, info, bstat, bf, rhs, X, R, D, nonconv, luws, solvews;
   JKBufs jk;
   SolveWS sws;
-  int ensure_solver(int n, int nrhs) {
-    if (ipiv.ensure((size_t)n * sizeof(int)) || info.ensure(sizeof(int))) return -3;
-    if (luws.ensure(std::max(pss_lu_ws_bytes(n, 0), pss_lu_ws_bytes(n, 1)))) return -3;
-    if (solvews.ensure(pss_solve_ws_bytes(n))) return -3;
-    sws.bind(solvews.p, n);
-    const size_t v = (size_t)n * nrhs * sizeof(cd);
+  int ensure_solver(int n, int nrhs, int nb) {
+    if (ipiv.ensure((size_t)nb * n * sizeof(int)) || info.ensure((size_t)nb * sizeof(int)) ||
+        bstat.ensure((size_t)nb * sizeof(int)))
+      return -3;
+    if (luws.ensure(std::max(pss_lu_ws_bytes(n, 0, nb), pss_lu_ws_bytes(n, 1, nb)))) return -3;
+    if (solvews.ensure(pss_solve_ws_bytes(n, nb))) return -3;
+    sws.bind(solvews.p, n, nb);
+    const size_t v = (size_t)nb * n * nrhs * sizeof(cd);
     if (rhs.ensure(v) || X.ensure(v) || R.ensure(v) || D.ensure(v)) return -3;
     return 0;
   }
-  // LU of the worker's matrix (FP64 in z64, or FP32 planes zr/zi) and solve rhs -> X,
-  // refined against z64 in FP32 mode.  Status bits go to *status (device).
-  int factor_solve(int n, long long ld, int prec, int nrhs, int maxit, int *status) {
+  // LU of the worker's first nb matrices (FP64 in z64, or FP32 planes zr/zi) and solves
+  // rhs -> X, refined against z64 in FP32 mode.  Status bits go to status[0..nb) (device).
+  int factor_solve(int n, int nb, int prec, int nrhs, int maxit, int *status) {
     int rc;
-    if (prec == PSS_FP64) rc = pss_lu64(n, z64.as<cd>(), ld, ipiv.as<int>(), info.as<int>(), luws.p, luws.n, st);
-    else rc = pss_lu32(n, zr.as<float>(), zi.as<float>(), ld, ipiv.as<int>(), info.as<int>(), luws.p, luws.n, st);
+    const long long ld = n, ms = (long long)n * n, vs = (long long)n * nrhs;
+    if (prec == PSS_FP64)
+      rc = pss_lu64_batched(n, nb, z64.as<cd>(), ld, ms, ipiv.as<int>(), info.as<int>(), luws.p, luws.n, st);
+    else
+      rc = pss_lu32_batched(n, nb, zr.as<float>(), zi.as<float>(), ld, ms, ipiv.as<int>(), info.as<int>(), luws.p,
+                            luws.n, st);
     if (rc) return rc;
     pss_count_launch();
-    k_info_to_status<<<1, 1, 0, st>>>(info.as<int>(), status);
+    k_info_to_status<<<1, 32, 0, st>>>(nb, info.as<int>(), status);
     const cd *L64 = prec == PSS_FP64 ? z64.as<cd>() : nullptr;
     const float *Lr = prec == PSS_FP64 ? nullptr : zr.as<float>();
     const float *Li = prec == PSS_FP64 ? nullptr : zi.as<float>();
-    if ((rc = pss_solve_prepare(sws, L64, Lr, Li, ld, ipiv.as<int>(), st))) return rc;
-    if ((rc = pss_solve_lu(sws, L64, Lr, Li, ld, nrhs, rhs.as<cd>(), X.as<cd>(), nullptr, st))) return rc;
+    if ((rc = pss_solve_prepare(sws, nb, L64, Lr, Li, ld, ms, ipiv.as<int>(), st))) return rc;
+    if ((rc = pss_solve_lu(sws, nb, L64, Lr, Li, ld, ms, nrhs, rhs.as<cd>(), X.as<cd>(), vs, 0, st))) return rc;
     if (prec == PSS_FP32_REFINE &&
-        (rc = pss_refine(sws, z64.as<cd>(), ld, Lr, Li, nrhs, rhs.as<cd>(), X.as<cd>(), R.as<cd>(), D.as<cd>(),
-                         maxit, status, st)))
+        (rc = pss_refine(sws, nb, z64.as<cd>(), ld, ms, Lr, Li, nrhs, rhs.as<cd>(), X.as<cd>(), R.as<cd>(),
+                         D.as<cd>(), vs, maxit, status, st)))
       return rc;
-    pss_solve_status(sws, status, st);
+    pss_solve_status(sws, nb, status, st);
     return 0;
   }
 };
 
-__global__ void k_info_to_status(int *info, int *status) {
-  if (*info > 0) *status |= PSS_ST_SINGULAR;
-  if (*info < 0) *status |= PSS_ST_DEVICE_TIMEOUT;
-  *info = 0;
+// Batch-local status words OR-ed into the points' status words.
+constexpr int kMaxBatch = 32;
+struct StatusMap {
+  int idx[kMaxBatch];
+};
+__global__ void k_status_scatter(int cnt, const int *bstat, int *status, StatusMap sm) {
+  for (int b = threadIdx.x; b < cnt; b += blockDim.x) status[sm.idx[b]] |= bstat[b];
+}
+
+__global__ void k_info_to_status(int nb, int *info, int *status) {
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+    if (info[b] > 0) status[b] |= PSS_ST_SINGULAR;
+    if (info[b] < 0) status[b] |= PSS_ST_DEVICE_TIMEOUT;
+    info[b] = 0;
+  }
 }
 __global__ void k_nonconv_to_status(int *nonconv, int *status) {
   if (*nonconv) *status |= PSS_ST_JK_NOCONV;
@@ -180,6 +202,7 @@ cd hcis(double a) { return mkcd(std::cos(a), std::sin(a)); }
 struct pss_ctx {
   int device = 0;
   int nworkers = 1;
+  int batch = 8;  // points per batched factorisation (PSS_BATCH, 1..32)
   std::vector<Worker> w;
   DevBuf params, dense, conv, mm, stage, tables, bigdense, modes, dS, status;
   std::vector<DevBuf> bigtables;
@@ -374,18 +397,18 @@ int refresh_jk_cache(pss_sheet *sh, double psi1, double psi2, double ulocal, cud
   return 0;
 }
 
-int ensure_worker(Worker &w, const pss_sheet *sh, int nm, int precision, bool own_jk) {
+int ensure_worker(Worker &w, const pss_sheet *sh, int nm, int precision, bool own_jk, int nb) {
   const size_t n = sh->nbf;
   if (w.zb.ensure((size_t)sh->nufp * 9 * sizeof(cd))) return -3;
-  if (w.z64.ensure(n * n * sizeof(cd))) return -3;
+  if (w.z64.ensure((size_t)nb * n * n * sizeof(cd))) return -3;
   if (precision == PSS_FP32_REFINE) {
-    if (w.zr.ensure(n * n * sizeof(float)) || w.zi.ensure(n * n * sizeof(float))) return -3;
+    if (w.zr.ensure((size_t)nb * n * n * sizeof(float)) || w.zi.ensure((size_t)nb * n * n * sizeof(float))) return -3;
   }
   if (w.nonconv.ensure(sizeof(int))) return -3;
-  if (w.bf.ensure((size_t)nm * n * 2 * sizeof(cd))) return -3;
-  if (w.ensure_solver((int)n, nm)) return -3;
+  if (w.bf.ensure((size_t)nb * nm * n * 2 * sizeof(cd))) return -3;
+  if (w.ensure_solver((int)n, nm, nb)) return -3;
   if (own_jk && w.jk.ensure(sh->nufp)) return -3;
-  PSS_CUDA_TRY(cudaMemsetAsync(w.info.p, 0, sizeof(int), w.st));
+  PSS_CUDA_TRY(cudaMemsetAsync(w.info.p, 0, (size_t)nb * sizeof(int), w.st));
   PSS_CUDA_TRY(cudaMemsetAsync(w.nonconv.p, 0, sizeof(int), w.st));
   return 0;
 }
@@ -413,6 +436,7 @@ int pss_ctx_create(int device, int nworkers, pss_ctx **out) {
   pss_ctx *c = new pss_ctx();
   c->device = device;
   c->nworkers = std::max(1, std::min(nworkers, 16));
+  if (const char *bs = std::getenv("PSS_BATCH")) c->batch = std::max(1, std::min(atoi(bs), kMaxBatch));
   if (set_device(c)) { delete c; return -3; }
   c->w.resize(c->nworkers);
   for (auto &w : c->w) {
@@ -431,7 +455,7 @@ int pss_ctx_destroy(pss_ctx *c) {
   cudaSetDevice(c->device);
   cudaDeviceSynchronize();
   for (auto &w : c->w) {
-    for (DevBuf *b : {&w.zb, &w.z64, &w.zr, &w.zi, &w.ipiv, &w.info, &w.bf, &w.rhs, &w.X, &w.R, &w.D, &w.nonconv,
+    for (DevBuf *b : {&w.zb, &w.z64, &w.zr, &w.zi, &w.ipiv, &w.info, &w.bstat, &w.bf, &w.rhs, &w.X, &w.R, &w.D, &w.nonconv,
                       &w.luws, &w.solvews})
       b->release();
     w.jk.buf.release();
@@ -631,56 +655,77 @@ int pss_partial_gsms(pss_sheet *sh, int nl, const double *eps, const double *mu,
       for (int i = 0; i < npts; ++i) hstatus[i] |= PSS_ST_JK_NOCONV;
   }
   const int nw = c->nworkers;
+  const int B = std::max(1, std::min(c->batch, npts));  // points factored together per worker
   for (int k = 0; k < nw; ++k)
-    if ((rc = ensure_worker(c->w[k], sh, nmodes, precision, !same_psi))) return rc;
+    if ((rc = ensure_worker(c->w[k], sh, nmodes, precision, !same_psi, B))) return rc;
 
   const int n = sh->nbf;
-  const long long ld = n;
-  std::vector<cudaEvent_t> ev;  // phase events of worker 0's points (pushed by its thread only)
+  const long long ld = n, msz = (long long)n * n, vsz = (long long)n * nmodes;
+  std::vector<cudaEvent_t> ev;  // phase events of worker 0's batches (pushed by its thread only)
   std::vector<KProf> kprofs(nw);
-  // One point through fill, LU, transforms, solve(s) and projection on worker w's stream.
-  auto run_point = [&](int i, int prec, Worker &w, bool rec) -> int {
+  // A batch of cnt points (indices idx[0..cnt)) on worker w: per point face integrals (when
+  // ψ varies), fill into matrix slot b, basis transforms and right-hand sides; then one
+  // batched LU + solve (+ refinement) of all cnt matrices; then per point the projection.
+  auto run_batch = [&](const int *idx, int cnt, int prec, Worker &w, bool rec) -> int {
     cudaStream_t st = w.st;
-    const PointParams *Pi = dP + i;
-    const double p1 = psi[2 * i], p2 = psi[2 * i + 1];
     cudaEvent_t e[8];
     if (rec) {
       for (int q = 0; q < 8; ++q) { cudaEventCreate(&e[q]); ev.push_back(e[q]); }
       cudaEventRecord(e[0], st);
+      cudaEventRecord(e[1], st);
     }
-    JKDev jk;
-    if (same_psi) {
-      jk = sh->cache.jk;
-    } else {
-      jk = w.jk.jk;
-      pss_filljk(sh->G, ulocal, p1, p2, sh->s1, sh->s2, jk, w.nonconv.as<int>(), st);
-      pss_count_launch();
-      k_nonconv_to_status<<<1, 1, 0, st>>>(w.nonconv.as<int>(), dstatus + i);
-    }
-    if (rec) cudaEventRecord(e[1], st);
-    pss_fill_pairs(sh->G, Pi, jk, tabs[i].t1, tabs[i].t2, tabs[i].mmax, w.zb.as<cd>(), st);
     float *zr = prec == PSS_FP32_REFINE ? w.zr.as<float>() : nullptr;
     float *zi = prec == PSS_FP32_REFINE ? w.zi.as<float>() : nullptr;
-    pss_fill_assemble(sh->G, Pi, w.zb.as<cd>(), w.z64.as<cd>(), zr, zi, ld, st);
+    for (int b = 0; b < cnt; ++b) {
+      const int i = idx[b];
+      const PointParams *Pi = dP + i;
+      JKDev jk;
+      if (same_psi) {
+        jk = sh->cache.jk;
+      } else {
+        jk = w.jk.jk;
+        pss_filljk(sh->G, ulocal, psi[2 * i], psi[2 * i + 1], sh->s1, sh->s2, jk, w.nonconv.as<int>(), st);
+        pss_count_launch();
+        k_nonconv_to_status<<<1, 1, 0, st>>>(w.nonconv.as<int>(), dstatus + i);
+      }
+      pss_fill_pairs(sh->G, Pi, jk, tabs[i].t1, tabs[i].t2, tabs[i].mmax, w.zb.as<cd>(), st);
+      pss_fill_assemble(sh->G, Pi, w.zb.as<cd>(), w.z64.as<cd>() + b * msz, zr ? zr + b * msz : nullptr,
+                        zi ? zi + b * msz : nullptr, ld, st);
+    }
     if (rec) cudaEventRecord(e[2], st);
-    const double *kv = (const double *)(mb + off_k) + (size_t)i * nmodes * 2;
-    const cd *sv = (const cd *)(mb + off_s) + (size_t)i * nmodes * 2;
-    const double *tv = (const double *)(mb + off_t) + (size_t)i * nmodes * 2;
-    const cd *wv = (const cd *)(mb + off_w) + (size_t)i * nmodes;
-    pss_bfft(sh->G, nmodes, kv, p1, p2, w.bf.as<cd>(), st);
-    pss_rhs(n, nmodes, w.bf.as<cd>(), sv, w.rhs.as<cd>(), st);
+    for (int b = 0; b < cnt; ++b) {
+      const int i = idx[b];
+      const double *kv = (const double *)(mb + off_k) + (size_t)i * nmodes * 2;
+      const cd *sv = (const cd *)(mb + off_s) + (size_t)i * nmodes * 2;
+      cd *bf = w.bf.as<cd>() + (size_t)b * nmodes * n * 2;
+      pss_bfft(sh->G, nmodes, kv, psi[2 * i], psi[2 * i + 1], bf, st);
+      pss_rhs(n, nmodes, bf, sv, w.rhs.as<cd>() + b * vsz, st);
+    }
     if (rec) { cudaEventRecord(e[3], st); cudaEventRecord(e[4], st); }
-    int rc2 = w.factor_solve(n, ld, prec, nmodes, kMaxRefine, dstatus + i);
+    PSS_CUDA_TRY(cudaMemsetAsync(w.bstat.p, 0, (size_t)cnt * sizeof(int), st));
+    int rc2 = w.factor_solve(n, cnt, prec, nmodes, kMaxRefine, w.bstat.as<int>());
     if (rc2) return rc2;
+    StatusMap sm{};
+    for (int b = 0; b < cnt; ++b) sm.idx[b] = idx[b];
+    pss_count_launch();
+    k_status_scatter<<<1, 32, 0, st>>>(cnt, w.bstat.as<int>(), dstatus, sm);
     if (rec) cudaEventRecord(e[5], st);
-    pss_project(n, nmodes, w.bf.as<cd>(), tv, wv, w.X.as<cd>(), c->dS.as<cd>() + (size_t)i * nm2, st);
+    for (int b = 0; b < cnt; ++b) {
+      const int i = idx[b];
+      const double *tv = (const double *)(mb + off_t) + (size_t)i * nmodes * 2;
+      const cd *wv = (const cd *)(mb + off_w) + (size_t)i * nmodes;
+      pss_project(n, nmodes, w.bf.as<cd>() + (size_t)b * nmodes * n * 2, tv, wv, w.X.as<cd>() + b * vsz,
+                  c->dS.as<cd>() + (size_t)i * nm2, st);
+    }
     if (rec) { cudaEventRecord(e[6], st); cudaEventRecord(e[7], st); }
     PSS_CUDA_TRY(cudaGetLastError());
     return 0;
   };
-  // One host thread per worker stream: each enqueues its own points (i = k, k + nw, ...), so
-  // a stream whose launch queue is full blocks only its own thread, not the other streams.
+  // One host thread per worker stream: each enqueues its own batches (batch q holds points
+  // [q*B, q*B + B), worker k takes q = k, k + nw, ...), so a stream whose launch queue is full
+  // blocks only its own thread, not the other streams.
   {
+    const int nbat = (npts + B - 1) / B;
     std::vector<int> wrc(nw, 0);
     std::vector<std::string> werr(nw);
     auto feed = [&](int k) {
@@ -690,7 +735,12 @@ int pss_partial_gsms(pss_sheet *sh, int nl, const double *eps, const double *mu,
         return;
       }
       g_kprof = c->prof_on ? &kprofs[k] : nullptr;
-      for (int i = k; i < npts && !wrc[k]; i += nw) wrc[k] = run_point(i, precision, c->w[k], k == 0);
+      int idx[kMaxBatch];
+      for (int q = k; q < nbat && !wrc[k]; q += nw) {
+        const int i0 = q * B, cnt = std::min(B, npts - i0);
+        for (int b = 0; b < cnt; ++b) idx[b] = i0 + b;
+        wrc[k] = run_batch(idx, cnt, precision, c->w[k], k == 0);
+      }
       g_kprof = nullptr;
       if (wrc[k]) werr[k] = pss_last_error();
     };
@@ -716,8 +766,10 @@ int pss_partial_gsms(pss_sheet *sh, int nl, const double *eps, const double *mu,
       std::vector<int> cleared(npts);
       for (int i = 0; i < npts; ++i) cleared[i] = status[i] & ~(PSS_ST_REFINE_NOCONV | PSS_ST_NONFINITE);
       PSS_CUDA_TRY(cudaMemcpy(c->status.p, cleared.data(), (size_t)npts * sizeof(int), cudaMemcpyHostToDevice));
-      for (size_t q = 0; q < redo.size(); ++q)
-        if ((rc = run_point(redo[q], PSS_FP64, c->w[q % nw], false))) return rc;
+      for (size_t q0 = 0, k = 0; q0 < redo.size(); q0 += B, ++k) {
+        const int cnt = (int)std::min<size_t>(B, redo.size() - q0);
+        if ((rc = run_batch(redo.data() + q0, cnt, PSS_FP64, c->w[k % nw], false))) return rc;
+      }
       for (auto &w : c->w) PSS_CUDA_TRY(cudaStreamSynchronize(w.st));
       PSS_CUDA_TRY(cudaMemcpy(status, c->status.p, (size_t)npts * sizeof(int), cudaMemcpyDeviceToHost));
       for (int i : redo) status[i] |= PSS_ST_FP64_FALLBACK;
@@ -803,7 +855,7 @@ int pss_fill_matrix(pss_sheet *sh, int nl, const double *eps, const double *mu, 
   if (rc) return rc;
   Worker &w = c->w[0];
   if ((rc = refresh_jk_cache(sh, psi1, psi2, u / sh->upm, w.st))) return rc;
-  if ((rc = ensure_worker(w, sh, 1, PSS_FP64, false))) return rc;
+  if ((rc = ensure_worker(w, sh, 1, PSS_FP64, false, 1))) return rc;
   pss_fill_pairs(sh->G, c->params.as<PointParams>(), sh->cache.jk, tabs[0].t1, tabs[0].t2, tabs[0].mmax,
                  w.zb.as<cd>(), w.st);
   pss_fill_assemble(sh->G, c->params.as<PointParams>(), w.zb.as<cd>(), w.z64.as<cd>(), nullptr, nullptr, sh->nbf,
@@ -891,7 +943,7 @@ int pss_lu_solve(pss_ctx *c, int n, const double *Z, int nrhs, const double *B, 
   std::vector<cd> h(nn);
   for (size_t m = 0; m < (size_t)n; ++m)
     for (size_t q = 0; q < (size_t)n; ++q) h[m * n + q] = mkcd(Z[2 * (m + q * n)], Z[2 * (m + q * n) + 1]);
-  if (w.z64.ensure(nn * sizeof(cd)) || w.ensure_solver(n, nrhs)) return -3;
+  if (w.z64.ensure(nn * sizeof(cd)) || w.ensure_solver(n, nrhs, 1)) return -3;
   DevBuf st_buf;
   if (st_buf.ensure(sizeof(int))) return -3;
   PSS_CUDA_TRY(cudaMemset(st_buf.p, 0, sizeof(int)));
@@ -906,7 +958,7 @@ int pss_lu_solve(pss_ctx *c, int n, const double *Z, int nrhs, const double *B, 
     PSS_CUDA_TRY(cudaMemcpy(w.zr.p, hr.data(), nn * sizeof(float), cudaMemcpyHostToDevice));
     PSS_CUDA_TRY(cudaMemcpy(w.zi.p, hi.data(), nn * sizeof(float), cudaMemcpyHostToDevice));
   }
-  if ((rc = w.factor_solve(n, n, precision, nrhs, kMaxRefine, st_buf.as<int>()))) return rc;
+  if ((rc = w.factor_solve(n, 1, precision, nrhs, kMaxRefine, st_buf.as<int>()))) return rc;
   PSS_CUDA_TRY(cudaStreamSynchronize(st));
   PSS_CUDA_TRY(cudaGetLastError());
   int hs = 0;
@@ -915,7 +967,7 @@ int pss_lu_solve(pss_ctx *c, int n, const double *Z, int nrhs, const double *B, 
     // stalled refinement: FP64 factorisation of the original matrix
     PSS_CUDA_TRY(cudaMemset(st_buf.p, 0, sizeof(int)));
     PSS_CUDA_TRY(cudaMemcpy(w.z64.p, h.data(), nn * sizeof(cd), cudaMemcpyHostToDevice));
-    if ((rc = w.factor_solve(n, n, PSS_FP64, nrhs, 0, st_buf.as<int>()))) return rc;
+    if ((rc = w.factor_solve(n, 1, PSS_FP64, nrhs, 0, st_buf.as<int>()))) return rc;
     PSS_CUDA_TRY(cudaStreamSynchronize(st));
     PSS_CUDA_TRY(cudaMemcpy(&hs, st_buf.p, sizeof(int), cudaMemcpyDeviceToHost));
     hs |= PSS_ST_FP64_FALLBACK;
@@ -956,7 +1008,7 @@ int pss_schur_update(pss_ctx *c, int m, int n, int k, const float *Lr, const flo
   PSS_CUDA_TRY(cudaMemcpyAsync(ar.p, hr.data(), total * sizeof(float), cudaMemcpyHostToDevice, st));
   PSS_CUDA_TRY(cudaMemcpyAsync(ai.p, hi.data(), total * sizeof(float), cudaMemcpyHostToDevice, st));
   PSS_CUDA_TRY(cudaMemsetAsync(err.p, 0, sizeof(int), st));
-  int rc = pss_cgemm_tc(ar.as<float>(), ai.as<float>(), ld, k, m, k, n, 0, k, ws.p, ws.n, err.as<int>(), st);
+  int rc = pss_cgemm_tc(ar.as<float>(), ai.as<float>(), ld, 0, 1, k, m, k, n, 0, k, ws.p, ws.n, err.as<int>(), st);
   if (rc) return rc;
   PSS_CUDA_TRY(cudaMemcpyAsync(hr.data(), ar.p, total * sizeof(float), cudaMemcpyDeviceToHost, st));
   PSS_CUDA_TRY(cudaMemcpyAsync(hi.data(), ai.p, total * sizeof(float), cudaMemcpyDeviceToHost, st));

@@ -123,12 +123,18 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
 
 struct GemmArgs {
   float *Cr, *Ci;
-  long long ldc;
-  int m0, n0;   // C offset of the update (rows, columns)
-  int M, N;     // extent of the update
-  int nk;       // number of BK slices (K / 16, K padded with zeros)
-  int *err;
+  long long ldc, ms;  // leading dimension; elements between the matrices of the batch
+  int m0, n0;         // C offset of the update (rows, columns)
+  int M, N;           // extent of the update
+  int nk;             // number of BK slices (K / 16, K padded with zeros)
+  int nb;             // matrices in the batch
+  int *err;           // one error word per matrix
 };
+
+// A bounded wait gave up: every matrix of the batch is marked (its update is incomplete).
+__device__ __forceinline__ void fail_all(const GemmArgs &g) {
+  for (int b = 0; b < g.nb; ++b) atomicExch(g.err + b, kErrTimeout);
+}
 
 __global__ void __launch_bounds__(192, 1) k_cgemm_tf32x3(const __grid_constant__ CUtensorMap mapA,
                                                          const __grid_constant__ CUtensorMap mapB, GemmArgs g) {
@@ -144,7 +150,8 @@ __global__ void __launch_bounds__(192, 1) k_cgemm_tf32x3(const __grid_constant__
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int tiles_m = (g.M + BM - 1) / BM, tiles_n = (g.N + BN - 1) / BN;
-  const int ntiles = tiles_m * tiles_n;
+  const int per = tiles_m * tiles_n;  // tiles per matrix
+  const int ntiles = per * g.nb;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
@@ -170,20 +177,22 @@ __global__ void __launch_bounds__(192, 1) k_cgemm_tf32x3(const __grid_constant__
       int last_ph[STAGES];  // parity of the last phase each stage was loaded for (-1: never)
       for (int q = 0; q < STAGES; ++q) last_ph[q] = -1;
       for (int t = blockIdx.x; t < ntiles && !*(volatile int *)abort_flag; t += gridDim.x) {
-        const int mt = t / tiles_n, nt = t % tiles_n;
+        const int b = t / per, tt = t % per;
+        const int mt = tt / tiles_n, nt = tt % tiles_n;
         for (int kb = 0; kb < g.nk; ++kb) {
-          if (!mbar_wait(&empty[s], ph ^ 1)) { atomicExch(g.err, kErrTimeout); *(volatile int *)abort_flag = 1; break; }
+          if (!mbar_wait(&empty[s], ph ^ 1)) { fail_all(g); *(volatile int *)abort_flag = 1; break; }
           mbar_expect_tx(&full[s], STAGE_BYTES);
           unsigned char *st = base + s * STAGE_BYTES;
-          for (int p = 0; p < 4; ++p) tma_load_3d(st + p * TILE_BYTES, &mapA, &full[s], kb * BK, mt * BM, p);
-          for (int p = 0; p < 4; ++p) tma_load_3d(st + (4 + p) * TILE_BYTES, &mapB, &full[s], kb * BK, nt * BN, p);
+          for (int p = 0; p < 4; ++p) tma_load_3d(st + p * TILE_BYTES, &mapA, &full[s], kb * BK, mt * BM, 4 * b + p);
+          for (int p = 0; p < 4; ++p)
+            tma_load_3d(st + (4 + p) * TILE_BYTES, &mapB, &full[s], kb * BK, nt * BN, 4 * b + p);
           last_ph[s] = (int)ph;
           if (++s == STAGES) { s = 0; ph ^= 1; }
         }
       }
       // Copies still in flight land before the shared memory is released (bounded).
       for (int q = 0; q < STAGES; ++q)
-        if (last_ph[q] >= 0 && !mbar_wait(&full[q], (uint32_t)last_ph[q])) atomicExch(g.err, kErrTimeout);
+        if (last_ph[q] >= 0 && !mbar_wait(&full[q], (uint32_t)last_ph[q])) fail_all(g);
     }
   } else if (warp == 1) {
     if (lane == 0) {  // ---------------- MMA issuer ----------------
@@ -194,7 +203,7 @@ __global__ void __launch_bounds__(192, 1) k_cgemm_tf32x3(const __grid_constant__
       for (int t = blockIdx.x; t < ntiles && !*(volatile int *)abort_flag; t += gridDim.x, ++local) {
         const int ab = local & 1;
         const uint32_t aph = (local >> 1) & 1;
-        if (!mbar_wait(&acce[ab], aph ^ 1)) { atomicExch(g.err, kErrTimeout); *(volatile int *)abort_flag = 1; break; }
+        if (!mbar_wait(&acce[ab], aph ^ 1)) { fail_all(g); *(volatile int *)abort_flag = 1; break; }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t dr = tmem + ab * 256, di = dr + 128;
         bool ok = true;
@@ -225,12 +234,12 @@ __global__ void __launch_bounds__(192, 1) k_cgemm_tf32x3(const __grid_constant__
           mma_commit(&empty[s]);  // stage s free once these MMAs have read it
           if (++s == STAGES) { s = 0; ph ^= 1; }
         }
-        if (!ok) { atomicExch(g.err, kErrTimeout); *(volatile int *)abort_flag = 1; break; }
+        if (!ok) { fail_all(g); *(volatile int *)abort_flag = 1; break; }
         mma_commit(&accf[ab]);    // accumulators ready for the epilogue
       }
       // Every MMA this thread issued completes before the accumulators are freed (bounded).
       mma_commit(drain);
-      if (!mbar_wait(drain, 0)) atomicExch(g.err, kErrTimeout);
+      if (!mbar_wait(drain, 0)) fail_all(g);
     }
   } else {  // ---------------- epilogue: warps 2..5 ----------------
     const int lg = warp & 3;             // TMEM lane group this warp may access
@@ -244,12 +253,14 @@ __global__ void __launch_bounds__(192, 1) k_cgemm_tf32x3(const __grid_constant__
       if (stop) break;
       const bool ok = __all_sync(0xffffffffu, mbar_wait(&accf[ab], aph));
       if (!ok) {
-        if (lane == 0) { atomicExch(g.err, kErrTimeout); *(volatile int *)abort_flag = 1; }
+        if (lane == 0) { fail_all(g); *(volatile int *)abort_flag = 1; }
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const int mt = t / tiles_n, nt = t % tiles_n;
+      const int b = t / per, tt = t % per;
+      const int mt = tt / tiles_n, nt = tt % tiles_n;
       const int r = mt * BM + row_in_tile;
+      float *Cr = g.Cr + b * g.ms, *Ci = g.Ci + b * g.ms;
       const uint32_t trow = tmem + ((uint32_t)(lg * 32) << 16) + ab * 256;
       for (int ch = 0; ch < BN / 32; ++ch) {
         float vr[32], vi[32];
@@ -257,8 +268,8 @@ __global__ void __launch_bounds__(192, 1) k_cgemm_tf32x3(const __grid_constant__
         tmem_ld32(trow + 128 + ch * 32, vi);
         const int c = nt * BN + ch * 32;
         if (r < g.M) {
-          float *pr = g.Cr + (long long)(g.m0 + r) * g.ldc + g.n0 + c;
-          float *pi = g.Ci + (long long)(g.m0 + r) * g.ldc + g.n0 + c;
+          float *pr = Cr + (long long)(g.m0 + r) * g.ldc + g.n0 + c;
+          float *pi = Ci + (long long)(g.m0 + r) * g.ldc + g.n0 + c;
           if (c + 32 <= g.N && (((uintptr_t)pr | (uintptr_t)pi) & 15) == 0) {
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
@@ -293,9 +304,11 @@ __device__ __forceinline__ float tf32_rna(float x) {
   return __uint_as_float(r);
 }
 
-// A planes [4][M][KP]: rows r of L21 (matrix rows m0 + r, columns k0 .. k0+K-1).
-__global__ void k_split_a(const float *__restrict__ Ar, const float *__restrict__ Ai, long long ld, int m0, int M,
-                          int k0, int K, int KP, float *__restrict__ out) {
+// A planes [nb][4][M][KP]: rows r of L21 (matrix rows m0 + r, columns k0 .. k0+K-1).
+__global__ void k_split_a(const float *__restrict__ Ar0, const float *__restrict__ Ai0, long long ld, long long ms,
+                          int m0, int M, int k0, int K, int KP, float *__restrict__ out0) {
+  const float *Ar = Ar0 + blockIdx.y * ms, *Ai = Ai0 + blockIdx.y * ms;
+  float *out = out0 + (long long)blockIdx.y * 4 * M * KP;
   const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (idx >= (long long)M * KP) return;
   const int r = (int)(idx / KP), k = (int)(idx % KP);
@@ -312,10 +325,12 @@ __global__ void k_split_a(const float *__restrict__ Ar, const float *__restrict_
   out[3 * pl + idx] = tf32_rna(xi - hi);
 }
 
-// B planes [4][N][KP]: B[n][k] = U12[k][n] (matrix rows k0 + k, columns n0 + n).
-__global__ void k_split_b(const float *__restrict__ Ar, const float *__restrict__ Ai, long long ld, int k0, int K,
-                          int n0, int N, int KP, float *__restrict__ out) {
+// B planes [nb][4][N][KP]: B[n][k] = U12[k][n] (matrix rows k0 + k, columns n0 + n).
+__global__ void k_split_b(const float *__restrict__ Ar0, const float *__restrict__ Ai0, long long ld, long long ms,
+                          int k0, int K, int n0, int N, int KP, float *__restrict__ out0) {
   __shared__ float tr[32][33], ti[32][33];
+  const float *Ar = Ar0 + blockIdx.z * ms, *Ai = Ai0 + blockIdx.z * ms;
+  float *out = out0 + (long long)blockIdx.z * 4 * N * KP;
   const int nb = blockIdx.x * 32, kb = blockIdx.y * 32;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
   for (int y = ty; y < 32; y += 8) {
@@ -354,8 +369,8 @@ int get_encoder() {
   return 0;
 }
 
-int make_map(CUtensorMap *m, const float *planes, int rows, int KP) {
-  cuuint64_t dims[3] = {(cuuint64_t)KP, (cuuint64_t)rows, 4};
+int make_map(CUtensorMap *m, const float *planes, int rows, int KP, int nplanes) {
+  cuuint64_t dims[3] = {(cuuint64_t)KP, (cuuint64_t)rows, (cuuint64_t)nplanes};
   cuuint64_t strides[2] = {(cuuint64_t)KP * 4, (cuuint64_t)rows * KP * 4};
   cuuint32_t box[3] = {BK, BM, 1};
   cuuint32_t es[3] = {1, 1, 1};
@@ -375,17 +390,19 @@ DeviceOnce g_setup;
 
 }  // namespace
 
-// Workspace for the split operands of an update with up to Mmax rows / Nmax columns, K<=KP.
-size_t pss_tc_ws_bytes(int Mmax, int Nmax, int KP) {
-  return 4 * sizeof(float) * ((size_t)Mmax * KP + (size_t)Nmax * KP) + 1024;
+// Workspace for the split operands of a batch of nb updates with up to Mmax rows / Nmax
+// columns, K <= KP.
+size_t pss_tc_ws_bytes(int Mmax, int Nmax, int KP, int nb) {
+  return 4 * sizeof(float) * ((size_t)Mmax * KP + (size_t)Nmax * KP) * nb + 1024;
 }
 
+// For each matrix b < nb (at Ar/Ai + b*ms):
 // C[m0:m0+M, n0:n0+N] -= A[m0:m0+M, k0:k0+K] * A[k0:k0+K, n0:n0+N] on FP32 planes.
-int pss_cgemm_tc(float *Ar, float *Ai, long long ld, int m0, int M, int n0, int N, int k0, int K, void *ws,
-                 size_t ws_bytes, int *err, cudaStream_t st) {
-  if (M <= 0 || N <= 0 || K <= 0) return 0;
+int pss_cgemm_tc(float *Ar, float *Ai, long long ld, long long ms, int nb, int m0, int M, int n0, int N, int k0,
+                 int K, void *ws, size_t ws_bytes, int *err, cudaStream_t st) {
+  if (M <= 0 || N <= 0 || K <= 0 || nb <= 0) return 0;
   const int KP = ((K + BK - 1) / BK) * BK;
-  if (ws_bytes < pss_tc_ws_bytes(M, N, KP)) { pss_set_error("tensor-core GEMM workspace too small"); return -4; }
+  if (ws_bytes < pss_tc_ws_bytes(M, N, KP, nb)) { pss_set_error("tensor-core GEMM workspace too small"); return -4; }
   if (get_encoder()) return -3;
   int dev = 0;
   PSS_CUDA_TRY(cudaGetDevice(&dev));
@@ -399,21 +416,21 @@ int pss_cgemm_tc(float *Ar, float *Ai, long long ld, int m0, int M, int n0, int 
       }))
     return rc;
   float *pa = (float *)(((uintptr_t)ws + 255) & ~(uintptr_t)255);
-  float *pb = pa + 4 * (size_t)M * KP;
+  float *pb = pa + 4 * (size_t)M * KP * nb;
   pb = (float *)(((uintptr_t)pb + 255) & ~(uintptr_t)255);
   pss_count_launch();
-  k_split_a<<<cdiv_u((long long)M * KP, 256), 256, 0, st>>>(Ar, Ai, ld, m0, M, k0, K, KP, pa);
+  k_split_a<<<dim3(cdiv_u((long long)M * KP, 256), nb), 256, 0, st>>>(Ar, Ai, ld, ms, m0, M, k0, K, KP, pa);
   pss_count_launch();
-  k_split_b<<<dim3(cdiv_u(N, 32), cdiv_u(KP, 32)), 256, 0, st>>>(Ar, Ai, ld, k0, K, n0, N, KP, pb);
+  k_split_b<<<dim3(cdiv_u(N, 32), cdiv_u(KP, 32), nb), 256, 0, st>>>(Ar, Ai, ld, ms, k0, K, n0, N, KP, pb);
   CUtensorMap ma, mb;
-  if (make_map(&ma, pa, M, KP) || make_map(&mb, pb, N, KP)) return -3;
-  GemmArgs g{Ar, Ai, ld, m0, n0, M, N, KP / BK, err};
-  const int tiles = ((M + BM - 1) / BM) * ((N + BN - 1) / BN);
+  if (make_map(&ma, pa, M, KP, 4 * nb) || make_map(&mb, pb, N, KP, 4 * nb)) return -3;
+  GemmArgs g{Ar, Ai, ld, ms, m0, n0, M, N, KP / BK, nb, err};
+  const int tiles = ((M + BM - 1) / BM) * ((N + BN - 1) / BN) * nb;
   const int grid = std::min(tiles, g_num_sms[dev]);
   const int tok = pss_prof_begin(st);
   pss_count_launch();
   k_cgemm_tf32x3<<<grid, 192, SMEM_BYTES, st>>>(ma, mb, g);
-  pss_prof_end(tok, st, PSS_PROF_TC_UPDATE, 8.0 * M * (double)N * K);
+  pss_prof_end(tok, st, PSS_PROF_TC_UPDATE, 8.0 * nb * M * (double)N * K);
   PSS_CUDA_TRY(cudaGetLastError());
   return 0;
 }

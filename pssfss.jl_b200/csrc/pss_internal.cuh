@@ -147,34 +147,46 @@ void pss_project(int nbf, int nmodes, const cd *bf, const double *tobs, const cd
                  cudaStream_t st);
 
 // Dense complex LU and solves (pss_lu.cu); matrices row-major with leading dimension ld.
+// Batched forms factor nb matrices of order n at A + b*ms (elements), pivots at ipiv + b*n,
+// info words at info + b; all matrices advance together, one launch per step.
 int pss_lu64(int n, cd *A, long long ld, int *ipiv, int *info, void *ws, size_t ws_bytes, cudaStream_t st);
 int pss_lu32(int n, float *Ar, float *Ai, long long ld, int *ipiv, int *info, void *ws, size_t ws_bytes,
              cudaStream_t st);
-size_t pss_lu_ws_bytes(int n, int precision);
+int pss_lu64_batched(int n, int nb, cd *A, long long ld, long long ms, int *ipiv, int *info, void *ws,
+                     size_t ws_bytes, cudaStream_t st);
+int pss_lu32_batched(int n, int nb, float *Ar, float *Ai, long long ld, long long ms, int *ipiv, int *info,
+                     void *ws, size_t ws_bytes, cudaStream_t st);
+size_t pss_lu_ws_bytes(int n, int precision, int nb = 1);
 
-// Tensor-core (tcgen05, 3xTF32) complex Schur update on FP32 planes (pss_gemm_tc.cu):
-// A[m0:m0+M, n0:n0+N] -= A[m0:m0+M, k0:k0+K] * A[k0:k0+K, n0:n0+N], row-major, leading
-// dimension ld; ws holds the split operands (pss_tc_ws_bytes(M, N, K rounded up to 16)).
-// A bounded pipeline wait that gives up writes -1 to *err.
-size_t pss_tc_ws_bytes(int Mmax, int Nmax, int KP);
-int pss_cgemm_tc(float *Ar, float *Ai, long long ld, int m0, int M, int n0, int N, int k0, int K, void *ws,
-                 size_t ws_bytes, int *err, cudaStream_t st);
+// Tensor-core (tcgen05, 3xTF32) complex Schur update on FP32 planes (pss_gemm_tc.cu), for
+// each of nb matrices A_b = A + b*ms (elements):
+//   A_b[m0:m0+M, n0:n0+N] -= A_b[m0:m0+M, k0:k0+K] * A_b[k0:k0+K, n0:n0+N],
+// row-major, leading dimension ld; ws holds the split operands
+// (pss_tc_ws_bytes(M, N, K rounded up to 16, nb)).  A bounded pipeline wait that gives up
+// writes -1 to err[b].
+size_t pss_tc_ws_bytes(int Mmax, int Nmax, int KP, int nb = 1);
+int pss_cgemm_tc(float *Ar, float *Ai, long long ld, long long ms, int nb, int m0, int M, int n0, int N, int k0,
+                 int K, void *ws, size_t ws_bytes, int *err, cudaStream_t st);
 
 // Triangular solves and refinement (pss_trsv.cu).  The factor is either FP64 (LU64) or
 // FP32 planes (Lr, Li); pass the other as null.
 struct SolveWS {
-  int n = 0, nblk = 0, epoch = 0;
-  cd *Dinv = nullptr;      // inverses of the 64x64 diagonal blocks (L and U)
-  int *perm = nullptr;     // pivot permutation
-  int *ctrl = nullptr;     // ticket, error flag, done flag, per-block epoch flags
-  double *norms = nullptr; // refinement norms
-  void bind(void *base, int n_);
+  int n = 0, nblk = 0, nb = 0, epoch = 0;
+  long long dstride = 0;   // elements between the matrices' diagonal-block inverses
+  int cstride = 0;         // ints between the matrices' control words
+  cd *Dinv = nullptr;      // inverses of the 64x64 diagonal blocks (L and U), per matrix
+  int *perm = nullptr;     // pivot permutations
+  int *ctrl = nullptr;     // per matrix: ticket, error flag, converged flag, per-block epoch flags
+  double *norms = nullptr; // refinement norms, per matrix
+  void bind(void *base, int n_, int nb_ = 1);
 };
-size_t pss_solve_ws_bytes(int n);
-int pss_solve_prepare(SolveWS &ws, const cd *LU64, const float *Lr, const float *Li, long long ld, const int *ipiv,
-                      cudaStream_t st);
-int pss_solve_lu(SolveWS &ws, const cd *LU64, const float *Lr, const float *Li, long long ld, int nrhs, const cd *B,
-                 cd *X, const int *done, cudaStream_t st);
-int pss_refine(SolveWS &ws, const cd *A, long long ld, const float *Lr, const float *Li, int nrhs, const cd *B,
-               cd *X, cd *R, cd *D, int maxit, int *status, cudaStream_t st);
-void pss_solve_status(SolveWS &ws, int *status, cudaStream_t st);
+// Batched over nb matrices: factors at LU64 (or Lr/Li) + b*ms, ipiv + b*n, right-hand sides
+// and solutions (n x nrhs column-major) at B/X + b*vs, status[b].
+size_t pss_solve_ws_bytes(int n, int nb = 1);
+int pss_solve_prepare(SolveWS &ws, int nb, const cd *LU64, const float *Lr, const float *Li, long long ld,
+                      long long ms, const int *ipiv, cudaStream_t st);
+int pss_solve_lu(SolveWS &ws, int nb, const cd *LU64, const float *Lr, const float *Li, long long ld, long long ms,
+                 int nrhs, const cd *B, cd *X, long long vs, int use_done, cudaStream_t st);
+int pss_refine(SolveWS &ws, int nb, const cd *A, long long ld, long long ms, const float *Lr, const float *Li,
+               int nrhs, const cd *B, cd *X, cd *R, cd *D, long long vs, int maxit, int *status, cudaStream_t st);
+void pss_solve_status(SolveWS &ws, int nb, int *status, cudaStream_t st);

@@ -60,6 +60,20 @@ struct Mat {
     if constexpr (F32) { ((float *)a)[r * ld + c] = v.x; ai[r * ld + c] = v.y; }
     else ((cd *)a)[r * ld + c] = cd{v.x, v.y};
   }
+  // matrix b of a batch whose matrices are ms elements apart
+  __host__ __device__ __forceinline__ Mat at(int b, long long ms) const {
+    if constexpr (F32) return Mat{(float *)a + b * ms, ai + b * ms, ld};
+    else return Mat{(cd *)a + b * ms, nullptr, ld};
+  }
+};
+
+// A batch of independent factorisations of the same order: matrix b at M.at(b, ms), its
+// pivots at ipiv + b*n, its info word at info + b, its panel interchange list at
+// xlist + b*kListInts.  Every kernel below takes the matrix index from its grid.
+struct LuBatch {
+  long long ms;
+  int n;
+  int *ipiv, *info, *xlist;
 };
 
 constexpr int kPanelRows = 512;     // panel rows per CTA
@@ -116,13 +130,16 @@ __device__ __forceinline__ unsigned long long warp_max_key(unsigned long long k,
 // the live columns only.  Multipliers overwrite the rows in place, pivot rows keep their U
 // entries, so the final write-back is a coalesced copy to the permuted positions.
 template <bool F32, int W>
-__global__ void __launch_bounds__(kPanelThreads) k_panel(Mat<F32> M, int row0, int nrows, int col0, int w,
-                                                         int *ipiv, int *info, int *xlist) {
+__global__ void __launch_bounds__(kPanelThreads) k_panel(Mat<F32> M0, LuBatch bt, int row0, int nrows, int col0,
+                                                         int w) {
   using E = typename Prec<F32>::E;
   using Rl = typename Prec<F32>::R;
   cg::cluster_group cluster = cg::this_cluster();
   const int cs = (int)cluster.num_blocks();
   const int crank = (int)cluster.block_rank();
+  const int bidx = blockIdx.x / cs;  // one cluster per matrix of the batch
+  const Mat<F32> M = M0.at(bidx, bt.ms);
+  int *ipiv = bt.ipiv + (long long)bidx * bt.n, *info = bt.info + bidx, *xlist = bt.xlist + bidx * kListInts;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   constexpr int NW = kPanelThreads / 32;
   extern __shared__ __align__(16) unsigned char panel_smem[];
@@ -261,9 +278,11 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(Mat<F32> M, int row0, i
 // rows xlist[1+kMaxMov..]) to columns [0, ncol) except the panel's own [skip0, skip0 + w):
 // every thread gathers its column's moved entries first and scatters them after.
 template <bool F32>
-__global__ void __launch_bounds__(kSwpThreads) k_laswp(Mat<F32> M, const int *__restrict__ xlist, int ncol,
-                                                       int skip0, int w) {
+__global__ void __launch_bounds__(kSwpThreads) k_laswp(Mat<F32> M0, long long ms, const int *__restrict__ xlist0,
+                                                       int ncol, int skip0, int w) {
   using E = typename Prec<F32>::E;
+  const Mat<F32> M = M0.at(blockIdx.y, ms);
+  const int *xlist = xlist0 + blockIdx.y * kListInts;
   constexpr int MOV = F32 ? 2 * 32 : 2 * 16;  // 2 x panel width
   __shared__ int dst[MOV], src[MOV];
   __shared__ E stage[MOV][kSwpThreads];
@@ -287,8 +306,9 @@ __global__ void __launch_bounds__(kSwpThreads) k_laswp(Mat<F32> M, const int *__
 // Runtime loops keep the code small: each instruction of a fully unrolled triangle would
 // run once per launch and miss the instruction cache.
 template <bool F32, int W>
-__global__ void __launch_bounds__(128) k_trsm_small(Mat<F32> M, int k0, int w, int c0, int c1) {
+__global__ void __launch_bounds__(128) k_trsm_small(Mat<F32> M0, long long ms, int k0, int w, int c0, int c1) {
   using E = typename Prec<F32>::E;
+  const Mat<F32> M = M0.at(blockIdx.y, ms);
   __shared__ E L[W][W];
   __shared__ E xs[W][128];
   for (int e = threadIdx.x; e < W * W; e += blockDim.x) {
@@ -318,7 +338,9 @@ __global__ void __launch_bounds__(128) k_trsm_small(Mat<F32> M, int k0, int w, i
 }
 
 // C[r0:r1, c0:c1] -= A[r0:r1, k0:k0+kb] * A[k0:k0+kb, c0:c1]  (FP64 complex, SIMT, 64x64 tiles)
-__global__ void __launch_bounds__(256) k_gemm64(cd *A, long long ld, int r0, int r1, int c0, int c1, int k0, int kb) {
+__global__ void __launch_bounds__(256) k_gemm64(cd *A0, long long ms, long long ld, int r0, int r1, int c0, int c1,
+                                                int k0, int kb) {
+  cd *A = A0 + blockIdx.z * ms;
   __shared__ cd As[16][64 + 1];
   __shared__ cd Bs[16][64 + 1];
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
@@ -362,8 +384,9 @@ __global__ void __launch_bounds__(256) k_gemm64(cd *A, long long ld, int r0, int
 }
 
 // FP32 planes variant (SIMT).
-__global__ void __launch_bounds__(256) k_gemm32(float *Ar, float *Ai, long long ld, int r0, int r1, int c0, int c1,
-                                                int k0, int kb) {
+__global__ void __launch_bounds__(256) k_gemm32(float *Ar0, float *Ai0, long long ms, long long ld, int r0, int r1,
+                                                int c0, int c1, int k0, int kb) {
+  float *Ar = Ar0 + blockIdx.z * ms, *Ai = Ai0 + blockIdx.z * ms;
   __shared__ float Asr[16][128 + 4], Asi[16][128 + 4];
   __shared__ float Bsr[16][128 + 4], Bsi[16][128 + 4];
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
@@ -412,9 +435,9 @@ __global__ void __launch_bounds__(256) k_gemm32(float *Ar, float *Ai, long long 
 }
 
 // ------------------------------- host side -------------------------------
+// Every launcher runs one step for all nb matrices of a batch (grid dimension = matrix).
 template <bool F32>
-int launch_panel(Mat<F32> M, int row0, int nrows, int col0, int w, int *ipiv, int *info, int *xlist,
-                 cudaStream_t st) {
+int launch_panel(Mat<F32> M, const LuBatch &bt, int nb, int row0, int nrows, int col0, int w, cudaStream_t st) {
   const int cs = (nrows + kPanelRows - 1) / kPanelRows;
   const int Wt = F32 ? 32 : 16;
   if (cs > kMaxCluster || w > Wt) {
@@ -422,7 +445,7 @@ int launch_panel(Mat<F32> M, int row0, int nrows, int col0, int w, int *ipiv, in
     return -6;
   }
   auto kern = k_panel<F32, (F32 ? 32 : 16)>;
-  constexpr int smem = kPanelRows * (F32 ? 32 : 16) * (int)sizeof(typename Prec<F32>::E);  // multipliers
+  constexpr int smem = kPanelRows * (F32 ? 32 : 16) * (int)sizeof(typename Prec<F32>::E);  // the panel rows
   static DeviceOnce once;
   if (int rc = device_once(once, [&] {
         PSS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
@@ -431,7 +454,7 @@ int launch_panel(Mat<F32> M, int row0, int nrows, int col0, int w, int *ipiv, in
       }))
     return rc;
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(cs);
+  cfg.gridDim = dim3(cs * nb);  // one cluster of cs CTAs per matrix
   cfg.blockDim = dim3(kPanelThreads);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
@@ -444,68 +467,71 @@ int launch_panel(Mat<F32> M, int row0, int nrows, int col0, int w, int *ipiv, in
   cfg.numAttrs = 1;
   pss_count_launch();
   const int tok = pss_prof_begin(st);
-  PSS_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, M, row0, nrows, col0, w, ipiv, info, xlist));
-  // algorithmic bytes: the panel read once and written once
-  pss_prof_end(tok, st, PSS_PROF_PANEL, 2.0 * nrows * w * (F32 ? 8.0 : 16.0));
+  PSS_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, M, bt, row0, nrows, col0, w));
+  // algorithmic bytes: every panel read once and written once
+  pss_prof_end(tok, st, PSS_PROF_PANEL, 2.0 * nb * nrows * w * (F32 ? 8.0 : 16.0));
   return 0;
 }
 
 template <bool F32>
-void launch_laswp(Mat<F32> M, const int *xlist, int n, int k0, int w, cudaStream_t st) {
+void launch_laswp(Mat<F32> M, const LuBatch &bt, int nb, int n, int k0, int w, cudaStream_t st) {
   if (n - w <= 0) return;
   pss_count_launch();
-  k_laswp<F32><<<cdiv_u(n - w, kSwpThreads), kSwpThreads, 0, st>>>(M, xlist, n, k0, w);
+  k_laswp<F32><<<dim3(cdiv_u(n - w, kSwpThreads), nb), kSwpThreads, 0, st>>>(M, bt.ms, bt.xlist, n, k0, w);
 }
 
 template <bool F32>
-void launch_trsm(Mat<F32> M, int k0, int w, int c0, int c1, cudaStream_t st) {
+void launch_trsm(Mat<F32> M, long long ms, int nb, int k0, int w, int c0, int c1, cudaStream_t st) {
   if (c1 <= c0) return;
   pss_count_launch();
+  const dim3 grid(cdiv_u(c1 - c0, 128), nb);
   if constexpr (F32) {
-    if (w <= 16) k_trsm_small<true, 16><<<cdiv_u(c1 - c0, 128), 128, 0, st>>>(M, k0, w, c0, c1);
-    else k_trsm_small<true, 32><<<cdiv_u(c1 - c0, 128), 128, 0, st>>>(M, k0, w, c0, c1);
+    if (w <= 16) k_trsm_small<true, 16><<<grid, 128, 0, st>>>(M, ms, k0, w, c0, c1);
+    else k_trsm_small<true, 32><<<grid, 128, 0, st>>>(M, ms, k0, w, c0, c1);
   } else {  // FP64 panels are at most 16 wide
-    k_trsm_small<false, 16><<<cdiv_u(c1 - c0, 128), 128, 0, st>>>(M, k0, w, c0, c1);
+    k_trsm_small<false, 16><<<grid, 128, 0, st>>>(M, ms, k0, w, c0, c1);
   }
 }
 
-void launch_gemm(Mat<false> M, int r0, int r1, int c0, int c1, int k0, int kb, cudaStream_t st) {
+void launch_gemm(Mat<false> M, long long ms, int nb, int r0, int r1, int c0, int c1, int k0, int kb,
+                 cudaStream_t st) {
   if (r1 <= r0 || c1 <= c0) return;
   int tok = pss_prof_begin(st);
   pss_count_launch();
-  k_gemm64<<<dim3(cdiv_u(c1 - c0, 64), cdiv_u(r1 - r0, 64)), 256, 0, st>>>((cd *)M.a, M.ld, r0, r1, c0, c1, k0, kb);
-  pss_prof_end(tok, st, PSS_PROF_SIMT_UPDATE, 8.0 * (r1 - r0) * (double)(c1 - c0) * kb);
+  k_gemm64<<<dim3(cdiv_u(c1 - c0, 64), cdiv_u(r1 - r0, 64), nb), 256, 0, st>>>((cd *)M.a, ms, M.ld, r0, r1, c0, c1,
+                                                                              k0, kb);
+  pss_prof_end(tok, st, PSS_PROF_SIMT_UPDATE, 8.0 * nb * (r1 - r0) * (double)(c1 - c0) * kb);
 }
-void launch_gemm(Mat<true> M, int r0, int r1, int c0, int c1, int k0, int kb, cudaStream_t st) {
+void launch_gemm(Mat<true> M, long long ms, int nb, int r0, int r1, int c0, int c1, int k0, int kb,
+                 cudaStream_t st) {
   if (r1 <= r0 || c1 <= c0) return;
   int tok = pss_prof_begin(st);
   pss_count_launch();
-  k_gemm32<<<dim3(cdiv_u(c1 - c0, 128), cdiv_u(r1 - r0, 128)), 256, 0, st>>>((float *)M.a, M.ai, M.ld, r0, r1, c0,
-                                                                             c1, k0, kb);
-  pss_prof_end(tok, st, PSS_PROF_SIMT_UPDATE, 8.0 * (r1 - r0) * (double)(c1 - c0) * kb);
+  k_gemm32<<<dim3(cdiv_u(c1 - c0, 128), cdiv_u(r1 - r0, 128), nb), 256, 0, st>>>((float *)M.a, M.ai, ms, M.ld, r0,
+                                                                                r1, c0, c1, k0, kb);
+  pss_prof_end(tok, st, PSS_PROF_SIMT_UPDATE, 8.0 * nb * (r1 - r0) * (double)(c1 - c0) * kb);
 }
 
-// Tensor-core workspace of an FP32 factorisation (split operand planes) and its error word.
+// Tensor-core workspace of an FP32 factorisation (split operand planes); pipeline errors
+// go to the matrices' info words (-1).
 struct TcWs {
   void *ws = nullptr;
   size_t bytes = 0;
-  int *err = nullptr;
 };
 
-void launch_gemm(Mat<false> M, int r0, int r1, int c0, int c1, int k0, int kb, const TcWs &, cudaStream_t st,
-                 int *rc) {
-  *rc = 0;
-  launch_gemm(M, r0, r1, c0, c1, k0, kb, st);
+int launch_update(Mat<false> M, const LuBatch &bt, int nb, int r0, int r1, int c0, int c1, int k0, int kb,
+                  const TcWs &, cudaStream_t st) {
+  launch_gemm(M, bt.ms, nb, r0, r1, c0, c1, k0, kb, st);
+  return 0;
 }
 // FP32: updates of at least kTcMinRows x kTcMinCols go to the tcgen05 kernel, smaller ones SIMT.
-void launch_gemm(Mat<true> M, int r0, int r1, int c0, int c1, int k0, int kb, const TcWs &tc, cudaStream_t st,
-                 int *rc) {
-  *rc = 0;
-  if (r1 - r0 >= kTcMinRows && c1 - c0 >= kTcMinCols && tc.ws) {
-    *rc = pss_cgemm_tc((float *)M.a, M.ai, M.ld, r0, r1 - r0, c0, c1 - c0, k0, kb, tc.ws, tc.bytes, tc.err, st);
-    return;
-  }
-  launch_gemm(M, r0, r1, c0, c1, k0, kb, st);
+int launch_update(Mat<true> M, const LuBatch &bt, int nb, int r0, int r1, int c0, int c1, int k0, int kb,
+                  const TcWs &tc, cudaStream_t st) {
+  if (r1 - r0 >= kTcMinRows && c1 - c0 >= kTcMinCols && tc.ws)
+    return pss_cgemm_tc((float *)M.a, M.ai, M.ld, bt.ms, nb, r0, r1 - r0, c0, c1 - c0, k0, kb, tc.ws, tc.bytes,
+                        bt.info, st);
+  launch_gemm(M, bt.ms, nb, r0, r1, c0, c1, k0, kb, st);
+  return 0;
 }
 
 // Outer blocks of NB columns, inner panels of W columns (LAPACK dgetrf order):
@@ -514,35 +540,29 @@ void launch_gemm(Mat<true> M, int r0, int r1, int c0, int c1, int k0, int kb, co
 //   2. once all interchanges of the outer block are applied, the block row of the
 //      trailing columns, U12 = L11^{-1} A12, as W-row solves plus block-row updates;
 //   3. the trailing matrix A22 -= L21 U12, one GEMM with K = NB.
+// All nb matrices of the batch advance together, one launch per step.
 template <bool F32>
-int lu_blocked(int n, Mat<F32> M, int *ipiv, int *info, int NB, int W, int *pscratch, void *tcws,
-               size_t tcws_bytes, cudaStream_t st) {
-  const TcWs tc{tcws, tcws_bytes, info};  // a pipeline timeout writes -1 to info
+int lu_blocked(int n, int nb, Mat<F32> M, const LuBatch &bt, int NB, int W, const TcWs &tc, cudaStream_t st) {
   int rc = 0;
   for (int K0 = 0; K0 < n; K0 += NB) {
     const int JB = min(NB, n - K0);
     const int E = K0 + JB;
     for (int k0 = K0; k0 < E; k0 += W) {
       const int w = min(W, E - k0);
-      if ((rc = launch_panel<F32>(M, k0, n - k0, k0, w, ipiv, info, pscratch, st))) return rc;
-      launch_laswp<F32>(M, pscratch, n, k0, w, st);
+      if ((rc = launch_panel<F32>(M, bt, nb, k0, n - k0, k0, w, st))) return rc;
+      launch_laswp<F32>(M, bt, nb, n, k0, w, st);
       if (k0 + w < E) {
-        launch_trsm<F32>(M, k0, w, k0 + w, E, st);
-        launch_gemm(M, k0 + w, n, k0 + w, E, k0, w, tc, st, &rc);
-        if (rc) return rc;
+        launch_trsm<F32>(M, bt.ms, nb, k0, w, k0 + w, E, st);
+        if ((rc = launch_update(M, bt, nb, k0 + w, n, k0 + w, E, k0, w, tc, st))) return rc;
       }
     }
     if (E < n) {
       for (int k0 = K0; k0 < E; k0 += W) {
         const int w = min(W, E - k0);
-        launch_trsm<F32>(M, k0, w, E, n, st);
-        if (k0 + w < E) {
-          launch_gemm(M, k0 + w, E, E, n, k0, w, tc, st, &rc);
-          if (rc) return rc;
-        }
+        launch_trsm<F32>(M, bt.ms, nb, k0, w, E, n, st);
+        if (k0 + w < E && (rc = launch_update(M, bt, nb, k0 + w, E, E, n, k0, w, tc, st))) return rc;
       }
-      launch_gemm(M, E, n, E, n, K0, JB, tc, st, &rc);
-      if (rc) return rc;
+      if ((rc = launch_update(M, bt, nb, E, n, E, n, K0, JB, tc, st))) return rc;
     }
   }
   PSS_CUDA_TRY(cudaGetLastError());
@@ -556,29 +576,44 @@ int pick_panel_width(int n, int want) {
 }
 
 constexpr int kNB64 = 64, kNB32 = 128;
-size_t scratch_bytes(int) { return (kListInts * sizeof(int) + 255) & ~(size_t)255; }
+size_t list_bytes(int nb) { return ((size_t)nb * kListInts * sizeof(int) + 255) & ~(size_t)255; }
 }  // namespace
 
-// Workspace: the panel's interchange list (kListInts ints), then for the FP32 factorisation
-// the split operand planes of the tensor-core trailing update.
-size_t pss_lu_ws_bytes(int n, int precision) {
-  return scratch_bytes(n) + (precision == 0 ? 0 : pss_tc_ws_bytes(n, n, kNB32));
+// Workspace of a batch of nb factorisations: the panels' interchange lists (kListInts ints
+// per matrix), then for the FP32 factorisation the split operand planes of one batched
+// tensor-core update.
+size_t pss_lu_ws_bytes(int n, int precision, int nb) {
+  return list_bytes(nb) + (precision == 0 ? 0 : pss_tc_ws_bytes(n, n, kNB32, nb));
 }
 
-int pss_lu64(int n, cd *A, long long ld, int *ipiv, int *info, void *ws, size_t ws_bytes, cudaStream_t st) {
-  if (ws_bytes < pss_lu_ws_bytes(n, 0)) { pss_set_error("LU workspace too small"); return -4; }
+int pss_lu64_batched(int n, int nb, cd *A, long long ld, long long ms, int *ipiv, int *info, void *ws,
+                     size_t ws_bytes, cudaStream_t st) {
+  if (nb <= 0) return 0;
+  if (ws_bytes < pss_lu_ws_bytes(n, 0, nb)) { pss_set_error("LU workspace too small"); return -4; }
   Mat<false> M{A, nullptr, ld};
   int W = pick_panel_width<false>(n, 16);
   if (W < 0) { pss_set_error("matrix order %d too large for the cluster panel", n); return -6; }
-  return lu_blocked<false>(n, M, ipiv, info, kNB64, W, (int *)ws, nullptr, 0, st);
+  const LuBatch bt{ms, n, ipiv, info, (int *)ws};
+  return lu_blocked<false>(n, nb, M, bt, kNB64, W, TcWs{}, st);
+}
+
+int pss_lu32_batched(int n, int nb, float *Ar, float *Ai, long long ld, long long ms, int *ipiv, int *info,
+                     void *ws, size_t ws_bytes, cudaStream_t st) {
+  if (nb <= 0) return 0;
+  if (ws_bytes < pss_lu_ws_bytes(n, 1, nb)) { pss_set_error("LU workspace too small"); return -4; }
+  Mat<true> M{Ar, Ai, ld};
+  int W = pick_panel_width<true>(n, 32);
+  if (W < 0) { pss_set_error("matrix order %d too large for the cluster panel", n); return -6; }
+  const size_t lb = list_bytes(nb);
+  const LuBatch bt{ms, n, ipiv, info, (int *)ws};
+  return lu_blocked<true>(n, nb, M, bt, kNB32, W, TcWs{(char *)ws + lb, ws_bytes - lb}, st);
+}
+
+int pss_lu64(int n, cd *A, long long ld, int *ipiv, int *info, void *ws, size_t ws_bytes, cudaStream_t st) {
+  return pss_lu64_batched(n, 1, A, ld, 0, ipiv, info, ws, ws_bytes, st);
 }
 
 int pss_lu32(int n, float *Ar, float *Ai, long long ld, int *ipiv, int *info, void *ws, size_t ws_bytes,
              cudaStream_t st) {
-  if (ws_bytes < pss_lu_ws_bytes(n, 1)) { pss_set_error("LU workspace too small"); return -4; }
-  Mat<true> M{Ar, Ai, ld};
-  int W = pick_panel_width<true>(n, 32);
-  if (W < 0) { pss_set_error("matrix order %d too large for the cluster panel", n); return -6; }
-  const size_t sb = scratch_bytes(n);
-  return lu_blocked<true>(n, M, ipiv, info, kNB32, W, (int *)ws, (char *)ws + sb, ws_bytes - sb, st);
+  return pss_lu32_batched(n, 1, Ar, Ai, ld, 0, ipiv, info, ws, ws_bytes, st);
 }

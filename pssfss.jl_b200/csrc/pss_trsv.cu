@@ -29,10 +29,21 @@ struct Fac {  // row-major factor access: FP64 interleaved or FP32 planes
   const cd *a64;
   const float *ar, *ai;
   long long ld;
+  long long ms;  // elements between the factors of a batch
   __device__ __forceinline__ cd at(long long r, long long c) const {
     if (a64) return a64[r * ld + c];
     return mkcd((double)ar[r * ld + c], (double)ai[r * ld + c]);
   }
+  __device__ __forceinline__ Fac of(int b) const {  // factor b of the batch
+    return Fac{a64 ? a64 + b * ms : nullptr, ar ? ar + b * ms : nullptr, ai ? ai + b * ms : nullptr, ld, ms};
+  }
+};
+
+// Per-matrix control words of a batch: [0] ticket, [1] error, [2] converged, [8..] flags.
+struct Ctrl {
+  int *base;
+  int stride;
+  __device__ __forceinline__ int *of(int b) const { return base + (long long)b * stride; }
 };
 
 __device__ __forceinline__ double cabs1(cd z) { return fabs(z.x) + fabs(z.y); }
@@ -65,8 +76,10 @@ __device__ __forceinline__ void post_flag(int *flags, int b, int epoch) {
 
 // Inverses of the 64x64 diagonal blocks: Dinv[(2*blk + 0)] = L_bb^{-1} (unit lower),
 // Dinv[(2*blk + 1)] = U_bb^{-1}; each 64x64 row-major FP64.
-__global__ void __launch_bounds__(64) k_diag_inv(Fac F, int n, cd *Dinv) {
+__global__ void __launch_bounds__(64) k_diag_inv(Fac F0, int n, cd *Dinv0, long long dstride) {
   const int blk = blockIdx.x, upper = blockIdx.y;
+  const Fac F = F0.of(blockIdx.z);
+  cd *Dinv = Dinv0 + blockIdx.z * dstride;
   const int r0 = blk * BS, nb = min(BS, n - r0);
   extern __shared__ cd sm[];
   cd *T = sm;            // 64 x 64 block
@@ -93,8 +106,10 @@ __global__ void __launch_bounds__(64) k_diag_inv(Fac F, int n, cd *Dinv) {
 }
 
 // perm[i] = original row that ends in position i after the LAPACK swap sequence ipiv.
-__global__ void __launch_bounds__(1024) k_ipiv_to_perm(int n, const int *ipiv, int *perm) {
+__global__ void __launch_bounds__(1024) k_ipiv_to_perm(int n, const int *ipiv0, int *perm0) {
   extern __shared__ int sp[];
+  const int *ipiv = ipiv0 + (long long)blockIdx.x * n;
+  int *perm = perm0 + (long long)blockIdx.x * n;
   for (int i = threadIdx.x; i < n; i += blockDim.x) sp[i] = i;
   __syncthreads();
   if (threadIdx.x == 0)
@@ -139,13 +154,21 @@ __device__ __forceinline__ C czero() { return C{0, 0}; }
 // the load; Dinv_b (dynamic shared memory) and the block's right-hand side are staged at
 // the start.  Blocks of X written by other CTAs are read with L1-bypassing loads.
 template <bool LOWER, bool F32, int NJ>
-__global__ void __launch_bounds__(256) k_trsv(Fac F, int n, const int *__restrict__ perm, const cd *__restrict__ B,
-                                              cd *__restrict__ X, int nrhs, int j0, const cd *__restrict__ Dinv,
-                                              int *ticket, int *flags, int epoch, int *err,
-                                              const int *__restrict__ done) {
+__global__ void __launch_bounds__(256) k_trsv(Fac F0, int n, const int *__restrict__ perm0, const cd *__restrict__ B0,
+                                              cd *__restrict__ X0, long long vs, int nrhs, int j0,
+                                              const cd *__restrict__ Dinv0, long long dstride, Ctrl ctrl, int epoch,
+                                              int use_done) {
   using T = SolveT<F32>;
   using C = typename T::C;
-  if (done && *done) return;
+  const int bm = blockIdx.y;  // matrix of the batch
+  int *cw = ctrl.of(bm);
+  if (use_done && cw[2]) return;
+  const Fac F = F0.of(bm);
+  const int *perm = perm0 + (long long)bm * n;
+  const cd *B = B0 + bm * vs;
+  cd *X = X0 + bm * vs;
+  const cd *Dinv = Dinv0 + bm * dstride;
+  int *ticket = cw, *err = cw + 1, *flags = cw + 8;
   extern __shared__ __align__(16) unsigned char smraw[];
   C *Ds = (C *)smraw;  // BS x BS, row-major
   __shared__ C y[BS][NJ];
@@ -234,10 +257,14 @@ __global__ void __launch_bounds__(256) k_trsv(Fac F, int n, const int *__restric
 }
 
 // R = B - A X with max|r_j| (norms[j]), max|x_j| (norms[kNX + j]) and ||A||_inf (norms[kNA]).
-__global__ void __launch_bounds__(256) k_resid(int n, const cd *__restrict__ A, long long ld, int nrhs,
-                                               const cd *__restrict__ X, const cd *__restrict__ B,
-                                               cd *__restrict__ R, double *norms, const int *__restrict__ done) {
-  if (done && *done) return;
+__global__ void __launch_bounds__(256) k_resid(int n, const cd *__restrict__ A0, long long ld, long long ms, int nrhs,
+                                               const cd *__restrict__ X0, const cd *__restrict__ B0,
+                                               cd *__restrict__ R0, long long vs, double *norms0, Ctrl ctrl) {
+  const int bm = blockIdx.y;
+  if (ctrl.of(bm)[2]) return;
+  const cd *A = A0 + bm * ms, *X = X0 + bm * vs, *B = B0 + bm * vs;
+  cd *R = R0 + bm * vs;
+  double *norms = norms0 + (long long)bm * kNormCount;
   const int lane = threadIdx.x & 31;
   const int row = blockIdx.x * 8 + (threadIdx.x >> 5);
   if (row < n) {
@@ -275,7 +302,10 @@ __global__ void __launch_bounds__(256) k_resid(int n, const cd *__restrict__ A, 
   }
 }
 
-__global__ void k_ir_check(int n, int nrhs, double *norms, int *done, int *status, int last, int *err) {
+__global__ void k_ir_check(int n, int nrhs, double *norms0, Ctrl ctrl, int *status0, int last) {
+  int *cw = ctrl.of(blockIdx.x);
+  int *done = cw + 2, *err = cw + 1, *status = status0 + blockIdx.x;
+  double *norms = norms0 + (long long)blockIdx.x * kNormCount;
   if (*done) return;
   const double cte = 1.1102230246251565e-16 * sqrt((double)n) * norms[kNA];
   int ok = 1, bad = 0;
@@ -292,13 +322,17 @@ __global__ void k_ir_check(int n, int nrhs, double *norms, int *done, int *statu
   norms[kNA] = 0.0;
 }
 
-__global__ void k_err_status(int *err, int *status) {
-  if (*err) *status |= PSS_ST_DEVICE_TIMEOUT;
+__global__ void k_err_status(Ctrl ctrl, int *status0) {
+  int *err = ctrl.of(blockIdx.x) + 1;
+  if (*err) status0[blockIdx.x] |= PSS_ST_DEVICE_TIMEOUT;
   *err = 0;
 }
 
-__global__ void k_axpy(long long total, cd *X, const cd *D, const int *done) {
-  if (done && *done) return;
+__global__ void k_axpy(long long total, cd *X0, const cd *D0, long long vs, Ctrl ctrl) {
+  const int bm = blockIdx.y;
+  if (ctrl.of(bm)[2]) return;
+  cd *X = X0 + bm * vs;
+  const cd *D = D0 + bm * vs;
   long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i < total) X[i] = X[i] + D[i];
 }
@@ -316,32 +350,37 @@ cudaError_t set_trsv_smem() {
 
 // ------------------------------- host side -------------------------------
 
-size_t pss_solve_ws_bytes(int n) {
+size_t pss_solve_ws_bytes(int n, int nb) {
   int nblk = (n + BS - 1) / BS;
-  return (size_t)nblk * 2 * BS * BS * sizeof(cd) + (size_t)n * sizeof(int) + (size_t)(nblk + 64) * sizeof(int) +
-         kNormCount * sizeof(double) + 256;
+  return (size_t)nb * ((size_t)nblk * 2 * BS * BS * sizeof(cd) + (size_t)n * sizeof(int) +
+                       (size_t)(nblk + 64) * sizeof(int) + kNormCount * sizeof(double)) + 512;
 }
 
-void SolveWS::bind(void *base, int n_) {
+void SolveWS::bind(void *base, int n_, int nb_) {
   n = n_;
+  nb = nb_;
   nblk = (n + BS - 1) / BS;
+  dstride = (long long)nblk * 2 * BS * BS;
+  cstride = nblk + 64;
   char *p = (char *)base;
   Dinv = (cd *)p;
-  p += (size_t)nblk * 2 * BS * BS * sizeof(cd);
+  p += (size_t)nb * dstride * sizeof(cd);
   perm = (int *)p;
-  p += (size_t)n * sizeof(int);
-  ctrl = (int *)p;  // [0] ticket, [1] err, [2] done, [8..8+nblk) flags
-  p += (size_t)(nblk + 64) * sizeof(int);
+  p += (size_t)nb * n * sizeof(int);
+  ctrl = (int *)p;  // per matrix: [0] ticket, [1] error, [2] converged, [8..8+nblk) flags
+  p += (size_t)nb * cstride * sizeof(int);
   p = (char *)(((uintptr_t)p + 15) & ~(uintptr_t)15);
   norms = (double *)p;
 }
 
-// After the LU: pivot permutation and diagonal-block inverses.  flags/epoch reset.
-int pss_solve_prepare(SolveWS &ws, const cd *LU64, const float *Lr, const float *Li, long long ld, const int *ipiv,
-                      cudaStream_t st) {
-  Fac F{LU64, Lr, Li, ld};
+// After the LU of nb matrices: pivot permutations and diagonal-block inverses; control
+// words and norms cleared, epoch reset.
+int pss_solve_prepare(SolveWS &ws, int nb, const cd *LU64, const float *Lr, const float *Li, long long ld,
+                      long long ms, const int *ipiv, cudaStream_t st) {
+  if (nb > ws.nb) { pss_set_error("solve workspace holds %d matrices, %d asked", ws.nb, nb); return -4; }
+  Fac F{LU64, Lr, Li, ld, ms};
   pss_count_launch();
-  k_ipiv_to_perm<<<1, 1024, ws.n * sizeof(int), st>>>(ws.n, ipiv, ws.perm);
+  k_ipiv_to_perm<<<nb, 1024, ws.n * sizeof(int), st>>>(ws.n, ipiv, ws.perm);
   static DeviceOnce once;
   if (int rc = device_once(once, [] {
         PSS_CUDA_TRY(
@@ -350,18 +389,19 @@ int pss_solve_prepare(SolveWS &ws, const cd *LU64, const float *Lr, const float 
       }))
     return rc;
   pss_count_launch();
-  k_diag_inv<<<dim3(ws.nblk, 2), BS, 2 * BS * BS * sizeof(cd), st>>>(F, ws.n, ws.Dinv);
-  PSS_CUDA_TRY(cudaMemsetAsync(ws.ctrl, 0, (size_t)(ws.nblk + 64) * sizeof(int), st));
-  PSS_CUDA_TRY(cudaMemsetAsync(ws.norms, 0, kNormCount * sizeof(double), st));
+  k_diag_inv<<<dim3(ws.nblk, 2, nb), BS, 2 * BS * BS * sizeof(cd), st>>>(F, ws.n, ws.Dinv, ws.dstride);
+  PSS_CUDA_TRY(cudaMemsetAsync(ws.ctrl, 0, (size_t)nb * ws.cstride * sizeof(int), st));
+  PSS_CUDA_TRY(cudaMemsetAsync(ws.norms, 0, (size_t)nb * kNormCount * sizeof(double), st));
   ws.epoch = 0;
   return 0;
 }
 
-// X = (LU)^{-1} P B (B and X distinct, n x nrhs column-major).
-int pss_solve_lu(SolveWS &ws, const cd *LU64, const float *Lr, const float *Li, long long ld, int nrhs, const cd *B,
-                 cd *X, const int *done, cudaStream_t st) {
-  Fac F{LU64, Lr, Li, ld};
-  int *ticket = ws.ctrl, *err = ws.ctrl + 1, *flags = ws.ctrl + 8;
+// X = (LU)^{-1} P B for each of nb matrices (B and X distinct, n x nrhs column-major, vs
+// elements apart).  use_done: skip matrices whose refinement has converged.
+int pss_solve_lu(SolveWS &ws, int nb, const cd *LU64, const float *Lr, const float *Li, long long ld, long long ms,
+                 int nrhs, const cd *B, cd *X, long long vs, int use_done, cudaStream_t st) {
+  Fac F{LU64, Lr, Li, ld, ms};
+  const Ctrl ctrl{ws.ctrl, ws.cstride};
   static DeviceOnce once;
   if (int rc = device_once(once, [] {
         PSS_CUDA_TRY(set_trsv_smem<true>());
@@ -373,12 +413,14 @@ int pss_solve_lu(SolveWS &ws, const cd *LU64, const float *Lr, const float *Li, 
   for (int pass = 0; pass < 2; ++pass)
     for (int j0 = 0; j0 < nrhs; j0 += kMaxRhs) {
       ++ws.epoch;
-      PSS_CUDA_TRY(cudaMemsetAsync(ticket, 0, sizeof(int), st));
+      // tickets of every matrix back to zero (the flags keep their epochs)
+      PSS_CUDA_TRY(cudaMemset2DAsync(ws.ctrl, ws.cstride * sizeof(int), 0, sizeof(int), nb, st));
       pss_count_launch();
       const bool small = nrhs - j0 <= 4;
+      const dim3 grid(ws.nblk, nb);
       auto go = [&](auto kern, size_t smem) {
-        kern<<<ws.nblk, 256, smem, st>>>(F, ws.n, ws.perm, B, X, nrhs, j0, ws.Dinv, ticket, flags, ws.epoch, err,
-                                         done);
+        kern<<<grid, 256, smem, st>>>(F, ws.n, ws.perm, B, X, vs, nrhs, j0, ws.Dinv, ws.dstride, ctrl, ws.epoch,
+                                      use_done);
       };
       const size_t s64 = BS * BS * sizeof(cd), s32 = BS * BS * sizeof(cf);
       if (pass == 0) {
@@ -393,29 +435,31 @@ int pss_solve_lu(SolveWS &ws, const cd *LU64, const float *Lr, const float *Li, 
   return 0;
 }
 
-// A timed-out wait in a solve (never expected) marks the point non-finite.
-void pss_solve_status(SolveWS &ws, int *status, cudaStream_t st) {
+// A timed-out wait in a solve (never expected) marks the point (status[b]).
+void pss_solve_status(SolveWS &ws, int nb, int *status, cudaStream_t st) {
   pss_count_launch();
-  k_err_status<<<1, 1, 0, st>>>(ws.ctrl + 1, status);
+  k_err_status<<<nb, 1, 0, st>>>(Ctrl{ws.ctrl, ws.cstride}, status);
 }
 
-// Iterative refinement of X against the FP64 matrix A (FP32 factors), up to maxit steps.
-int pss_refine(SolveWS &ws, const cd *A, long long ld, const float *Lr, const float *Li, int nrhs, const cd *B,
-               cd *X, cd *R, cd *D, int maxit, int *status, cudaStream_t st) {
-  int *done = ws.ctrl + 2, *err = ws.ctrl + 1;
+// Iterative refinement of each X_b against its FP64 matrix A_b (FP32 factors), up to
+// maxit steps; matrices that converge drop out (their converged word).
+int pss_refine(SolveWS &ws, int nb, const cd *A, long long ld, long long ms, const float *Lr, const float *Li,
+               int nrhs, const cd *B, cd *X, cd *R, cd *D, long long vs, int maxit, int *status, cudaStream_t st) {
   if (nrhs > kMaxRefRhs) { pss_set_error("refinement supports at most %d right-hand sides", kMaxRefRhs); return -1; }
-  PSS_CUDA_TRY(cudaMemsetAsync(done, 0, sizeof(int), st));
+  const Ctrl ctrl{ws.ctrl, ws.cstride};
+  // converged words of every matrix cleared
+  PSS_CUDA_TRY(cudaMemset2DAsync(ws.ctrl + 2, ws.cstride * sizeof(int), 0, sizeof(int), nb, st));
   const long long total = (long long)ws.n * nrhs;
   for (int it = 0; it <= maxit; ++it) {
     pss_count_launch();
-    k_resid<<<cdiv_u(ws.n, 8), 256, 0, st>>>(ws.n, A, ld, nrhs, X, B, R, ws.norms, done);
+    k_resid<<<dim3(cdiv_u(ws.n, 8), nb), 256, 0, st>>>(ws.n, A, ld, ms, nrhs, X, B, R, vs, ws.norms, ctrl);
     pss_count_launch();
-    k_ir_check<<<1, 1, 0, st>>>(ws.n, nrhs, ws.norms, done, status, it == maxit, err);
+    k_ir_check<<<nb, 1, 0, st>>>(ws.n, nrhs, ws.norms, ctrl, status, it == maxit);
     if (it == maxit) break;
-    int rc = pss_solve_lu(ws, nullptr, Lr, Li, ld, nrhs, R, D, done, st);
+    int rc = pss_solve_lu(ws, nb, nullptr, Lr, Li, ld, ms, nrhs, R, D, vs, 1, st);
     if (rc) return rc;
     pss_count_launch();
-    k_axpy<<<cdiv_u(total, 256), 256, 0, st>>>(total, X, D, done);
+    k_axpy<<<dim3(cdiv_u(total, 256), nb), 256, 0, st>>>(total, X, D, vs, ctrl);
   }
   PSS_CUDA_TRY(cudaGetLastError());
   return 0;
