@@ -27,7 +27,9 @@ constexpr int BM = 128, BN = 128, BK = 16, KSUB = 8;
 constexpr int STAGES = 3;
 constexpr int TILE_BYTES = BM * BK * 4;          // 8 KB per plane tile
 constexpr int STAGE_BYTES = 8 * TILE_BYTES;      // 4 A + 4 B planes
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+constexpr int EPI_BYTES = 2 * BM * 32 * 4;  // epilogue staging: 32 columns of the tile, both planes
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + EPI_BYTES + 1024 + 256;
+static_assert(SMEM_BYTES <= 232448, "dynamic shared memory of one CTA");
 constexpr uint32_t TMEM_COLS = 512;
 constexpr long long kWaitCap = 1LL << 24;
 // Written to *err when a bounded wait gives up: negative, like LAPACK's argument errors, so an
@@ -129,7 +131,30 @@ struct GemmArgs {
   int nk;             // number of BK slices (K / 16, K padded with zeros)
   int nb;             // matrices in the batch
   int *err;           // one error word per matrix
+  int tma_epi;        // C -= D by TMA reduce-add (mapCr / mapCi), else by loads and stores
 };
+
+// OR / AND of a predicate over the 128 epilogue threads (named barrier 1).
+__device__ __forceinline__ bool epi_any(bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 q, %1, 0;\n\tbar.red.or.pred p, 1, 128, q;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)v)
+      : "memory");
+  return r != 0;
+}
+__device__ __forceinline__ bool epi_all(bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 q, %1, 0;\n\tbar.red.and.pred p, 1, 128, q;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)v)
+      : "memory");
+  return r != 0;
+}
 
 // A bounded wait gave up: every matrix of the batch is marked (its update is incomplete).
 __device__ __forceinline__ void fail_all(const GemmArgs &g) {
@@ -137,10 +162,13 @@ __device__ __forceinline__ void fail_all(const GemmArgs &g) {
 }
 
 __global__ void __launch_bounds__(192, 1) k_cgemm_tf32x3(const __grid_constant__ CUtensorMap mapA,
-                                                         const __grid_constant__ CUtensorMap mapB, GemmArgs g) {
+                                                         const __grid_constant__ CUtensorMap mapB,
+                                                         const __grid_constant__ CUtensorMap mapCr,
+                                                         const __grid_constant__ CUtensorMap mapCi, GemmArgs g) {
   extern __shared__ __align__(1024) unsigned char smraw[];
   unsigned char *base = (unsigned char *)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
-  uint64_t *full = (uint64_t *)(base + STAGES * STAGE_BYTES);
+  unsigned char *epi = base + STAGES * STAGE_BYTES;  // [2 planes][128 rows][32 floats], 128-byte swizzle
+  uint64_t *full = (uint64_t *)(epi + EPI_BYTES);
   uint64_t *empty = full + STAGES;
   uint64_t *accf = empty + STAGES;  // [2]
   uint64_t *acce = accf + 2;        // [2]
@@ -248,12 +276,11 @@ __global__ void __launch_bounds__(192, 1) k_cgemm_tf32x3(const __grid_constant__
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++local) {
       const int ab = local & 1;
       const uint32_t aph = (local >> 1) & 1;
-      // warp-uniform decisions: tcgen05.ld below needs the whole warp converged
-      const bool stop = __shfl_sync(0xffffffffu, *(volatile int *)abort_flag, 0) != 0;
-      if (stop) break;
-      const bool ok = __all_sync(0xffffffffu, mbar_wait(&accf[ab], aph));
-      if (!ok) {
-        if (lane == 0) { fail_all(g); *(volatile int *)abort_flag = 1; }
+      // decisions uniform over the 4 epilogue warps: tcgen05.ld needs whole warps and the
+      // staging tile's named barrier needs all 128 threads
+      if (epi_any(*(volatile int *)abort_flag != 0)) break;
+      if (!epi_all(mbar_wait(&accf[ab], aph))) {
+        if (threadIdx.x == 64) { fail_all(g); *(volatile int *)abort_flag = 1; }
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -267,7 +294,36 @@ __global__ void __launch_bounds__(192, 1) k_cgemm_tf32x3(const __grid_constant__
         tmem_ld32(trow + ch * 32, vr);
         tmem_ld32(trow + 128 + ch * 32, vi);
         const int c = nt * BN + ch * 32;
-        if (r < g.M) {
+        if (g.tma_epi) {
+          // -D into the staging tile (128-byte swizzle: 16-byte chunk q of row r at q ^ (r & 7)),
+          // then one thread adds it to C in L2 with a TMA reduce per plane.
+          if (threadIdx.x == 64) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+          asm volatile("bar.sync 1, 128;" ::: "memory");  // staging free (previous reduce has read it)
+          float4 *sr = reinterpret_cast<float4 *>(epi + row_in_tile * 128);
+          float4 *si = reinterpret_cast<float4 *>(epi + BM * 128 + row_in_tile * 128);
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const int pq = q ^ (row_in_tile & 7);
+            sr[pq] = make_float4(-vr[4 * q], -vr[4 * q + 1], -vr[4 * q + 2], -vr[4 * q + 3]);
+            si[pq] = make_float4(-vi[4 * q], -vi[4 * q + 1], -vi[4 * q + 2], -vi[4 * q + 3]);
+          }
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          asm volatile("bar.sync 1, 128;" ::: "memory");
+          if (threadIdx.x == 64) {
+            const int x = g.n0 + c, y = g.m0 + mt * BM;
+            asm volatile(
+                "cp.reduce.async.bulk.tensor.3d.global.shared::cta.add.tile.bulk_group [%0, {%2, %3, %4}], [%1];" ::"l"(
+                    &mapCr),
+                "r"(smem_u32(epi)), "r"(x), "r"(y), "r"(b)
+                : "memory");
+            asm volatile(
+                "cp.reduce.async.bulk.tensor.3d.global.shared::cta.add.tile.bulk_group [%0, {%2, %3, %4}], [%1];" ::"l"(
+                    &mapCi),
+                "r"(smem_u32(epi + BM * 128)), "r"(x), "r"(y), "r"(b)
+                : "memory");
+            asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+          }
+        } else if (r < g.M) {
           float *pr = Cr + (long long)(g.m0 + r) * g.ldc + g.n0 + c;
           float *pi = Ci + (long long)(g.m0 + r) * g.ldc + g.n0 + c;
           if (c + 32 <= g.N && (((uintptr_t)pr | (uintptr_t)pi) & 15) == 0) {
@@ -289,6 +345,8 @@ __global__ void __launch_bounds__(192, 1) k_cgemm_tf32x3(const __grid_constant__
       __syncwarp();
       if (lane == 0) mbar_arrive(&acce[ab]);
     }
+    // the reduces complete (and stop reading the staging tile) before the CTA exits
+    if (threadIdx.x == 64) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -369,6 +427,23 @@ int get_encoder() {
   return 0;
 }
 
+// C plane of every matrix of the batch for the reduce-add epilogue: columns [0, cols),
+// rows [0, rows), matrix z; 32 x 128 boxes with the 128-byte swizzle of the staging tile.
+int make_cmap(CUtensorMap *m, const float *c, long long ld, long long ms, int rows, int cols, int nb) {
+  cuuint64_t dims[3] = {(cuuint64_t)cols, (cuuint64_t)rows, (cuuint64_t)nb};
+  cuuint64_t strides[2] = {(cuuint64_t)ld * 4, (cuuint64_t)(nb > 1 ? ms : ld * rows) * 4};
+  cuuint32_t box[3] = {32, BM, 1};
+  cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = g_encode.load(std::memory_order_acquire)(
+      m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)c, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+      CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    pss_set_error("cuTensorMapEncodeTiled (C) failed (%d)", (int)r);
+    return -3;
+  }
+  return 0;
+}
+
 int make_map(CUtensorMap *m, const float *planes, int rows, int KP, int nplanes) {
   cuuint64_t dims[3] = {(cuuint64_t)KP, (cuuint64_t)rows, (cuuint64_t)nplanes};
   cuuint64_t strides[2] = {(cuuint64_t)KP * 4, (cuuint64_t)rows * KP * 4};
@@ -422,14 +497,22 @@ int pss_cgemm_tc(float *Ar, float *Ai, long long ld, long long ms, int nb, int m
   k_split_a<<<dim3(cdiv_u((long long)M * KP, 256), nb), 256, 0, st>>>(Ar, Ai, ld, ms, m0, M, k0, K, KP, pa);
   pss_count_launch();
   k_split_b<<<dim3(cdiv_u(N, 32), cdiv_u(KP, 32), nb), 256, 0, st>>>(Ar, Ai, ld, ms, k0, K, n0, N, KP, pb);
-  CUtensorMap ma, mb;
+  CUtensorMap ma, mb, mcr, mci;
   if (make_map(&ma, pa, M, KP, 4 * nb) || make_map(&mb, pb, N, KP, 4 * nb)) return -3;
-  GemmArgs g{Ar, Ai, ld, ms, m0, n0, M, N, KP / BK, nb, err};
+  // TMA reduce-add epilogue when every box start and stride is 16-byte aligned
+  const bool tma_epi = ld % 4 == 0 && (nb == 1 || ms % 4 == 0) && n0 % 4 == 0 &&
+                       (((uintptr_t)Ar | (uintptr_t)Ai) & 15) == 0;
+  if (tma_epi) {
+    if (make_cmap(&mcr, Ar, ld, ms, m0 + M, n0 + N, nb) || make_cmap(&mci, Ai, ld, ms, m0 + M, n0 + N, nb)) return -3;
+  } else {
+    mcr = mci = ma;  // not read
+  }
+  GemmArgs g{Ar, Ai, ld, ms, m0, n0, M, N, KP / BK, nb, err, tma_epi ? 1 : 0};
   const int tiles = ((M + BM - 1) / BM) * ((N + BN - 1) / BN) * nb;
   const int grid = std::min(tiles, g_num_sms[dev]);
   const int tok = pss_prof_begin(st);
   pss_count_launch();
-  k_cgemm_tf32x3<<<grid, 192, SMEM_BYTES, st>>>(ma, mb, g);
+  k_cgemm_tf32x3<<<grid, 192, SMEM_BYTES, st>>>(ma, mb, mcr, mci, g);
   pss_prof_end(tok, st, PSS_PROF_TC_UPDATE, 8.0 * nb * M * (double)N * K);
   PSS_CUDA_TRY(cudaGetLastError());
   return 0;
