@@ -241,72 +241,46 @@ __global__ void __launch_bounds__(128) k_pairs(SheetDev G, const PointParams *__
 }
 
 // Z[m, n] (m = test / match basis function, n = source).  Row-major, leading dimension ld.
-// One matrix entry (m, n) per thread: the <= 4 x 4 face-pair terms are gathered with all
-// their index loads, then all their zb loads, in flight together (the gathers, not the
-// arithmetic, bound this kernel).
-__global__ void __launch_bounds__(256, 2) k_assemble(SheetDev G, const PointParams *__restrict__ Pp,
+__global__ void __launch_bounds__(256) k_assemble(SheetDev G, const PointParams *__restrict__ Pp,
                                                   const cd *__restrict__ zb, cd *__restrict__ z64,
                                                   float *__restrict__ zr, float *__restrict__ zi, long long ld) {
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  const int m = blockIdx.y * blockDim.y + threadIdx.y;
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  int m = blockIdx.y * blockDim.y + threadIdx.y;
   if (m >= G.nbf || n >= G.nbf) return;
   const PointParams &P = *Pp;
-  const int cm = G.inc_cnt[m], cn = G.inc_cnt[n];
-  int fa[4], ka[4], fb[4], kb[4];
-  cd mf[4], sf[4];
-#pragma unroll
-  for (int a = 0; a < 4; ++a) {
-    if (a < cm) {
-      fa[a] = G.inc_face[4 * m + a];
-      ka[a] = G.inc_loc[4 * m + a];
-      const cd ffa = P.ff[G.inc_eci[4 * m + a]];
-      mf[a] = G.inc_sgn[4 * m + a] > 0 ? conjd(ffa) : -conjd(ffa);
-    }
-    if (a < cn) {
-      fb[a] = G.inc_face[4 * n + a];
-      kb[a] = G.inc_loc[4 * n + a];
-      const cd ffb = P.ff[G.inc_eci[4 * n + a]];
-      sf[a] = G.inc_sgn[4 * n + a] > 0 ? ffb : -ffb;
-    }
-  }
-  int iu[4][4];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b)
-      iu[a][b] = (a < cm && b < cn) ? G.ufpm[(size_t)fa[a] + (size_t)fb[b] * G.nface] : 0;
-  cd v[4][4];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b)
-      v[a][b] = (a < cm && b < cn) ? zb[(size_t)iu[a][b] * 9 + 3 * kb[b] + ka[a]] : mkcd(0, 0);
-  cd acc = mkcd(0, 0);
   const int nx[3] = {1, 2, 0}, pv[3] = {2, 0, 1};
   const int third[3][3] = {{0, 2, 1}, {2, 0, 0}, {1, 0, 0}};
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      if (!(a < cm && b < cn)) continue;
-      acc = acc + (mf[a] * sf[b]) * v[a][b];
-      if (!P.magnetic && fa[a] == fb[b]) {  // surface loading (FillZY.jl:221-230)
-        const double fr = G.fr[fa[a]];
+  cd acc = mkcd(0, 0);
+  const int cm = G.inc_cnt[m], cn = G.inc_cnt[n];
+  for (int a = 0; a < cm; ++a) {
+    const int fa = G.inc_face[4 * m + a], ka = G.inc_loc[4 * m + a];
+    const cd ffa = P.ff[G.inc_eci[4 * m + a]];
+    const cd mflag = G.inc_sgn[4 * m + a] > 0 ? conjd(ffa) : -conjd(ffa);
+    for (int b = 0; b < cn; ++b) {
+      const int fb = G.inc_face[4 * n + b], kb = G.inc_loc[4 * n + b];
+      const cd ffb = P.ff[G.inc_eci[4 * n + b]];
+      const cd sflag = G.inc_sgn[4 * n + b] > 0 ? ffb : -ffb;
+      const int iu = G.ufpm[(size_t)fa + (size_t)fb * G.nface];
+      const cd v = zb[(size_t)iu * 9 + 3 * kb + ka];
+      acc = acc + (mflag * sflag) * v;
+      if (!P.magnetic && fa == fb) {
+        const double fr = G.fr[fa];
         if (fr != 0.0) {
-          const double *ls = G.face_ls + 3 * fa[a];
-          const double g = fr / G.face_a48[fa[a]];
-          if (ka[a] == kb[b]) {
-            const double l1 = ls[nx[kb[b]]], l2 = ls[pv[kb[b]]], l0 = ls[kb[b]];
+          const double *ls = G.face_ls + 3 * fa;
+          const double g = fr / G.face_a48[fa];
+          if (ka == kb) {
+            double l1 = ls[nx[kb]], l2 = ls[pv[kb]], l0 = ls[kb];
             acc = acc + mkcd(g * (3 * (l1 * l1 + l2 * l2) - l0 * l0), 0.0);
           } else {
-            const double lt = ls[third[kb[b]][ka[a]]];
-            const double geo = ls[kb[b]] * ls[kb[b]] + ls[ka[a]] * ls[ka[a]] - 3 * (lt * lt);
-            acc = acc + geo * ((g * sf[b]) * mf[a]);
+            double lt = ls[third[kb][ka]];
+            double geo = ls[kb] * ls[kb] + ls[ka] * ls[ka] - 3 * (lt * lt);
+            acc = acc + geo * ((g * sflag) * mflag);
           }
         }
       }
     }
-  const size_t o = (size_t)m * ld + n;
+  }
+  size_t o = (size_t)m * ld + n;
   if (z64) z64[o] = acc;
   if (zr) {
     zr[o] = (float)acc.x;
