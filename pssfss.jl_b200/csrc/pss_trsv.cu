@@ -302,6 +302,81 @@ __global__ void __launch_bounds__(256) k_resid(int n, const cd *__restrict__ A0,
   }
 }
 
+// Residual for up to 4 right-hand sides (the sweep's usual case): a CTA of 8 warps takes 32
+// rows, each warp 4 of them; the columns go in chunks whose X block (4 x 256) is staged in
+// shared memory and reused by the 4 rows of every warp, so the matrix rows are the only
+// HBM stream (each read once) and the kernel runs at the memory roofline.
+constexpr int kResRows = 4, kResChunk = 256;
+__global__ void __launch_bounds__(256) k_resid4(int n, const cd *__restrict__ A0, long long ld, long long ms, int nrhs,
+                                                const cd *__restrict__ X0, const cd *__restrict__ B0,
+                                                cd *__restrict__ R0, long long vs, double *norms0, Ctrl ctrl) {
+  const int bm = blockIdx.y;
+  if (ctrl.of(bm)[2]) return;
+  const cd *A = A0 + bm * ms, *X = X0 + bm * vs, *B = B0 + bm * vs;
+  cd *R = R0 + bm * vs;
+  double *norms = norms0 + (long long)bm * kNormCount;
+  __shared__ cd xs[4][kResChunk];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int r0 = blockIdx.x * (8 * kResRows) + warp * kResRows;
+  cd acc[kResRows][4];
+  double rs[kResRows];
+#pragma unroll
+  for (int i = 0; i < kResRows; ++i) {
+    rs[i] = 0.0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = mkcd(0, 0);
+  }
+  for (int t0 = 0; t0 < n; t0 += kResChunk) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < 4 * kResChunk; e += blockDim.x) {
+      const int j = e / kResChunk, t = e % kResChunk;
+      xs[j][t] = (j < nrhs && t0 + t < n) ? X[(size_t)j * n + t0 + t] : mkcd(0, 0);
+    }
+    __syncthreads();
+#pragma unroll 2
+    for (int q = 0; q < kResChunk / 32; ++q) {
+      const int t = q * 32 + lane;
+      if (t0 + t >= n) break;
+      cd xv[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) xv[j] = xs[j][t];
+#pragma unroll
+      for (int i = 0; i < kResRows; ++i) {
+        if (r0 + i >= n) continue;
+        const cd av = A[(long long)(r0 + i) * ld + t0 + t];
+        rs[i] += cabs1(av);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = acc[i][j] + av * xv[j];
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < kResRows; ++i) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      rs[i] += __shfl_xor_sync(0xffffffff, rs[i], o);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        acc[i][j].x += __shfl_xor_sync(0xffffffff, acc[i][j].x, o);
+        acc[i][j].y += __shfl_xor_sync(0xffffffff, acc[i][j].y, o);
+      }
+    }
+    const int row = r0 + i;
+    if (row >= n) continue;
+    if (lane == 0) atomicMax((unsigned long long *)&norms[kNA], (unsigned long long)__double_as_longlong(rs[i]));
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      if (j < nrhs && lane == j) {
+        const cd r = B[(size_t)j * n + row] - acc[i][j];
+        R[(size_t)j * n + row] = r;
+        atomicMax((unsigned long long *)&norms[j], (unsigned long long)__double_as_longlong(cabs1(r)));
+        const double xv = cabs1(X[(size_t)j * n + row]);
+        atomicMax((unsigned long long *)&norms[kNX + j], (unsigned long long)__double_as_longlong(xv));
+      }
+    }
+  }
+}
+
 __global__ void k_ir_check(int n, int nrhs, double *norms0, Ctrl ctrl, int *status0, int last) {
   int *cw = ctrl.of(blockIdx.x);
   int *done = cw + 2, *err = cw + 1, *status = status0 + blockIdx.x;
@@ -452,7 +527,11 @@ int pss_refine(SolveWS &ws, int nb, const cd *A, long long ld, long long ms, con
   const long long total = (long long)ws.n * nrhs;
   for (int it = 0; it <= maxit; ++it) {
     pss_count_launch();
-    k_resid<<<dim3(cdiv_u(ws.n, 8), nb), 256, 0, st>>>(ws.n, A, ld, ms, nrhs, X, B, R, vs, ws.norms, ctrl);
+    if (nrhs <= 4)
+      k_resid4<<<dim3(cdiv_u(ws.n, 8 * kResRows), nb), 256, 0, st>>>(ws.n, A, ld, ms, nrhs, X, B, R, vs, ws.norms,
+                                                                     ctrl);
+    else
+      k_resid<<<dim3(cdiv_u(ws.n, 8), nb), 256, 0, st>>>(ws.n, A, ld, ms, nrhs, X, B, R, vs, ws.norms, ctrl);
     pss_count_launch();
     k_ir_check<<<nb, 1, 0, st>>>(ws.n, nrhs, ws.norms, ctrl, status, it == maxit);
     if (it == maxit) break;
