@@ -306,7 +306,8 @@ __global__ void __launch_bounds__(256) k_resid(int n, const cd *__restrict__ A0,
 // rows, each warp 4 of them; the columns go in chunks whose X block (4 x 256) is staged in
 // shared memory and reused by the 4 rows of every warp, so the matrix rows are the only
 // HBM stream (each read once) and the kernel runs at the memory roofline.
-constexpr int kResRows = 4, kResChunk = 256;
+constexpr int kResRows = 4, kResChunk = 1024;
+constexpr int kResSmem = 4 * kResChunk * (int)sizeof(cd);  // 64 KB
 __global__ void __launch_bounds__(256) k_resid4(int n, const cd *__restrict__ A0, long long ld, long long ms, int nrhs,
                                                 const cd *__restrict__ X0, const cd *__restrict__ B0,
                                                 cd *__restrict__ R0, long long vs, double *norms0, Ctrl ctrl) {
@@ -315,7 +316,8 @@ __global__ void __launch_bounds__(256) k_resid4(int n, const cd *__restrict__ A0
   const cd *A = A0 + bm * ms, *X = X0 + bm * vs, *B = B0 + bm * vs;
   cd *R = R0 + bm * vs;
   double *norms = norms0 + (long long)bm * kNormCount;
-  __shared__ cd xs[4][kResChunk];
+  extern __shared__ __align__(16) unsigned char res_smem[];
+  cd(*xs)[kResChunk] = reinterpret_cast<cd(*)[kResChunk]>(res_smem);  // [4][kResChunk]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int r0 = blockIdx.x * (8 * kResRows) + warp * kResRows;
   cd acc[kResRows][4];
@@ -333,7 +335,7 @@ __global__ void __launch_bounds__(256) k_resid4(int n, const cd *__restrict__ A0
       xs[j][t] = (j < nrhs && t0 + t < n) ? X[(size_t)j * n + t0 + t] : mkcd(0, 0);
     }
     __syncthreads();
-#pragma unroll 2
+#pragma unroll 4
     for (int q = 0; q < kResChunk / 32; ++q) {
       const int t = q * 32 + lane;
       if (t0 + t >= n) break;
@@ -522,14 +524,20 @@ int pss_refine(SolveWS &ws, int nb, const cd *A, long long ld, long long ms, con
                int nrhs, const cd *B, cd *X, cd *R, cd *D, long long vs, int maxit, int *status, cudaStream_t st) {
   if (nrhs > kMaxRefRhs) { pss_set_error("refinement supports at most %d right-hand sides", kMaxRefRhs); return -1; }
   const Ctrl ctrl{ws.ctrl, ws.cstride};
+  static DeviceOnce once;
+  if (int rc = device_once(once, [] {
+        PSS_CUDA_TRY(cudaFuncSetAttribute(k_resid4, cudaFuncAttributeMaxDynamicSharedMemorySize, kResSmem));
+        return 0;
+      }))
+    return rc;
   // converged words of every matrix cleared
   PSS_CUDA_TRY(cudaMemset2DAsync(ws.ctrl + 2, ws.cstride * sizeof(int), 0, sizeof(int), nb, st));
   const long long total = (long long)ws.n * nrhs;
   for (int it = 0; it <= maxit; ++it) {
     pss_count_launch();
     if (nrhs <= 4)
-      k_resid4<<<dim3(cdiv_u(ws.n, 8 * kResRows), nb), 256, 0, st>>>(ws.n, A, ld, ms, nrhs, X, B, R, vs, ws.norms,
-                                                                     ctrl);
+      k_resid4<<<dim3(cdiv_u(ws.n, 8 * kResRows), nb), 256, kResSmem, st>>>(ws.n, A, ld, ms, nrhs, X, B, R, vs,
+                                                                            ws.norms, ctrl);
     else
       k_resid<<<dim3(cdiv_u(ws.n, 8), nb), 256, 0, st>>>(ws.n, A, ld, ms, nrhs, X, B, R, vs, ws.norms, ctrl);
     pss_count_launch();
