@@ -3,9 +3,13 @@
 ``rectstrip`` (``:149-186``) and ``meander`` (``:617-729``) are built from ``recttri``
 and ``combine`` exactly as in the reference, so node numbering, edge numbering and
 coordinates are identical.  ``pecsheet``/``pmcsheet`` (``:108-126``) are the null
-sheets.  Constructors that call Shewchuk's Triangle in the reference (``polyring``,
-``diagstrip`` end caps, ``loadedcross``, ``jerusalemcross``) are not provided: their
-meshes cannot be reproduced without that third-party mesher.
+sheets.
+
+``polyring`` (``:368-558``) and ``jerusalemcross`` (``:963-...``) take the reference's
+geometry arguments but are meshed here with structured meshes of their own (a polar grid
+per ring; a rectilinear grid over the union of rectangles), because the reference meshes
+them with Shewchuk's Triangle, which is not available: same shapes, different
+triangulations, so results agree with the reference only to discretisation accuracy.
 """
 import math
 
@@ -172,3 +176,174 @@ def meander(*, a, b, h, w1, w2, ntri, units, orient=0.0, **kwarg):
         sheet.rho = np.array([[kwargs["dx"] + x, kwargs["dy"] + y] for x, y in sheet.rho])
     sheet.xi_eta_check = True
     return sheet
+
+
+def _sheet_from_triangles(rho, tris):
+    """RWGSheet topology from node coordinates (nnode, 2) and counter-clockwise triangles
+    (nface, 3) of 0-based node indices: 1-based ``fv``, ``fe`` with ``fe[k]`` the edge
+    opposite ``fv[k]``, and edges ``e1``/``e2`` numbered in order of first appearance."""
+    from .sheets import RWGSheet
+    rho = np.asarray(rho, float)
+    tris = np.asarray(tris, np.int64)
+    area = ((rho[tris[:, 1], 0] - rho[tris[:, 0], 0]) * (rho[tris[:, 2], 1] - rho[tris[:, 0], 1]) -
+            (rho[tris[:, 2], 0] - rho[tris[:, 0], 0]) * (rho[tris[:, 1], 1] - rho[tris[:, 0], 1]))
+    if np.any(area <= 0):
+        raise ValueError("triangles must be counter-clockwise and non-degenerate")
+    edges = {}
+    e1, e2 = [], []
+    fe = np.zeros((3, len(tris)), np.int64)
+    for f, (a, b, c) in enumerate(tris):
+        for k, (p, q) in enumerate(((b, c), (c, a), (a, b))):  # edge opposite vertex k
+            key = (min(p, q), max(p, q))
+            if key not in edges:
+                edges[key] = len(e1) + 1
+                e1.append(key[0] + 1)
+                e2.append(key[1] + 1)
+            fe[k, f] = edges[key]
+    sh = RWGSheet()
+    sh.rho = rho
+    sh.fv = (tris.T + 1).astype(np.int64)
+    sh.fe = fe
+    sh.e1 = np.array(e1, np.int64)
+    sh.e2 = np.array(e2, np.int64)
+    return sh
+
+
+def _finish_sheet(sheet, style, units, s1, s2, kwargs):
+    sheet.style = style
+    sheet.units = units
+    sheet.s1 = np.asarray(s1, float)
+    sheet.s2 = np.asarray(s2, float)
+    sheet.beta1, sheet.beta2 = s1s2_to_b1b2(sheet.s1, sheet.s2)
+    sheet.fr = np.full(sheet.nface, float(kwargs["Rsheet"]))
+    sheet.fufp = kwargs["fufp"]
+    sheet.cls = kwargs["cls"]
+    rotate(sheet, kwargs["rot"])
+    if kwargs["dx"] != 0 or kwargs["dy"] != 0:
+        sheet.rho = np.array([[kwargs["dx"] + x, kwargs["dy"] + y] for x, y in sheet.rho])
+    sheet.xi_eta_check = False
+    return sheet
+
+
+def polyring(*, s1, s2, a, b, sides, ntri, units, orient=0.0, **kwarg):
+    """Concentric regular-polygon rings (``Elements.jl:368-558``): ring i spans radii
+    a[i]..b[i] (a[i] = 0: a solid polygon), centred in the cell, first vertex at angle
+    ``orient`` (degrees).  Structured polar mesh of about ``ntri`` triangles in total,
+    shared among the rings by area; rings that fill the cell (b[-1] < 0) are not
+    supported by this mesher."""
+    kwargs = dict(kwarg)
+    kwargs.setdefault("fufp", False)
+    _check_kwargs(kwargs)
+    _testpos(sides=sides, ntri=ntri)
+    a = [float(x) for x in a]
+    b = [float(x) for x in b]
+    if len(a) != len(b):
+        raise ValueError("length(a) !== length(b)")
+    if b[-1] < 0:
+        raise ValueError("rings that fill the unit cell (b[end] < 0) need the reference's mesher")
+    for i in range(len(a)):
+        if a[i] >= b[i]:
+            raise ValueError(f"a[{i + 1}] >= b[{i + 1}]")
+        if i + 1 < len(a) and b[i] >= a[i + 1]:
+            raise ValueError(f"b[{i + 1}] >= a[{i + 2}]")
+    s1 = np.asarray(s1, float)
+    s2 = np.asarray(s2, float)
+    rho0 = 0.5 * (s1 + s2)
+    alpha = 2 * math.pi / sides
+    area_factor = 0.5 * sides * math.sin(alpha)
+    areas = [(bb * bb - aa * aa) * area_factor for aa, bb in zip(a, b)]
+    rho, tris = [], []
+    for aa, bb, ar in zip(a, b, areas):
+        nt = max(2 * sides, round(ntri * ar / sum(areas)))
+        # ns segments per polygon side, nr radial layers, cells as close to square as the
+        # triangle budget allows: 2 * sides * ns * nr ~ nt with (bb - aa) / nr ~ side(rmid) / ns
+        rmid = 0.5 * (aa + bb)
+        side = 2 * rmid * math.sin(alpha / 2)
+        ratio = (bb - aa) / side  # nr / ns
+        ns = max(1, round(math.sqrt(nt / (2 * sides * ratio))))
+        nr = max(1, round(nt / (2 * sides * ns)))
+        m = sides * ns  # nodes per layer
+        verts = [np.array([math.cos(math.radians(orient) + i * alpha), math.sin(math.radians(orient) + i * alpha)])
+                 for i in range(sides)]
+        dirs = [verts[i] + (verts[(i + 1) % sides] - verts[i]) * (t / ns) for i in range(sides) for t in range(ns)]
+        layers = []
+        r_in = aa if aa > 0 else bb / (nr + 1)
+        nl = nr + 1 if aa > 0 else nr
+        for k in range(nl + (0 if aa > 0 else 1)):
+            r = (aa + (bb - aa) * k / nr) if aa > 0 else bb * (k + 1) / (nr + 1)
+            base = len(rho)
+            rho.extend(rho0 + r * d for d in dirs)
+            layers.append(base)
+        if aa == 0:  # centre node and its fan to the first layer
+            c = len(rho)
+            rho.append(rho0.copy())
+            for i in range(m):
+                tris.append((c, layers[0] + i, layers[0] + (i + 1) % m))
+        for k in range(len(layers) - 1):
+            lo, hi = layers[k], layers[k + 1]
+            for i in range(m):
+                i1 = (i + 1) % m
+                tris.append((lo + i, hi + i, hi + i1))
+                tris.append((lo + i, hi + i1, lo + i1))
+    sheet = _sheet_from_triangles(rho, tris)
+    return _finish_sheet(sheet, "polyring", units, s1, s2, kwargs)
+
+
+def _rect_union_mesh(rects, h):
+    """Conforming triangulation of a union of axis-aligned rectangles (x0, y0, x1, y1):
+    grid lines at every rectangle edge, refined to steps <= h, cells inside the union
+    split along the lower-left/upper-right diagonal."""
+    def lines(vals):
+        vals = sorted(set(round(v, 12) for v in vals))
+        out = [vals[0]]
+        for lo, hi in zip(vals, vals[1:]):
+            k = max(1, math.ceil((hi - lo) / h - 1e-9))
+            out.extend(lo + (hi - lo) * (i + 1) / k for i in range(k))
+        return np.array(out)
+    xs = lines([r[0] for r in rects] + [r[2] for r in rects])
+    ys = lines([r[1] for r in rects] + [r[3] for r in rects])
+    inside = np.zeros((len(xs) - 1, len(ys) - 1), bool)
+    xc = 0.5 * (xs[:-1] + xs[1:])
+    yc = 0.5 * (ys[:-1] + ys[1:])
+    for x0, y0, x1, y1 in rects:
+        inside |= ((xc > x0) & (xc < x1))[:, None] & ((yc > y0) & (yc < y1))[None, :]
+    nid = -np.ones((len(xs), len(ys)), np.int64)
+    rho, tris = [], []
+
+    def node(i, j):
+        if nid[i, j] < 0:
+            nid[i, j] = len(rho)
+            rho.append((xs[i], ys[j]))
+        return nid[i, j]
+    for j in range(len(ys) - 1):
+        for i in range(len(xs) - 1):
+            if inside[i, j]:
+                ll, lr, ur, ul = node(i, j), node(i + 1, j), node(i + 1, j + 1), node(i, j + 1)
+                tris.append((ll, ur, ul))
+                tris.append((ll, lr, ur))
+    return np.array(rho), np.array(tris)
+
+
+def jerusalemcross(*, P, L1, L2, A, B, w, ntri, units, **kwarg):
+    """Jerusalem cross in a square cell of period P (``Elements.jl:963``): arms of length L1
+    (tip to tip) and width L2, end caps of length A and width B.  Meshed here as the solid
+    cross (the reference's ``w >= L2/2`` and ``w >= B/2`` case); a hollow outline of width
+    w < L2/2 is not supported by this mesher."""
+    kwargs = dict(kwarg)
+    kwargs.setdefault("fufp", False)
+    _check_kwargs(kwargs)
+    _testpos(P=P, L1=L1, L2=L2, A=A, B=B, w=w, ntri=ntri)
+    if w < L2 / 2 or w < B / 2:
+        raise ValueError("only the solid cross (w >= L2/2 and w >= B/2) is meshed here")
+    if not (L1 < P and A < P and L2 < A and 2 * B < L1):
+        raise ValueError("inconsistent Jerusalem-cross dimensions")
+    c = P / 2
+    h1, h2, hA = L1 / 2, L2 / 2, A / 2
+    rects = [(c - h1, c - h2, c + h1, c + h2), (c - h2, c - h1, c + h2, c + h1),   # arms
+             (c - h1, c - hA, c - h1 + B, c + hA), (c + h1 - B, c - hA, c + h1, c + hA),  # caps
+             (c - hA, c - h1, c + hA, c - h1 + B), (c - hA, c + h1 - B, c + hA, c + h1)]
+    area = 2 * L1 * L2 - L2 * L2 + 4 * (A * B - L2 * B)
+    h = math.sqrt(2 * area / ntri)  # two triangles per h x h cell
+    rho, tris = _rect_union_mesh(rects, h)
+    sheet = _sheet_from_triangles(rho, tris)
+    return _finish_sheet(sheet, "jerusalemcross", units, [float(P), 0.0], [0.0, float(P)], kwargs)

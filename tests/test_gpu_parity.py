@@ -259,3 +259,41 @@ def test_two_sheet_cascade_oblique_scan():
     ref = oracle.analyze(strata, freqs, steer)
     assert _gsm_relerr(analyze(strata, freqs, steer), ref) < 1e-9
     assert _gsm_relerr(analyze(strata, freqs, steer, precision="fp32r"), ref) <= 1e-6
+
+
+def test_config2_jerusalem_cross_and_aperture_cascade():
+    """Two-sheet cascade in the shape of the plain-FP64 config 2: a (solid) Jerusalem-cross
+    conductor on 0.5 mm eps_r = 3 (tan d = 0.002), a 2 mm air gap, then a 6 mm square
+    aperture (M-type) in an 8 mm cell; scan theta = 30, phi = 45 (face-pair integrals per
+    point).  Own structured meshes (the reference meshes these with Triangle), coarse enough
+    for the oracle; CUDA vs oracle GSMs to 1e-9."""
+    from pssfss_b200 import analyze
+    from pssfss_b200.elements import jerusalemcross
+    jc = jerusalemcross(P=8, L1=6, L2=0.5, A=3, B=0.5, w=0.5, ntri=300, units=mm)
+    ap = rectstrip(Lx=6, Ly=6, Px=8, Py=8, Nx=6, Ny=6, units=mm, **{"class": "M"})
+    strata = [Layer(), jc, Layer(epsr=3.0, tandel=0.002, width=Length(0.5, mm)), Layer(width=Length(2, mm)), ap,
+              Layer()]
+    freqs = [7.0, 16.0]
+    steer = {"θ": 30, "ϕ": 45}
+    ref = oracle.analyze(strata, freqs, steer)
+    assert _gsm_relerr(analyze(strata, freqs, steer), ref) < 1e-9
+    assert _gsm_relerr(analyze(strata, freqs, steer, precision="fp32r"), ref) <= 1e-6
+
+
+@pytest.mark.parametrize("period,ro,ntri,theta", [(6.0, 0.40, 160, 0.0), (9.0, 0.36, 260, 15.0),
+                                                  (12.0, 0.44, 360, 45.0)])
+def test_config4_ring_patches(period, ro, ntri, theta):
+    """Ring-patch problems in the style of the batched config 4 (period, outer radius and
+    triangle count vary per problem, so do the unknown counts; scan theta in {0, 15, 45}),
+    free-standing, 2 frequencies each, FP32 + refinement against the FP64 oracle."""
+    from pssfss_b200 import analyze
+    from pssfss_b200.elements import polyring
+    r_out = ro * period
+    sh = polyring(s1=[period, 0], s2=[0, period], a=[r_out - 0.05 * period], b=[r_out], sides=24, ntri=ntri,
+                  units=mm)
+    strata = [Layer(), sh, Layer()]
+    freqs = [10.0, 20.0]
+    steer = {"θ": theta, "ϕ": 0}
+    ref = oracle.analyze(strata, freqs, steer)
+    assert _gsm_relerr(analyze(strata, freqs, steer, precision="fp32r"), ref) <= 1e-6
+    assert _gsm_relerr(analyze(strata, freqs, steer), ref) < 1e-9

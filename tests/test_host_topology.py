@@ -127,3 +127,27 @@ def test_cascade_identities():
     cascade_layer(b, layer)
     for x, y in ((a.s12, be * prop), (a.s22, al * prop ** 2), (b.s21, be * prop)):
         assert abs(x[0, 0] - y) <= 1e-16
+
+
+def test_structured_ring_and_cross_meshes():
+    """Own meshes for the shapes the reference meshes with Triangle: counter-clockwise
+    faces, every interior edge shared by exactly two faces, total area equal to the shape's."""
+    from pssfss_b200.elements import jerusalemcross, polyring
+    from pssfss_b200.units import mm as MM
+    import math as _m
+    ring = polyring(s1=[10, 0], s2=[0, 10], a=[2.0], b=[3.0], sides=24, ntri=400, units=MM)
+    patch = polyring(s1=[10, 0], s2=[0, 10], a=[0], b=[4.0], sides=4, ntri=300, units=MM, orient=45)
+    cross = jerusalemcross(P=8, L1=6, L2=0.5, A=3, B=0.5, w=0.5, ntri=600, units=MM)
+    af = 0.5 * 24 * _m.sin(2 * _m.pi / 24)
+    for sh, area in ((ring, (9 - 4) * af), (patch, 16 * 0.5 * 4 * _m.sin(_m.pi / 2)),
+                     (cross, 2 * 6 * 0.5 - 0.25 + 4 * (3 * 0.5 - 0.5 * 0.5))):
+        rho = sh.rho
+        fv = sh.fv - 1
+        a = 0.5 * ((rho[fv[1], 0] - rho[fv[0], 0]) * (rho[fv[2], 1] - rho[fv[0], 1]) -
+                   (rho[fv[2], 0] - rho[fv[0], 0]) * (rho[fv[1], 1] - rho[fv[0], 1]))
+        assert (a > 0).all()
+        assert abs(a.sum() - area) < 1e-9 * area
+        counts = np.bincount(sh.fe.ravel(), minlength=sh.nedge + 1)[1:]
+        assert counts.min() >= 1 and counts.max() <= 2
+        rwg = setup_rwg(sh)
+        assert rwg.nbf == int((counts == 2).sum())
