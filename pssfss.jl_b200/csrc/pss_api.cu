@@ -202,7 +202,7 @@ cd hcis(double a) { return mkcd(std::cos(a), std::sin(a)); }
 struct pss_ctx {
   int device = 0;
   int nworkers = 1;
-  int batch = 8;  // points per batched factorisation (PSS_BATCH, 1..32)
+  int batch = 12;  // points per batched factorisation (PSS_BATCH, 1..32)
   std::vector<Worker> w;
   DevBuf params, dense, conv, mm, stage, tables, bigdense, modes, dS, status;
   std::vector<DevBuf> bigtables;

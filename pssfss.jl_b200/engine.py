@@ -115,10 +115,10 @@ def context(device=0, nworkers=None):
     """Per-device ``pss_ctx`` (created once)."""
     if nworkers is None:
         # one stream per worker, each factoring a batch of points at a time (PSS_BATCH,
-        # default 8, read by the library); more streams than the process's hardware work
+        # default 12, read by the library); more streams than the process's hardware work
         # queues (CUDA_DEVICE_MAX_CONNECTIONS, default 8) would share queues
         queues = int(os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS", "8"))
-        nworkers = int(os.environ.get("PSS_WORKERS", str(max(1, min(4, queues)))))
+        nworkers = int(os.environ.get("PSS_WORKERS", str(max(1, min(3, queues)))))
     key = (device, nworkers)
     with _lock:
         c = _ctx.get(key)
