@@ -76,16 +76,18 @@ struct LuBatch {
   int *ipiv, *info, *xlist;
 };
 
-constexpr int kPanelRows = 512;     // panel rows per CTA
-constexpr int kPanelThreads = 256;  // two panel rows per thread
+constexpr int kPanelRows = 512;  // panel rows per CTA
+#ifndef PSS_PANEL_RPT
+#define PSS_PANEL_RPT 2
+#endif
+constexpr int kPanelRpt = PSS_PANEL_RPT;  // panel rows per thread
 constexpr int kMaxCluster = 16;
 constexpr int kMaxW = 32;
 constexpr int kMaxMov = 2 * kMaxW;  // rows one panel's interchanges can move
 constexpr int kSwpThreads = 64;
 constexpr int kListInts = 1 + 2 * kMaxMov;  // interchange list: count, destinations, sources
 constexpr int kTcMinRows = 64, kTcMinCols = 32;  // smallest FP32 update sent to the tensor cores
-static_assert(kPanelThreads / 32 <= 32 && kMaxCluster <= 32, "panel reductions run over one warp's lanes");
-static_assert(kPanelRows == 2 * kPanelThreads, "two rows per panel thread");
+static_assert(kPanelRows / kPanelRpt / 32 <= 32 && kMaxCluster <= 32, "panel reductions run over one warp's lanes");
 
 // Pivot keys: LAPACK's izamax order (largest |re|+|im|, then the lowest row) as one 64-bit
 // unsigned key per candidate, 0 = no candidate, 1 = an exactly zero candidate.  The bits
@@ -129,11 +131,12 @@ __device__ __forceinline__ unsigned long long warp_max_key(unsigned long long k,
 // one cluster barrier; every CTA picks the same winner and updates its active rows over
 // the live columns only.  Multipliers overwrite the rows in place, pivot rows keep their U
 // entries, so the final write-back is a coalesced copy to the permuted positions.
-template <bool F32, int W>
-__global__ void __launch_bounds__(kPanelThreads) k_panel(Mat<F32> M0, LuBatch bt, int row0, int nrows, int col0,
-                                                         int w) {
+template <bool F32, int W, int RPT>
+__global__ void __launch_bounds__(kPanelRows / RPT) k_panel(Mat<F32> M0, LuBatch bt, int row0, int nrows, int col0,
+                                                            int w) {
   using E = typename Prec<F32>::E;
   using Rl = typename Prec<F32>::R;
+  constexpr int T = kPanelRows / RPT;  // threads; thread t works on local rows t + k*T, k < RPT
   cg::cluster_group cluster = cg::this_cluster();
   const int cs = (int)cluster.num_blocks();
   const int crank = (int)cluster.block_rank();
@@ -141,7 +144,7 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(Mat<F32> M0, LuBatch bt
   const Mat<F32> M = M0.at(bidx, bt.ms);
   int *ipiv = bt.ipiv + (long long)bidx * bt.n, *info = bt.info + bidx, *xlist = bt.xlist + bidx * kListInts;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  constexpr int NW = kPanelThreads / 32;
+  constexpr int NW = T / 32;
   extern __shared__ __align__(16) unsigned char panel_smem[];
   E *R = (E *)panel_smem;                      // [W][kPanelRows] the CTA's panel rows
   __shared__ E srow[2][kMaxCluster][W];        // candidate rows pushed by every CTA (double-buffered)
@@ -157,17 +160,22 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(Mat<F32> M0, LuBatch bt
   // coalesced load: one row per warp step, one column per lane
   for (int r = warp; r < kPanelRows; r += NW)
     if (lane < W) R[lane * kPanelRows + r] = (r < nloc && lane < w) ? M.get(row0 + base + r, col0 + lane) : E{0, 0};
-  const int ta = tid, tb = kPanelThreads + tid;  // local rows of this thread
-  bool acta = ta < nloc, actb = tb < nloc;
+  bool act[RPT];
+#pragma unroll
+  for (int k = 0; k < RPT; ++k) act[k] = tid + k * T < nloc;
   __syncthreads();
 
   for (int j = 0; j < w; ++j) {
     const int par = j & 1;
-    const E va = R[j * kPanelRows + ta], vb = R[j * kPanelRows + tb];
-    unsigned long long k = piv_key<F32>(va, acta);
-    int r = base + ta;
-    const unsigned long long kb = piv_key<F32>(vb, actb);
-    if (kb > k) { k = kb; r = base + tb; }  // equal keys keep the lower row
+    E v[RPT];
+    unsigned long long k = 0ull;
+    int r = base + tid;
+#pragma unroll
+    for (int q = 0; q < RPT; ++q) {
+      v[q] = R[j * kPanelRows + tid + q * T];
+      const unsigned long long kq = piv_key<F32>(v[q], act[q]);
+      if (kq > k) { k = kq; r = base + tid + q * T; }  // equal keys keep the lower row
+    }
     int wr;
     k = warp_max_key<F32>(k, r, wr);
     if (lane == 0) { wkey[warp] = k; wrow[warp] = wr; }
@@ -177,10 +185,10 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(Mat<F32> M0, LuBatch bt
       const unsigned long long kc =
           warp_max_key<F32>(lane < NW ? wkey[lane] : 0ull, lane < NW ? wrow[lane] : 0x7fffffff, cr);
       const int lr = kc ? cr - base : 0;
-      const E v = (lane < W && j + lane < w) ? R[(j + lane) * kPanelRows + lr] : E{0, 0};
+      const E pv = (lane < W && j + lane < w) ? R[(j + lane) * kPanelRows + lr] : E{0, 0};
       if (lane < W && j + lane < w)
         for (int dst = 0; dst < cs; ++dst)
-          cluster.map_shared_rank(&srow[0][0][0], dst)[(par * kMaxCluster + crank) * W + j + lane] = v;
+          cluster.map_shared_rank(&srow[0][0][0], dst)[(par * kMaxCluster + crank) * W + j + lane] = pv;
       if (lane < cs) {
         cluster.map_shared_rank(&skey[0][0], lane)[par * kMaxCluster + crank] = kc;
         cluster.map_shared_rank(&sidx[0][0], lane)[par * kMaxCluster + crank] = cr;
@@ -196,9 +204,13 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(Mat<F32> M0, LuBatch bt
       if (tid == 0 && crank == 0) atomicCAS(info, 0, col0 + j + 1);
       continue;
     }
-    if (base + ta == grow) acta = false;  // the pivot row keeps its entries (row of U)
-    if (base + tb == grow) actb = false;
-    if (!(acta || actb)) continue;
+    bool any = false;
+#pragma unroll
+    for (int q = 0; q < RPT; ++q) {
+      if (base + tid + q * T == grow) act[q] = false;  // the pivot row keeps its entries (row of U)
+      any = any || act[q];
+    }
+    if (!any) continue;
     const E *prow = srow[par][grow / kPanelRows];
     const E piv = prow[j];
     E inv;  // 1/pivot (LAPACK zgetf2 scales the column by the reciprocal)
@@ -209,14 +221,18 @@ __global__ void __launch_bounds__(kPanelThreads) k_panel(Mat<F32> M0, LuBatch bt
       const Rl rr = piv.x / piv.y, d = piv.y + piv.x * rr;
       inv = E{rr / d, (Rl)-1 / d};
     }
-    const E la = cmulE(va, inv), lb = cmulE(vb, inv);
-    if (acta) R[j * kPanelRows + ta] = la;
-    if (actb) R[j * kPanelRows + tb] = lb;
+    E l[RPT];
+#pragma unroll
+    for (int q = 0; q < RPT; ++q) {
+      l[q] = cmulE(v[q], inv);
+      if (act[q]) R[j * kPanelRows + tid + q * T] = l[q];
+    }
 #pragma unroll 4
     for (int c = j + 1; c < w; ++c) {
       const E p = prow[c];
-      if (acta) R[c * kPanelRows + ta] = csubE(R[c * kPanelRows + ta], cmulE(la, p));
-      if (actb) R[c * kPanelRows + tb] = csubE(R[c * kPanelRows + tb], cmulE(lb, p));
+#pragma unroll
+      for (int q = 0; q < RPT; ++q)
+        if (act[q]) R[c * kPanelRows + tid + q * T] = csubE(R[c * kPanelRows + tid + q * T], cmulE(l[q], p));
     }
   }
   __syncthreads();
@@ -444,7 +460,7 @@ int launch_panel(Mat<F32> M, const LuBatch &bt, int nb, int row0, int nrows, int
     pss_set_error("panel %d x %d exceeds a %d-CTA cluster", nrows, w, kMaxCluster);
     return -6;
   }
-  auto kern = k_panel<F32, (F32 ? 32 : 16)>;
+  auto kern = k_panel<F32, (F32 ? 32 : 16), kPanelRpt>;
   constexpr int smem = kPanelRows * (F32 ? 32 : 16) * (int)sizeof(typename Prec<F32>::E);  // the panel rows
   static DeviceOnce once;
   if (int rc = device_once(once, [&] {
@@ -455,7 +471,7 @@ int launch_panel(Mat<F32> M, const LuBatch &bt, int nb, int row0, int nrows, int
     return rc;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(cs * nb);  // one cluster of cs CTAs per matrix
-  cfg.blockDim = dim3(kPanelThreads);
+  cfg.blockDim = dim3(kPanelRows / kPanelRpt);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   cudaLaunchAttribute at[1];
