@@ -187,6 +187,7 @@ __global__ void __launch_bounds__(128) k_pairs(SheetDev G, const PointParams *__
   int ifm = fp % G.nface, ifs = fp / G.nface;
   const double inv = 1.0 / G.upm;
   double rs[3][2], rm[3][2];
+#pragma unroll
   for (int k = 0; k < 3; ++k) {
     int vs = G.fv[3 * ifs + k], vm = G.fv[3 * ifm + k];
     rs[k][0] = G.rho[2 * vs] / G.upm;
@@ -217,15 +218,18 @@ __global__ void __launch_bounds__(128) k_pairs(SheetDev G, const PointParams *__
   cd phi = (C.cI2 * I2 + u * (mkcd(rinv, 0) + J)) + C.cKP * K;
   cd zphi = C.zP * phi;
   double rc2[3][2];
+#pragma unroll
   for (int i = 0; i < 3; ++i) {
     rc2[i][0] = 0.5 * (rmc[0] - rm[i][0]);
     rc2[i][1] = 0.5 * (rmc[1] - rm[i][1]);
   }
   cd *out = zb + (size_t)iu * 9;
+#pragma unroll
   for (int isl = 0; isl < 3; ++isl) {
     double sing0 = rr0 + (u * rinv) * (rmc[0] - rs[isl][0]);
     double sing1 = rr1 + (u * rinv) * (rmc[1] - rs[isl][1]);
     cd av[2];
+#pragma unroll
     for (int d = 0; d < 2; ++d) {
       cd Ii = ((rs[0][d] * I1x + rs[1][d] * I1e) + rs[2][d] * I1z) - rs[isl][d] * I1;
       cd Ji = ((rs[0][d] * Jx + rs[1][d] * Je) + rs[2][d] * Jz) - rs[isl][d] * J;
@@ -233,6 +237,7 @@ __global__ void __launch_bounds__(128) k_pairs(SheetDev G, const PointParams *__
       double sg = d == 0 ? sing0 : sing1;
       av[d] = ((C.cI1 * Ii + mkcd(sg, 0)) + u * Ji) + C.cK * Ki;
     }
+#pragma unroll
     for (int iml = 0; iml < 3; ++iml) {
       cd dp = rc2[iml][0] * av[0] + rc2[iml][1] * av[1];
       out[3 * isl + iml] = C.zA * dp - zphi;
@@ -248,8 +253,6 @@ __global__ void __launch_bounds__(256) k_assemble(SheetDev G, const PointParams 
   int m = blockIdx.y * blockDim.y + threadIdx.y;
   if (m >= G.nbf || n >= G.nbf) return;
   const PointParams &P = *Pp;
-  const int nx[3] = {1, 2, 0}, pv[3] = {2, 0, 1};
-  const int third[3][3] = {{0, 2, 1}, {2, 0, 0}, {1, 0, 0}};
   cd acc = mkcd(0, 0);
   const int cm = G.inc_cnt[m], cn = G.inc_cnt[n];
   for (int a = 0; a < cm; ++a) {
@@ -268,11 +271,11 @@ __global__ void __launch_bounds__(256) k_assemble(SheetDev G, const PointParams 
         if (fr != 0.0) {
           const double *ls = G.face_ls + 3 * fa;
           const double g = fr / G.face_a48[fa];
-          if (ka == kb) {
-            double l1 = ls[nx[kb]], l2 = ls[pv[kb]], l0 = ls[kb];
+          if (ka == kb) {  // the other two edges of the face: next and previous slot
+            double l1 = ls[(kb + 1) % 3], l2 = ls[(kb + 2) % 3], l0 = ls[kb];
             acc = acc + mkcd(g * (3 * (l1 * l1 + l2 * l2) - l0 * l0), 0.0);
           } else {
-            double lt = ls[third[kb][ka]];
+            double lt = ls[3 - ka - kb];  // the third edge
             double geo = ls[kb] * ls[kb] + ls[ka] * ls[ka] - 3 * (lt * lt);
             acc = acc + geo * ((g * sflag) * mflag);
           }

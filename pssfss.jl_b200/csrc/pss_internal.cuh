@@ -86,9 +86,9 @@ __device__ __forceinline__ cd sigma_interp(const cd *__restrict__ T, int mmax, c
   if (fabs(x1o) < 1e-8) x1o = 0.0;
   double x2o = (P.b2[0] * rx + P.b2[1] * ry) / PSS_TWOPI;
   if (fabs(x2o) < 1e-8) x2o = 0.0;
-  double r1 = fmod(x1o, 1.0), r2 = fmod(x2o, 1.0);
-  double x1 = (r1 == 0.0) ? 0.0 : (r1 < 0.0 ? r1 + 1.0 : r1);
-  double x2 = (r2 == 0.0) ? 0.0 : (r2 < 0.0 ? r2 + 1.0 : r2);
+  // Julia's mod(x, 1) in [0, 1]: x - floor(x) rounds once, exactly as fmod(x, 1) (exact)
+  // followed by + 1 for negative x, so the result is bit-identical and avoids fmod
+  const double x1 = x1o - floor(x1o), x2 = x2o - floor(x2o);
   double ms = rint(x1o - x1), ns = rint(x2o - x2);
   int m = (int)trunc(mmax * x1);
   double p = mmax * x1 - m;
