@@ -110,8 +110,9 @@ int pss_basis_transforms(pss_sheet *sheet, int nmodes, const double *kvec, doubl
 int pss_lu_solve(pss_ctx *ctx, int n, const double *Z, int nrhs, const double *B, int precision, double *X,
                  int *status);
 
-/* Accumulated per-phase device milliseconds of the last pss_partial_gsms call on worker 0:
- * [tables, face_integrals, fill, factor, transforms+rhs, solve+refine, projection, total]. */
+/* Device milliseconds of the last pss_partial_gsms call, summed over worker 0's batches:
+ * [tables, face_integrals (0: folded into fill), fill, transforms+rhs, 0, factor+solve+refine,
+ *  projection, total span of the call over all workers]. */
 int pss_last_timings(pss_ctx *ctx, double *ms8);
 
 /* Per-launch CUDA-event timing (on each launch's own stream) of the factorisation's main
