@@ -76,10 +76,13 @@ struct LuBatch {
   int *ipiv, *info, *xlist;
 };
 
-constexpr int kPanelRows = 512;  // panel rows per CTA
+#ifndef PSS_PANEL_ROWS
+#define PSS_PANEL_ROWS 512
+#endif
 #ifndef PSS_PANEL_RPT
 #define PSS_PANEL_RPT 2
 #endif
+constexpr int kPanelRows = PSS_PANEL_ROWS;  // panel rows per CTA
 constexpr int kPanelRpt = PSS_PANEL_RPT;  // panel rows per thread
 constexpr int kMaxCluster = 16;
 constexpr int kMaxW = 32;

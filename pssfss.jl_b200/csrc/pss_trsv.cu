@@ -154,7 +154,7 @@ __device__ __forceinline__ C czero() { return C{0, 0}; }
 // the load; Dinv_b (dynamic shared memory) and the block's right-hand side are staged at
 // the start.  Blocks of X written by other CTAs are read with L1-bypassing loads.
 template <bool LOWER, bool F32, int NJ>
-__global__ void __launch_bounds__(256) k_trsv(Fac F0, int n, const int *__restrict__ perm0, const cd *__restrict__ B0,
+__global__ void __launch_bounds__(256, F32 ? 4 : 1) k_trsv(Fac F0, int n, const int *__restrict__ perm0, const cd *__restrict__ B0,
                                               cd *__restrict__ X0, long long vs, int nrhs, int j0,
                                               const cd *__restrict__ Dinv0, long long dstride, Ctrl ctrl, int epoch,
                                               int use_done) {
