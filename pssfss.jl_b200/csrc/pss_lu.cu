@@ -156,13 +156,24 @@ __global__ void __launch_bounds__(kPanelRows / RPT) k_panel(Mat<F32> M0, LuBatch
   __shared__ unsigned long long wkey[NW];      // per-warp winners
   __shared__ int wrow[NW];
   __shared__ int chosen[kMaxW];
-  __shared__ int mpos[2 * kMaxW], morig[2 * kMaxW];  // moved positions and the row each now holds
-  __shared__ int nmoved;
+  __shared__ int sdst[kPanelRows];             // final panel position of each local row
   const int base = crank * kPanelRows;
   const int nloc = max(0, min(kPanelRows, nrows - base));  // rows this CTA owns
-  // coalesced load: one row per warp step, one column per lane
-  for (int r = warp; r < kPanelRows; r += NW)
-    if (lane < W) R[lane * kPanelRows + r] = (r < nloc && lane < w) ? M.get(row0 + base + r, col0 + lane) : E{0, 0};
+  // coalesced load: one row per warp step, one column per lane, LB rows of a warp in flight
+  constexpr int LB = F32 ? 16 : 8;
+  static_assert(kPanelRows % (NW * LB) == 0, "panel rows split evenly into load batches");
+  for (int r0 = warp; r0 < kPanelRows; r0 += NW * LB) {
+    E t[LB];
+#pragma unroll
+    for (int u = 0; u < LB; ++u) {
+      const int r = r0 + u * NW;
+      t[u] = (r < nloc && lane < w) ? M.get(row0 + base + r, col0 + lane) : E{0, 0};
+    }
+    if (lane < W) {
+#pragma unroll
+      for (int u = 0; u < LB; ++u) R[lane * kPanelRows + r0 + u * NW] = t[u];
+    }
+  }
   bool act[RPT];
 #pragma unroll
   for (int k = 0; k < RPT; ++k) act[k] = tid + k * T < nloc;
@@ -218,11 +229,11 @@ __global__ void __launch_bounds__(kPanelRows / RPT) k_panel(Mat<F32> M0, LuBatch
     const E piv = prow[j];
     E inv;  // 1/pivot (LAPACK zgetf2 scales the column by the reciprocal)
     if (fabs((double)piv.y) <= fabs((double)piv.x)) {
-      const Rl rr = piv.y / piv.x, d = piv.x + piv.y * rr;
-      inv = E{(Rl)1 / d, -rr / d};
+      const Rl rr = piv.y / piv.x, id = (Rl)1 / (piv.x + piv.y * rr);
+      inv = E{id, -rr * id};
     } else {
-      const Rl rr = piv.x / piv.y, d = piv.y + piv.x * rr;
-      inv = E{rr / d, (Rl)-1 / d};
+      const Rl rr = piv.x / piv.y, id = (Rl)1 / (piv.y + piv.x * rr);
+      inv = E{rr * id, -id};
     }
     E l[RPT];
 #pragma unroll
@@ -238,58 +249,62 @@ __global__ void __launch_bounds__(kPanelRows / RPT) k_panel(Mat<F32> M0, LuBatch
         if (act[q]) R[c * kPanelRows + tid + q * T] = csubE(R[c * kPanelRows + tid + q * T], cmulE(l[q], p));
     }
   }
+#pragma unroll
+  for (int q = 0; q < RPT; ++q) sdst[tid + q * T] = base + tid + q * T;
   __syncthreads();
-  // Replay the interchanges (LAPACK semantics) in shared memory, by warp 0 of every CTA
-  // (each holds the same chosen[]): a sparse map of the <= 2w positions whose row changed.
+  // Replay the interchanges (LAPACK semantics) by warp 0 of every CTA (each holds the same
+  // chosen[]).  Only the w top rows can be displaced before they are chosen (a row leaves
+  // position j only when step j swaps it out), and a chosen row stays at its pivot
+  // position, so lane r < w keeps the position of original top row r and the original row
+  // now at top position r; one step is two shuffles.
   if (warp == 0) {
-    int cnt = 0;  // warp-uniform
-    auto find = [&](const int *keys, int key) -> int {  // index of key in keys[0..cnt), or -1
-      const bool h0 = lane < cnt && keys[lane] == key;
-      const bool h1 = lane + 32 < cnt && keys[lane + 32] == key;
-      const unsigned b0 = __ballot_sync(0xffffffffu, h0), b1 = __ballot_sync(0xffffffffu, h1);
-      return b0 ? __ffs(b0) - 1 : (b1 ? 32 + __ffs(b1) - 1 : -1);
-    };
+    constexpr unsigned full = 0xffffffffu;
+    int pos_top = lane, row_at = lane;
+    const int ch = lane < w ? chosen[lane] : -1;
     for (int j = 0; j < w; ++j) {
-      const int r = chosen[j];
-      int p = j;
-      if (r >= 0) {  // current position of original row r
-        const int e = find(morig, r);
-        p = e >= 0 ? mpos[e] : r;
+      const int c = __shfl_sync(full, ch, j);  // original row chosen at step j, -1 = zero column
+      const int pc = __shfl_sync(full, pos_top, c & 31);
+      const int x = __shfl_sync(full, row_at, j);  // original row at position j (a top row)
+      const int p = c < 0 ? j : (c < w ? pc : c);   // current position of row c
+      if (c >= 0 && p != j) {  // row c -> position j, row x -> position p
+        if (lane == j) row_at = c;
+        if (lane == c) pos_top = j;
+        if (lane == p) row_at = x;
+        if (lane == x) pos_top = p;
       }
       if (crank == 0 && lane == 0) ipiv[col0 + j] = row0 + p;
-      if (p != j) {
-        const int ej = find(mpos, j), ep = find(mpos, p);
-        const int x = ej >= 0 ? morig[ej] : j;  // row now at position j
-        const int y = ep >= 0 ? morig[ep] : p;  // row now at position p
-        __syncwarp();
-        if (lane == 0) {
-          if (ej >= 0) morig[ej] = y; else { mpos[cnt] = j; morig[cnt] = y; }
-          if (ep >= 0) morig[ep] = x; else { mpos[cnt + (ej < 0)] = p; morig[cnt + (ej < 0)] = x; }
-        }
-        cnt += (ej < 0) + (ep < 0);
-        __syncwarp();
-      }
     }
-    if (lane == 0) nmoved = cnt;
-    // Interchange list for the other columns: dst = row0 + position, src = row0 + original row.
+    // final positions of this CTA's moved rows: top rows and chosen rows below them
+    if (lane < w && lane >= base && lane < base + nloc) sdst[lane - base] = pos_top;
+    if (ch >= w && ch >= base && ch < base + nloc) sdst[ch - base] = lane;
+    // interchange list for the other columns: dst = row0 + position, src = row0 + original row
     if (crank == 0) {
-      int m = 0;
-      for (int e = 0; e < cnt; ++e)
-        if (mpos[e] != morig[e]) {
-          if (lane == 0) { xlist[1 + m] = row0 + mpos[e]; xlist[1 + kMaxMov + m] = row0 + morig[e]; }
-          ++m;
-        }
-      if (lane == 0) xlist[0] = m;
+      const unsigned lt = (1u << lane) - 1u;
+      const bool m1 = lane < w && row_at != lane;  // top position holding another row
+      const bool m2 = lane < w && pos_top >= w;    // top row moved below the top rows
+      const unsigned b1 = __ballot_sync(full, m1), b2 = __ballot_sync(full, m2);
+      const int n1 = __popc(b1);
+      if (m1) {
+        const int i = __popc(b1 & lt);
+        xlist[1 + i] = row0 + lane;
+        xlist[1 + kMaxMov + i] = row0 + row_at;
+      }
+      if (m2) {
+        const int i = n1 + __popc(b2 & lt);
+        xlist[1 + i] = row0 + pos_top;
+        xlist[1 + kMaxMov + i] = row0 + lane;
+      }
+      if (lane == 0) xlist[0] = n1 + __popc(b2);
     }
   }
   __syncthreads();
   // coalesced write-back: one row per warp step, one column per lane, to its final position
-  for (int r = warp; r < nloc; r += NW) {
-    const int g = base + r;
-    const unsigned h0 = __ballot_sync(0xffffffffu, lane < nmoved && morig[lane] == g);
-    const unsigned h1 = __ballot_sync(0xffffffffu, lane + 32 < nmoved && morig[lane + 32] == g);
-    const int dst = h0 ? mpos[__ffs(h0) - 1] : (h1 ? mpos[32 + __ffs(h1) - 1] : g);
-    if (lane < w) M.put(row0 + dst, col0 + lane, R[lane * kPanelRows + r]);
+  for (int r0 = warp; r0 < nloc; r0 += NW * 8) {
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int r = r0 + u * NW;
+      if (r < nloc && lane < w) M.put(row0 + sdst[r], col0 + lane, R[lane * kPanelRows + r]);
+    }
   }
 }
 
