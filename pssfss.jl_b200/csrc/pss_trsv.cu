@@ -302,12 +302,18 @@ __global__ void __launch_bounds__(256) k_resid(int n, const cd *__restrict__ A0,
   }
 }
 
-// Residual for up to 4 right-hand sides (the sweep's usual case): a CTA of 8 warps takes 32
-// rows, each warp 4 of them; the columns go in chunks whose X block (4 x 256) is staged in
-// shared memory and reused by the 4 rows of every warp, so the matrix rows are the only
-// HBM stream (each read once) and the kernel runs at the memory roofline.
-constexpr int kResRows = 4, kResChunk = 1024;
+// Residual for up to 4 right-hand sides (the sweep's usual case): a CTA of 8 warps takes 16
+// rows, each warp 2 of them; the columns go in chunks whose X block (4 x 1024) is staged in
+// shared memory and reused by the rows of every warp, so the matrix rows are the only HBM
+// stream (each read once, streaming loads).  The column loop has no early exit (the ragged
+// last chunk is predicated), so the loads of several steps are in flight per lane; rows past
+// n are clamped to row n-1 for their loads and dropped at the end.
+constexpr int kResRows = 2, kResChunk = 1024;
 constexpr int kResSmem = 4 * kResChunk * (int)sizeof(cd);  // 64 KB
+__device__ __forceinline__ cd ldcs(const cd *p) {
+  const double2 v = __ldcs(reinterpret_cast<const double2 *>(p));
+  return cd{v.x, v.y};
+}
 __global__ void __launch_bounds__(256) k_resid4(int n, const cd *__restrict__ A0, long long ld, long long ms, int nrhs,
                                                 const cd *__restrict__ X0, const cd *__restrict__ B0,
                                                 cd *__restrict__ R0, long long vs, double *norms0, Ctrl ctrl) {
@@ -320,35 +326,40 @@ __global__ void __launch_bounds__(256) k_resid4(int n, const cd *__restrict__ A0
   cd(*xs)[kResChunk] = reinterpret_cast<cd(*)[kResChunk]>(res_smem);  // [4][kResChunk]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int r0 = blockIdx.x * (8 * kResRows) + warp * kResRows;
+  const cd *arow[kResRows];
   cd acc[kResRows][4];
   double rs[kResRows];
 #pragma unroll
   for (int i = 0; i < kResRows; ++i) {
+    arow[i] = A + (long long)min(r0 + i, n - 1) * ld;
     rs[i] = 0.0;
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = mkcd(0, 0);
   }
   for (int t0 = 0; t0 < n; t0 += kResChunk) {
+    const int len = min(kResChunk, n - t0);
     __syncthreads();
     for (int e = threadIdx.x; e < 4 * kResChunk; e += blockDim.x) {
       const int j = e / kResChunk, t = e % kResChunk;
-      xs[j][t] = (j < nrhs && t0 + t < n) ? X[(size_t)j * n + t0 + t] : mkcd(0, 0);
+      xs[j][t] = (j < nrhs && t < len) ? X[(size_t)j * n + t0 + t] : mkcd(0, 0);
     }
     __syncthreads();
+    const int qn = (len + 31) >> 5;
 #pragma unroll 4
-    for (int q = 0; q < kResChunk / 32; ++q) {
+    for (int q = 0; q < qn; ++q) {
       const int t = q * 32 + lane;
-      if (t0 + t >= n) break;
+      const bool ok = t < len;
+      cd av[kResRows];
+#pragma unroll
+      for (int i = 0; i < kResRows; ++i) av[i] = ok ? ldcs(arow[i] + t0 + t) : mkcd(0, 0);
       cd xv[4];
 #pragma unroll
       for (int j = 0; j < 4; ++j) xv[j] = xs[j][t];
 #pragma unroll
       for (int i = 0; i < kResRows; ++i) {
-        if (r0 + i >= n) continue;
-        const cd av = A[(long long)(r0 + i) * ld + t0 + t];
-        rs[i] += cabs1(av);
+        rs[i] += cabs1(av[i]);
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = acc[i][j] + av * xv[j];
+        for (int j = 0; j < 4; ++j) acc[i][j] = acc[i][j] + av[i] * xv[j];
       }
     }
   }
