@@ -158,3 +158,67 @@ def test_strip_grating_analytic(cls):
     g = res[0].gsm
     for k in ex:
         assert np.abs(g[k] - ex[k]).max() < 0.01
+
+
+def _simplex_integral(f, singular_at_origin, tol=1e-12):
+    """Integral of f(xi, eta) over the unit simplex xi, eta >= 0, xi + eta <= 1.
+
+    A 1/r singularity at the vertex (0, 0) is removed by the Duffy map xi = s(1-t), eta = s t
+    (Jacobian s); otherwise the plain iterated integral is used.  Adaptive QUADPACK (scipy).
+    """
+    from scipy.integrate import dblquad
+    if singular_at_origin:
+        val, _ = dblquad(lambda t, s: s * f(s * (1 - t), s * t), 0, 1, 0, 1, epsabs=0, epsrel=tol)
+    else:
+        val, _ = dblquad(lambda eta, xi: f(xi, eta), 0, 1, 0, lambda xi: 1 - xi, epsabs=0, epsrel=tol)
+    return val
+
+
+def test_filljk_singular_terms_vs_cubature():
+    # test/Zint_test.jl:70-101: the closed-form singular integrals of filljk! (the smoothing-
+    # normalised rinv = (1/u) ∫∫ 1/|r| and ρ_r = ∫∫ r/|r| over the source simplex, observation
+    # at the match centroid) against adaptive cubature, 1e-7 relative.  Same ring geometry and
+    # u = 0.4 max|β|; this mesh is the structured one of elements.polyring.
+    from pssfss_b200.elements import polyring
+    sheet = polyring(ntri=100, sides=32, a=[0.4957], b=[0.5557], s1=[1.1414, 0.0],
+                     s2=[0.5707, 0.9885], units=inch)
+    rwg = setup_rwg(sheet)
+    nface, nufp = sheet.nface, rwg.nufp
+    u = 0.4 * max(np.linalg.norm(sheet.beta1), np.linalg.norm(sheet.beta2))
+    jk = oracle.filljk(sheet, rwg, u, 0.0, 0.0)
+    rho = np.asarray(sheet.rho, float)
+    fv = np.asarray(sheet.fv) - 1
+
+    def vtx(f):
+        return [rho[fv[k, f]] for k in range(3)]
+
+    def twice_area(r):
+        a, b = r[1] - r[0], r[2] - r[0]
+        return abs(a[0] * b[1] - a[1] * b[0])
+
+    def integrals(rm, rs, singular):
+        def pt(xi, eta):
+            return rs[0] + xi * (rs[1] - rs[0]) + eta * (rs[2] - rs[0]) - rm
+        inv = _simplex_integral(lambda x, e: 1 / np.linalg.norm(pt(x, e)), singular)
+        rr = [_simplex_integral(lambda x, e, c=c: pt(x, e)[c] / np.linalg.norm(pt(x, e)), singular)
+              for c in (0, 1)]
+        return inv, np.array(rr)
+
+    for iufp in (1, 2, 3, nufp - 3, nufp - 2, nufp - 1, nufp):
+        lin = int(rwg.ufp2fp[iufp - 1][0]) - 1  # column-major (match, source)
+        ifm, ifs = lin % nface, lin // nface
+        rs = vtx(ifs)
+        rm = sum(vtx(ifm)) / 3
+        if ifm == ifs:  # split at the centroid so the singular point is a vertex
+            inv, rr, a2 = 0.0, np.zeros(2), twice_area(rs)
+            for p, q in ((0, 1), (0, 2), (1, 2)):
+                sub = [rm, rs[p], rs[q]]
+                i1, r1 = integrals(rm, sub, True)
+                w = twice_area(sub) / a2
+                inv += w * i1
+                rr += w * r1
+        else:
+            inv, rr = integrals(rm, rs, False)
+        assert abs((u * jk.rinv[iufp - 1] - inv) / inv) < 1e-7
+        got = jk.rho_r[2 * (iufp - 1):2 * iufp]
+        assert np.linalg.norm((got - rr) / rr) < 1e-7
