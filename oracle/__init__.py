@@ -206,12 +206,18 @@ def fill(k0, u, layers, s, psi1, psi2, sheet, rwg, jk=None):
     tabs = modal_tables(magnetic, k0, u, psi1, psi2, layers, s, b1, b2, b00, 1e-7)
     key = id(sheet)
     if jk is None:
-        jk = _jk_cache.get(key)
+        # the entry keeps its sheet alive, so a hit is this very sheet (an id is reused only
+        # after its object is gone)
+        held, jk = _jk_cache.get(key, (None, None))
+        if held is not sheet:
+            jk = None
         # FillZY.jl:97-99 cache test
         if (jk is None or psi1 != jk.psi1 or psi2 != jk.psi2 or jk.u == 0
                 or abs((u / upm - jk.u) / jk.u) > 1e-4):
             jk = filljk(sheet, rwg, u / upm, psi1, psi2)
-            _jk_cache[key] = jk
+            if len(_jk_cache) >= 16:
+                _jk_cache.clear()
+            _jk_cache[key] = (sheet, jk)
     a = sheet_arrays(sheet, rwg)
     eps, mu, w = _layer_arrays(layers)
     nbf = rwg.nbf

@@ -1,0 +1,34 @@
+"""Finite-difference gradient driver of the meander differentiation workload, run through
+the oracle's analyze on a small mesh (the CUDA sweep is the same call with the default
+``analyze_fn``).  Objective Σ_f (|S21_TE|² − |S21_TM|²) with respect to trace width, pitch
+and substrate permittivity, central differences with a 1e-4 relative step."""
+import pytest
+
+import oracle
+from pssfss_b200.gradient import (fd_gradient, meander_gradient, meander_strata, meander_topology,
+                                  te_tm_transmission_objective)
+
+P0 = {"w": 0.3, "a": 5.0, "epsr": 2.2}
+FREQS = [9.0, 15.0]
+NTRI = 120
+
+
+def test_meander_fd_gradient_converges_in_step():
+    f0, g4 = meander_gradient(P0, FREQS, ntri=NTRI, rel_step=1e-4, analyze_fn=oracle.analyze)
+    direct = te_tm_transmission_objective(
+        oracle.analyze(meander_strata(P0, ntri=NTRI), FREQS, {"θ": 0.0, "ϕ": 0.0}))
+    assert abs(f0 - direct) <= 1e-12 * max(1.0, abs(direct))
+    _, g3 = meander_gradient(P0, FREQS, ntri=NTRI, rel_step=1e-3, analyze_fn=oracle.analyze)
+    for k in P0:
+        assert g4[k] != 0.0
+        # central differences: O(h^2) truncation, so the two steps agree closely
+        assert abs(g4[k] - g3[k]) <= 1e-4 * abs(g4[k]) + 1e-9, (k, g4[k], g3[k])
+
+
+def test_fd_gradient_rejects_topology_change():
+    # a 20% width step changes the meander's segment counts
+    assert meander_topology({**P0, "w": 0.36}, ntri=NTRI) != meander_topology(P0, ntri=NTRI)
+    with pytest.raises(ValueError, match="topology"):
+        fd_gradient(lambda p: meander_strata(p, ntri=NTRI), P0, FREQS, {"θ": 0.0, "ϕ": 0.0},
+                    te_tm_transmission_objective, rel_step=0.2,
+                    topology=lambda p: meander_topology(p, ntri=NTRI), analyze_fn=oracle.analyze)
