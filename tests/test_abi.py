@@ -40,3 +40,33 @@ def test_no_device_error_is_reported_not_raised_in_c():
     rc = engine.lib().pss_ctx_create(0, 1, ctypes.byref(h))
     assert rc != 0
     assert b"device" in engine.lib().pss_last_error().lower() or b"cuda" in engine.lib().pss_last_error().lower()
+
+
+def test_entry_points_reject_bad_arguments_before_any_device_use():
+    # Every export returns 0 or a negative code with a message and never aborts; these checks
+    # run before a device is touched, so they hold on a machine without a GPU.
+    import ctypes
+    L = engine.lib()
+    nul = None
+    buf = (ctypes.c_double * 8)()
+    ibuf = (ctypes.c_int * 8)()
+
+    def err():
+        return L.pss_last_error().decode()
+
+    assert L.pss_ctx_destroy(nul) == 0 and L.pss_sheet_destroy(nul) == 0
+    assert L.pss_partial_gsms(nul, 1, buf, buf, buf, 1, 1.0, 1, buf, buf, 1, buf, buf, buf, buf, 0,
+                              buf, ibuf) == -1 and "null" in err()
+    assert L.pss_fill_matrix(nul, 1, buf, buf, buf, 1, 1.0, 1.0, 0.0, 0.0, buf,
+                             ctypes.byref(ctypes.c_int())) == -1 and "null" in err()
+    assert L.pss_face_integrals(nul, 1.0, 0.0, 0.0, *([buf] * 9)) == -1 and "null" in err()
+    assert L.pss_basis_transforms(nul, 1, buf, 0.0, 0.0, buf) == -1 and "invalid" in err()
+    assert L.pss_lu_solve(nul, 4, buf, 1, buf, 0, buf, ibuf) == -1 and "invalid" in err()
+    assert L.pss_profile(nul, 1) == -1 and L.pss_last_timings(nul, buf) == -1
+    h = ctypes.c_void_p()
+    assert L.pss_sheet_create(nul, b"J", 1.0, buf, buf, buf, buf, 0, buf, 0, ibuf, ibuf, buf, 0, 0, ibuf,
+                              ibuf, ibuf, 0, ibuf, ibuf, ctypes.byref(h)) == -1 and "null" in err()
+    # the no-allocation LU: invalid shapes and orders beyond its fixed scratch array
+    assert L.pss_lu_factor_noalloc(0, buf, 1, ibuf, ibuf, nul) == -1 and "invalid" in err()
+    assert L.pss_lu_factor_noalloc(4, buf, 2, ibuf, ibuf, nul) == -1 and "invalid" in err()
+    assert L.pss_lu_factor_noalloc(9000, buf, 9000, ibuf, ibuf, nul) == -1 and "exceeds" in err()
