@@ -3,6 +3,7 @@
 There is no CPU fallback: if the library cannot be loaded or no CUDA device is present,
 every call raises ``RuntimeError``.
 """
+import collections
 import ctypes
 import os
 import threading
@@ -23,7 +24,10 @@ FATAL_STATUS = 4 | 16 | 64
 _lib = None
 _lock = threading.Lock()
 _ctx = {}
-_sheets = {}
+# uploaded sheets, most recently used last; a sheet's device arrays (its face-pair integral
+# cache grows as nface^2 for unstructured sheets) are freed when it falls out
+_sheets = collections.OrderedDict()
+SHEET_CACHE = max(1, int(os.environ.get("PSS_SHEET_CACHE", "8")))
 
 _P = ctypes.c_void_p
 _D = ctypes.c_double
@@ -120,14 +124,13 @@ def context(device=0, nworkers=None):
         queues = int(os.environ.get("CUDA_DEVICE_MAX_CONNECTIONS", "8"))
         nworkers = int(os.environ.get("PSS_WORKERS", str(max(1, min(3, queues)))))
     key = (device, nworkers)
+    L = lib()
     with _lock:
         c = _ctx.get(key)
-    if c is None:
-        h = ctypes.c_void_p()
-        _check(lib().pss_ctx_create(device, nworkers, ctypes.byref(h)), "pss_ctx_create")
-        c = h
-        with _lock:
-            _ctx[key] = c
+        if c is None:
+            h = ctypes.c_void_p()
+            _check(L.pss_ctx_create(device, nworkers, ctypes.byref(h)), "pss_ctx_create")
+            c = _ctx[key] = h
     return c
 
 
@@ -171,10 +174,18 @@ class DeviceSheet:
 def device_sheet(sheet, rwg, device=0, nworkers=None):
     ctx = context(device, nworkers)
     key = (id(sheet), id(rwg), ctx.value)
-    ds = _sheets.get(key)
-    if ds is None or ds.sheet is not sheet or ds.rwg is not rwg:
-        ds = DeviceSheet(ctx, sheet, rwg)
+    evicted = []
+    with _lock:
+        ds = _sheets.get(key)
+        if ds is not None and ds.sheet is sheet and ds.rwg is rwg:
+            _sheets.move_to_end(key)
+            return ds
+    ds = DeviceSheet(ctx, sheet, rwg)
+    with _lock:
         _sheets[key] = ds
+        while len(_sheets) > SHEET_CACHE:
+            evicted.append(_sheets.popitem(last=False)[1])
+    del evicted  # pss_sheet_destroy runs here, outside the lock
     return ds
 
 

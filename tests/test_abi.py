@@ -70,3 +70,33 @@ def test_entry_points_reject_bad_arguments_before_any_device_use():
     assert L.pss_lu_factor_noalloc(0, buf, 1, ibuf, ibuf, nul) == -1 and "invalid" in err()
     assert L.pss_lu_factor_noalloc(4, buf, 2, ibuf, ibuf, nul) == -1 and "invalid" in err()
     assert L.pss_lu_factor_noalloc(9000, buf, 9000, ibuf, ibuf, nul) == -1 and "exceeds" in err()
+
+
+def test_device_sheet_cache_is_bounded_and_reuses_entries(monkeypatch):
+    # Host logic of the binding: an uploaded sheet is reused while cached, and the least
+    # recently used one is released once more than SHEET_CACHE sheets were uploaded.
+    import ctypes
+    made, freed = [], []
+
+    class FakeDeviceSheet:
+        def __init__(self, ctx, sheet, rwg):
+            self.sheet, self.rwg = sheet, rwg
+            made.append(sheet)
+
+        def __del__(self):
+            freed.append(self.sheet)
+
+    monkeypatch.setattr(engine, "context", lambda device=0, nworkers=None: ctypes.c_void_p(1))
+    monkeypatch.setattr(engine, "DeviceSheet", FakeDeviceSheet)
+    monkeypatch.setattr(engine, "SHEET_CACHE", 2)
+    monkeypatch.setattr(engine, "_sheets", engine.collections.OrderedDict())
+    s = [object() for _ in range(3)]
+    r = object()
+    a = engine.device_sheet(s[0], r)
+    assert engine.device_sheet(s[0], r) is a and made == [s[0]]
+    engine.device_sheet(s[1], r)
+    engine.device_sheet(s[0], r)          # s[0] becomes the most recent
+    engine.device_sheet(s[2], r)          # evicts s[1]
+    assert made == [s[0], s[1], s[2]] and freed == [s[1]]
+    assert [v.sheet for v in engine._sheets.values()] == [s[0], s[2]]
+    del a
