@@ -278,3 +278,51 @@ def analyze(strata, flist, steering):
             out.append(A.add_scattered(io, dS))
         partial[ig] = out
     return A.assemble(plan, partial)
+
+
+def partial_dS_linearized(sheet, rwg, region, s, k0, u, io, perturbed):
+    """Scattered partial GSM at a point and, for each perturbed input set, its first-order
+    (in the perturbation) value from the unperturbed factorisation:
+
+        dS_k = wobs_k * (P_k Z^-1 R_k - Lambda^T (Z_k - Z) X),  X = Z^-1 R,  Lambda = Z^-T P^T,
+
+    exact to O(h^2), so central differences of dS_k give dS/dp to O(h^2) with one
+    factorisation.  ``perturbed``: list of (sheet_k, rwg_k, region_k, u_k, io_k) with the
+    topology of ``sheet``.  The same projection as ``partial_dS`` (PSSFSS.jl:391-457)."""
+    import scipy.linalg as sl
+    Z, _ = fill(k0, u, region, s, io.psi1, io.psi2, sheet, rwg)
+    nm = len(io.wobs)
+
+    def rp(sh, rw, io_):
+        bf = [rwgbfft(rw, sh, io_.kvec[j], io_.psi1, io_.psi2) for j in range(nm)]
+        R = np.stack([np.conj(bf[j]) @ io_.src[j] for j in range(nm)], axis=1)
+        P = np.stack([bf[i] @ io_.tobs[i] for i in range(nm)])
+        return R, P
+
+    R, P = rp(sheet, rwg, io)
+    lu = sl.lu_factor(Z, check_finite=False)
+    X = sl.lu_solve(lu, R, check_finite=False)
+    Lam = sl.lu_solve(lu, P.T, trans=1, check_finite=False)  # Z^T Lambda = P^T
+    dS = io.wobs[:, None] * (P @ X)
+    out = []
+    for sh_k, rw_k, region_k, u_k, io_k in perturbed:
+        Zk, _ = fill(k0, u_k, region_k, s, io_k.psi1, io_k.psi2, sh_k, rw_k)
+        Rk, Pk = rp(sh_k, rw_k, io_k)
+        Xk = sl.lu_solve(lu, Rk, check_finite=False)
+        out.append(io_k.wobs[:, None] * (Pk @ Xk - Lam.T @ ((Zk - Z) @ X)))
+    return dS, out
+
+
+def partial_gsms_linearized(sheet, rwg, points, region_rng, s, u, ios, perturbed):
+    """``partial_dS_linearized`` over the points of one sheet Gblock.  ``perturbed``: list
+    of (sheet_k, rwg_k, points_k, u_k, ios_k).  Returns (dS per point, [dS_k per point])."""
+    i1, i2 = region_rng
+    dS, lin = [], [[] for _ in perturbed]
+    for p, pt in enumerate(points):
+        pk = [(sh_k, rw_k, pts_k[p].layers[i1 - 1:i2], u_k, ios_k[p])
+              for sh_k, rw_k, pts_k, u_k, ios_k in perturbed]
+        d, ds_k = partial_dS_linearized(sheet, rwg, pt.layers[i1 - 1:i2], s, pt.k0, u, ios[p], pk)
+        dS.append(d)
+        for k, v in enumerate(ds_k):
+            lin[k].append(v)
+    return dS, lin

@@ -7,13 +7,20 @@ differences with a relative step (1e-4 by default): two whole sweeps per paramet
 through `analyze` (the CUDA path), so it is the finite-difference check an adjoint gradient is
 held to and a gradient in its own right.
 
+`linearized_gradient` needs one factorisation per point instead of 2·P: the partial GSM at
+p ± h is taken to first order from the factors at p (the perturbed matrices enter only through
+Λᵀ (Z± − Z) X with Λ = Z⁻ᵀ Pᵀ, and the perturbed sources through extra right-hand sides), while
+the cheap host parts (modes, incident GSMs, cascade) are recomputed at p ± h.  The device
+form of that linearised partial GSM is not built yet; its contract is the ``partial_lin``
+argument.
+
 Geometry steps must leave the mesh topology unchanged, so that vertices move affinely and the
 difference is smooth: `topology(params)` returns a key (for the meander, its segment counts,
 `Elements.jl:634-646`) that must agree at p − h, p and p + h, else `fd_gradient` raises.
 """
 import numpy as np
 
-from .analyze import analyze
+from .analyze import add_scattered, analyze, assemble, make_plan, sheet_gblocks, sheet_io
 from .elements import meander, meander_counts
 from .layers import TE, TM, Layer
 from .outputs import getsijmn
@@ -73,3 +80,62 @@ def meander_gradient(params, flist, *, ntri=4000, rel_step=1e-4, analyze_fn=None
                        {"θ": 0.0, "ϕ": 0.0}, te_tm_transmission_objective,
                        rel_step=rel_step, topology=lambda p: meander_topology(p, ntri=ntri),
                        analyze_fn=analyze_fn, **kw)
+
+
+def linearized_gradient(build, params, flist, steering, objective, partial_lin, *, rel_step=1e-4,
+                        topology=None):
+    """Objective and central-difference gradient with one factorisation per point.
+
+    ``partial_lin(sheet, rwg, points, (i1, i2), s, u, ios, perturbed)`` returns the scattered
+    partial GSMs of one sheet Gblock at ``points`` and, for each entry (sheet_k, rwg_k,
+    points_k, u_k, ios_k) of ``perturbed``, their first-order values at that perturbation
+    from the unperturbed factorisation.  Every perturbed plan must keep the points, Gblocks,
+    modes and mesh topology of the unperturbed one.  Returns ``(f(params), {name: df/dp})``.
+    """
+    p0 = {k: float(v) for k, v in params.items()}
+    key0 = topology(p0) if topology is not None else None
+    steps = []
+    for name, v in p0.items():
+        h = rel_step * abs(v) if v != 0 else rel_step
+        for sgn in (1.0, -1.0):
+            p = {**p0, name: v + sgn * h}
+            if topology is not None and topology(p) != key0:
+                raise ValueError(f"step changes the mesh topology: {topology(p)} != {key0} at {p}")
+            steps.append((name, h, p))
+    plan0 = make_plan(build(p0), flist, steering)
+    plans = [make_plan(build(p), flist, steering) for _, _, p in steps]
+    blocks = sheet_gblocks(plan0)
+    for pl in plans:
+        if (sheet_gblocks(pl) != blocks or len(pl.points) != len(plan0.points)
+                or any(len(a.layers[0].P) != len(b.layers[0].P) or len(a.layers[-1].P) != len(b.layers[-1].P)
+                       for a, b in zip(pl.points, plan0.points))):
+            raise ValueError("a step changes the points, Gblocks or modes of the sweep")
+    partial0, partials = {}, [{} for _ in steps]
+    for ig, (i1, i2), isht, s in blocks:
+        sheet, rwg = plan0.sheets[isht - 1], plan0.rwgdat[isht - 1]
+        ios0 = [sheet_io(pt.layers[i1 - 1:i2], sheet, s, pt.k0, pt.beta00) for pt in plan0.points]
+        pert = []
+        for pl in plans:
+            sh_k = pl.sheets[isht - 1]
+            if pl.rwgdat[isht - 1].nbf != rwg.nbf:
+                raise ValueError("a step changes the number of basis functions")
+            ios_k = [sheet_io(pt.layers[i1 - 1:i2], sh_k, s, pt.k0, pt.beta00) for pt in pl.points]
+            pert.append((sh_k, pl.rwgdat[isht - 1], pl.points, pl.uvec[isht - 1], ios_k))
+        dS0, lin = partial_lin(sheet, rwg, plan0.points, (i1, i2), s, plan0.uvec[isht - 1], ios0, pert)
+        partial0[ig] = [add_scattered(io, d) for io, d in zip(ios0, dS0)]
+        for k in range(len(steps)):
+            partials[k][ig] = [add_scattered(io, d) for io, d in zip(pert[k][4], lin[k])]
+    f0 = float(objective(assemble(plan0, partial0)))
+    fs = [float(objective(assemble(pl, partials[k]))) for k, pl in enumerate(plans)]
+    grad = {}
+    for k in range(0, len(steps), 2):
+        name, h, _ = steps[k]
+        grad[name] = (fs[k] - fs[k + 1]) / (2 * h)
+    return f0, grad
+
+
+def meander_linearized_gradient(params, flist, partial_lin, *, ntri=4000, rel_step=1e-4):
+    """`meander_gradient` with one factorisation per point (see `linearized_gradient`)."""
+    return linearized_gradient(lambda p: meander_strata(p, ntri=ntri), params, np.asarray(flist, float),
+                               {"θ": 0.0, "ϕ": 0.0}, te_tm_transmission_objective, partial_lin,
+                               rel_step=rel_step, topology=lambda p: meander_topology(p, ntri=ntri))

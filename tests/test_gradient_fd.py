@@ -32,3 +32,16 @@ def test_fd_gradient_rejects_topology_change():
         fd_gradient(lambda p: meander_strata(p, ntri=NTRI), P0, FREQS, {"θ": 0.0, "ϕ": 0.0},
                     te_tm_transmission_objective, rel_step=0.2,
                     topology=lambda p: meander_topology(p, ntri=NTRI), analyze_fn=oracle.analyze)
+
+
+def test_linearized_gradient_matches_full_central_differences():
+    # One factorisation per point (perturbed matrices enter as Λᵀ ΔZ X, perturbed sources as
+    # extra right-hand sides) against two full sweeps per parameter; both are central
+    # differences with the same step, so they agree to the O(h²) of the linearisation.
+    from pssfss_b200.gradient import meander_linearized_gradient
+    f_fd, g_fd = meander_gradient(P0, FREQS, ntri=NTRI, rel_step=1e-4, analyze_fn=oracle.analyze)
+    f_lin, g_lin = meander_linearized_gradient(P0, FREQS, oracle.partial_gsms_linearized, ntri=NTRI,
+                                               rel_step=1e-4)
+    assert abs(f_lin - f_fd) <= 1e-12 * abs(f_fd)
+    for k in P0:
+        assert abs(g_lin[k] - g_fd[k]) <= 1e-5 * abs(g_fd[k]), (k, g_lin[k], g_fd[k])
