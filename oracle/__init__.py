@@ -192,6 +192,11 @@ def filljk(sheet, rwg, ulocal, psi1, psi2):
 _jk_cache = {}
 
 
+def prime_jk_cache(sheet, jk):
+    """Make ``jk`` (from ``filljk``) the cached face integrals of ``sheet`` for ``fill``."""
+    _jk_cache[id(sheet)] = (sheet, jk)
+
+
 def fill(k0, u, layers, s, psi1, psi2, sheet, rwg, jk=None):
     """``fillz`` (FillZY.jl:50) for class 'J' sheets, ``filly`` (FillZY.jl:273) for 'M'.
 
