@@ -220,7 +220,7 @@ def fill(k0, u, layers, s, psi1, psi2, sheet, rwg, jk=None):
         if (jk is None or psi1 != jk.psi1 or psi2 != jk.psi2 or jk.u == 0
                 or abs((u / upm - jk.u) / jk.u) > 1e-4):
             jk = filljk(sheet, rwg, u / upm, psi1, psi2)
-            if len(_jk_cache) >= 16:
+            if len(_jk_cache) >= 4:
                 _jk_cache.clear()
             _jk_cache[key] = (sheet, jk)
     a = sheet_arrays(sheet, rwg)
