@@ -45,4 +45,4 @@ def golden(key):
         with open(os.path.join(ROOT, "tests", "golden", "reference_golden.json")) as f:
             _GOLDEN = json.load(f)
     g = _GOLDEN[key]
-    return [complex(re_, im) for re_, im in g["values"]], g
+    return [complex(re_, im) for re_, im in g.get("values", [])], g

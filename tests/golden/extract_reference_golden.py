@@ -45,6 +45,15 @@ def main(ref):
         "rwgbfft_inch": {"source": "test/RWGData_test.jl:56-58", "k": [20.0, -30.3], "psi": [0.8, -0.7],
                          "values": cplx_on(rwg, 56, 58)},
     }
+    # mode counts per layer after choose_layer_modes! (test/Modes_test.jl, three testsets)
+    md = read("Modes_test.jl")
+    counts = []
+    for i, ln in enumerate(md, 1):
+        m = re.search(r"@test \[length\(l\.P\) for l in strata if l isa Layer\] == \[([\d,\s]+)\]", ln)
+        if m:
+            counts.append({"line": i, "counts": [int(x) for x in m.group(1).split(",")]})
+    gold["layer_mode_counts"] = {"source": "test/Modes_test.jl", "cases": counts}
+    assert len(counts) == 3, counts
     for key, n in (("fillz", 2), ("filly", 2), ("modal_series_electric", 4), ("modal_series_magnetic", 4),
                    ("rwgbfft_mm", 6), ("rwgbfft_inch", 6)):
         assert len(gold[key]["values"]) == n, (key, gold[key]["values"])

@@ -151,3 +151,45 @@ def test_structured_ring_and_cross_meshes():
         assert counts.min() >= 1 and counts.max() <= 2
         rwg = setup_rwg(sh)
         assert rwg.nbf == int((counts == 2).sum())
+
+
+def _duroid():
+    from pssfss_b200.units import mil
+    return Layer(name="Duroid 6035", epsr=3.6, tandel=0.0013, width=Length(20, mil))
+
+
+def test_choose_layer_modes_counts():
+    # test/Modes_test.jl: modes kept per layer by choose_layer_modes! for two ring screens on
+    # Duroid with vacuum gaps, 2-8 GHz, dbmin = 25 (the count depends on the lattices and the
+    # layers, not on the ring's triangulation).
+    from pssfss_b200.constants import C0, TWOPI
+    from pssfss_b200.elements import polyring
+    from pssfss_b200.gsms import choose_gblocks
+    from pssfss_b200.modes import choose_layer_modes
+    from pssfss_b200.sheets import RWGSheet
+
+    def ring(p):
+        return polyring(sides=4, orient=45, a=[0.1902], b=[0.2169], units=inch, s1=[p, 0], s2=[0, p], ntri=100)
+
+    vac = lambda w=None: Layer(name="Vacuum") if w is None else Layer(name="Vacuum", width=Length(w, inch))
+    cases = [
+        [vac(), _duroid(), ring(0.5117), _duroid(), vac(0.2), _duroid(), ring(0.5117), _duroid(), vac()],
+        [vac(), _duroid(), ring(0.5117), _duroid(), vac(0.1), vac(0.1), _duroid(), ring(0.9005), _duroid(), vac()],
+        [vac(), _duroid(), ring(0.5117), _duroid(), vac(0.1), vac(0.1), _duroid(), ring(0.5117), _duroid(), vac()],
+    ]
+    want = [c["counts"] for c in golden("layer_mode_counts")[1]["cases"]]
+    for strata, expect in zip(cases, want):
+        layers = [s for s in strata if isinstance(s, Layer)]
+        sheets = [s for s in strata if isinstance(s, RWGSheet)]
+        junc = [0] * (len(layers) - 1)
+        nlay = ns = 0
+        for s in strata:
+            if isinstance(s, Layer):
+                nlay += 1
+            else:
+                ns += 1
+                junc[nlay - 1] = ns
+        k0min, k0max = TWOPI * 2e9 / C0, TWOPI * 8e9 / C0
+        gbl = choose_gblocks(layers, sheets, junc, k0min)
+        choose_layer_modes(layers, sheets, junc, gbl, k0max, 25.0)
+        assert [len(l.P) for l in layers] == expect
