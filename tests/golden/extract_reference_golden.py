@@ -54,6 +54,21 @@ def main(ref):
             counts.append({"line": i, "counts": [int(x) for x in m.group(1).split(",")]})
     gold["layer_mode_counts"] = {"source": "test/Modes_test.jl", "cases": counts}
     assert len(counts) == 3, counts
+    # Gblocks chosen by choose_gblocks (test/GSMs_test.jl, testsets choose_gblocks1..4):
+    # Gblock(first:last, j) literals of each testset's @test lines, in order
+    gs = read("GSMs_test.jl")
+    starts = [i for i, ln in enumerate(gs, 1) if re.search(r'@testset "choose_gblocks\d"', ln)]
+    cases = []
+    for k, lo in enumerate(starts):
+        hi = starts[k + 1] - 1 if k + 1 < len(starts) else len(gs)
+        blocks = []
+        for i in range(lo, hi + 1):
+            if "@test" in gs[i - 1] and "@testset" not in gs[i - 1]:
+                blocks += [[int(a), int(b), int(j)] for a, b, j in
+                           re.findall(r"Gblock\((\d+):(\d+),\s*(\d+)\)", gs[i - 1])]
+        cases.append({"lines": [lo, hi], "gblocks": blocks})
+    gold["gblocks"] = {"source": "test/GSMs_test.jl", "cases": cases}
+    assert [len(c["gblocks"]) for c in cases] == [2, 2, 2, 3], cases
     for key, n in (("fillz", 2), ("filly", 2), ("modal_series_electric", 4), ("modal_series_magnetic", 4),
                    ("rwgbfft_mm", 6), ("rwgbfft_inch", 6)):
         assert len(gold[key]["values"]) == n, (key, gold[key]["values"])

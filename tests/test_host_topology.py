@@ -153,6 +153,28 @@ def test_structured_ring_and_cross_meshes():
         assert rwg.nbf == int((counts == 2).sum())
 
 
+def _split_strata(strata):
+    """Layers, sheets and junc (sheet number at each interface, 0 = none) as in
+    PSSFSS.jl:205-213."""
+    from pssfss_b200.sheets import RWGSheet
+    layers = [s for s in strata if isinstance(s, Layer)]
+    sheets = [s for s in strata if isinstance(s, RWGSheet)]
+    junc = [0] * (len(layers) - 1)
+    nlay = ns = 0
+    for s in strata:
+        if isinstance(s, Layer):
+            nlay += 1
+        else:
+            ns += 1
+            junc[nlay - 1] = ns
+    return layers, sheets, junc
+
+
+def _ring(p):
+    from pssfss_b200.elements import polyring
+    return polyring(sides=4, orient=45, a=[0.1902], b=[0.2169], units=inch, s1=[p, 0], s2=[0, p], ntri=100)
+
+
 def _duroid():
     from pssfss_b200.units import mil
     return Layer(name="Duroid 6035", epsr=3.6, tandel=0.0013, width=Length(20, mil))
@@ -163,33 +185,45 @@ def test_choose_layer_modes_counts():
     # Duroid with vacuum gaps, 2-8 GHz, dbmin = 25 (the count depends on the lattices and the
     # layers, not on the ring's triangulation).
     from pssfss_b200.constants import C0, TWOPI
-    from pssfss_b200.elements import polyring
     from pssfss_b200.gsms import choose_gblocks
     from pssfss_b200.modes import choose_layer_modes
-    from pssfss_b200.sheets import RWGSheet
-
-    def ring(p):
-        return polyring(sides=4, orient=45, a=[0.1902], b=[0.2169], units=inch, s1=[p, 0], s2=[0, p], ntri=100)
 
     vac = lambda w=None: Layer(name="Vacuum") if w is None else Layer(name="Vacuum", width=Length(w, inch))
     cases = [
-        [vac(), _duroid(), ring(0.5117), _duroid(), vac(0.2), _duroid(), ring(0.5117), _duroid(), vac()],
-        [vac(), _duroid(), ring(0.5117), _duroid(), vac(0.1), vac(0.1), _duroid(), ring(0.9005), _duroid(), vac()],
-        [vac(), _duroid(), ring(0.5117), _duroid(), vac(0.1), vac(0.1), _duroid(), ring(0.5117), _duroid(), vac()],
+        [vac(), _duroid(), _ring(0.5117), _duroid(), vac(0.2), _duroid(), _ring(0.5117), _duroid(), vac()],
+        [vac(), _duroid(), _ring(0.5117), _duroid(), vac(0.1), vac(0.1), _duroid(), _ring(0.9005), _duroid(), vac()],
+        [vac(), _duroid(), _ring(0.5117), _duroid(), vac(0.1), vac(0.1), _duroid(), _ring(0.5117), _duroid(), vac()],
     ]
     want = [c["counts"] for c in golden("layer_mode_counts")[1]["cases"]]
     for strata, expect in zip(cases, want):
-        layers = [s for s in strata if isinstance(s, Layer)]
-        sheets = [s for s in strata if isinstance(s, RWGSheet)]
-        junc = [0] * (len(layers) - 1)
-        nlay = ns = 0
-        for s in strata:
-            if isinstance(s, Layer):
-                nlay += 1
-            else:
-                ns += 1
-                junc[nlay - 1] = ns
+        layers, sheets, junc = _split_strata(strata)
         k0min, k0max = TWOPI * 2e9 / C0, TWOPI * 8e9 / C0
         gbl = choose_gblocks(layers, sheets, junc, k0min)
         choose_layer_modes(layers, sheets, junc, gbl, k0max, 25.0)
         assert [len(l.P) for l in layers] == expect
+
+
+def test_choose_gblocks():
+    # test/GSMs_test.jl choose_gblocks1..4: Gblock(first:last, j) for sheets on thin layers
+    # and separated by gaps (a gap whose evanescent modes decay enough splits the Gblocks).
+    from pssfss_b200.constants import C0, TWOPI
+    from pssfss_b200.gsms import choose_gblocks
+    from pssfss_b200.units import cm, mil
+
+    def strip():
+        return rectstrip(units=cm, Px=1, Py=1, Lx=0.5, Ly=0.5, Nx=10, Ny=10)
+
+    vac = lambda w=None, u=inch: Layer(name="Vacuum") if w is None else Layer(name="Vacuum", width=Length(w, u))
+    cases = [
+        ([Layer(), strip(), Layer(width=Length(1, mil), epsr=2.2), Layer(width=Length(1, mil)),
+          Layer(width=Length(3, mm)), strip(), Layer(width=Length(1, mil), epsr=2.2), Layer()], 10e9),
+        ([vac(), _duroid(), _ring(0.5117), _duroid(), vac(0.05), _duroid(), _ring(0.5117), _duroid(), vac()], 2e9),
+        ([vac(), _duroid(), _ring(0.5117), _duroid(), _duroid(), _ring(0.5117), _duroid(), vac()], 2e9),
+        ([vac(), _duroid(), _ring(0.5117), _duroid(), vac(5, mil), _duroid(), _ring(0.5117), _duroid(),
+          vac(5, mil), _duroid(), _ring(0.5117), _duroid(), vac()], 2e9),
+    ]
+    want = [c["gblocks"] for c in golden("gblocks")[1]["cases"]]
+    for (strata, f), expect in zip(cases, want):
+        layers, sheets, junc = _split_strata(strata)
+        gbl = choose_gblocks(layers, sheets, junc, TWOPI * f / C0)
+        assert [[g.first, g.last, g.j] for g in gbl] == expect
