@@ -15,7 +15,7 @@ import math
 
 import numpy as np
 
-from .sheets import RWGSheet, combine, recttri, rotate, s1s2_to_b1b2
+from .sheets import RWGSheet, combine, recttri, rotate, s1s2_to_b1b2, translate
 
 _DEFAULTS = dict(cls="J", dx=0.0, dy=0.0, rot=0.0, Rsheet=0.0, save="", fufp=False)
 
@@ -174,6 +174,89 @@ def meander(*, a, b, h, w1, w2, ntri, units, orient=0.0, **kwarg):
     rotate(sheet, kwargs["rot"])
     if kwargs["dx"] != 0 or kwargs["dy"] != 0:
         sheet.rho = np.array([[kwargs["dx"] + x, kwargs["dy"] + y] for x, y in sheet.rho])
+    sheet.xi_eta_check = True
+    return sheet
+
+
+def _tritri(w, nw):
+    """Isosceles right triangle, apex at the origin, base of length ``w`` on x = w/2
+    bisected by the x-axis (``Elements.jl:296``).  Nodes on the grid of the reference's
+    layout (spacing w/nw; for odd nw the columns sit at half steps and the apex is alone);
+    the columns are joined by squares split on a diagonal and one half-square at each end,
+    a structured triangulation of the region the reference hands to Triangle."""
+    dxy = w / nw
+    cols = []
+    if nw % 2 == 0:
+        k = nw // 2
+        for i in range(k + 1):
+            cols.append([(i * dxy, j * dxy) for j in range(-i, i + 1)])
+    else:
+        k = (nw + 1) // 2
+        cols.append([(0.0, 0.0)])
+        for mx in range(1, k + 1):
+            x = (2 * mx - 1) / 2 * dxy
+            cols.append([(x, -x + t * dxy) for t in range(2 * mx)])
+    rho, ids = [], []
+    for col in cols:
+        ids.append(list(range(len(rho), len(rho) + len(col))))
+        rho.extend(col)
+    tris = []
+    for a, b in zip(ids[:-1], ids[1:]):
+        if len(b) == 2:  # odd nw: the lone apex and the first half-step column
+            tris.append((a[0], b[0], b[1]))
+            continue
+        # column b has two more nodes than a, one beyond each end; node a[t] aligns with b[t+1]
+        tris.append((a[0], b[0], b[1]))                  # lower end
+        for t in range(len(a) - 1):                       # squares
+            tris.append((a[t], b[t + 1], b[t + 2]))
+            tris.append((a[t], b[t + 2], a[t + 1]))
+        tris.append((a[-1], b[-2], b[-1]))               # upper end
+    rho = np.array(rho, float)
+    out = []
+    for t in tris:
+        p0, p1, p2 = (rho[i] for i in t)
+        cross = (p1[0] - p0[0]) * (p2[1] - p0[1]) - (p2[0] - p0[0]) * (p1[1] - p0[1])
+        out.append(t if cross > 0 else (t[0], t[2], t[1]))
+    return _sheet_from_triangles(rho, out)
+
+
+def diagstrip(*, P, w, orient, Nl, Nw, units, **kwarg):
+    """Strip along a diagonal of a square cell of side ``P`` (``Elements.jl:218-294``):
+    width ``w``, ``orient`` 45 (lower left to upper right) or -45, ``Nl`` x ``Nw`` cells on
+    the rectangular middle part; the ends taper to the cell corners as right isosceles
+    triangles (``_tritri``), and the two opposite corners carry the matching pieces so the
+    strip is continuous from cell to cell."""
+    kwargs = dict(kwarg)
+    kwargs.setdefault("fufp", True)
+    _check_kwargs(kwargs)
+    _testpos(P=P, w=w, Nl=Nl, Nw=Nw)
+    if kwargs["dx"] != 0 or kwargs["dy"] != 0:
+        raise ValueError("Translation not allowed for this style of sheet")
+    if abs(orient) != 45:
+        raise ValueError("orient must be 45 or -45")
+    r2 = math.sqrt(2.0)
+    xbl = w / 2 - (r2 * P if orient < 0 else 0.0)
+    rhobl = np.array([xbl, -w / 2])
+    rhotr = rhobl + np.array([r2 * P - w, w])
+    sh1 = recttri(rhobl, rhotr, Nl, Nw)
+    sh2 = translate(rotate(_tritri(w, Nw), 180.0), rhotr[0] + w / 2, 0.0)
+    sh3 = combine(sh1, sh2, "x", rhotr[0])
+    sh2 = translate(_tritri(w, Nw), xbl - w / 2, 0.0)
+    sh1 = combine(sh3, sh2, "x", xbl)
+    rotate(sh1, orient)
+    if orient < 0:
+        translate(sh1, P, 0.0)
+    if orient > 0:
+        sh2 = translate(rotate(_tritri(w, Nw), -45.0), 0.0, P)      # top left corner
+        sh3 = combine(sh1, sh2, " ", 0.0)
+        sh1 = translate(rotate(_tritri(w, Nw), 135.0), P, 0.0)     # bottom right corner
+    else:
+        sh2 = translate(rotate(_tritri(w, Nw), -135.0), P, P)      # top right corner
+        sh3 = combine(sh1, sh2, " ", 0.0)
+        sh1 = translate(rotate(_tritri(w, Nw), 45.0), 0.0, 0.0)    # bottom left corner
+    sheet = combine(sh3, sh1, " ", 0.0)
+    sheet.rot = 0.0
+    _finish_sheet(sheet, "diagstrip", units, [P, 0.0], [0.0, P], kwargs)
     sheet.xi_eta_check = True
     return sheet
 

@@ -227,3 +227,35 @@ def test_choose_gblocks():
         layers, sheets, junc = _split_strata(strata)
         gbl = choose_gblocks(layers, sheets, junc, TWOPI * f / C0)
         assert [[g.first, g.last, g.j] for g in gbl] == expect
+
+
+def test_diagstrip_mesh_and_mirror_symmetry():
+    # diagstrip (Elements.jl:218-294): the strip along the cell diagonal tapers into the two
+    # corners it runs to; the other two corners carry the matching pieces, so the sheet has
+    # three pieces joined only through the periodic boundary.  Its area is √2·P·w, and the
+    # -45° strip is the mirror image of the +45° one: the co-polarised transmissions swap
+    # and the cross-polarised ones swap with a change of sign.
+    from pssfss_b200.elements import _tritri, diagstrip
+    from pssfss_b200.outputs import getsijmn
+
+    def area(sh):
+        r, f = sh.rho, sh.fv - 1
+        return sum(abs((r[b][0] - r[a][0]) * (r[c][1] - r[a][1]) - (r[c][0] - r[a][0]) * (r[b][1] - r[a][1])) / 2
+                   for a, b, c in f.T)
+
+    for nw in range(1, 7):
+        t = _tritri(2.0, nw)
+        assert math.isclose(area(t), 1.0, rel_tol=1e-12) and t.nnode - t.nedge + t.nface == 1
+    res = {}
+    for o in (45, -45):
+        d = diagstrip(P=10, w=1, orient=o, Nl=16, Nw=2, units=mm)
+        assert math.isclose(area(d), math.sqrt(2) * 10, rel_tol=1e-12)
+        assert d.nnode - d.nedge + d.nface == 3
+        r = setup_rwg(d)
+        assert np.bincount(r.eci, minlength=5)[1:].tolist() == [2, 2, 2, 2]  # one edge per corner leg
+        res[o] = oracle.analyze([Layer(), d, Layer()], [12.0], {"θ": 0.0, "ϕ": 0.0})[0]
+    s = lambda o, m, n: getsijmn(2, 1, m, n, res[o])
+    # (to the modal tables' 1e-7 convergence; TE and TM of one orientation differ by ~3e-4)
+    assert abs(s(45, 1, 1) - s(-45, 2, 2)) < 1e-7 and abs(s(45, 2, 2) - s(-45, 1, 1)) < 1e-7
+    assert abs(s(45, 1, 2) + s(-45, 2, 1)) < 1e-7 and abs(s(45, 2, 1) + s(-45, 1, 2)) < 1e-7
+    assert abs(s(45, 1, 2)) > 0.1
