@@ -372,10 +372,10 @@ def polyring(*, s1, s2, a, b, sides, ntri, units, orient=0.0, **kwarg):
     return _finish_sheet(sheet, "polyring", units, s1, s2, kwargs)
 
 
-def _rect_union_mesh(rects, h):
-    """Conforming triangulation of a union of axis-aligned rectangles (x0, y0, x1, y1):
-    grid lines at every rectangle edge, refined to steps <= h, cells inside the union
-    split along the lower-left/upper-right diagonal."""
+def _rect_union_mesh(rects, h, holes=()):
+    """Conforming triangulation of a union of axis-aligned rectangles (x0, y0, x1, y1) less
+    the union of the ``holes`` rectangles: grid lines at every rectangle edge, refined to
+    steps <= h, cells inside the region split along the lower-left/upper-right diagonal."""
     def lines(vals):
         vals = sorted(set(round(v, 12) for v in vals))
         out = [vals[0]]
@@ -383,13 +383,16 @@ def _rect_union_mesh(rects, h):
             k = max(1, math.ceil((hi - lo) / h - 1e-9))
             out.extend(lo + (hi - lo) * (i + 1) / k for i in range(k))
         return np.array(out)
-    xs = lines([r[0] for r in rects] + [r[2] for r in rects])
-    ys = lines([r[1] for r in rects] + [r[3] for r in rects])
+    allr = list(rects) + list(holes)
+    xs = lines([r[0] for r in allr] + [r[2] for r in allr])
+    ys = lines([r[1] for r in allr] + [r[3] for r in allr])
     inside = np.zeros((len(xs) - 1, len(ys) - 1), bool)
     xc = 0.5 * (xs[:-1] + xs[1:])
     yc = 0.5 * (ys[:-1] + ys[1:])
     for x0, y0, x1, y1 in rects:
         inside |= ((xc > x0) & (xc < x1))[:, None] & ((yc > y0) & (yc < y1))[None, :]
+    for x0, y0, x1, y1 in holes:
+        inside &= ~(((xc > x0) & (xc < x1))[:, None] & ((yc > y0) & (yc < y1))[None, :])
     nid = -np.ones((len(xs), len(ys)), np.int64)
     rho, tris = [], []
 
@@ -405,6 +408,40 @@ def _rect_union_mesh(rects, h):
                 tris.append((ll, ur, ul))
                 tris.append((ll, lr, ur))
     return np.array(rho), np.array(tris)
+
+
+def loadedcross(*, s1, s2, L1, L2, w, ntri, units, orient=0.0, **kwarg):
+    """Loaded cross (``Elements.jl:794-961``): a cross of arm length ``L1`` (tip to tip) and
+    arm width ``L2`` centred in the cell, hollowed to a loop of trace width ``w`` when
+    2w < L2 (solid otherwise), rotated by ``orient`` degrees about its centre.  The outline
+    is axis-aligned before the rotation, so it is meshed by a conforming grid (cells of
+    about equal area, ~``ntri`` triangles) instead of the reference's Triangle mesh."""
+    kwargs = dict(kwarg)
+    kwargs.setdefault("fufp", False)
+    _check_kwargs(kwargs)
+    _testpos(L1=L1, L2=L2, w=w, ntri=ntri)
+    s1 = np.asarray(s1, float)
+    s2 = np.asarray(s2, float)
+    if s1.shape != (2,) or s2.shape != (2,):
+        raise ValueError("s1 and s2 must be 2-vectors")
+    if not L2 < L1:
+        raise ValueError("L2 must be smaller than L1")
+    h1, h2 = L1 / 2, L2 / 2
+    rects = [(-h1, -h2, h1, h2), (-h2, -h1, h2, h1)]
+    area = 2 * L1 * L2 - L2 * L2
+    holes = []
+    if 2 * w < L2:
+        holes = [(-h1 + w, -h2 + w, h1 - w, h2 - w), (-h2 + w, -h1 + w, h2 - w, h1 - w)]
+        a1, a2 = L1 - 2 * w, L2 - 2 * w
+        area -= 2 * a1 * a2 - a2 * a2
+    h = math.sqrt(2 * area / ntri)
+    rho, tris = _rect_union_mesh(rects, min(h, w if holes else h), holes)
+    if orient != 0:
+        sn, cs = math.sin(math.radians(orient)), math.cos(math.radians(orient))
+        rho = rho @ np.array([[cs, sn], [-sn, cs]])
+    rho = rho + 0.5 * (s1 + s2)
+    sheet = _sheet_from_triangles(rho, tris)
+    return _finish_sheet(sheet, "loadedcross", units, s1, s2, kwargs)
 
 
 def jerusalemcross(*, P, L1, L2, A, B, w, ntri, units, **kwarg):

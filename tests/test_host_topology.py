@@ -259,3 +259,31 @@ def test_diagstrip_mesh_and_mirror_symmetry():
     assert abs(s(45, 1, 1) - s(-45, 2, 2)) < 1e-7 and abs(s(45, 2, 2) - s(-45, 1, 1)) < 1e-7
     assert abs(s(45, 1, 2) + s(-45, 2, 1)) < 1e-7 and abs(s(45, 2, 1) + s(-45, 1, 2)) < 1e-7
     assert abs(s(45, 1, 2)) > 0.1
+
+
+def test_loadedcross_mesh_and_lossless_balance():
+    # loadedcross (Elements.jl:794-961): a cross loop of trace width w (an annulus, Euler
+    # characteristic 0) or, for 2w >= L2, a solid cross (1), with the exact area.  Through the
+    # oracle at normal incidence, below the first grating lobe and with no sheet resistance,
+    # the power of each incident polarisation is conserved, and the four-fold symmetric
+    # element transmits TE and TM alike with almost no cross-polarisation (the grid mesh
+    # is symmetric only up to its diagonals).
+    from pssfss_b200.elements import loadedcross
+    from pssfss_b200.outputs import getsijmn
+
+    def area(sh):
+        r, f = sh.rho, sh.fv - 1
+        return sum(abs((r[b][0] - r[a][0]) * (r[c][1] - r[a][1]) - (r[c][0] - r[a][0]) * (r[b][1] - r[a][1])) / 2
+                   for a, b, c in f.T)
+
+    for w, orient, euler in ((0.5, 0.0, 0), (0.5, 30.0, 0), (3.0, 0.0, 1)):
+        sh = loadedcross(s1=[10, 0], s2=[0, 10], L1=8, L2=3, w=w, ntri=200, units=mm, orient=orient)
+        a2 = 3 - 2 * w
+        want = 2 * 8 * 3 - 9 - ((2 * (8 - 2 * w) * a2 - a2 * a2) if a2 > 0 else 0)
+        assert math.isclose(area(sh), want, rel_tol=1e-12)
+        assert sh.nnode - sh.nedge + sh.nface == euler
+        r = oracle.analyze([Layer(), sh, Layer()], [12.0], {"θ": 0.0, "ϕ": 0.0})[0]
+        S = lambda i, j, m, n: getsijmn(i, j, m, n, r)
+        for n in (1, 2):
+            assert abs(sum(abs(S(i, 1, m, n)) ** 2 for i in (1, 2) for m in (1, 2)) - 1) < 1e-5
+        assert abs(S(2, 1, 1, 1) - S(2, 1, 2, 2)) < 2e-3 and abs(S(2, 1, 1, 2)) < 5e-3
