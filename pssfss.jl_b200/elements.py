@@ -446,16 +446,17 @@ def loadedcross(*, s1, s2, L1, L2, w, ntri, units, orient=0.0, **kwarg):
 
 def jerusalemcross(*, P, L1, L2, A, B, w, ntri, units, **kwarg):
     """Jerusalem cross in a square cell of period P (``Elements.jl:963``): arms of length L1
-    (tip to tip) and width L2, end caps of length A and width B.  Meshed here as the solid
-    cross (the reference's ``w >= L2/2`` and ``w >= B/2`` case); a hollow outline of width
-    w < L2/2 is not supported by this mesher."""
+    (tip to tip) and width L2, end caps of length A and width B, drawn as an outline of
+    trace width w.  As in the reference, a part whose width is at most 2w is solid: w >= L2/2
+    fills the arms, w >= B/2 the caps, both fill the whole cross.  With hollow arms and
+    solid caps the arm slot stops a trace width short of the caps; with both hollow the
+    slot runs into the caps' openings.  The outline is axis-aligned, so it is meshed by a
+    conforming grid (about ``ntri`` triangles) instead of the reference's Triangle mesh."""
     kwargs = dict(kwarg)
     kwargs.setdefault("fufp", False)
     _check_kwargs(kwargs)
     _testpos(P=P, L1=L1, L2=L2, A=A, B=B, w=w, ntri=ntri)
-    if w < L2 / 2 or w < B / 2:
-        raise ValueError("only the solid cross (w >= L2/2 and w >= B/2) is meshed here")
-    if not (L1 < P and A < P and L2 < A and 2 * B < L1):
+    if not (L1 < P and A < P and L2 < A and (L1 - L2) / 2 > B):
         raise ValueError("inconsistent Jerusalem-cross dimensions")
     c = P / 2
     h1, h2, hA = L1 / 2, L2 / 2, A / 2
@@ -463,7 +464,17 @@ def jerusalemcross(*, P, L1, L2, A, B, w, ntri, units, **kwarg):
              (c - h1, c - hA, c - h1 + B, c + hA), (c + h1 - B, c - hA, c + h1, c + hA),  # caps
              (c - hA, c - h1, c + hA, c - h1 + B), (c - hA, c + h1 - B, c + hA, c + h1)]
     area = 2 * L1 * L2 - L2 * L2 + 4 * (A * B - L2 * B)
+    hollow_arms, hollow_caps = 2 * w < L2, 2 * w < B
+    holes = []
+    if hollow_arms:
+        reach = h1 - w if hollow_caps else h1 - B - w   # the slot's half length
+        g = h2 - w
+        holes += [(c - reach, c - g, c + reach, c + g), (c - g, c - reach, c + g, c + reach)]
+    if hollow_caps:
+        a_, b_ = hA - w, h1 - w
+        holes += [(c - b_, c - a_, c - h1 + B - w, c + a_), (c + h1 - B + w, c - a_, c + b_, c + a_),
+                  (c - a_, c - b_, c + a_, c - h1 + B - w), (c - a_, c + h1 - B + w, c + a_, c + b_)]
     h = math.sqrt(2 * area / ntri)  # two triangles per h x h cell
-    rho, tris = _rect_union_mesh(rects, h)
+    rho, tris = _rect_union_mesh(rects, min(h, w) if holes else h, holes)
     sheet = _sheet_from_triangles(rho, tris)
     return _finish_sheet(sheet, "jerusalemcross", units, [float(P), 0.0], [0.0, float(P)], kwargs)

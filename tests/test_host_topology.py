@@ -287,3 +287,41 @@ def test_loadedcross_mesh_and_lossless_balance():
         for n in (1, 2):
             assert abs(sum(abs(S(i, 1, m, n)) ** 2 for i in (1, 2) for m in (1, 2)) - 1) < 1e-5
         assert abs(S(2, 1, 1, 1) - S(2, 1, 2, 2)) < 2e-3 and abs(S(2, 1, 1, 2)) < 5e-3
+
+
+def test_hollow_jerusalemcross_outlines():
+    # jerusalemcross (Elements.jl:963): parts no wider than 2w are solid.  Hollow arms and
+    # caps give one connected opening (Euler characteristic 0), hollow arms with solid caps
+    # a cross-shaped slot (0), hollow caps on solid arms four openings (-3), all solid 1;
+    # the meshed area is exact, and through the oracle a hollow cross keeps the power of
+    # each polarisation and its TE/TM degeneracy at normal incidence.
+    from pssfss_b200.elements import jerusalemcross
+    from pssfss_b200.outputs import getsijmn
+
+    def area(sh):
+        r, f = sh.rho, sh.fv - 1
+        return sum(abs((r[b][0] - r[a][0]) * (r[c][1] - r[a][1]) - (r[c][0] - r[a][0]) * (r[b][1] - r[a][1])) / 2
+                   for a, b, c in f.T)
+
+    L1, L2, A, B = 6.0, 1.0, 3.0, 0.8
+    h1, h2, hA = L1 / 2, L2 / 2, A / 2
+    solid = 2 * L1 * L2 - L2 * L2 + 4 * (A * B - L2 * B)
+    for w, euler in ((0.1, 0), (0.3, 0), (0.45, 0), (0.6, 1)):
+        sh = jerusalemcross(P=8, L1=L1, L2=L2, A=A, B=B, w=w, ntri=600, units=mm)
+        g = 2 * (h2 - w)
+        if 2 * w < B:      # slots through the arms into the caps' openings
+            hole = 2 * (2 * (h1 - w) * g) - g * g + 4 * (B - 2 * w) * (2 * (hA - w) - g)
+        elif 2 * w < L2:   # slot stopping a trace width short of the solid caps
+            hole = 2 * (2 * (h1 - B - w) * g) - g * g
+        else:
+            hole = 0.0
+        assert math.isclose(area(sh), solid - hole, rel_tol=1e-12)
+        assert sh.nnode - sh.nedge + sh.nface == euler
+    caps = jerusalemcross(P=8, L1=6, L2=0.5, A=3, B=1.2, w=0.3, ntri=300, units=mm)
+    assert caps.nnode - caps.nedge + caps.nface == -3
+    sh = jerusalemcross(P=8, L1=L1, L2=L2, A=A, B=B, w=0.1, ntri=300, units=mm)
+    r = oracle.analyze([Layer(), sh, Layer()], [14.0], {"θ": 0.0, "ϕ": 0.0})[0]
+    S = lambda i, j, m, n: getsijmn(i, j, m, n, r)
+    for n in (1, 2):
+        assert abs(sum(abs(S(i, 1, m, n)) ** 2 for i in (1, 2) for m in (1, 2)) - 1) < 1e-5
+    assert abs(S(2, 1, 1, 1) - S(2, 1, 2, 2)) < 1e-6 and abs(S(2, 1, 1, 2)) < 1e-3
