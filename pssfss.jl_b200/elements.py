@@ -312,8 +312,11 @@ def polyring(*, s1, s2, a, b, sides, ntri, units, orient=0.0, **kwarg):
     """Concentric regular-polygon rings (``Elements.jl:368-558``): ring i spans radii
     a[i]..b[i] (a[i] = 0: a solid polygon), centred in the cell, first vertex at angle
     ``orient`` (degrees).  Structured polar mesh of about ``ntri`` triangles in total,
-    shared among the rings by area; rings that fill the cell (b[-1] < 0) are not
-    supported by this mesher."""
+    shared among the rings by area.  ``b[-1] < 0`` makes the last ring fill the cell out to
+    its boundary, with ``-b[-1]`` edges along the shorter lattice vector (the longer one in
+    proportion): its polygonal inner edge is joined to the cell boundary by layers blended
+    along rays from the centre, the last of them zipped to the boundary nodes by angle, and
+    the sheet is periodic across the cell edges."""
     kwargs = dict(kwarg)
     kwargs.setdefault("fufp", False)
     _check_kwargs(kwargs)
@@ -322,10 +325,9 @@ def polyring(*, s1, s2, a, b, sides, ntri, units, orient=0.0, **kwarg):
     b = [float(x) for x in b]
     if len(a) != len(b):
         raise ValueError("length(a) !== length(b)")
-    if b[-1] < 0:
-        raise ValueError("rings that fill the unit cell (b[end] < 0) need the reference's mesher")
+    fillcell = b[-1] < 0
     for i in range(len(a)):
-        if a[i] >= b[i]:
+        if a[i] >= b[i] and not (fillcell and i == len(a) - 1):
             raise ValueError(f"a[{i + 1}] >= b[{i + 1}]")
         if i + 1 < len(a) and b[i] >= a[i + 1]:
             raise ValueError(f"b[{i + 1}] >= a[{i + 2}]")
@@ -335,9 +337,16 @@ def polyring(*, s1, s2, a, b, sides, ntri, units, orient=0.0, **kwarg):
     alpha = 2 * math.pi / sides
     area_factor = 0.5 * sides * math.sin(alpha)
     areas = [(bb * bb - aa * aa) * area_factor for aa, bb in zip(a, b)]
+    if fillcell:
+        if a[-1] <= 0:
+            raise ValueError("a cell-filling ring needs a[end] > 0")
+        areas[-1] = abs(s1[0] * s2[1] - s1[1] * s2[0]) - area_factor * a[-1] * a[-1]
     rho, tris = [], []
-    for aa, bb, ar in zip(a, b, areas):
+    for iring, (aa, bb, ar) in enumerate(zip(a, b, areas)):
         nt = max(2 * sides, round(ntri * ar / sum(areas)))
+        if fillcell and iring == len(a) - 1:
+            _cell_ring(rho, tris, rho0, s1, s2, int(round(-bb)), aa, sides, orient, nt)
+            continue
         # ns segments per polygon side, nr radial layers, cells as close to square as the
         # triangle budget allows: 2 * sides * ns * nr ~ nt with (bb - aa) / nr ~ side(rmid) / ns
         rmid = 0.5 * (aa + bb)
@@ -369,7 +378,78 @@ def polyring(*, s1, s2, a, b, sides, ntri, units, orient=0.0, **kwarg):
                 tris.append((lo + i, hi + i, hi + i1))
                 tris.append((lo + i, hi + i1, lo + i1))
     sheet = _sheet_from_triangles(rho, tris)
-    return _finish_sheet(sheet, "polyring", units, s1, s2, kwargs)
+    _finish_sheet(sheet, "polyring", units, s1, s2, kwargs)
+    sheet.xi_eta_check = fillcell
+    return sheet
+
+
+def _cell_ring(rho, tris, rho0, s1, s2, nshort, a, sides, orient, nt):
+    """Append the mesh of the region between the regular polygon of radius ``a`` (centred at
+    ``rho0``, first vertex at ``orient`` degrees) and the boundary of the cell spanned by
+    ``s1``, ``s2`` from the origin.  Boundary nodes are uniform, ``nshort`` edges along the
+    shorter lattice vector and the longer one in proportion (``Elements.jl:393-403``), so
+    opposite edges match for the periodic basis functions.  The polygon, with about as many
+    nodes as the boundary, is carried outward in layers along the rays through its nodes
+    (quad strips split on a diagonal); the last layer is joined to the boundary nodes by a
+    merge in angle about the centre."""
+    if nshort < 1:
+        raise ValueError("-b[end] must be a positive number of edges")
+    n1, n2 = np.linalg.norm(s1), np.linalg.norm(s2)
+    ns1, ns2 = (nshort, round(nshort * n2 / n1)) if n1 <= n2 else (round(nshort * n1 / n2), nshort)
+    outer = ([i / ns1 * s1 for i in range(ns1)] + [s1 + i / ns2 * s2 for i in range(ns2)] +
+             [s1 + s2 - i / ns1 * s1 for i in range(ns1)] + [s2 - i / ns2 * s2 for i in range(ns2)])
+    M = len(outer)
+    ns = max(1, round(M / sides))
+    m = sides * ns
+    alpha = 2 * math.pi / sides
+    verts = [rho0 + a * np.array([math.cos(math.radians(orient) + i * alpha), math.sin(math.radians(orient) + i * alpha)])
+             for i in range(sides)]
+    poly = [verts[i] + (verts[(i + 1) % sides] - verts[i]) * (t / ns) for i in range(sides) for t in range(ns)]
+    Binv = np.linalg.inv(np.column_stack([s1, s2]))
+
+    def reach(d):  # distance from the centre to the cell boundary along direction d
+        q = Binv @ d
+        return 0.5 / max(abs(q[0]), abs(q[1]))
+    rays = []
+    for p in poly:
+        v = p - rho0
+        r0 = np.linalg.norm(v)
+        rays.append((r0, v / r0, reach(v / r0)))
+    nlayer = max(1, 1 + round((nt - m - M) / (2 * m)))
+    layers = []
+    for k in range(nlayer):
+        base = len(rho)
+        rho.extend(rho0 + (r0 + (R - r0) * k / nlayer) * d for r0, d, R in rays)
+        layers.append(base)
+    for k in range(nlayer - 1):
+        lo, hi = layers[k], layers[k + 1]
+        for i in range(m):
+            i1 = (i + 1) % m
+            tris.append((lo + i, hi + i, hi + i1))
+            tris.append((lo + i, hi + i1, lo + i1))
+    obase = len(rho)
+    rho.extend(outer)
+
+    def ang(p):
+        return math.atan2(p[1] - rho0[1], p[0] - rho0[0])
+    ref = ang(outer[0])
+    inner = [layers[-1] + i for i in range(m)]
+    ai = [(ang(rho[q]) - ref) % (2 * math.pi) for q in inner]
+    s0 = int(np.argmin(ai))
+    inner, ai = inner[s0:] + inner[:s0], ai[s0:] + ai[:s0]
+    ao = [(ang(p) - ref) % (2 * math.pi) for p in outer]
+    ao[0] = 0.0
+    i = j = 0
+    while i < m or j < M:
+        nxt_i = ai[(i + 1) % m] + (2 * math.pi if i + 1 >= m else 0.0)
+        nxt_o = ao[(j + 1) % M] + (2 * math.pi if j + 1 >= M else 0.0)
+        I, O = inner[i % m], obase + j % M
+        if j < M and (i >= m or nxt_o <= nxt_i):
+            tris.append((I, O, obase + (j + 1) % M))
+            j += 1
+        else:
+            tris.append((I, O, inner[(i + 1) % m]))
+            i += 1
 
 
 def _rect_union_mesh(rects, h, holes=()):

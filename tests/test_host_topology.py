@@ -325,3 +325,38 @@ def test_hollow_jerusalemcross_outlines():
     for n in (1, 2):
         assert abs(sum(abs(S(i, 1, m, n)) ** 2 for i in (1, 2) for m in (1, 2)) - 1) < 1e-5
     assert abs(S(2, 1, 1, 1) - S(2, 1, 2, 2)) < 1e-6 and abs(S(2, 1, 1, 2)) < 1e-3
+
+
+def test_cell_filling_polyring():
+    # polyring with b[end] < 0 (Elements.jl:392-403, 440-482): the last ring fills the cell
+    # out to its boundary with -b[end] edges along the shorter lattice vector, so the sheet
+    # is a periodic screen with polygonal openings.  Exact area; matching edge counts on
+    # opposite cell edges (periodic basis functions); through the oracle a square opening
+    # in a square cell keeps the power of each polarisation and its TE/TM degeneracy.
+    from pssfss_b200.elements import polyring
+    from pssfss_b200.outputs import getsijmn
+
+    def area(sh):
+        r, f = sh.rho, sh.fv - 1
+        return sum(abs((r[b][0] - r[a][0]) * (r[c][1] - r[a][1]) - (r[c][0] - r[a][0]) * (r[b][1] - r[a][1])) / 2
+                   for a, b, c in f.T)
+
+    cases = [(dict(s1=[10, 0], s2=[0, 10], a=[3.0], b=[-10], sides=4, orient=45, ntri=300), [10, 10, 10, 10]),
+             (dict(s1=[10, 0], s2=[0, 10], a=[2.0, 3.5], b=[3.0, -12], sides=32, ntri=800), [12, 12, 12, 12]),
+             (dict(s1=[1.1414, 0.0], s2=[0.5707, 0.9885], a=[0.3], b=[-8], sides=6, ntri=500), [8, 8, 8, 8]),
+             (dict(s1=[10, 0], s2=[0, 14], a=[4.0], b=[-6], sides=24, ntri=300), [8, 8, 6, 6])]
+    for kw, eci in cases:
+        sh = polyring(units=mm, **kw)
+        s1, s2 = np.array(kw["s1"], float), np.array(kw["s2"], float)
+        af = 0.5 * kw["sides"] * math.sin(2 * math.pi / kw["sides"])
+        want = (abs(s1[0] * s2[1] - s1[1] * s2[0]) - af * kw["a"][-1] ** 2 +
+                sum((bb * bb - aa * aa) * af for aa, bb in zip(kw["a"][:-1], kw["b"][:-1])))
+        assert math.isclose(area(sh), want, rel_tol=1e-12)
+        assert sh.xi_eta_check and np.bincount(setup_rwg(sh).eci, minlength=5)[1:].tolist() == eci
+    sh = polyring(units=mm, **cases[0][0])
+    r = oracle.analyze([Layer(), sh, Layer()], [12.0], {"θ": 0.0, "ϕ": 0.0})[0]
+    S = lambda i, j, m, n: getsijmn(i, j, m, n, r)
+    for n in (1, 2):
+        assert abs(sum(abs(S(i, 1, m, n)) ** 2 for i in (1, 2) for m in (1, 2)) - 1) < 1e-6
+    assert abs(S(2, 1, 1, 1) - S(2, 1, 2, 2)) < 1e-3 and abs(S(2, 1, 1, 2)) < 1e-3
+    assert 0.05 < abs(S(2, 1, 1, 1)) < 0.5   # an opening well below its cutoff passes little
