@@ -1,0 +1,71 @@
+"""Result extraction (Outputs.jl): polarisation basis changes, derived outputs and the
+@outputs-style request parsing, on results of the oracle's analyze (CPU)."""
+import cmath
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+from pssfss_b200.elements import diagstrip, rectstrip
+from pssfss_b200.layers import Layer
+from pssfss_b200.outputs import (H, L, R, TE, TM, V, extract_result, getsijmn, obsmat, outputs,
+                                 sourcemat)
+from pssfss_b200.units import Length, mm
+
+NORMAL = {"θ": 0.0, "ϕ": 0.0}
+
+
+@pytest.fixture(scope="module")
+def patch_result():
+    sh = rectstrip(Lx=6, Ly=6, Px=10, Py=10, Nx=6, Ny=6, units=mm)
+    return oracle.analyze([Layer(), sh, Layer(epsr=2.2, width=Length(1, mm)), Layer()], [12.0], NORMAL)[0]
+
+
+def test_basis_changes_at_normal_incidence(patch_result):
+    r = patch_result
+    S = lambda i, j, m, n: getsijmn(i, j, m, n, r)
+    # with ϕ = 0 the Ludwig-3 horizontal field is the TM mode's and the vertical the TE mode's
+    for i, j in ((1, 1), (2, 1), (1, 2), (2, 2)):
+        assert S(i, j, H, H) == S(i, j, TM, TM) and S(i, j, V, V) == S(i, j, TE, TE)
+    for mat in (sourcemat(1, R, r), sourcemat(2, L, r), obsmat(1, R, r), obsmat(2, H, r)):
+        assert np.abs(mat.conj().T @ mat - np.eye(2)).max() < 1e-15
+    # power of each incident wave in every basis, to the GSM's own unitarity
+    g = np.block([[r.gsm[(1, 1)], r.gsm[(1, 2)]], [r.gsm[(2, 1)], r.gsm[(2, 2)]]])
+    err = np.abs(g.conj().T @ g - np.eye(4)).max()
+    for basis in ((TE, TM), (H, V), (R, L)):
+        for n in basis:
+            assert abs(sum(abs(S(i, 1, m, n)) ** 2 for i in (1, 2) for m in basis) - 1) <= 2 * err + 1e-12
+    # a square patch treats both hands alike: transmission keeps the hand, reflection reverses it
+    assert abs(abs(S(2, 1, R, R)) - abs(S(2, 1, TE, TE))) < 1e-3 and abs(S(2, 1, L, R)) < 1e-2
+    assert abs(abs(S(1, 1, L, R)) - abs(S(1, 1, TE, TE))) < 1e-3 and abs(S(1, 1, R, R)) < 1e-2
+
+
+def test_derived_outputs_and_extraction(patch_result):
+    r = patch_result
+    ops = outputs("FGHz", "theta", "phi", "s21db(te,te)", "S21ANG(TE,TE)", "s11mag(1,1)", "ar21db(h)",
+                  "dipd21", "ΔIL21", "s21real(r,h)", "psi1")
+    row = extract_result(r, ops)
+    assert row.shape == (1, len(ops))
+    s = getsijmn(2, 1, 1, 1, r)
+    assert row[0, 0] == 12.0 and row[0, 1] == 0.0 and row[0, 2] == 0.0
+    assert math.isclose(row[0, 3], 20 * math.log10(abs(s)), rel_tol=1e-14)
+    assert math.isclose(row[0, 4], math.degrees(cmath.phase(s)), rel_tol=1e-14)
+    assert math.isclose(row[0, 5], abs(getsijmn(1, 1, 1, 1, r)), rel_tol=1e-14)
+    assert row[0, 6] > 30          # a square patch passes a linear wave nearly linear
+    ratio = getsijmn(2, 1, 1, 1, r) / getsijmn(2, 1, 2, 2, r)
+    assert math.isclose(row[0, 7], math.degrees(cmath.phase(ratio)), abs_tol=1e-12)
+    assert math.isclose(row[0, 8], 10 * math.log10(abs(ratio) ** 2), abs_tol=1e-12)
+    assert row[0, 9] == getsijmn(2, 1, R, H, r).real and math.isnan(row[0, 10])
+    assert extract_result([r, r], ops).shape == (2, len(ops))
+    with pytest.raises(ValueError):
+        outputs("s21xx(te,te)")
+
+
+def test_axial_ratio_of_a_diagonal_polariser():
+    # a strip along the cell diagonal splits a horizontal wave into unequal, dephased
+    # components along and across the strip: an elliptical transmitted wave
+    d = diagstrip(P=10, w=1, orient=45, Nl=12, Nw=2, units=mm)
+    r = oracle.analyze([Layer(), d, Layer()], [12.0], NORMAL)[0]
+    ar_h, ar_v = extract_result(r, outputs("ar21db(h)", "ar21db(v)"))[0]
+    assert 3 < ar_h < 20 and abs(ar_h - ar_v) < 0.1
