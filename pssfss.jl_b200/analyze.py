@@ -320,9 +320,14 @@ def analyze(strata, flist, steering, *, precision="fp64", device=0, outlist=(),
     ``flist``: frequencies in GHz.  ``steering``: dict with keys (θ, ϕ) or (ψ₁, ψ₂) in
     degrees (first key = outer loop).  ``precision``: ``"fp64"`` (plain FP64 LU) or
     ``"fp32r"`` (complex64 LU with FP64 iterative refinement).
+    ``outlist``: (csv file name, ``outputs(...)`` tuple) pairs, each written as a header of
+    output labels and one row per result (PSSFSS.jl:316-325).  ``resultfile``: where to
+    save the results for ``read_result_file`` / ``extract_result_file`` (none by default;
+    the reference's JLD2 file is not written).
     Returns a list of ``Result``.
     """
     from . import engine
+    from .outputs import write_outlist
     plan = make_plan(strata, flist, steering, plan_flist)
     partial = {}
     for ig, (i1, i2), isht, s in sheet_gblocks(plan):
@@ -332,4 +337,6 @@ def analyze(strata, flist, steering, *, precision="fp64", device=0, outlist=(),
                                  plan.uvec[isht - 1], ios, precision=precision, device=device,
                                  stats=stats)
         partial[ig] = [add_scattered(io, d) for io, d in zip(ios, dS)]
-    return assemble(plan, partial)
+    results = assemble(plan, partial)
+    write_outlist(results, outlist, resultfile)
+    return results

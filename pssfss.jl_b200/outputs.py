@@ -260,3 +260,47 @@ def extract_result(results, ops):
     if isinstance(results, Result):
         results = [results]
     return np.array([[o(r) for o in ops] for r in results])
+
+
+def _cell(v):
+    if isinstance(v, complex):
+        return f"{v.real!r}{'+' if v.imag >= 0 else '-'}{abs(v.imag)!r}im"
+    return repr(float(v))
+
+
+def write_outputs_csv(fname, results, ops):
+    """A CSV of the outputs ``ops`` of ``results``: a header of their labels, then one row
+    per result (the reference's ``outlist`` files, ``PSSFSS.jl:316-325``)."""
+    with open(fname, "w", encoding="utf-8") as f:
+        f.write(",".join(o.label for o in ops) + "\n")
+        for r in results:
+            f.write(",".join(_cell(o(r)) for o in ops) + "\n")
+
+
+def save_results(fname, results):
+    """Save results for ``read_result_file`` (a pickle of the list; the reference's file is
+    JLD2, ``Outputs.jl:396-409``)."""
+    import pickle
+    with open(fname, "wb") as f:
+        pickle.dump(list(results), f)
+
+
+def read_result_file(fname):
+    """The results saved by ``save_results`` (``Outputs.jl:411-421``)."""
+    import pickle
+    with open(fname, "rb") as f:
+        return pickle.load(f)
+
+
+def extract_result_file(fname, ops):
+    """``extract_result`` of the results in a result file (``Outputs.jl:428-431``)."""
+    return extract_result(read_result_file(fname), ops)
+
+
+def write_outlist(results, outlist=(), resultfile=None):
+    """The file outputs of ``analyze``: every (csv name, ops) of ``outlist``, and the result
+    file when one is named."""
+    for fname, ops in outlist:
+        write_outputs_csv(fname, results, ops)
+    if resultfile:
+        save_results(resultfile, results)

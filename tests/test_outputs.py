@@ -69,3 +69,19 @@ def test_axial_ratio_of_a_diagonal_polariser():
     r = oracle.analyze([Layer(), d, Layer()], [12.0], NORMAL)[0]
     ar_h, ar_v = extract_result(r, outputs("ar21db(h)", "ar21db(v)"))[0]
     assert 3 < ar_h < 20 and abs(ar_h - ar_v) < 0.1
+
+
+def test_outlist_csv_and_result_file(patch_result, tmp_path):
+    # analyze's file outputs: each outlist CSV gets a header of labels and a row per result;
+    # a result file reads back to the same extracted numbers
+    from pssfss_b200.outputs import extract_result_file, read_result_file, write_outlist
+    ops = outputs("FGHz", "s21db(te,te)", "s11(h,h)")
+    csv, res = tmp_path / "out.csv", tmp_path / "pssfss.res"
+    write_outlist([patch_result, patch_result], [(str(csv), ops)], str(res))
+    lines = csv.read_text().splitlines()
+    assert lines[0] == "FGHZ,S21DB(TE,TE),S11(H,H)" and len(lines) == 3
+    cells = lines[1].split(",")
+    assert float(cells[0]) == 12.0 and float(cells[1]) == extract_result(patch_result, ops)[0, 1].real
+    assert complex(cells[2].replace("im", "j")) == getsijmn(1, 1, H, H, patch_result)
+    assert len(read_result_file(str(res))) == 2
+    assert np.array_equal(extract_result_file(str(res), ops), extract_result([patch_result] * 2, ops))
