@@ -197,3 +197,19 @@ def unique_face_pairs(sheet):
     ufpm = cls.reshape((nface, nface), order="F")
     rep_sorted = np.sort(rep) + 1
     return ufpm, rep_sorted.astype(np.int64), len(rep)
+
+
+def edge_current_unit_vector(ie, rwgdat, sheet):
+    """Unit vector of the positive reference direction of the basis function on edge ``ie``
+    (1-based; ``RWG.jl:339-363``): normal to the edge, pointing out of the basis function's
+    plus face (away from that face's free vertex)."""
+    bf = int(rwgdat.ebf[ie - 1])
+    if bf == 0:
+        raise ValueError(f"No basis function for edge {ie}")
+    n1, n2 = int(sheet.e1[ie - 1]), int(sheet.e2[ie - 1])
+    r21 = sheet.rho[n2 - 1] - sheet.rho[n1 - 1]
+    t = r21 / math.hypot(r21[0], r21[1])
+    u = np.array([-t[1], t[0]])  # ẑ × edge direction
+    f = int(rwgdat.bff[0, bf - 1])
+    nfree = next(int(v) for v in sheet.fv[:, f - 1] if v != n1 and v != n2)
+    return -u if (sheet.rho[n1 - 1] - sheet.rho[nfree - 1]) @ u < 0 else u

@@ -1,11 +1,13 @@
 """Host-side geometry, topology, modes and GSM algebra against the reference's tests.
 
 test/RWGData_test.jl, test/RWGSheet_test.jl, test/Elements_test.jl, test/Rings_test.jl,
-test/GSMs_test.jl (cascade identities).
+test/GSMs_test.jl (cascade identities, choose_gblocks), test/Modes_test.jl; the element
+constructors the reference meshes with Triangle, checked by area, topology and physics.
 """
 import math
 
 import numpy as np
+import pytest
 
 import oracle
 from conftest import golden
@@ -360,3 +362,23 @@ def test_cell_filling_polyring():
         assert abs(sum(abs(S(i, 1, m, n)) ** 2 for i in (1, 2) for m in (1, 2)) - 1) < 1e-6
     assert abs(S(2, 1, 1, 1) - S(2, 1, 2, 2)) < 1e-3 and abs(S(2, 1, 1, 2)) < 1e-3
     assert 0.05 < abs(S(2, 1, 1, 1)) < 0.5   # an opening well below its cutoff passes little
+
+
+def test_edge_current_unit_vector():
+    # RWG.jl:339-363: a unit normal to the edge, pointing out of the plus face of its basis
+    # function (from that face's free vertex across the edge)
+    from pssfss_b200.rwg import edge_current_unit_vector
+    sh = meander(a=5, b=10, h=6, w1=0.3, w2=0.3, ntri=200, units=mm)
+    r = setup_rwg(sh)
+    for ie in range(1, sh.nedge + 1):
+        bf = int(r.ebf[ie - 1])
+        if bf == 0:
+            with pytest.raises(ValueError):
+                edge_current_unit_vector(ie, r, sh)
+            continue
+        u = edge_current_unit_vector(ie, r, sh)
+        n1, n2 = int(sh.e1[ie - 1]), int(sh.e2[ie - 1])
+        f = int(r.bff[0, bf - 1])
+        nfree = [int(v) for v in sh.fv[:, f - 1] if v not in (n1, n2)][0]
+        assert abs(np.linalg.norm(u) - 1) < 1e-14 and abs(u @ (sh.rho[n2 - 1] - sh.rho[n1 - 1])) < 1e-12
+        assert u @ (sh.rho[n1 - 1] - sh.rho[nfree - 1]) > 0
