@@ -4,7 +4,8 @@ Host-side: ``GSM`` (``:16-29``), ``cascade`` (``:125-141``), ``cascade_layer``
 (``cascade!``, ``:155-176``), the incident partial GSMs and transmission-line Green's
 functions of a Gblock (``gsm_electric_gblock`` ``:213-370``, ``gsm_magnetic_gblock``
 ``:401-526``), ``gsm_slab_interface`` (``:545-620``), ``translate_gsm`` (``:717-750``),
-``choose_gblocks`` (``:771-868``) and ``find_mode_index`` (``:884-891``).  These are
+``choose_gblocks`` (``:771-868``), ``find_mode_index`` (``:884-891``) and the GSM files
+(``:623-696``).  These are
 per-mode scalar recursions and n_modes-sized dense algebra; the O(N^2)/O(N^3) work of a
 sheet's partial GSM is done by the CUDA library.
 """
@@ -480,3 +481,57 @@ def choose_gblocks(layers, sheets, junc, k0min):
     if cover != list(range(1, nj + 1)):
         raise RuntimeError(f"Bad Gblock vector: {out}")
     return out
+
+
+# GSM files (GSMs.jl:623-700): a header with the end regions' unit cells and mode lists, then
+# one group per frequency / scan case.  The reference writes JLD2; here the same keys are
+# kept in a pickled dict.
+def _load_gsm_dict(fname):
+    import pickle
+    with open(fname, "rb") as f:
+        return pickle.load(f)
+
+
+def _save_gsm_dict(fname, dat):
+    import pickle
+    with open(fname, "wb") as f:
+        pickle.dump(dat, f)
+
+
+def initialize_gsm_file(fname, layer1, layer2, sh1=None, sh2=None):
+    """Start a GSM file with the unit cells of the input and output regions (a 1 m square
+    cell when no sheets are given) and their mode lists (``GSMs.jl:623-665``)."""
+    if (sh1 is None) != (sh2 is None):
+        raise ValueError("give both sheets or neither")
+    cells = []
+    for sh in (sh1, sh2):
+        if sh is None:
+            cells.append((np.array([1.0, 0.0]), np.array([0.0, 1.0]), "m"))
+        else:
+            cells.append((np.array(sh.s1, float), np.array(sh.s2, float), sh.units))
+    _save_gsm_dict(fname, {
+        "FileType": "GSMFile", "FileTypeVersion": "0.0.1",
+        "s1in": cells[0][0], "s2in": cells[0][1], "unitsin": cells[0][2],
+        "s1out": cells[1][0], "s2out": cells[1][1], "unitsout": cells[1][2],
+        "ModelistIn": (list(layer1.P), list(layer1.M), list(layer1.N)),
+        "ModelistOut": (list(layer2.P), list(layer2.M), list(layer2.N)),
+    })
+
+
+def append_gsm_data(fname, gname, gsm, l1, l2, case):
+    """Add the GSM of one frequency / scan case (``case``: "FGHz" and θ, ϕ or ψ₁, ψ₂) under
+    group ``gname``, with the end regions' (εr, μr) (``GSMs.jl:667-690``)."""
+    dat = read_gsm_file(fname)
+    dat[f"{gname}/case"] = dict(case)
+    dat[f"{gname}/epsmu1"] = (complex(l1.epsr), complex(l1.mur))
+    dat[f"{gname}/epsmu2"] = (complex(l2.epsr), complex(l2.mur))
+    dat[f"{gname}/gsm"] = gsm
+    _save_gsm_dict(fname, dat)
+
+
+def read_gsm_file(fname):
+    """The contents of a GSM file as a dict keyed like the reference's (``GSMs.jl:692-696``)."""
+    dat = _load_gsm_dict(fname)
+    if dat.get("FileType") != "GSMFile":
+        raise ValueError(f"{fname} is not a GSM file")
+    return dat

@@ -382,3 +382,36 @@ def test_edge_current_unit_vector():
         nfree = [int(v) for v in sh.fv[:, f - 1] if v not in (n1, n2)][0]
         assert abs(np.linalg.norm(u) - 1) < 1e-14 and abs(u @ (sh.rho[n2 - 1] - sh.rho[n1 - 1])) < 1e-12
         assert u @ (sh.rho[n1 - 1] - sh.rho[nfree - 1]) > 0
+
+
+def test_gsm_file_round_trip(tmp_path):
+    # test/GSMs_test.jl "GSM file": header (cells, units, mode lists) and one case group
+    from pssfss_b200.gsms import append_gsm_data, initialize_gsm_file, read_gsm_file
+    from pssfss_b200.layers import TE, TM
+    alpha = 0.35
+    beta = math.sqrt(1 - alpha ** 2)
+    a = GSM.identity(1, 1)
+    a.s11[:] = a.s22[:] = alpha
+    a.s12[:] = a.s21[:] = beta
+    l1 = Layer(epsr=2.0)
+    l1.P, l1.M, l1.N = [TE, TM], [0, 0], [0, 0]
+    l2 = Layer(epsr=2.0)
+    l2.P, l2.M, l2.N = [TE, TM], [0, 0], [0, 0]
+    l2.epsr = 1.0
+    sh = rectstrip(Lx=1, Ly=1, Px=1, Py=1, Nx=2, Ny=1, units=mm, fufp=True)
+    fname = str(tmp_path / "gsmfile.gsm")
+    initialize_gsm_file(fname, l1, l2, sh, sh)
+    case = {"θ": 0.0, "ϕ": 0.0, "FGHz": 2.0}
+    append_gsm_data(fname, "1", a, l1, l2, case)
+    dat = read_gsm_file(fname)
+    assert dat["ModelistIn"] == ([TE, TM], [0, 0], [0, 0]) and dat["ModelistOut"] == ([TE, TM], [0, 0], [0, 0])
+    assert dat["s1in"].tolist() == [1.0, 0.0] and dat["s2out"].tolist() == [0.0, 1.0]
+    for k in ("s11", "s12", "s21", "s22"):
+        assert np.array_equal(getattr(dat["1/gsm"], k), getattr(a, k))
+    assert dat["1/epsmu1"] == (2.0 + 0j, 1.0 + 0j) and dat["1/epsmu2"] == (1.0 + 0j, 1.0 + 0j)
+    assert dat["1/case"] == case and dat["unitsin"] == mm and dat["unitsout"] == mm
+    import pickle
+    other = tmp_path / "other.gsm"
+    other.write_bytes(pickle.dumps({"FileType": "ResultFile"}))
+    with pytest.raises(ValueError, match="not a GSM file"):
+        read_gsm_file(str(other))
