@@ -269,3 +269,21 @@ def combine(sh1, sh2, dup_coor, dup_coor_value):
             fe[fe > eoffset + ecen2[i]] -= 1
     sh3.fe = fe
     return sh3
+
+
+def write_sheet_data(filename, sheet):
+    """Save a sheet's geometry for ``read_sheet_data`` (``Sheets.jl:113-117``; the reference
+    writes JLD2, here a pickled ``{"sheet": sheet}``)."""
+    import pickle
+    with open(filename, "wb") as f:
+        pickle.dump({"sheet": sheet}, f)
+
+
+def read_sheet_data(filename):
+    """The sheet saved by ``write_sheet_data`` (``Sheets.jl:98-106``)."""
+    import pickle
+    with open(filename, "rb") as f:
+        dat = pickle.load(f)
+    if not isinstance(dat, dict) or "sheet" not in dat:
+        raise ValueError(f"{filename} does not contain sheet data")
+    return dat["sheet"]

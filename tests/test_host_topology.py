@@ -415,3 +415,15 @@ def test_gsm_file_round_trip(tmp_path):
     other.write_bytes(pickle.dumps({"FileType": "ResultFile"}))
     with pytest.raises(ValueError, match="not a GSM file"):
         read_gsm_file(str(other))
+
+
+def test_sheet_file_round_trip(tmp_path):
+    # test/RWGSheet_test.jl "read and write": a combined sheet written and read back
+    from pssfss_b200.sheets import read_sheet_data, write_sheet_data
+    sh = combine(recttri([0., 0.], [1., 1.], 2, 2), recttri([1., 0.], [2., 1.], 2, 2), "x", 1.0)
+    fname = str(tmp_path / "sheet.dat")
+    write_sheet_data(fname, sh)
+    back = read_sheet_data(fname)
+    for k in ("rho", "e1", "e2", "fv", "fe"):
+        assert np.array_equal(getattr(back, k), getattr(sh, k))
+    assert back.units == sh.units and back.style == sh.style
