@@ -312,6 +312,76 @@ def assemble(plan, partial):
     return results
 
 
+class AnalysisLog:
+    """The ``logfile`` of ``analyze`` (``Log.jl``; messages of ``PSSFSS.jl:212-332`` and the
+    layer / sheet report of ``:706-745``).  Without a file name every call is a no-op."""
+
+    def __init__(self, logfile):
+        self.fname = logfile
+        if logfile:
+            open(logfile, "w").close()
+
+    def __call__(self, msg):
+        if self.fname:
+            with open(self.fname, "a", encoding="utf-8") as f:
+                f.write(msg + "\n")
+
+    def start(self):
+        import datetime
+        now = datetime.datetime.now()
+        self(f"\n\nStarting pssfss_b200 analysis on {now:%Y-%m-%d} at {now:%H:%M:%S}\n\n")
+
+    def report(self, plan):
+        """Layer and sheet tables of ``report_layers_sheets`` (PSSFSS.jl:706-745)."""
+        if not self.fname:
+            return
+        from .gsms import find_unique_periods
+        usi = find_unique_periods(plan.junc, plan.sheets)
+        usi = [usi[plan.junc.index(k + 1)] if (k + 1) in plan.junc else 0 for k in range(len(plan.sheets))]
+        self("Dielectric layer information... \n")
+        self(" Layer  Width  units  epsr   tandel   mur  mtandel modes  beta1x  beta1y  beta2x  beta2y")
+        self(" ----- ------------- ------- ------ ------- ------ ----- ------- ------- ------- -------")
+        for jl, l in enumerate(plan.layers, 1):
+            eps, mu = l.epsr.real, l.mur.real
+            uw = l.user_width
+            units = "in" if uw.unit.name == "inch" else uw.unit.name
+            self(" %5i %9.4f %3s %7.2f %6.4f %7.2f %6.4f %5i %7.1f %7.1f %7.1f %7.1f" % (
+                jl, float(uw.value), units, eps, -l.epsr.imag / eps, mu, -l.mur.imag / mu, len(l.P),
+                l.beta1[0], l.beta1[1], l.beta2[0], l.beta2[1]))
+            if jl < len(plan.layers) and plan.junc[jl - 1] != 0:
+                js = plan.junc[jl - 1]
+                sh = plan.sheets[js - 1]
+                om = sh.units.units_per_meter
+                self(" ==================  Sheet %3i  ======================== %7.1f %7.1f %7.1f %7.1f" % (
+                    usi[js - 1], sh.beta1[0] * om, sh.beta1[1] * om, sh.beta2[0] * om, sh.beta2[1] * om))
+        sint = [i + 1 for i, j in enumerate(plan.junc) if j != 0]
+        self("\n\n\nPSS/FSS sheet information...\n")
+        self("Sheet  Loc         Style      Rot  J/M Faces Edges Nodes Unknowns  NUFP")
+        self("-----  ---  ---------------- ----- --- ----- ----- ----- -------- ------")
+        for js, sh in enumerate(plan.sheets, 1):
+            rw = plan.rwgdat[js - 1]
+            self("%4i   %3i  %16s %5.1f  %1s  %5i %5i %5i  %6i %7i" % (
+                usi[js - 1], sint[js - 1], sh.style, sh.rot, sh.cls, sh.nface, sh.nedge, sh.nnode,
+                rw.nbf if rw is not None else 0, rw.nufp if rw is not None else 0))
+        self("\n\n")
+
+    def skipped(self, plan, flist):
+        planned = {pt.fghz for pt in plan.points}
+        for f in np.atleast_1d(np.asarray(flist, float)):
+            if float(f) not in planned:
+                self(f"  Skipping {float(f)} GHz due to cutoff principal modes in ambient medium")
+
+    def sheet_sweep(self, isht, npts, timings):
+        self(f"    Sheet {isht}: {npts} points on the GPU")
+        for k, v in (timings or {}).items():
+            self(f"      {v:.3f} ms {k}")
+
+    def finish(self):
+        import datetime
+        now = datetime.datetime.now()
+        self(f"\n\n pssfss_b200 analysis exiting on {now:%Y-%m-%d} at {now:%H:%M:%S}\n\n")
+
+
 def analyze(strata, flist, steering, *, precision="fp64", device=0, outlist=(),
             logfile=None, resultfile=None, showprogress=False, stats=None, plan_flist=None):
     """Analyze a layered FSS/PSS over frequencies and steering (PSSFSS.jl:114).
@@ -320,6 +390,7 @@ def analyze(strata, flist, steering, *, precision="fp64", device=0, outlist=(),
     ``flist``: frequencies in GHz.  ``steering``: dict with keys (θ, ϕ) or (ψ₁, ψ₂) in
     degrees (first key = outer loop).  ``precision``: ``"fp64"`` (plain FP64 LU) or
     ``"fp32r"`` (complex64 LU with FP64 iterative refinement).
+    ``logfile``: a log of the layers, sheets and per-sheet device timings (none by default).
     ``outlist``: (csv file name, ``outputs(...)`` tuple) pairs, each written as a header of
     output labels and one row per result (PSSFSS.jl:316-325).  ``resultfile``: where to
     save the results for ``read_result_file`` / ``extract_result_file`` (none by default;
@@ -328,15 +399,22 @@ def analyze(strata, flist, steering, *, precision="fp64", device=0, outlist=(),
     """
     from . import engine
     from .outputs import write_outlist
+    log = AnalysisLog(logfile)
+    log.start()
     plan = make_plan(strata, flist, steering, plan_flist)
+    log.report(plan)
+    log.skipped(plan, flist)
     partial = {}
     for ig, (i1, i2), isht, s in sheet_gblocks(plan):
         sheet = plan.sheets[isht - 1]
         ios = [sheet_io(pt.layers[i1 - 1:i2], sheet, s, pt.k0, pt.beta00) for pt in plan.points]
+        st = stats if stats is not None else ({} if logfile else None)
         dS = engine.partial_gsms(sheet, plan.rwgdat[isht - 1], plan.points, (i1, i2), s,
                                  plan.uvec[isht - 1], ios, precision=precision, device=device,
-                                 stats=stats)
+                                 stats=st)
+        log.sheet_sweep(isht, len(plan.points), (st or {}).get("timings_ms"))
         partial[ig] = [add_scattered(io, d) for io, d in zip(ios, dS)]
     results = assemble(plan, partial)
     write_outlist(results, outlist, resultfile)
+    log.finish()
     return results

@@ -85,3 +85,29 @@ def test_outlist_csv_and_result_file(patch_result, tmp_path):
     assert complex(cells[2].replace("im", "j")) == getsijmn(1, 1, H, H, patch_result)
     assert len(read_result_file(str(res))) == 2
     assert np.array_equal(extract_result_file(str(res), ops), extract_result([patch_result] * 2, ops))
+
+
+def test_analysis_log_report(tmp_path):
+    # the logfile of analyze: banner, the layer / sheet tables of report_layers_sheets
+    # (PSSFSS.jl:706-745), skipped points, per-sheet timings; nothing without a file name
+    from pssfss_b200.analyze import AnalysisLog, make_plan
+    from pssfss_b200.elements import meander
+    strata = [Layer(), meander(a=5, b=10, h=6, w1=0.3, w2=0.3, ntri=300, units=mm),
+              Layer(epsr=2.2, tandel=0.001, width=Length(1, mm)), Layer()]
+    plan = make_plan(strata, [8.0, 12.0], NORMAL)
+    fn = str(tmp_path / "pssfss.log")
+    log = AnalysisLog(fn)
+    log.start()
+    log.report(plan)
+    log.skipped(plan, [8.0, 12.0])
+    log.sheet_sweep(1, 2, {"fill": 1.5})
+    log.finish()
+    text = open(fn).read()
+    assert "Starting pssfss_b200 analysis" in text and "exiting" in text
+    assert "     2    1.0000  mm    2.20 0.0010    1.00 0.0000     0" in text
+    assert "   1     1           meander   0.0  J    368   646   279     460   62556" in text
+    assert "1.500 ms fill" in text and "Skipping" not in text
+    quiet = AnalysisLog(None)
+    quiet.start()
+    quiet.report(plan)
+    quiet.finish()
