@@ -285,14 +285,15 @@ def analyze(strata, flist, steering):
     return A.assemble(plan, partial)
 
 
-def partial_dS_linearized(sheet, rwg, region, s, k0, u, io, perturbed):
+def partial_dS_linearized(sheet, rwg, region, s, k0, u, io, perturbed, tangent=False):
     """Scattered partial GSM at a point and, for each perturbed input set, its first-order
     (in the perturbation) value from the unperturbed factorisation:
 
         dS_k = wobs_k * (P_k Z^-1 R_k - Lambda^T (Z_k - Z) X),  X = Z^-1 R,  Lambda = Z^-T P^T,
 
     exact to O(h^2), so central differences of dS_k give dS/dp to O(h^2) with one
-    factorisation.  ``perturbed``: list of (sheet_k, rwg_k, region_k, u_k, io_k) with the
+    factorisation.  ``tangent``: the same through forward solves only, Lambda^T (Z_k - Z) X
+    = P Z^-1 (Z_k X - R) (the form a device implementation takes).  ``perturbed``: list of (sheet_k, rwg_k, region_k, u_k, io_k) with the
     topology of ``sheet``.  The same projection as ``partial_dS`` (PSSFSS.jl:391-457)."""
     import scipy.linalg as sl
     Z, _ = fill(k0, u, region, s, io.psi1, io.psi2, sheet, rwg)
@@ -314,11 +315,15 @@ def partial_dS_linearized(sheet, rwg, region, s, k0, u, io, perturbed):
         Zk, _ = fill(k0, u_k, region_k, s, io_k.psi1, io_k.psi2, sh_k, rw_k)
         Rk, Pk = rp(sh_k, rw_k, io_k)
         Xk = sl.lu_solve(lu, Rk, check_finite=False)
-        out.append(io_k.wobs[:, None] * (Pk @ Xk - Lam.T @ ((Zk - Z) @ X)))
+        if tangent:  # no transposed solve: Lambda^T (Z_k - Z) X = P Z^-1 (Z_k X - R)
+            Wk = sl.lu_solve(lu, R - Zk @ X, check_finite=False)
+            out.append(io_k.wobs[:, None] * (Pk @ Xk + P @ Wk))
+        else:
+            out.append(io_k.wobs[:, None] * (Pk @ Xk - Lam.T @ ((Zk - Z) @ X)))
     return dS, out
 
 
-def partial_gsms_linearized(sheet, rwg, points, region_rng, s, u, ios, perturbed):
+def partial_gsms_linearized(sheet, rwg, points, region_rng, s, u, ios, perturbed, tangent=False):
     """``partial_dS_linearized`` over the points of one sheet Gblock.  ``perturbed``: list
     of (sheet_k, rwg_k, points_k, u_k, ios_k).  Returns (dS per point, [dS_k per point])."""
     i1, i2 = region_rng
@@ -326,7 +331,7 @@ def partial_gsms_linearized(sheet, rwg, points, region_rng, s, u, ios, perturbed
     for p, pt in enumerate(points):
         pk = [(sh_k, rw_k, pts_k[p].layers[i1 - 1:i2], u_k, ios_k[p])
               for sh_k, rw_k, pts_k, u_k, ios_k in perturbed]
-        d, ds_k = partial_dS_linearized(sheet, rwg, pt.layers[i1 - 1:i2], s, pt.k0, u, ios[p], pk)
+        d, ds_k = partial_dS_linearized(sheet, rwg, pt.layers[i1 - 1:i2], s, pt.k0, u, ios[p], pk, tangent)
         dS.append(d)
         for k, v in enumerate(ds_k):
             lin[k].append(v)

@@ -45,3 +45,15 @@ def test_linearized_gradient_matches_full_central_differences():
     assert abs(f_lin - f_fd) <= 1e-12 * abs(f_fd)
     for k in P0:
         assert abs(g_lin[k] - g_fd[k]) <= 1e-5 * abs(g_fd[k]), (k, g_lin[k], g_fd[k])
+
+
+def test_tangent_form_equals_adjoint_form():
+    # the forward-solve form (perturbed matrices through P Z^-1 (R - Z_k X)) gives the same
+    # linearised partial GSMs as the transposed-solve form, to rounding
+    import functools
+    from pssfss_b200.gradient import meander_linearized_gradient
+    _, g_adj = meander_linearized_gradient(P0, FREQS, oracle.partial_gsms_linearized, ntri=NTRI)
+    _, g_tan = meander_linearized_gradient(P0, FREQS, functools.partial(oracle.partial_gsms_linearized,
+                                                                        tangent=True), ntri=NTRI)
+    for k in P0:
+        assert abs(g_tan[k] - g_adj[k]) <= 1e-9 * abs(g_adj[k]), (k, g_tan[k], g_adj[k])
