@@ -87,6 +87,27 @@ int pss_partial_gsms(pss_sheet *sheet, int nl, const double *eps, const double *
                      const double *kvec, const double *src, const double *tobs, const double *wobs,
                      int precision, double *dS, int *status);
 
+/* Linearised partial GSMs for gradients with one factorisation per point (no counterpart in
+ * the reference, which has no gradients).  The unperturbed inputs are those of
+ * pss_partial_gsms.  For each of npert perturbed input sets k (a sheet psheets[k] of the same
+ * context, class and basis count - the same sheet for a layer parameter - layers
+ * peps/pmu/pwidth + k*nl, smoothing parameter pu[k], per point ppsi[(k*npts+i)*2 ..] and per
+ * point and mode pkvec, psrc, ptobs, pwobs laid out like kvec .. wobs with index
+ * (k*npts+i)*nmodes + j) it returns
+ *     dSp[k][i] = wobs_k o (P_k Z^-1 R_k + P Z^-1 (R - Z_k X)),   X = Z^-1 R,
+ * the first-order value of the perturbed partial GSM from the factors of the unperturbed Z
+ * (P, R: projection and right-hand sides as in pss_partial_gsms), so central differences
+ * of dSp over +/- steps give dS/dp to O(h^2).  dS: as pss_partial_gsms; dSp: npert * npts *
+ * nmodes^2 complex.  Points run one at a time on the context's first stream; calls on one
+ * context must not overlap. */
+int pss_partial_gsms_lin(pss_sheet *sheet, int nl, const double *eps, const double *mu, const double *width,
+                         int s, double u, int npts, const double *k0, const double *psi, int nmodes,
+                         const double *kvec, const double *src, const double *tobs, const double *wobs,
+                         int npert, pss_sheet *const *psheets, const double *peps, const double *pmu,
+                         const double *pwidth, const double *pu, const double *ppsi, const double *pkvec,
+                         const double *psrc, const double *ptobs, const double *pwobs, int precision,
+                         double *dS, double *dSp, int *status);
+
 /* The MoM matrix of one point: Z (nbf x nbf complex, column-major like zorymat). */
 int pss_fill_matrix(pss_sheet *sheet, int nl, const double *eps, const double *mu, const double *width, int s,
                     double u, double k0, double psi1, double psi2, double *Z, int *mmax_out);

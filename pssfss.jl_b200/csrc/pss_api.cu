@@ -1025,3 +1025,231 @@ int pss_schur_update(pss_ctx *c, int m, int n, int k, const float *Lr, const flo
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Linearised partial GSMs for gradients with one factorisation per point.  For each perturbed
+// input set k (another sheet of the same topology, other layers, smoothing parameter, modes):
+//     dS_k = wobs_k o (P_k Z^-1 R_k + P Z^-1 (R - Z_k X)),   X = Z^-1 R,
+// the first-order value of the perturbed partial GSM from the factors of Z, so that central
+// differences of dS_k give dS/dp to O(h^2).  Forward solves only: R_k are extra right-hand
+// sides of the first solve, R - Z_k X those of a second solve on the same factors.
+namespace {
+
+// Y[:, j] = B[:, j] - A X[:, j] for row-major A (n x n, row stride ld): one warp per row.
+__global__ void k_lin_resid(int n, int nrhs, const cd *__restrict__ A, long long ld, const cd *__restrict__ X,
+                            const cd *__restrict__ B, cd *__restrict__ Y) {
+  const int row = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (row >= n) return;  // uniform per warp
+  const cd *a = A + (long long)row * ld;
+  for (int j = 0; j < nrhs; ++j) {
+    const cd *x = X + (long long)j * n;
+    double sr = 0.0, si = 0.0;
+    for (int c = lane; c < n; c += 32) {
+      const cd p = a[c] * x[c];
+      sr += p.x;
+      si += p.y;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      sr += __shfl_xor_sync(0xffffffffu, sr, o);
+      si += __shfl_xor_sync(0xffffffffu, si, o);
+    }
+    if (lane == 0) Y[(long long)j * n + row] = B[(long long)j * n + row] - mkcd(sr, si);
+  }
+}
+
+// The tables of one point, copied out of the context's table buffers (which the next
+// build_tables call reuses).
+int point_tables(pss_ctx *c, const StackParams &S, const PointParams *dP, DevBuf &own, TableDev &t, int &hstat) {
+  std::vector<TableDev> tabs;
+  std::vector<int> hs(1, 0);
+  if (int rc = build_tables(c, S, dP, 1, 1e-7, tabs, hs)) return rc;
+  const size_t used = (size_t)(tabs[0].mmax + 2) * (tabs[0].mmax + 2);
+  if (own.ensure(2 * used * sizeof(cd))) return -3;
+  cudaStream_t st = c->w[0].st;
+  PSS_CUDA_TRY(cudaMemcpyAsync(own.p, tabs[0].t1, used * sizeof(cd), cudaMemcpyDeviceToDevice, st));
+  PSS_CUDA_TRY(cudaMemcpyAsync(own.as<cd>() + used, tabs[0].t2, used * sizeof(cd), cudaMemcpyDeviceToDevice, st));
+  t.t1 = own.as<cd>();
+  t.t2 = own.as<cd>() + used;
+  t.mmax = tabs[0].mmax;
+  hstat |= hs[0];
+  return 0;
+}
+
+}  // namespace
+
+extern "C" int pss_partial_gsms_lin(pss_sheet *sh, int nl, const double *eps, const double *mu, const double *width,
+                                    int s, double u, int npts, const double *k0, const double *psi, int nmodes,
+                                    const double *kvec, const double *src, const double *tobs, const double *wobs,
+                                    int npert, pss_sheet *const *psh, const double *peps, const double *pmu,
+                                    const double *pwidth, const double *pu, const double *ppsi, const double *pkvec,
+                                    const double *psrc, const double *ptobs, const double *pwobs, int precision,
+                                    double *dS, double *dSp, int *status) {
+  if (!sh || !k0 || !psi || !dS || !status || !kvec || !src || !tobs || !wobs) {
+    pss_set_error("null argument");
+    return -1;
+  }
+  if (npts <= 0 || nmodes <= 0 || nmodes > 4096 || npert < 0 || npert > 64) {
+    pss_set_error("invalid npts/nmodes/npert");
+    return -1;
+  }
+  if (npert > 0 && (!psh || !peps || !pmu || !pwidth || !pu || !ppsi || !pkvec || !psrc || !ptobs || !pwobs || !dSp)) {
+    pss_set_error("null perturbation argument");
+    return -1;
+  }
+  if (precision != PSS_FP64 && precision != PSS_FP32_REFINE) { pss_set_error("unknown precision %d", precision); return -1; }
+  for (int k = 0; k < npert; ++k)
+    if (!psh[k] || psh[k]->ctx != sh->ctx || psh[k]->nbf != sh->nbf || psh[k]->cls != sh->cls) {
+      pss_set_error("perturbed sheet %d is not a sheet of the same context, class and basis count", k);
+      return -1;
+    }
+  if (!(u > 0)) { pss_set_error("smoothing parameter u must be positive"); return -1; }
+  pss_ctx *c = sh->ctx;
+  if (set_device(c)) return -3;
+  const int magnetic = sh->cls == 'M';
+  const int n = sh->nbf, nm = nmodes, K = npert;
+  const long long ld = n, msz = (long long)n * n;
+  StackParams S;
+  if (make_stack(nl, eps, mu, width, s, S)) return -1;
+  std::vector<StackParams> Sk(K);
+  for (int k = 0; k < K; ++k) {
+    if (make_stack(nl, peps + 2 * (size_t)k * nl, pmu + 2 * (size_t)k * nl, pwidth + (size_t)k * nl, s, Sk[k]))
+      return -1;
+    if (!(pu[k] > 0)) { pss_set_error("perturbed smoothing parameter %d must be positive", k); return -1; }
+  }
+  Worker &w = c->w[0];
+  cudaStream_t st = w.st;
+  const int nrhs1 = nm * (1 + K), nrhs2 = nm * K;
+  int rc = ensure_worker(w, sh, nm, precision, false, 1 + K);
+  if (rc) return rc;
+  if ((rc = w.ensure_solver(n, std::max(nrhs1, 1), 1 + K))) return rc;
+  int maxufp = sh->nufp;
+  for (int k = 0; k < K; ++k) maxufp = std::max(maxufp, psh[k]->nufp);
+  if (w.zb.ensure((size_t)maxufp * 9 * sizeof(cd))) return -3;
+  DevBuf pbuf, tb0, mbuf, Ybuf, Wbuf, out;
+  std::vector<DevBuf> tbk(K);
+  if (pbuf.ensure((size_t)(1 + K) * sizeof(PointParams)) ||
+      mbuf.ensure((size_t)(1 + K) * nm * (2 * sizeof(double) + 2 * sizeof(cd) + 2 * sizeof(double) + sizeof(cd))) ||
+      Ybuf.ensure((size_t)n * std::max(nrhs2, 1) * sizeof(cd)) || Wbuf.ensure((size_t)n * std::max(nrhs2, 1) * sizeof(cd)) ||
+      out.ensure((size_t)(1 + 2 * K) * nm * nm * sizeof(cd)))
+    return -3;
+  const size_t nmk = (size_t)nm * 2;  // doubles of one mode set's kvec / tobs; cd of its src
+  // per mode set q (0 = unperturbed, k + 1 = perturbation k): kvec, src, tobs, wobs
+  char *mb = mbuf.as<char>();
+  auto kv_of = [&](int q) { return (double *)mb + (size_t)q * nmk; };
+  auto src_of = [&](int q) { return (cd *)(mb + (size_t)(1 + K) * nmk * sizeof(double)) + (size_t)q * nmk; };
+  auto tob_of = [&](int q) {
+    return (double *)(mb + (size_t)(1 + K) * nmk * (sizeof(double) + sizeof(cd))) + (size_t)q * nmk;
+  };
+  auto wob_of = [&](int q) {
+    return (cd *)(mb + (size_t)(1 + K) * nmk * (2 * sizeof(double) + sizeof(cd))) + (size_t)q * nm;
+  };
+  std::vector<cd> hdS((size_t)(1 + 2 * K) * nm * nm);
+  float *zr = precision == PSS_FP32_REFINE ? w.zr.as<float>() : nullptr;
+  float *zi = precision == PSS_FP32_REFINE ? w.zi.as<float>() : nullptr;
+  const cd *L64 = precision == PSS_FP64 ? w.z64.as<cd>() : nullptr;
+  for (int i = 0; i < npts; ++i) {
+    if (!(k0[i] > 0) || !std::isfinite(psi[2 * i]) || !std::isfinite(psi[2 * i + 1])) {
+      pss_set_error("invalid k0/psi at point %d", i);
+      return -1;
+    }
+    int hst = 0;
+    // point parameters and mode data of every set
+    std::vector<PointParams> hP(1 + K);
+    {
+      const double b1m[2] = {sh->b1[0] * sh->upm, sh->b1[1] * sh->upm};
+      const double b2m[2] = {sh->b2[0] * sh->upm, sh->b2[1] * sh->upm};
+      make_params(magnetic, S, b1m, b2m, u, k0[i], psi[2 * i], psi[2 * i + 1], hP[0]);
+    }
+    for (int k = 0; k < K; ++k) {
+      const pss_sheet *q = psh[k];
+      const double b1m[2] = {q->b1[0] * q->upm, q->b1[1] * q->upm};
+      const double b2m[2] = {q->b2[0] * q->upm, q->b2[1] * q->upm};
+      const double *pp = ppsi + 2 * ((size_t)k * npts + i);
+      make_params(magnetic, Sk[k], b1m, b2m, pu[k], k0[i], pp[0], pp[1], hP[1 + k]);
+    }
+    PSS_CUDA_TRY(cudaMemcpy(pbuf.p, hP.data(), hP.size() * sizeof(PointParams), cudaMemcpyHostToDevice));
+    const PointParams *dP = pbuf.as<PointParams>();
+    for (int q = 0; q <= K; ++q) {
+      const size_t off = q == 0 ? (size_t)i * nm : ((size_t)(q - 1) * npts + i) * nm;
+      const double *kv = q == 0 ? kvec : pkvec;
+      const double *sv = q == 0 ? src : psrc;
+      const double *tv = q == 0 ? tobs : ptobs;
+      const double *wv = q == 0 ? wobs : pwobs;
+      PSS_CUDA_TRY(cudaMemcpy(kv_of(q), kv + 2 * off, nm * 2 * sizeof(double), cudaMemcpyHostToDevice));
+      PSS_CUDA_TRY(cudaMemcpy(src_of(q), sv + 4 * off, nm * 2 * sizeof(cd), cudaMemcpyHostToDevice));
+      PSS_CUDA_TRY(cudaMemcpy(tob_of(q), tv + 2 * off, nm * 2 * sizeof(double), cudaMemcpyHostToDevice));
+      PSS_CUDA_TRY(cudaMemcpy(wob_of(q), wv + 2 * off, nm * sizeof(cd), cudaMemcpyHostToDevice));
+    }
+    // tables and face-pair integrals of every set
+    TableDev t0;
+    std::vector<TableDev> tk(K);
+    if ((rc = point_tables(c, S, dP, tb0, t0, hst))) return rc;
+    for (int k = 0; k < K; ++k)
+      if ((rc = point_tables(c, Sk[k], dP + 1 + k, tbk[k], tk[k], hst))) return rc;
+    if ((rc = refresh_jk_cache(sh, psi[2 * i], psi[2 * i + 1], u / sh->upm, st))) return rc;
+    if (sh->jk_nonconv) hst |= PSS_ST_JK_NOCONV;
+    // Z into slot 0 (and the FP32 planes), fills and transforms of every set
+    pss_fill_pairs(sh->G, dP, sh->cache.jk, t0.t1, t0.t2, t0.mmax, w.zb.as<cd>(), st);
+    pss_fill_assemble(sh->G, dP, w.zb.as<cd>(), w.z64.as<cd>(), zr, zi, ld, st);
+    cd *bf = w.bf.as<cd>();
+    const size_t bfs = (size_t)nm * n * 2;
+    pss_bfft(sh->G, nm, kv_of(0), psi[2 * i], psi[2 * i + 1], bf, st);
+    pss_rhs(n, nm, bf, src_of(0), w.rhs.as<cd>(), st);
+    for (int k = 0; k < K; ++k) {
+      pss_sheet *q = psh[k];
+      const double *pp = ppsi + 2 * ((size_t)k * npts + i);
+      if ((rc = refresh_jk_cache(q, pp[0], pp[1], pu[k] / q->upm, st))) return rc;
+      if (q->jk_nonconv) hst |= PSS_ST_JK_NOCONV;
+      pss_fill_pairs(q->G, dP + 1 + k, q->cache.jk, tk[k].t1, tk[k].t2, tk[k].mmax, w.zb.as<cd>(), st);
+      pss_fill_assemble(q->G, dP + 1 + k, w.zb.as<cd>(), w.z64.as<cd>() + (1 + k) * msz, nullptr, nullptr, ld, st);
+      pss_bfft(q->G, nm, kv_of(1 + k), pp[0], pp[1], bf + (1 + k) * bfs, st);
+      pss_rhs(n, nm, bf + (1 + k) * bfs, src_of(1 + k), w.rhs.as<cd>() + (size_t)(1 + k) * nm * n, st);
+    }
+    // one factorisation; solves of R and every R_k
+    PSS_CUDA_TRY(cudaMemsetAsync(w.bstat.p, 0, sizeof(int), st));
+    if ((rc = w.factor_solve(n, 1, precision, nrhs1, kMaxRefine, w.bstat.as<int>()))) return rc;
+    // R - Z_k X (slot k + 1), then its solve on the same factors
+    cd *X = w.X.as<cd>();
+    for (int k = 0; k < K; ++k) {
+      pss_count_launch();
+      k_lin_resid<<<cdiv_u((long long)n * 32, 256), 256, 0, st>>>(n, nm, w.z64.as<cd>() + (1 + k) * msz, ld, X,
+                                                                   w.rhs.as<cd>(), Ybuf.as<cd>() + (size_t)k * nm * n);
+    }
+    if (K > 0) {
+      const long long vs2 = (long long)n * nrhs2;
+      if ((rc = pss_solve_lu(w.sws, 1, L64, zr, zi, ld, msz, nrhs2, Ybuf.as<cd>(), Wbuf.as<cd>(), vs2, 0, st)))
+        return rc;
+      if (precision == PSS_FP32_REFINE &&
+          (rc = pss_refine(w.sws, 1, w.z64.as<cd>(), ld, msz, zr, zi, nrhs2, Ybuf.as<cd>(), Wbuf.as<cd>(),
+                           w.R.as<cd>(), w.D.as<cd>(), vs2, kMaxRefine, w.bstat.as<int>(), st)))
+        return rc;
+      pss_solve_status(w.sws, 1, w.bstat.as<int>(), st);
+    }
+    // projections: dS; P_k X_k' and P W_k for every k
+    cd *o = out.as<cd>();
+    const size_t nm2 = (size_t)nm * nm;
+    pss_project(n, nm, bf, tob_of(0), wob_of(0), X, o, st);
+    for (int k = 0; k < K; ++k) {
+      pss_project(n, nm, bf + (1 + k) * bfs, tob_of(1 + k), wob_of(1 + k), X + (size_t)(1 + k) * nm * n,
+                  o + (1 + 2 * k) * nm2, st);
+      pss_project(n, nm, bf, tob_of(0), wob_of(1 + k), Wbuf.as<cd>() + (size_t)k * nm * n, o + (2 + 2 * k) * nm2, st);
+    }
+    int bst = 0;
+    PSS_CUDA_TRY(cudaMemcpyAsync(hdS.data(), o, hdS.size() * sizeof(cd), cudaMemcpyDeviceToHost, st));
+    PSS_CUDA_TRY(cudaMemcpyAsync(&bst, w.bstat.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    PSS_CUDA_TRY(cudaStreamSynchronize(st));
+    status[i] = hst | bst;
+    for (size_t e = 0; e < nm2; ++e) {
+      dS[2 * ((size_t)i * nm2 + e)] = hdS[e].x;
+      dS[2 * ((size_t)i * nm2 + e) + 1] = hdS[e].y;
+    }
+    for (int k = 0; k < K; ++k)
+      for (size_t e = 0; e < nm2; ++e) {
+        const cd v = hdS[(1 + 2 * k) * nm2 + e] + hdS[(2 + 2 * k) * nm2 + e];
+        const size_t d = ((size_t)k * npts + i) * nm2 + e;
+        dSp[2 * d] = v.x;
+        dSp[2 * d + 1] = v.y;
+      }
+  }
+  return 0;
+}

@@ -46,6 +46,8 @@ SIGNATURES = {
                               _P, _P, _P]),
     "pss_sheet_destroy": (_I, [_P]),
     "pss_partial_gsms": (_I, [_P, _I, _P, _P, _P, _I, _D, _I, _P, _P, _I, _P, _P, _P, _P, _I, _P, _P]),
+    "pss_partial_gsms_lin": (_I, [_P, _I, _P, _P, _P, _I, _D, _I, _P, _P, _I, _P, _P, _P, _P, _I, _P, _P, _P,
+                                  _P, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P]),
     "pss_fill_matrix": (_I, [_P, _I, _P, _P, _P, _I, _D, _D, _D, _D, _P, _P]),
     "pss_modal_tables": (_I, [_P, _I, _I, _P, _P, _P, _I, _D, _D, _D, _D, _P, _P, _D, _L, _P, _P, _P, _P]),
     "pss_face_integrals": (_I, [_P, _D, _D, _D, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
@@ -220,6 +222,56 @@ def partial_gsms(sheet, rwg, points, region_rng, s, u, ios, precision="fp64", de
     if bad.any():
         raise RuntimeError(f"solver status {status.tolist()} (singular, non-finite or device timeout)")
     return [d.T.copy() for d in dS]
+
+
+def partial_gsms_linearized(sheet, rwg, points, region_rng, s, u, ios, perturbed, precision="fp64", device=0):
+    """Scattered partial GSMs of one sheet Gblock and their first-order values at each
+    perturbed input set (``pss_partial_gsms_lin``), the ``partial_lin`` form that
+    ``gradient.linearized_gradient`` takes.  ``perturbed``: (sheet_k, rwg_k, points_k, u_k,
+    ios_k) per set, with the topology of ``sheet``."""
+    i1, i2 = region_rng
+    region = points[0].layers[i1 - 1:i2]
+    eps, mu, w = region_arrays(region)
+    npts, nm, K = len(points), len(ios[0].wobs), len(perturbed)
+
+    def modes(ios_):
+        return (_f64(np.stack([io.kvec for io in ios_])), _c2d(np.stack([io.src for io in ios_])),
+                _f64(np.stack([io.tobs for io in ios_])), _c2d(np.stack([io.wobs for io in ios_])))
+    k0 = _f64([pt.k0 for pt in points])
+    psi = _f64([[io.psi1, io.psi2] for io in ios])
+    kvec, src, tobs, wobs = modes(ios)
+    ds = device_sheet(sheet, rwg, device)
+    held = [device_sheet(sh_k, rw_k, device) for sh_k, rw_k, _, _, _ in perturbed]
+    psh = (ctypes.c_void_p * max(K, 1))(*[d.h.value for d in held])
+    pe, pm, pw, pu, pp, pk, ps, pt, pwo = [], [], [], [], [], [], [], [], []
+    for (_, _, pts_k, u_k, ios_k) in perturbed:
+        e_, m_, w_ = region_arrays(pts_k[0].layers[i1 - 1:i2])
+        pe.append(e_)
+        pm.append(m_)
+        pw.append(w_)
+        pu.append(float(u_k))
+        pp.append([[io.psi1, io.psi2] for io in ios_k])
+        a, b, c, d = modes(ios_k)
+        pk.append(a)
+        ps.append(b)
+        pt.append(c)
+        pwo.append(d)
+    z = np.zeros(1)
+    arr = (lambda xs, f: f(np.stack(xs)) if xs else z)
+    peps, pmu, pwidth = arr(pe, _c2d), arr(pm, _c2d), arr(pw, _f64)
+    pu_, ppsi, pkvec = arr(pu, _f64), arr(pp, _f64), arr(pk, _f64)
+    psrc, ptobs, pwobs = arr(ps, _c2d), arr(pt, _f64), arr(pwo, _c2d)
+    dS = np.zeros((npts, nm, nm), complex)
+    dSp = np.zeros((max(K, 1), npts, nm, nm), complex)
+    status = np.zeros(npts, np.int32)
+    _check(lib().pss_partial_gsms_lin(ds.h, len(region), _p(eps), _p(mu), _p(w), s, float(u), npts, _p(k0), _p(psi),
+                                      nm, _p(kvec), _p(src), _p(tobs), _p(wobs), K, psh, _p(peps), _p(pmu),
+                                      _p(pwidth), _p(pu_), _p(ppsi), _p(pkvec), _p(psrc), _p(ptobs), _p(pwobs),
+                                      PRECISIONS[precision], _p(dS), _p(dSp), _p(status)), "pss_partial_gsms_lin")
+    if (status & FATAL_STATUS).any():
+        raise RuntimeError(f"solver status {status.tolist()} (singular, non-finite or device timeout)")
+    del held
+    return [d.T.copy() for d in dS], [[d.T.copy() for d in dSp[k]] for k in range(K)]
 
 
 def fill_matrix(sheet, rwg, layers, s, u, k0, psi1, psi2, device=0):

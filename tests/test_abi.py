@@ -57,6 +57,8 @@ def test_entry_points_reject_bad_arguments_before_any_device_use():
     assert L.pss_ctx_destroy(nul) == 0 and L.pss_sheet_destroy(nul) == 0
     assert L.pss_partial_gsms(nul, 1, buf, buf, buf, 1, 1.0, 1, buf, buf, 1, buf, buf, buf, buf, 0,
                               buf, ibuf) == -1 and "null" in err()
+    assert L.pss_partial_gsms_lin(nul, 1, buf, buf, buf, 1, 1.0, 1, buf, buf, 1, buf, buf, buf, buf, 0, nul,
+                                  *([nul] * 9), 0, buf, nul, ibuf) == -1 and "null" in err()
     assert L.pss_fill_matrix(nul, 1, buf, buf, buf, 1, 1.0, 1.0, 0.0, 0.0, buf,
                              ctypes.byref(ctypes.c_int())) == -1 and "null" in err()
     assert L.pss_face_integrals(nul, 1.0, 0.0, 0.0, *([buf] * 9)) == -1 and "null" in err()
