@@ -102,3 +102,51 @@ def test_device_sheet_cache_is_bounded_and_reuses_entries(monkeypatch):
     assert made == [s[0], s[1], s[2]] and freed == [s[1]]
     assert [v.sheet for v in engine._sheets.values()] == [s[0], s[2]]
     del a
+
+
+def test_linearized_binding_packs_the_header_layout(monkeypatch):
+    # Host side of engine.partial_gsms_linearized without a device: the arrays handed to
+    # pss_partial_gsms_lin follow the header's layout (perturbed set k, point i, mode j at
+    # (k*npts + i)*nmodes + j), and the outputs come back per point, transposed.
+    import ctypes
+    import types
+    import numpy as np
+    from pssfss_b200.layers import Layer
+
+    npts, nm, K, nl = 3, 2, 2, 3
+    rng = np.random.default_rng(0)
+
+    def io(seed):
+        r = np.random.default_rng(seed)
+        return types.SimpleNamespace(kvec=r.normal(size=(nm, 2)), src=r.normal(size=(nm, 2)) + 1j * r.normal(size=(nm, 2)),
+                                     tobs=r.normal(size=(nm, 2)), wobs=r.normal(size=nm) + 1j * r.normal(size=nm),
+                                     psi1=float(r.normal()), psi2=float(r.normal()))
+    layers = [Layer(), Layer(epsr=2.2), Layer()]
+    pts = [types.SimpleNamespace(layers=layers, k0=100.0 + i) for i in range(npts)]
+    ios = [io(i) for i in range(npts)]
+    pert = [(object(), object(), pts, 7.0 + k, [io(100 * (k + 1) + i) for i in range(npts)]) for k in range(K)]
+    seen = {}
+
+    def fake_call(*a):
+        names = ["sh", "nl", "eps", "mu", "width", "s", "u", "npts", "k0", "psi", "nm", "kvec", "src", "tobs", "wobs",
+                 "npert", "psh", "peps", "pmu", "pwidth", "pu", "ppsi", "pkvec", "psrc", "ptobs", "pwobs", "prec",
+                 "dS", "dSp", "status"]
+        seen.update(zip(names, a))
+        seen["dS"][:] = rng.normal(size=seen["dS"].shape)
+        seen["dSp"][:] = rng.normal(size=seen["dSp"].shape)
+        return 0
+
+    monkeypatch.setattr(engine, "_p", lambda x: x)
+    monkeypatch.setattr(engine, "lib", lambda: types.SimpleNamespace(pss_partial_gsms_lin=fake_call))
+    monkeypatch.setattr(engine, "device_sheet", lambda sh, rw, device=0: types.SimpleNamespace(h=ctypes.c_void_p(7)))
+    dS, lin = engine.partial_gsms_linearized(object(), object(), pts, (1, 3), 1, 5.0, ios, pert)
+    assert seen["nl"] == nl and seen["npert"] == K and seen["npts"] == npts and seen["nm"] == nm
+    pk = seen["pkvec"].reshape(K, npts, nm, 2)
+    ps = seen["psrc"].reshape(K, npts, nm, 2)
+    for k in range(K):
+        assert seen["pu"][k] == 7.0 + k
+        for i in range(npts):
+            assert np.array_equal(pk[k, i], pert[k][4][i].kvec) and np.array_equal(ps[k, i], pert[k][4][i].src)
+            assert tuple(seen["ppsi"][k, i]) == (pert[k][4][i].psi1, pert[k][4][i].psi2)
+    assert seen["peps"].shape == (K, nl) and seen["peps"][0, 1] == layers[1].epsr
+    assert np.array_equal(dS[1], seen["dS"][1].T) and np.array_equal(lin[1][2], seen["dSp"][1, 2].T)
