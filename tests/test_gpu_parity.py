@@ -232,8 +232,8 @@ def _gsm_relerr(res, ref):
     return worst
 
 
-def test_config1_square_patch_sweep():
-    """Plain FP64 config: 8 mm square patch in a 10 mm cell (structured, 512 triangles,
+def test_square_patch_sweep():
+    """8 mm square patch in a 10 mm cell (structured, 512 triangles,
     N = 736) in free space, normal incidence, 11 frequencies 10-20 GHz; the FP32 form is held
     to |dS| <= 1e-6 of the FP64 oracle on the same sweep."""
     from pssfss_b200 import analyze
@@ -261,8 +261,8 @@ def test_two_sheet_cascade_oblique_scan():
     assert _gsm_relerr(analyze(strata, freqs, steer, precision="fp32r"), ref) <= 1e-6
 
 
-def test_config2_jerusalem_cross_and_aperture_cascade():
-    """Two-sheet cascade in the shape of the plain-FP64 config 2: a (solid) Jerusalem-cross
+def test_jerusalem_cross_and_aperture_cascade():
+    """Two-sheet cascade: a (solid) Jerusalem-cross
     conductor on 0.5 mm eps_r = 3 (tan d = 0.002), a 2 mm air gap, then a 6 mm square
     aperture (M-type) in an 8 mm cell; scan theta = 30, phi = 45 (face-pair integrals per
     point).  Own structured meshes (the reference meshes these with Triangle), coarse enough
@@ -282,8 +282,8 @@ def test_config2_jerusalem_cross_and_aperture_cascade():
 
 @pytest.mark.parametrize("period,ro,ntri,theta", [(6.0, 0.40, 160, 0.0), (9.0, 0.36, 260, 15.0),
                                                   (12.0, 0.44, 360, 45.0)])
-def test_config4_ring_patches(period, ro, ntri, theta):
-    """Ring-patch problems in the style of the batched config 4 (period, outer radius and
+def test_ring_patches_of_varied_size(period, ro, ntri, theta):
+    """Ring-patch problems of a batch whose members differ (period, outer radius and
     triangle count vary per problem, so do the unknown counts; scan theta in {0, 15, 45}),
     free-standing, 2 frequencies each, FP32 + refinement against the FP64 oracle."""
     from pssfss_b200 import analyze
