@@ -21,10 +21,9 @@ difference is smooth: `topology(params)` returns a key (for the meander, its seg
 import numpy as np
 
 from .analyze import add_scattered, analyze, assemble, make_plan, sheet_gblocks, sheet_io
-from .elements import meander, meander_counts
-from .layers import TE, TM, Layer
+from .elements import meander_counts
+from .layers import TE, TM
 from .outputs import getsijmn
-from .units import Length, mm
 
 
 def fd_gradient(build, params, flist, steering, objective, *, rel_step=1e-4, topology=None,
@@ -61,16 +60,17 @@ def te_tm_transmission_objective(results):
                for r in results)
 
 
-def meander_strata(params, *, b=10.0, h=6.0, ntri=4000, sub_width_mm=1.0):
-    """Layers and sheet of the meander workload: ``params`` has ``w`` (trace width, both
-    w1 and w2, mm), ``a`` (cell period along the meander, mm) and ``epsr`` (substrate)."""
-    sheet = meander(a=params["a"], b=b, h=h, w1=params["w"], w2=params["w"], ntri=ntri, units=mm)
-    return [Layer(), sheet, Layer(epsr=params["epsr"], width=Length(sub_width_mm, mm)), Layer()]
+def meander_strata(params, *, ntri=4000):
+    """Layers and sheet of the meander workload (``workloads.meander_strata``): ``params`` has
+    ``w`` (trace width, both w1 and w2, mm), ``a`` (cell period along the meander, mm) and
+    ``epsr`` (the 1 mm substrate)."""
+    from .workloads import meander_strata as build
+    return build(w=params["w"], a=params["a"], epsr=params["epsr"], ntri=ntri)
 
 
-def meander_topology(params, *, b=10.0, h=6.0, ntri=4000):
+def meander_topology(params, *, ntri=4000):
     """Segment counts of the meander mesh at ``params`` (equal counts: same topology)."""
-    return meander_counts(params["a"], b, h, params["w"], params["w"], ntri)[:4]
+    return meander_counts(params["a"], 10.0, 6.0, params["w"], params["w"], ntri)[:4]
 
 
 def meander_gradient(params, flist, *, ntri=4000, rel_step=1e-4, analyze_fn=None, **kw):

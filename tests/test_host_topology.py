@@ -427,3 +427,24 @@ def test_sheet_file_round_trip(tmp_path):
     for k in ("rho", "e1", "e2", "fv", "fe"):
         assert np.array_equal(getattr(back, k), getattr(sh, k))
     assert back.units == sh.units and back.style == sh.style
+
+
+def test_benchmark_workloads_plan():
+    # the workloads build and plan on the host with the sizes they are quoted at
+    from pssfss_b200 import workloads
+    from pssfss_b200.analyze import make_plan
+    strata, f, st = workloads.square_patch_sweep()
+    plan = make_plan(strata, f, st)
+    assert plan.rwgdat[0].nbf == 736 and len(plan.points) == 11
+    strata, f, st = workloads.meander_precision_sweep()
+    assert setup_rwg(strata[1]).nbf == 3976 and len(f) == 101
+    strata, f, st = workloads.jerusalem_aperture_cascade(ntri_cross=300, ntri_aperture=200)
+    plan = make_plan(strata, f, st)
+    assert len(plan.sheets) == 2 and len(plan.points) == 51 and plan.sheets[1].cls == "M"
+    batch = workloads.ring_batch()
+    assert len(batch) == 64
+    sizes = [b[0][1].nface for b in batch]
+    assert min(sizes) >= 250 and max(sizes) <= 3600 and len({b[2]["θ"] for b in batch}) == 4
+    params, f, ntri = workloads.meander_gradient_workload()
+    sh = workloads.meander_strata(ntri=ntri, **params)[1]
+    assert sh.nface == 3960 and len(f) == 201
