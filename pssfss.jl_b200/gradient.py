@@ -10,9 +10,9 @@ held to and a gradient in its own right.
 `linearized_gradient` needs one factorisation per point instead of 2·P: the partial GSM at
 p ± h is taken to first order from the factors at p (the perturbed matrices enter only through
 Λᵀ (Z± − Z) X with Λ = Z⁻ᵀ Pᵀ, and the perturbed sources through extra right-hand sides), while
-the cheap host parts (modes, incident GSMs, cascade) are recomputed at p ± h.  The device
-form of that linearised partial GSM is not built yet; its contract is the ``partial_lin``
-argument.
+the cheap host parts (modes, incident GSMs, cascade) are recomputed at p ± h.  The
+linearised partial GSM comes from ``partial_lin``, by default the CUDA library's
+(``engine.partial_gsms_linearized``, forward solves on the factors of Z).
 
 Geometry steps must leave the mesh topology unchanged, so that vertices move affinely and the
 difference is smooth: `topology(params)` returns a key (for the meander, its segment counts,
@@ -82,7 +82,7 @@ def meander_gradient(params, flist, *, ntri=4000, rel_step=1e-4, analyze_fn=None
                        analyze_fn=analyze_fn, **kw)
 
 
-def linearized_gradient(build, params, flist, steering, objective, partial_lin, *, rel_step=1e-4,
+def linearized_gradient(build, params, flist, steering, objective, partial_lin=None, *, rel_step=1e-4,
                         topology=None):
     """Objective and central-difference gradient with one factorisation per point.
 
@@ -92,6 +92,8 @@ def linearized_gradient(build, params, flist, steering, objective, partial_lin, 
     from the unperturbed factorisation.  Every perturbed plan must keep the points, Gblocks,
     modes and mesh topology of the unperturbed one.  Returns ``(f(params), {name: df/dp})``.
     """
+    if partial_lin is None:
+        from .engine import partial_gsms_linearized as partial_lin
     p0 = {k: float(v) for k, v in params.items()}
     key0 = topology(p0) if topology is not None else None
     steps = []
@@ -134,7 +136,7 @@ def linearized_gradient(build, params, flist, steering, objective, partial_lin, 
     return f0, grad
 
 
-def meander_linearized_gradient(params, flist, partial_lin, *, ntri=4000, rel_step=1e-4):
+def meander_linearized_gradient(params, flist, partial_lin=None, *, ntri=4000, rel_step=1e-4):
     """`meander_gradient` with one factorisation per point (see `linearized_gradient`)."""
     return linearized_gradient(lambda p: meander_strata(p, ntri=ntri), params, np.asarray(flist, float),
                                {"θ": 0.0, "ϕ": 0.0}, te_tm_transmission_objective, partial_lin,

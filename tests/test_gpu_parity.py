@@ -7,6 +7,7 @@ bounds are 1e-10 relative (max-abs-difference over max-abs-value) for tables, in
 and matrices, and 1e-9 for S-parameters.  FP32+refinement results must agree with the
 FP64 oracle to |dS| <= 1e-6 absolute (the target of the precision form).
 """
+import functools
 import math
 
 import numpy as np
@@ -297,3 +298,43 @@ def test_ring_patches_of_varied_size(period, ro, ntri, theta):
     ref = oracle.analyze(strata, freqs, steer)
     assert _gsm_relerr(analyze(strata, freqs, steer, precision="fp32r"), ref) <= 1e-6
     assert _gsm_relerr(analyze(strata, freqs, steer), ref) < 1e-9
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32r"])
+def test_linearised_partial_gsms_and_gradient(precision):
+    """pss_partial_gsms_lin on a small meanderline (two perturbed sets: eps_r of the substrate,
+    and the trace width, a second sheet of the same topology) against the oracle's
+    forward-solve form, and the one-factorisation gradient through it against the oracle's."""
+    from pssfss_b200 import engine
+    from pssfss_b200.analyze import make_plan, sheet_gblocks, sheet_io
+    from pssfss_b200.gradient import meander_linearized_gradient, meander_strata
+    P0 = {"w": 0.3, "a": 5.0, "epsr": 2.2}
+    steps = [{**P0, "epsr": 2.2 * (1 + 1e-4)}, {**P0, "w": 0.3 * (1 + 1e-4)}]
+    freqs, st = [9.0, 15.0], {"θ": 0.0, "ϕ": 0.0}
+    plan0 = make_plan(meander_strata(P0, ntri=120), freqs, st)
+    plans = [make_plan(meander_strata(p, ntri=120), freqs, st) for p in steps]
+    (_, (i1, i2), _, s), = sheet_gblocks(plan0)
+    sh, rw = plan0.sheets[0], plan0.rwgdat[0]
+    ios0 = [sheet_io(pt.layers[i1 - 1:i2], sh, s, pt.k0, pt.beta00) for pt in plan0.points]
+    pert = []
+    for pl in plans:
+        shk = pl.sheets[0]
+        pert.append((shk, pl.rwgdat[0], pl.points, pl.uvec[0],
+                     [sheet_io(pt.layers[i1 - 1:i2], shk, s, pt.k0, pt.beta00) for pt in pl.points]))
+    ref0, refk = oracle.partial_gsms_linearized(sh, rw, plan0.points, (i1, i2), s, plan0.uvec[0], ios0, pert,
+                                                tangent=True)
+    got0, gotk = engine.partial_gsms_linearized(sh, rw, plan0.points, (i1, i2), s, plan0.uvec[0], ios0, pert,
+                                                precision=precision)
+    for i in range(len(freqs)):
+        assert relerr(got0[i], ref0[i]) < 1e-11
+        for k in range(len(pert)):
+            assert relerr(gotk[k][i], refk[k][i]) < 1e-11
+            # the perturbation itself (~1e-4 of dS) to 1e-6 of its size
+            d = refk[k][i] - ref0[i]
+            assert np.max(np.abs((gotk[k][i] - got0[i]) - d)) <= 1e-6 * np.max(np.abs(d))
+    part = functools.partial(engine.partial_gsms_linearized, precision=precision)
+    _, g_dev = meander_linearized_gradient(P0, freqs, part, ntri=120)
+    _, g_ref = meander_linearized_gradient(P0, freqs, functools.partial(oracle.partial_gsms_linearized, tangent=True),
+                                           ntri=120)
+    for k in P0:
+        assert abs(g_dev[k] - g_ref[k]) <= 1e-6 * abs(g_ref[k]), (k, g_dev[k], g_ref[k])
