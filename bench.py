@@ -205,6 +205,43 @@ def cpu_baseline_sample(case):
                                       f"({t_jk:.1f} s) amortised over {NFREQ} points"}
 
 
+def run_grads(args, rank):
+    """Gradients/s of Σ_f (|S21_TE|² − |S21_TM|²) in trace width, pitch and substrate eps_r of
+    the meanderline at ntri = 4000 (N ≈ 6000) over 201 frequencies 8-18 GHz: one FP32 +
+    refinement factorisation per point, the six perturbed sets through the same factors
+    (pss_partial_gsms_lin).  Wall-clock per gradient, device synchronised on both sides."""
+    if rank != 0:
+        return
+    import torch
+    torch.cuda.set_device(0)
+    load_package()
+    import functools
+    from pssfss_b200 import engine, workloads
+    from pssfss_b200.gradient import meander_linearized_gradient
+    params, flist, ntri = workloads.meander_gradient_workload()
+    if args.grad_npts:
+        flist = flist[:args.grad_npts]
+    part = functools.partial(engine.partial_gsms_linearized, precision="fp32r")
+    for _ in range(args.warmup):
+        meander_linearized_gradient(params, flist, part, ntri=ntri)
+    times = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        f, g = meander_linearized_gradient(params, flist, part, ntri=ntri)
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t)
+    sec = statistics.mean(times)
+    line = {"metric": "grads/s (one-factorisation central-difference gradient)", "value": 1.0 / sec,
+            "unit": "grads/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64+c128-refine",
+            "data": "synthetic (structured meander mesh built from the reference's element recipe)",
+            "config": {"workload": f"meanderline w=0.3 a=5 mm ntri={ntri} on 1 mm eps_r=2.2, "
+                                   f"{len(flist)} freqs 8-18 GHz, d/d(w, a, eps_r)", "objective": float(f),
+                       "gradient": {k: float(v) for k, v in g.items()}}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -215,12 +252,18 @@ def main():
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--npts", type=int, default=NFREQ,
                     help="sweep points per step (default: the full 101-point sweep; fewer only for profiling)")
+    ap.add_argument("--grads", action="store_true",
+                    help="time gradients of the meander gradient workload instead (grads/s)")
+    ap.add_argument("--grad-npts", type=int, default=0,
+                    help="frequencies of the gradient workload (default: all 201)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.grads:
+        return run_grads(args, rank)
 
     import torch
     dist = None
