@@ -119,11 +119,18 @@ def get_gbldup(gbls, layers, sheets, junc):
     return gd
 
 
-def make_plan(strata, flist, steering, plan_flist=None):
+def _geometry_key(sh):
+    return (sh.rho.tobytes(), np.asarray(sh.fv).tobytes(), np.asarray(sh.fe).tobytes(), bool(sh.fufp),
+            bool(sh.xi_eta_check), tuple(np.asarray(sh.s1, float)), tuple(np.asarray(sh.s2, float)))
+
+
+def make_plan(strata, flist, steering, plan_flist=None, rwg_cache=None):
     """Everything of ``_analyze`` (PSSFSS.jl:199-255) before the per-Gblock GSMs.
 
     ``plan_flist`` (default ``flist``): the frequencies whose extremes choose the Gblocks
-    and layer modes (PSSFSS.jl:215-221) - the whole sweep when ``flist`` is one shard."""
+    and layer modes (PSSFSS.jl:215-221) - the whole sweep when ``flist`` is one shard.
+    ``rwg_cache``: a dict reused across calls so that sheets of identical geometry share one
+    basis-function setup (gradients perturb layers as well as geometry)."""
     layers = [copy.deepcopy(s) for s in strata if isinstance(s, Layer)]
     sheets = [s for s in strata if isinstance(s, RWGSheet)]
     nl = len(layers)
@@ -146,7 +153,17 @@ def make_plan(strata, flist, steering, plan_flist=None):
     gbls = choose_gblocks(layers, sheets, junc, k0min)
     choose_layer_modes(layers, sheets, junc, gbls, k0max, DBMIN)
     gbldup = get_gbldup(gbls, layers, sheets, junc)
-    rwgdat = [setup_rwg(sh) if sh.style != "NULL" else None for sh in sheets]
+    rwgdat = []
+    for sh in sheets:
+        if sh.style == "NULL":
+            rwgdat.append(None)
+        elif rwg_cache is None:
+            rwgdat.append(setup_rwg(sh))
+        else:
+            key = _geometry_key(sh)
+            if key not in rwg_cache:
+                rwg_cache[key] = setup_rwg(sh)
+            rwgdat.append(rwg_cache[key])
     uvec = []
     for sh in sheets:
         if sh.style == "NULL":

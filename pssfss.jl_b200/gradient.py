@@ -104,8 +104,9 @@ def linearized_gradient(build, params, flist, steering, objective, partial_lin=N
             if topology is not None and topology(p) != key0:
                 raise ValueError(f"step changes the mesh topology: {topology(p)} != {key0} at {p}")
             steps.append((name, h, p))
-    plan0 = make_plan(build(p0), flist, steering)
-    plans = [make_plan(build(p), flist, steering) for _, _, p in steps]
+    cache = {}  # steps of layer parameters keep the sheet's geometry: one RWG setup serves them
+    plan0 = make_plan(build(p0), flist, steering, rwg_cache=cache)
+    plans = [make_plan(build(p), flist, steering, rwg_cache=cache) for _, _, p in steps]
     blocks = sheet_gblocks(plan0)
     for pl in plans:
         if (sheet_gblocks(pl) != blocks or len(pl.points) != len(plan0.points)

@@ -160,29 +160,52 @@ def setup_rwg(sheet):
     return RWGData(bfe, bff, ebf, eci, ufpm, rep, nufp)
 
 
-def unique_face_pairs(sheet):
-    """Translation-equivalence classes of face pairs (``RWG.jl:287-319``)."""
-    nface = sheet.nface
+def _ufp_keys(sheet):
+    """Per face pair (match m, source n): the source triangle's shape class and the offset of
+    the match centroid from the source's first vertex, quantised on a grid of 1e-6 of the
+    first two centroids' distance (the KD-tree radius of ``RWG.jl:305-315``)."""
     rho = sheet.rho
     r1 = rho[sheet.fv[0] - 1]
     r2 = rho[sheet.fv[1] - 1]
     r3 = rho[sheet.fv[2] - 1]
     cen = (r1 + r2 + r3) / 3
     d = cen[0] - cen[1]
-    rad = 1e-6 * math.sqrt(d[0] * d[0] + d[1] * d[1])
-    g = rad
-    # Source-triangle shape classes (edge vectors quantised on the same grid).
+    g = 1e-6 * math.sqrt(d[0] * d[0] + d[1] * d[1])
     shape_key = np.round(np.hstack([r2 - r1, r3 - r1]) / g).astype(np.int64)
     _, shape_id = np.unique(shape_key, axis=0, return_inverse=True)
     shape_id = shape_id.ravel().astype(np.int64)
-    # Column-major face pairs: match m fastest, source n slowest.
     dx = np.round((cen[:, None, 0] - r1[None, :, 0]) / g).astype(np.int64)  # [m, n]
     dy = np.round((cen[:, None, 1] - r1[None, :, 1]) / g).astype(np.int64)
-    sid = np.broadcast_to(shape_id[None, :], (nface, nface))
-    k0 = sid.ravel(order="F")
+    return shape_id, dx, dy
+
+
+def unique_face_pairs(sheet):
+    """Translation-equivalence classes of face pairs (``RWG.jl:287-319``), numbered in the
+    order of their first member in column-major (match fastest) order.  The three keys are
+    packed into one integer when they fit in 62 bits (one sort), else sorted together."""
+    nface = sheet.nface
+    shape_id, dx, dy = _ufp_keys(sheet)
+    dx -= dx.min()
+    dy -= dy.min()
+    bx, by, bs = int(dx.max()).bit_length(), int(dy.max()).bit_length(), int(shape_id.max()).bit_length()
+    if bx + by + bs > 62:
+        return _unique_face_pairs_sorted(nface, shape_id, dx, dy)
+    key = ((shape_id[None, :] << (bx + by)) | (dx << by) | dy).ravel(order="F")
+    del dx, dy
+    _, first, inv = np.unique(key, return_index=True, return_inverse=True)
+    rank = np.empty(len(first), np.int64)
+    rank[np.argsort(first, kind="stable")] = np.arange(len(first))
+    cls = rank[inv.ravel()]
+    # classes numbered by first appearance: a new class shows where cls passes its running max
+    rep = np.flatnonzero(np.r_[True, cls[1:] > np.maximum.accumulate(cls)[:-1]])
+    return (cls + 1).reshape((nface, nface), order="F"), (rep + 1).astype(np.int64), len(first)
+
+
+def _unique_face_pairs_sorted(nface, shape_id, dx, dy):
+    """``unique_face_pairs`` by a three-key sort (keys wider than one 62-bit integer)."""
+    k0 = np.broadcast_to(shape_id[None, :], (nface, nface)).ravel(order="F")
     k1 = dx.ravel(order="F")
     k2 = dy.ravel(order="F")
-    del dx, dy
     order = np.lexsort((k2, k1, k0))
     ks0, ks1, ks2 = k0[order], k1[order], k2[order]
     newgrp = np.ones(len(order), bool)

@@ -448,3 +448,18 @@ def test_benchmark_workloads_plan():
     params, f, ntri = workloads.meander_gradient_workload()
     sh = workloads.meander_strata(ntri=ntri, **params)[1]
     assert sh.nface == 3960 and len(f) == 201
+
+
+def test_unique_face_pair_paths_agree():
+    # the packed one-key classing and the three-key sort give the same classes, numbered by
+    # first member in column-major order (RWG.jl:287-319)
+    from pssfss_b200 import rwg
+    from pssfss_b200.elements import diagstrip
+    for sh in (meander(a=5, b=10, h=6, w1=0.3, w2=0.3, ntri=300, units=mm),
+               rectstrip(Lx=8, Ly=8, Px=10, Py=10, Nx=16, Ny=16, units=mm, fufp=True),
+               diagstrip(P=10, w=1, orient=45, Nl=12, Nw=3, units=mm)):
+        a = rwg.unique_face_pairs(sh)
+        sid, dx, dy = rwg._ufp_keys(sh)
+        b = rwg._unique_face_pairs_sorted(sh.nface, sid, dx, dy)
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and a[2] == b[2]
+        assert a[0][tuple(np.unravel_index(a[1] - 1, a[0].shape, order="F"))].tolist() == list(range(1, a[2] + 1))
