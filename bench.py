@@ -205,6 +205,43 @@ def cpu_baseline_sample(case):
                                       f"({t_jk:.1f} s) amortised over {NFREQ} points"}
 
 
+def run_rings(args, rank):
+    """Freq-points/s over the seeded batch of 64 ring problems (period 6-12 mm, 300-3000
+    triangles, theta in {0, 15, 30, 45}, 21 frequencies each), FP32 + refinement through
+    ``analyze``, one sweep call per problem.  Wall-clock per pass over the batch, device
+    synchronised on both sides."""
+    if rank != 0:
+        return
+    import torch
+    torch.cuda.set_device(0)
+    load_package()
+    from pssfss_b200 import workloads
+    from pssfss_b200.analyze import analyze
+    batch = workloads.ring_batch()
+    npts = sum(len(f) for _, f, _ in batch)
+
+    def one_pass():
+        for strata, flist, steer in batch:
+            analyze(strata, flist, steer, precision="fp32r")
+    for _ in range(args.warmup):
+        one_pass()
+    times = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        one_pass()
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t)
+    sec = statistics.mean(times)
+    line = {"metric": "freq-points/sec over a batch of ring problems of differing size", "value": npts / sec,
+            "unit": "freq-points/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64+c128-refine",
+            "data": "synthetic (seeded ring problems, structured meshes)",
+            "config": {"workload": f"64 ring problems, {npts} points, N {min(b[0][1].nface for b in batch)}.."
+                                   f"{max(b[0][1].nface for b in batch)} faces, host time included"}}
+    print(json.dumps(line), flush=True)
+
+
 def run_grads(args, rank):
     """Gradients/s of Σ_f (|S21_TE|² − |S21_TM|²) in trace width, pitch and substrate eps_r of
     the meanderline at ntri = 4000 (N ≈ 6000) over 201 frequencies 8-18 GHz: one FP32 +
@@ -256,6 +293,8 @@ def main():
                     help="time gradients of the meander gradient workload instead (grads/s)")
     ap.add_argument("--grad-npts", type=int, default=0,
                     help="frequencies of the gradient workload (default: all 201)")
+    ap.add_argument("--rings", action="store_true",
+                    help="time the seeded batch of 64 ring problems of differing size instead")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -264,6 +303,8 @@ def main():
         return run_reference(args, rank, world)
     if args.grads:
         return run_grads(args, rank)
+    if args.rings:
+        return run_rings(args, rank)
 
     import torch
     dist = None
