@@ -83,14 +83,16 @@ def meander_gradient(params, flist, *, ntri=4000, rel_step=1e-4, analyze_fn=None
 
 
 def linearized_gradient(build, params, flist, steering, objective, partial_lin=None, *, rel_step=1e-4,
-                        topology=None):
+                        topology=None, plan_flist=None):
     """Objective and central-difference gradient with one factorisation per point.
 
     ``partial_lin(sheet, rwg, points, (i1, i2), s, u, ios, perturbed)`` returns the scattered
     partial GSMs of one sheet Gblock at ``points`` and, for each entry (sheet_k, rwg_k,
     points_k, u_k, ios_k) of ``perturbed``, their first-order values at that perturbation
     from the unperturbed factorisation.  Every perturbed plan must keep the points, Gblocks,
-    modes and mesh topology of the unperturbed one.  Returns ``(f(params), {name: df/dp})``.
+    modes and mesh topology of the unperturbed one.  ``plan_flist``: the band that chooses
+    modes and Gblocks when ``flist`` is one shard of a sweep.  Returns ``(f(params), {name:
+    df/dp})``.
     """
     if partial_lin is None:
         from .engine import partial_gsms_linearized as partial_lin
@@ -105,8 +107,8 @@ def linearized_gradient(build, params, flist, steering, objective, partial_lin=N
                 raise ValueError(f"step changes the mesh topology: {topology(p)} != {key0} at {p}")
             steps.append((name, h, p))
     cache = {}  # steps of layer parameters keep the sheet's geometry: one RWG setup serves them
-    plan0 = make_plan(build(p0), flist, steering, rwg_cache=cache)
-    plans = [make_plan(build(p), flist, steering, rwg_cache=cache) for _, _, p in steps]
+    plan0 = make_plan(build(p0), flist, steering, plan_flist, rwg_cache=cache)
+    plans = [make_plan(build(p), flist, steering, plan_flist, rwg_cache=cache) for _, _, p in steps]
     blocks = sheet_gblocks(plan0)
     for pl in plans:
         if (sheet_gblocks(pl) != blocks or len(pl.points) != len(plan0.points)
@@ -142,3 +144,33 @@ def meander_linearized_gradient(params, flist, partial_lin=None, *, ntri=4000, r
     return linearized_gradient(lambda p: meander_strata(p, ntri=ntri), params, np.asarray(flist, float),
                                {"θ": 0.0, "ϕ": 0.0}, te_tm_transmission_objective, partial_lin,
                                rel_step=rel_step, topology=lambda p: meander_topology(p, ntri=ntri))
+
+
+def linearized_gradient_sharded(build, params, flist, steering, objective, partial_lin=None, *, group=None,
+                                **kw):
+    """``linearized_gradient`` over the ranks of the default (or given) process group for an
+    objective that is a sum over frequency points: rank k takes a contiguous block of
+    ``flist`` (planned with the whole band), and one all-reduce of the 1 + P partial sums
+    gives every rank the objective and gradient.  Without a process group it is plain
+    ``linearized_gradient``."""
+    import torch
+    import torch.distributed as dist
+
+    from .sweep import shard_range
+    flist = [float(f) for f in np.atleast_1d(np.asarray(flist, float))]
+    if not (dist.is_available() and dist.is_initialized()):
+        return linearized_gradient(build, params, flist, steering, objective, partial_lin, **kw)
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    lo, hi = shard_range(len(flist), rank, world)
+    names = list(params)
+    if hi > lo:
+        f0, g = linearized_gradient(build, params, flist[lo:hi], steering, objective, partial_lin,
+                                    plan_flist=flist, **kw)
+        part = [f0] + [g[k] for k in names]
+    else:
+        part = [0.0] * (1 + len(names))
+    dev = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+    t = torch.tensor(part, dtype=torch.float64, device=dev)
+    dist.all_reduce(t, group=group)
+    tot = t.cpu().tolist()
+    return tot[0], dict(zip(names, tot[1:]))

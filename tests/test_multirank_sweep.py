@@ -100,3 +100,61 @@ def test_merge_tagged_orders_by_steering_then_frequency():
     merged = merge_tagged([part1, part0])
     assert [(combos.index(r.steering), r.FGHz) for r in merged] == [(0, 1.0), (0, 2.0), (0, 3.0), (1, 1.0),
                                                                     (1, 3.0), (1, 4.0)]
+
+
+def _grad_worker(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), LOCAL_RANK=str(rank))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        import functools
+        import oracle
+        from pssfss_b200.gradient import (linearized_gradient_sharded, meander_strata, meander_topology,
+                                          te_tm_transmission_objective)
+        part = functools.partial(oracle.partial_gsms_linearized, tangent=True)
+        f, g = linearized_gradient_sharded(lambda p: meander_strata(p, ntri=120), GRAD_P0, GRAD_FREQS,
+                                           {"θ": 0.0, "ϕ": 0.0}, te_tm_transmission_objective, part,
+                                           topology=lambda p: meander_topology(p, ntri=120))
+        q.put((rank, (f, g)))
+    finally:
+        dist.destroy_process_group()
+
+
+GRAD_P0 = {"w": 0.3, "a": 5.0, "epsr": 2.2}
+GRAD_FREQS = [9.0, 12.0, 15.0]
+
+
+def test_linearized_gradient_sharded_gloo_matches_single_process():
+    # the gradient objective is a sum over frequencies: ranks take blocks of the sweep and one
+    # all-reduce of the partial sums gives the single-process objective and gradient
+    import functools
+    import oracle
+    from pssfss_b200.gradient import meander_linearized_gradient
+    part = functools.partial(oracle.partial_gsms_linearized, tangent=True)
+    f1, g1 = meander_linearized_gradient(GRAD_P0, GRAD_FREQS, part, ntri=120)
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_grad_worker, args=(k, world, port, q)) for k in range(world)]
+    for p in procs:
+        p.start()
+    got = {}
+    try:
+        for _ in range(480):
+            while not q.empty() and len(got) < world:
+                k, v = q.get()
+                got[k] = v
+            if len(got) == world or any(p.exitcode not in (None, 0) for p in procs):
+                break
+            procs[0].join(timeout=0.5)
+    finally:
+        for p in procs:
+            p.join(timeout=60)
+            if p.is_alive():
+                p.kill()
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    for k in range(world):
+        f, g = got[k]
+        assert abs(f - f1) <= 1e-12 * abs(f1)
+        for name in GRAD_P0:
+            assert abs(g[name] - g1[name]) <= 1e-9 * abs(g1[name]), (name, g[name], g1[name])
