@@ -10,7 +10,7 @@ import oracle
 from pssfss_b200.elements import diagstrip, rectstrip
 from pssfss_b200.layers import Layer
 from pssfss_b200.outputs import (H, L, R, TE, TM, V, extract_result, getsijmn, obsmat, outputs,
-                                 sourcemat)
+                                 sourcemat, theta_phi)
 from pssfss_b200.units import Length, mm
 
 NORMAL = {"θ": 0.0, "ϕ": 0.0}
@@ -111,3 +111,23 @@ def test_analysis_log_report(tmp_path):
     quiet.start()
     quiet.report(plan)
     quiet.finish()
+
+
+def test_psi_steering_equals_angle_steering():
+    # steering by the incremental phase shifts (ψ₁, ψ₂) - the branch of getsttuple that the
+    # reference leaves broken (PSSFSS.jl:612) - reproduces angle steering with the same β00
+    sh = rectstrip(Lx=6, Ly=0.5, Px=8, Py=8, Nx=8, Ny=2, units=mm)
+    strata = [Layer(), sh, Layer()]
+    f, th, ph = 12.0, 25.0, 30.0
+    k = 2 * math.pi * f * 1e9 / 299792458.0
+    b00 = k * math.sin(math.radians(th)) * np.array([math.cos(math.radians(ph)), math.sin(math.radians(ph))])
+    p = 8e-3  # cell period in metres
+    psi = {"ψ₁": math.degrees(b00[0] * p), "ψ₂": math.degrees(b00[1] * p)}
+    ra = oracle.analyze(strata, [f], {"θ": th, "ϕ": ph})[0]
+    rp = oracle.analyze(strata, [f], psi)[0]
+    assert np.allclose(rp.beta00, ra.beta00, rtol=1e-12)
+    for key in ((1, 1), (1, 2), (2, 1), (2, 2)):
+        assert np.abs(rp.gsm[key] - ra.gsm[key]).max() < 1e-9
+    assert rp.steering == psi and math.isnan(extract_result(rp, outputs("theta"))[0, 0])
+    th_rp, ph_rp = theta_phi(rp)   # the angles recovered from β00
+    assert math.isclose(th_rp, th, rel_tol=1e-9) and math.isclose(ph_rp, ph, rel_tol=1e-9)
