@@ -463,3 +463,40 @@ def test_unique_face_pair_paths_agree():
         b = rwg._unique_face_pairs_sorted(sh.nface, sid, dx, dy)
         assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and a[2] == b[2]
         assert a[0][tuple(np.unravel_index(a[1] - 1, a[0].shape, order="F"))].tolist() == list(range(1, a[2] + 1))
+
+
+def test_meshers_on_seeded_random_shapes():
+    # the structured meshers over seeded random valid parameters: counter-clockwise,
+    # non-degenerate triangles (checked when the sheet is built), exact areas, periodic
+    # edges that pair up (setup_rwg)
+    from pssfss_b200.elements import jerusalemcross, loadedcross, polyring
+
+    def area(sh):
+        r, f = sh.rho, sh.fv - 1
+        return sum(abs((r[b][0] - r[a][0]) * (r[c][1] - r[a][1]) - (r[c][0] - r[a][0]) * (r[b][1] - r[a][1])) / 2
+                   for a, b, c in f.T)
+
+    rng = np.random.default_rng(7)
+    for _ in range(20):
+        p1, p2, skew = rng.uniform(5, 15), rng.uniform(5, 15), rng.uniform(-0.5, 0.5)
+        s1, s2 = [p1, 0.0], [skew * p2, p2 * rng.uniform(0.7, 1.0)]
+        cell = abs(s1[0] * s2[1] - s1[1] * s2[0])
+        inr = 0.5 * min(cell / np.linalg.norm(s1), cell / np.linalg.norm(s2))
+        sides, a = int(rng.integers(3, 40)), rng.uniform(0.1, 0.8) * inr
+        sh = polyring(s1=s1, s2=s2, a=[a], b=[-int(rng.integers(2, 20))], sides=sides, orient=float(rng.uniform(0, 90)),
+                      ntri=int(rng.integers(100, 1000)), units=mm)
+        af = 0.5 * sides * math.sin(2 * math.pi / sides)
+        assert math.isclose(area(sh), cell - af * a * a, rel_tol=1e-9)
+        setup_rwg(sh)
+        P = rng.uniform(6, 12)
+        L1 = rng.uniform(0.4, 0.9) * P
+        L2 = rng.uniform(0.1, 0.5) * L1
+        w = rng.uniform(0.02, 0.6) * L2
+        lc = loadedcross(s1=[P, 0], s2=[0, P], L1=L1, L2=L2, w=w, ntri=int(rng.integers(100, 600)), units=mm,
+                         orient=float(rng.uniform(0, 90)))
+        a2 = L2 - 2 * w
+        assert math.isclose(area(lc), 2 * L1 * L2 - L2 * L2 - ((2 * (L1 - 2 * w) * a2 - a2 * a2) if a2 > 0 else 0),
+                            rel_tol=1e-9)
+        A, B = rng.uniform(1.05, 1.6) * L2, rng.uniform(0.1, 0.8) * (L1 - L2) / 2
+        if A < P:
+            setup_rwg(jerusalemcross(P=P, L1=L1, L2=L2, A=A, B=B, w=w, ntri=int(rng.integers(100, 600)), units=mm))
