@@ -20,7 +20,7 @@
  *                          batched over all frequency / steering points of a sweep.
  *   pss_fill_matrix    <- fillz / filly alone (src/FillZY.jl:50-245, 273-457).
  *   pss_modal_tables   <- electric_/magnetic_modal_sum_funcs tables (src/PGF.jl:196, 478).
- *   pss_face_integrals <- filljk! (src/Zint.jl:117-242).
+ *   pss_face_integrals <- filljk! (src/Zint.jl:54-179).
  *   pss_lu_solve       <- lu! followed by ldiv! on a caller matrix (LinearAlgebra).
  */
 #ifndef PSSFSS_B200_H
@@ -108,6 +108,24 @@ int pss_partial_gsms_lin(pss_sheet *sheet, int nl, const double *eps, const doub
                          const double *psrc, const double *ptobs, const double *pwobs, int precision,
                          double *dS, double *dSp, int *status);
 
+/* Adjoint form of pss_partial_gsms_lin (no counterpart in the reference, which has no
+ * gradients): the same arguments and output layout, with
+ *     dSp[k][i] = wobs_k o (P_k X + Lam^T (R_k - Z_k X)),   X = Z^-1 R,   Lam = Z^-T P^T,
+ * the first-order value of the perturbed partial GSM (central differences of dSp over
+ * +/- steps give dS/dp to O(h^2)).  Per point: one factorisation, the forward solves of R
+ * and the adjoint (transposed) solves of P^T on the same factors; each perturbed set then
+ * recomputes its pair terms (the Green's-function values of its sheet and layers) and
+ * contracts Lam^T Z_k X while assembling Z_k entry by entry - no perturbed matrix is stored
+ * and no further solve is taken.  Points run one at a time on the context's first stream;
+ * calls on one context must not overlap.  nmodes <= 1024. */
+int pss_partial_gsms_adj(pss_sheet *sheet, int nl, const double *eps, const double *mu, const double *width,
+                         int s, double u, int npts, const double *k0, const double *psi, int nmodes,
+                         const double *kvec, const double *src, const double *tobs, const double *wobs,
+                         int npert, pss_sheet *const *psheets, const double *peps, const double *pmu,
+                         const double *pwidth, const double *pu, const double *ppsi, const double *pkvec,
+                         const double *psrc, const double *ptobs, const double *pwobs, int precision,
+                         double *dS, double *dSp, int *status);
+
 /* The MoM matrix of one point: Z (nbf x nbf complex, column-major like zorymat). */
 int pss_fill_matrix(pss_sheet *sheet, int nl, const double *eps, const double *mu, const double *width, int s,
                     double u, double k0, double psi1, double psi2, double *Z, int *mmax_out);
@@ -154,17 +172,16 @@ int pss_profile_result(pss_ctx *ctx, double *out);
  * products: FP32-level accuracy), the kernel the PSS_FP32_REFINE factorisation uses for its
  * trailing updates.  Host arrays, row-major, real and imaginary parts separate: L m x k,
  * U k x n, C m x n (updated in place).  status: 0, or PSS_STATUS_DEVICE_TIMEOUT.
- * No counterpart in the reference, whose LU is LAPACK zgetrf behind `Z \ rhs`
- * (src/PSSFSS.jl:473); exposed so the kernel can be checked on its own. */
+ * No counterpart in the reference, whose LU is LAPACK zgetrf behind lu! (src/PSSFSS.jl:401,
+ * 526); exposed so the kernel can be checked on its own. */
 int pss_schur_update(pss_ctx *ctx, int m, int n, int k, const float *Lr, const float *Li, const float *Ur,
                      const float *Ui, float *Cr, float *Ci, int *status);
 
 /* FP64 complex LU factorisation, in place, on caller-owned device memory, allocating no
- * device memory at all (no cudaMalloc, cudaFree or allocating library routine).  No
- * counterpart in the reference (its factorisation is LAPACK zgetrf behind `Z \ rhs`,
- * src/PSSFSS.jl:473); it serves callers that cannot let a library allocate per call - a
- * host whose device memory is held by its own pool (Julia CUDA.jl, PyTorch), or a
- * latency-sensitive loop in which cudaFree's device-wide synchronisation would stall
+ * device memory at all (no cudaMalloc, cudaFree or allocating library routine).  It has
+ * no counterpart in the reference.  It serves callers that cannot let a library allocate
+ * per call - a host whose device memory is held by its own pool (Julia CUDA.jl, PyTorch),
+ * or a latency-sensitive loop in which cudaFree's device-wide synchronisation would stall
  * every other stream.
  *   A     device, n x n interleaved complex128, ROW-major, leading dimension ld >= n
  *         (elements), 16-byte aligned; overwritten by U (upper) and the unit-lower L.
@@ -179,7 +196,8 @@ int pss_schur_update(pss_ctx *ctx, int m, int n, int k, const float *Lr, const f
  * nothing in it has to start at zero, but calls that overlap in time on the same device
  * race on it - serialise them.  The first call on each device resolves that array's
  * address (cudaGetSymbolAddress); make that first call before any stream capture on the
- * device. */
+ * device.  The address is cached with the CUDA context it belongs to and looked up again
+ * when another context is current (after cudaDeviceReset, for instance). */
 int pss_lu_factor_noalloc(int n, double *A, int64_t ld, int *ipiv, int *info, void *stream);
 
 #ifdef __cplusplus

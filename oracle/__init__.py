@@ -162,7 +162,7 @@ def modal_tables(magnetic, k0, u, psi1, psi2, layers, s, b1, b2, b00, convtest=5
 
 
 class JKCache:
-    """Frequency-independent face-pair integrals of ``filljk!`` (Zint.jl:117)."""
+    """Frequency-independent face-pair integrals of ``filljk!`` (Zint.jl:54)."""
     __slots__ = ("J", "Jxi", "Jeta", "K", "Kxi", "Keta", "rho_r", "rinv", "psi1", "psi2", "u",
                  "nonconv")
 
@@ -266,26 +266,76 @@ def partial_dS(sheet, rwg, region, s, k0, u, io):
 
 
 def analyze(strata, flist, steering):
-    """Oracle ``analyze`` (PSSFSS.jl:114-334): the package's host plan and cascade with the
-    hot path (fill, LU/solve, transforms, projection) done by this restatement."""
+    """Oracle ``analyze`` (PSSFSS.jl:114-334), independent of the package's host numerics.
+
+    Only the *selection* steps come from the package's planner: the Gblocks, the layer mode
+    lists and the duplicate-Gblock map (``choose_gblocks``, ``choose_layer_modes!``,
+    ``get_gbldup``, pinned to the reference's golden values of test/GSMs_test.jl and
+    test/Modes_test.jl) and the basis-function topology (``setup_rwg``, pinned by
+    test/RWGData_test.jl).  Everything numeric is the oracle's own: modal constants,
+    incident GSMs and transmission-line Green's functions, source and projection factors
+    (``host.py``), the fill and basis transforms (``pssfss_oracle.c``), LAPACK's LU, the
+    cascade.  Returns the package's ``Result`` containers so outputs can be taken from them."""
     import importlib
+    from . import host
     A = importlib.import_module("pssfss_b200.analyze")
-    plan = A.make_plan(strata, flist, steering)
-    partial = {}
-    for ig, (i1, i2), isht, s in A.sheet_gblocks(plan):
-        sheet = plan.sheets[isht - 1]
-        out = []
-        for pt in plan.points:
-            region = pt.layers[i1 - 1:i2]
-            io = A.sheet_io(region, sheet, s, pt.k0, pt.beta00)
-            dS, _, _ = partial_dS(sheet, plan.rwgdat[isht - 1], region, s, pt.k0,
-                                  plan.uvec[isht - 1], io)
-            out.append(A.add_scattered(io, dS))
-        partial[ig] = out
-    return A.assemble(plan, partial)
+    O = importlib.import_module("pssfss_b200.outputs")
+    Gm = importlib.import_module("pssfss_b200.gsms")
+    plan = A.make_plan(strata, flist, steering)  # selection only: its points are not used
+    freqs = [float(f) for f in np.atleast_1d(np.asarray(flist, float))]
+    base = [host.ModalLayer(l.epsr, l.mur, l.width, list(l.P), list(l.M), list(l.N),
+                            np.array(l.beta1, float), np.array(l.beta2, float)) for l in plan.layers]
+    sh0 = plan.sheets[0]
+    upm0 = sh0.units.units_per_meter
+    points = host.steering_points(base, freqs, steering, (sh0.beta1 * upm0, sh0.beta2 * upm0))
+    uvec = [0.0 if sh.style == "NULL" else
+            0.5 * sh.units.units_per_meter * max(np.linalg.norm(sh.beta1), np.linalg.norm(sh.beta2))
+            for sh in plan.sheets]
+    saved = {}
+
+    def sheet_gsm(ig, p, region, s, k0):
+        g = plan.gbls[ig]
+        sheet = plan.sheets[plan.junc[g.j - 1] - 1]
+        if plan.gbldup[ig] > 0:
+            gb = {k: v.copy() for k, v in saved[(plan.gbldup[ig] - 1, p)].items()}
+        else:
+            if sheet.cls == "E":
+                gb = host.pec(region[0].nmodes, region[-1].nmodes)
+            elif sheet.cls == "H":
+                gb = host.pmc(region[0].nmodes, region[-1].nmodes)
+            elif sheet.style == "NULL":
+                gb = (host.electric_gblock if sheet.cls == "J" else host.magnetic_gblock)(region, s, k0)[0]
+            else:
+                upm = sheet.units.units_per_meter
+                rwg = plan.rwgdat[plan.junc[g.j - 1] - 1]
+                b00 = points[p][3]
+                psi1 = float(b00 @ np.asarray(sheet.s1, float)) / upm
+                psi2 = float(b00 @ np.asarray(sheet.s2, float)) / upm
+                Z, _ = fill(k0, uvec[plan.junc[g.j - 1] - 1], region, s, psi1, psi2, sheet, rwg)
+                import scipy.linalg as sl
+                lu = sl.lu_factor(Z, check_finite=False)
+                ends = (region[0], region[-1])
+                area = abs(sheet.s1[0] * sheet.s2[1] - sheet.s1[1] * sheet.s2[0]) / upm ** 2
+                gb = host.sheet_partial_gsm(
+                    sheet.cls, region, s, k0, area, lambda b: sl.lu_solve(lu, b, check_finite=False),
+                    lambda r, q: rwgbfft(rwg, sheet, ends[r].beta[q], psi1, psi2))
+            if plan.gbldup[ig] < 0:
+                saved[(ig, p)] = {k: v.copy() for k, v in gb.items()}
+        if sheet.dx != 0 or sheet.dy != 0:
+            upm = sheet.units.units_per_meter
+            host.translate(gb, sheet.dx / upm, sheet.dy / upm, region[0], region[-1])
+        return gb
+
+    gbls = [(g.first, g.last, g.j) for g in plan.gbls]
+    out = []
+    for steer, f, b00, g, L in host.cascade_points(points, gbls, plan.junc, sheet_gsm):
+        gsm = Gm.GSM(g["s11"], g["s12"], g["s21"], g["s22"])
+        out.append(O.Result(gsm, steer, np.array(b00, float), f, L[0].epsr, L[0].mur, L[0].beta1.copy(),
+                            L[0].beta2.copy(), L[-1].epsr, L[-1].mur, L[-1].beta1.copy(), L[-1].beta2.copy()))
+    return out
 
 
-def partial_dS_linearized(sheet, rwg, region, s, k0, u, io, perturbed, tangent=False):
+def partial_dS_linearized(sheet, rwg, region, s, k0, u, io, perturbed, tangent=False, form=None):
     """Scattered partial GSM at a point and, for each perturbed input set, its first-order
     (in the perturbation) value from the unperturbed factorisation:
 
@@ -293,7 +343,8 @@ def partial_dS_linearized(sheet, rwg, region, s, k0, u, io, perturbed, tangent=F
 
     exact to O(h^2), so central differences of dS_k give dS/dp to O(h^2) with one
     factorisation.  ``tangent``: the same through forward solves only, Lambda^T (Z_k - Z) X
-    = P Z^-1 (Z_k X - R) (the form a device implementation takes).  ``perturbed``: list of (sheet_k, rwg_k, region_k, u_k, io_k) with the
+    = P Z^-1 (Z_k X - R).  ``form="adjoint"``: the fully linearised form
+    dS_k = wobs_k * (P_k X + Lambda^T (R_k - Z_k X)), which needs no solve per set.  ``perturbed``: list of (sheet_k, rwg_k, region_k, u_k, io_k) with the
     topology of ``sheet``.  The same projection as ``partial_dS`` (PSSFSS.jl:391-457)."""
     import scipy.linalg as sl
     Z, _ = fill(k0, u, region, s, io.psi1, io.psi2, sheet, rwg)
@@ -315,7 +366,9 @@ def partial_dS_linearized(sheet, rwg, region, s, k0, u, io, perturbed, tangent=F
         Zk, _ = fill(k0, u_k, region_k, s, io_k.psi1, io_k.psi2, sh_k, rw_k)
         Rk, Pk = rp(sh_k, rw_k, io_k)
         Xk = sl.lu_solve(lu, Rk, check_finite=False)
-        if tangent:  # no transposed solve: Lambda^T (Z_k - Z) X = P Z^-1 (Z_k X - R)
+        if form == "adjoint":
+            out.append(io_k.wobs[:, None] * (Pk @ X + Lam.T @ (Rk - Zk @ X)))
+        elif tangent:  # no transposed solve: Lambda^T (Z_k - Z) X = P Z^-1 (Z_k X - R)
             Wk = sl.lu_solve(lu, R - Zk @ X, check_finite=False)
             out.append(io_k.wobs[:, None] * (Pk @ Xk + P @ Wk))
         else:
@@ -323,7 +376,7 @@ def partial_dS_linearized(sheet, rwg, region, s, k0, u, io, perturbed, tangent=F
     return dS, out
 
 
-def partial_gsms_linearized(sheet, rwg, points, region_rng, s, u, ios, perturbed, tangent=False):
+def partial_gsms_linearized(sheet, rwg, points, region_rng, s, u, ios, perturbed, tangent=False, form=None):
     """``partial_dS_linearized`` over the points of one sheet Gblock.  ``perturbed``: list
     of (sheet_k, rwg_k, points_k, u_k, ios_k).  Returns (dS per point, [dS_k per point])."""
     i1, i2 = region_rng
@@ -331,7 +384,7 @@ def partial_gsms_linearized(sheet, rwg, points, region_rng, s, u, ios, perturbed
     for p, pt in enumerate(points):
         pk = [(sh_k, rw_k, pts_k[p].layers[i1 - 1:i2], u_k, ios_k[p])
               for sh_k, rw_k, pts_k, u_k, ios_k in perturbed]
-        d, ds_k = partial_dS_linearized(sheet, rwg, pt.layers[i1 - 1:i2], s, pt.k0, u, ios[p], pk, tangent)
+        d, ds_k = partial_dS_linearized(sheet, rwg, pt.layers[i1 - 1:i2], s, pt.k0, u, ios[p], pk, tangent, form)
         dS.append(d)
         for k, v in enumerate(ds_k):
             lin[k].append(v)

@@ -424,7 +424,7 @@ cplx ora_sigma(const cplx *T, int mmax, const double b1[2], const double b2[2], 
     return s;
 }
 
-/* 7-point triangle rule (Zint.jl:118-125, 282-289) */
+/* 7-point triangle rule (Zint.jl:55-62, 219-225) */
 static const double QXI[7] = {0.33333333333333330, 0.10128650732345633, 0.79742698535308730,
                               0.10128650732345633, 0.47014206410511505, 0.05971587178976989,
                               0.47014206410511505};
@@ -442,7 +442,7 @@ static inline void vtx(const double *rho, const int64_t *fv, int64_t f, int k, d
     out[1] = rho[2 * v + 1];
 }
 
-/* Zint.jl:117-242 -- frequency-independent face-pair integrals for each unique pair.
+/* Zint.jl:54-179 (filljk!) -- frequency-independent face-pair integrals for each unique pair.
  * rho: 2 x nnode (sheet units), ufp_rep: 1-based column-major face-pair index of each
  * class's first member.  Outputs per class: J, Jxi, Jeta, K, Kxi, Keta, rho_r[2], rinv. */
 void ora_filljk(int64_t nface, const double *rho, const int64_t *fv, int64_t nufp,
@@ -576,7 +576,7 @@ void ora_fill(int magnetic, double k0, double u, int nl, const cplx *eps, const 
             rm[k][0] /= units_per_meter; rm[k][1] /= units_per_meter;
         }
         double rmc[2] = {((rm[0][0] + rm[1][0]) + rm[2][0]) / 3, ((rm[0][1] + rm[1][1]) + rm[2][1]) / 3};
-        /* zint (Zint.jl:281-308) */
+        /* zint (Zint.jl:218-245) */
         cplx I1 = 0, I1x = 0, I1e = 0, I2 = 0;
         for (int i = 0; i < 7; ++i) {
             double rt[2] = {(rs[0][0] + (rs[1][0] - rs[0][0]) * QXI[i]) + (rs[2][0] - rs[0][0]) * QETA[i],

@@ -1253,3 +1253,179 @@ extern "C" int pss_partial_gsms_lin(pss_sheet *sh, int nl, const double *eps, co
   }
   return 0;
 }
+
+// Adjoint form of the linearised partial GSMs (same inputs and outputs as
+// pss_partial_gsms_lin):  dSp[k] = wobs_k o (P_k X + Lam^T (R_k - Z_k X)),  X = Z^-1 R,
+// Lam = Z^-T P^T.  Per point: one fill of Z, one factorisation, nm forward and nm adjoint
+// solves on the same factors; each perturbed set then costs its pair terms (Green's-function
+// table interpolations recomputed for the set), its basis transforms and one fused
+// assemble-and-contract pass (pss_adj_contract) - no perturbed matrix is stored and no
+// further solve is taken.
+extern "C" int pss_partial_gsms_adj(pss_sheet *sh, int nl, const double *eps, const double *mu, const double *width,
+                                    int s, double u, int npts, const double *k0, const double *psi, int nmodes,
+                                    const double *kvec, const double *src, const double *tobs, const double *wobs,
+                                    int npert, pss_sheet *const *psh, const double *peps, const double *pmu,
+                                    const double *pwidth, const double *pu, const double *ppsi, const double *pkvec,
+                                    const double *psrc, const double *ptobs, const double *pwobs, int precision,
+                                    double *dS, double *dSp, int *status) {
+  if (!sh || !k0 || !psi || !dS || !status || !kvec || !src || !tobs || !wobs) {
+    pss_set_error("null argument");
+    return -1;
+  }
+  if (npts <= 0 || nmodes <= 0 || nmodes > 1024 || npert < 0 || npert > 64) {
+    pss_set_error("invalid npts/nmodes/npert");
+    return -1;
+  }
+  if (npert > 0 && (!psh || !peps || !pmu || !pwidth || !pu || !ppsi || !pkvec || !psrc || !ptobs || !pwobs || !dSp)) {
+    pss_set_error("null perturbation argument");
+    return -1;
+  }
+  if (precision != PSS_FP64 && precision != PSS_FP32_REFINE) { pss_set_error("unknown precision %d", precision); return -1; }
+  for (int k = 0; k < npert; ++k)
+    if (!psh[k] || psh[k]->ctx != sh->ctx || psh[k]->nbf != sh->nbf || psh[k]->cls != sh->cls) {
+      pss_set_error("perturbed sheet %d is not a sheet of the same context, class and basis count", k);
+      return -1;
+    }
+  if (!(u > 0)) { pss_set_error("smoothing parameter u must be positive"); return -1; }
+  pss_ctx *c = sh->ctx;
+  if (set_device(c)) return -3;
+  const int magnetic = sh->cls == 'M';
+  const int n = sh->nbf, nm = nmodes, K = npert;
+  const long long ld = n, msz = (long long)n * n, vsz = (long long)n * nm;
+  StackParams S;
+  if (make_stack(nl, eps, mu, width, s, S)) return -1;
+  std::vector<StackParams> Sk(K);
+  for (int k = 0; k < K; ++k) {
+    if (make_stack(nl, peps + 2 * (size_t)k * nl, pmu + 2 * (size_t)k * nl, pwidth + (size_t)k * nl, s, Sk[k]))
+      return -1;
+    if (!(pu[k] > 0)) { pss_set_error("perturbed smoothing parameter %d must be positive", k); return -1; }
+  }
+  Worker &w = c->w[0];
+  cudaStream_t st = w.st;
+  int rc = ensure_worker(w, sh, nm, precision, false, 1);
+  if (rc) return rc;
+  int maxufp = sh->nufp;
+  for (int k = 0; k < K; ++k) maxufp = std::max(maxufp, psh[k]->nufp);
+  if (w.zb.ensure((size_t)maxufp * 9 * sizeof(cd))) return -3;
+  DevBuf pbuf, tb0, mbuf, vbuf, rtw, part, gout, out;
+  std::vector<DevBuf> tbk(K);
+  const size_t nvec = (size_t)vsz;  // one n x nm block
+  // vectors: PT, Lam, W (adjoint scratch), Rk, bfk (nm x n x 2)
+  if (pbuf.ensure((size_t)(1 + K) * sizeof(PointParams)) ||
+      mbuf.ensure((size_t)(1 + K) * nm * (2 * sizeof(double) + 2 * sizeof(cd) + 2 * sizeof(double) + sizeof(cd))) ||
+      vbuf.ensure((4 * nvec + 2 * nvec) * sizeof(cd)) ||
+      rtw.ensure(precision == PSS_FP32_REFINE ? pss_refine_trans_ws_bytes(n, nm, 1) : 0) ||
+      part.ensure(pss_adj_part_bytes(n, nm)) || gout.ensure((size_t)std::max(K, 1) * nm * nm * sizeof(cd)) ||
+      out.ensure((size_t)(1 + K) * nm * nm * sizeof(cd)))
+    return -3;
+  cd *PT = vbuf.as<cd>(), *Lam = PT + nvec, *Wt = Lam + nvec, *Rk = Wt + nvec, *bfk = Rk + nvec;
+  const size_t nmk = (size_t)nm * 2;
+  char *mb = mbuf.as<char>();
+  auto kv_of = [&](int q) { return (double *)mb + (size_t)q * nmk; };
+  auto src_of = [&](int q) { return (cd *)(mb + (size_t)(1 + K) * nmk * sizeof(double)) + (size_t)q * nmk; };
+  auto tob_of = [&](int q) {
+    return (double *)(mb + (size_t)(1 + K) * nmk * (sizeof(double) + sizeof(cd))) + (size_t)q * nmk;
+  };
+  auto wob_of = [&](int q) {
+    return (cd *)(mb + (size_t)(1 + K) * nmk * (2 * sizeof(double) + sizeof(cd))) + (size_t)q * nm;
+  };
+  const size_t nm2 = (size_t)nm * nm;
+  std::vector<cd> hout((1 + K) * nm2), hG(std::max(K, 1) * nm2), hw((1 + K) * (size_t)nm);
+  float *zr = precision == PSS_FP32_REFINE ? w.zr.as<float>() : nullptr;
+  float *zi = precision == PSS_FP32_REFINE ? w.zi.as<float>() : nullptr;
+  const cd *L64 = precision == PSS_FP64 ? w.z64.as<cd>() : nullptr;
+  for (int i = 0; i < npts; ++i) {
+    if (!(k0[i] > 0) || !std::isfinite(psi[2 * i]) || !std::isfinite(psi[2 * i + 1])) {
+      pss_set_error("invalid k0/psi at point %d", i);
+      return -1;
+    }
+    int hst = 0;
+    std::vector<PointParams> hP(1 + K);
+    {
+      const double b1m[2] = {sh->b1[0] * sh->upm, sh->b1[1] * sh->upm};
+      const double b2m[2] = {sh->b2[0] * sh->upm, sh->b2[1] * sh->upm};
+      make_params(magnetic, S, b1m, b2m, u, k0[i], psi[2 * i], psi[2 * i + 1], hP[0]);
+    }
+    for (int k = 0; k < K; ++k) {
+      const pss_sheet *q = psh[k];
+      const double b1m[2] = {q->b1[0] * q->upm, q->b1[1] * q->upm};
+      const double b2m[2] = {q->b2[0] * q->upm, q->b2[1] * q->upm};
+      const double *pp = ppsi + 2 * ((size_t)k * npts + i);
+      make_params(magnetic, Sk[k], b1m, b2m, pu[k], k0[i], pp[0], pp[1], hP[1 + k]);
+    }
+    PSS_CUDA_TRY(cudaMemcpyAsync(pbuf.p, hP.data(), hP.size() * sizeof(PointParams), cudaMemcpyHostToDevice, st));
+    const PointParams *dP = pbuf.as<PointParams>();
+    for (int q = 0; q <= K; ++q) {
+      const size_t off = q == 0 ? (size_t)i * nm : ((size_t)(q - 1) * npts + i) * nm;
+      const double *kv = q == 0 ? kvec : pkvec;
+      const double *sv = q == 0 ? src : psrc;
+      const double *tv = q == 0 ? tobs : ptobs;
+      const double *wv = q == 0 ? wobs : pwobs;
+      PSS_CUDA_TRY(cudaMemcpyAsync(kv_of(q), kv + 2 * off, nm * 2 * sizeof(double), cudaMemcpyHostToDevice, st));
+      PSS_CUDA_TRY(cudaMemcpyAsync(src_of(q), sv + 4 * off, nm * 2 * sizeof(cd), cudaMemcpyHostToDevice, st));
+      PSS_CUDA_TRY(cudaMemcpyAsync(tob_of(q), tv + 2 * off, nm * 2 * sizeof(double), cudaMemcpyHostToDevice, st));
+      PSS_CUDA_TRY(cudaMemcpyAsync(wob_of(q), wv + 2 * off, nm * sizeof(cd), cudaMemcpyHostToDevice, st));
+      for (int a = 0; a < nm; ++a) hw[(size_t)q * nm + a] = mkcd(wv[2 * (off + a)], wv[2 * (off + a) + 1]);
+    }
+    // the unperturbed point: tables, face integrals, Z (+ FP32 planes), transforms, R
+    TableDev t0;
+    std::vector<TableDev> tk(K);
+    if ((rc = point_tables(c, S, dP, tb0, t0, hst))) return rc;
+    for (int k = 0; k < K; ++k)
+      if ((rc = point_tables(c, Sk[k], dP + 1 + k, tbk[k], tk[k], hst))) return rc;
+    if ((rc = refresh_jk_cache(sh, psi[2 * i], psi[2 * i + 1], u / sh->upm, st))) return rc;
+    if (sh->jk_nonconv) hst |= PSS_ST_JK_NOCONV;
+    pss_fill_pairs(sh->G, dP, sh->cache.jk, t0.t1, t0.t2, t0.mmax, w.zb.as<cd>(), st);
+    pss_fill_assemble(sh->G, dP, w.zb.as<cd>(), w.z64.as<cd>(), zr, zi, ld, st);
+    cd *bf = w.bf.as<cd>();
+    pss_bfft(sh->G, nm, kv_of(0), psi[2 * i], psi[2 * i + 1], bf, st);
+    pss_rhs(n, nm, bf, src_of(0), w.rhs.as<cd>(), st);
+    pss_proj_rows(n, nm, bf, tob_of(0), PT, st);
+    // one factorisation; X = Z^-1 R (forward) and Lam = Z^-T P^T (adjoint), both refined
+    // against the FP64 Z in the FP32 form
+    PSS_CUDA_TRY(cudaMemsetAsync(w.bstat.p, 0, sizeof(int), st));
+    if ((rc = w.factor_solve(n, 1, precision, nm, kMaxRefine, w.bstat.as<int>()))) return rc;
+    if ((rc = pss_solve_lu_trans(w.sws, 1, L64, zr, zi, ld, msz, nm, PT, Lam, Wt, vsz, 0, st))) return rc;
+    if (precision == PSS_FP32_REFINE &&
+        (rc = pss_refine_trans(w.sws, 1, w.z64.as<cd>(), ld, msz, zr, zi, nm, PT, Lam, w.R.as<cd>(), w.D.as<cd>(),
+                               Wt, rtw.p, rtw.n, vsz, kMaxRefine, w.bstat.as<int>(), st)))
+      return rc;
+    pss_solve_status(w.sws, 1, w.bstat.as<int>(), st);
+    cd *X = w.X.as<cd>();
+    cd *o = out.as<cd>();
+    pss_project(n, nm, bf, tob_of(0), wob_of(0), X, o, st);
+    // every perturbed set: its pair terms, transforms and right-hand sides, P_k X, and the
+    // contraction Lam^T (R_k - Z_k X) assembled on the fly
+    for (int k = 0; k < K; ++k) {
+      pss_sheet *q = psh[k];
+      const double *pp = ppsi + 2 * ((size_t)k * npts + i);
+      if ((rc = refresh_jk_cache(q, pp[0], pp[1], pu[k] / q->upm, st))) return rc;
+      if (q->jk_nonconv) hst |= PSS_ST_JK_NOCONV;
+      pss_fill_pairs(q->G, dP + 1 + k, q->cache.jk, tk[k].t1, tk[k].t2, tk[k].mmax, w.zb.as<cd>(), st);
+      pss_bfft(q->G, nm, kv_of(1 + k), pp[0], pp[1], bfk, st);
+      pss_rhs(n, nm, bfk, src_of(1 + k), Rk, st);
+      pss_project(n, nm, bfk, tob_of(1 + k), wob_of(1 + k), X, o + (1 + k) * nm2, st);
+      pss_adj_contract(q->G, dP + 1 + k, w.zb.as<cd>(), X, Rk, Lam, nm, part.as<cd>(), gout.as<cd>() + k * nm2, st);
+    }
+    int bst = 0;
+    PSS_CUDA_TRY(cudaMemcpyAsync(hout.data(), o, hout.size() * sizeof(cd), cudaMemcpyDeviceToHost, st));
+    if (K > 0)
+      PSS_CUDA_TRY(cudaMemcpyAsync(hG.data(), gout.p, (size_t)K * nm2 * sizeof(cd), cudaMemcpyDeviceToHost, st));
+    PSS_CUDA_TRY(cudaMemcpyAsync(&bst, w.bstat.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    PSS_CUDA_TRY(cudaStreamSynchronize(st));
+    status[i] = hst | bst;
+    for (size_t e = 0; e < nm2; ++e) {
+      dS[2 * ((size_t)i * nm2 + e)] = hout[e].x;
+      dS[2 * ((size_t)i * nm2 + e) + 1] = hout[e].y;
+    }
+    for (int k = 0; k < K; ++k)
+      for (size_t e = 0; e < nm2; ++e) {
+        const size_t a = e % nm;  // row (observation mode) of entry e, column-major
+        const cd v = hout[(1 + k) * nm2 + e] + hw[(size_t)(1 + k) * nm + a] * hG[k * nm2 + e];
+        const size_t d = ((size_t)k * npts + i) * nm2 + e;
+        dSp[2 * d] = v.x;
+        dSp[2 * d + 1] = v.y;
+      }
+  }
+  return 0;
+}

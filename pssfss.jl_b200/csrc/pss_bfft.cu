@@ -128,7 +128,21 @@ __global__ void k_project(int nbf, int nm, const cd *__restrict__ bf, const doub
   if (threadIdx.x == 0) dS[i + (size_t)j * nm] = wobs[i] * red[0];
 }
 
+// PT[n + i*nbf] = t_i · F_i[n]: the projection rows of dS = w ∘ (P X), transposed, which are
+// the right-hand sides of the adjoint solve Z^T Lam = P^T.
+__global__ void k_proj_rows(int nbf, const cd *__restrict__ bf, const double *__restrict__ tobs, cd *__restrict__ PT) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
+  if (n >= nbf) return;
+  const cd *F = bf + (size_t)i * nbf * 2;
+  PT[(size_t)i * nbf + n] = tobs[2 * i] * F[2 * n] + tobs[2 * i + 1] * F[2 * n + 1];
+}
+
 }  // namespace
+
+void pss_proj_rows(int nbf, int nmodes, const cd *bf, const double *tobs, cd *PT, cudaStream_t st) {
+  pss_count_launch();
+  k_proj_rows<<<dim3(cdiv_u(nbf, 256), nmodes), 256, 0, st>>>(nbf, bf, tobs, PT);
+}
 
 void pss_bfft(const SheetDev &G, int nmodes, const double *kvec, double psi1, double psi2, cd *bf,
               cudaStream_t st) {

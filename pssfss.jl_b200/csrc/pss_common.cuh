@@ -112,7 +112,7 @@ __host__ __device__ __forceinline__ void ring_mn(int r, int idx, int &m, int &n)
 }
 __host__ __device__ __forceinline__ int ring_len(int r) { return r == 0 ? 1 : 8 * r; }
 
-// 7-point triangle rule (Zint.jl:118-125)
+// 7-point triangle rule (Zint.jl:55-62)
 __constant__ static double c_qxi[7] = {0.33333333333333330, 0.10128650732345633, 0.79742698535308730,
                                        0.10128650732345633, 0.47014206410511505, 0.05971587178976989,
                                        0.47014206410511505};

@@ -1,9 +1,9 @@
 // K2 + K3: face-pair integrals and the MoM matrix fill.
 //
-// K2 k_filljk   restates Zint.jl:117-242 (filljk!) with PGF.jl:67-106 (jksums):
+// K2 k_filljk   restates Zint.jl:54-179 (filljk!) with PGF.jl:67-106 (jksums):
 //               one thread per unique face pair, the 7-point rule and each lattice
 //               ring summed in the reference's order, FP64.
-// K3a k_pairs   restates Zint.jl:281-308 (zint) and the per-edge algebra of
+// K3a k_pairs   restates Zint.jl:218-245 (zint) and the per-edge algebra of
 //               FillZY.jl:141-197 / 362-419: one thread per unique face pair computes
 //               the 3x3 unflagged edge-pair terms  zA*(ρc2[iml]·a_isl) - zP*φ.
 // K3b k_assemble replaces the spin-locked scatter of FillZY.jl:160-239 by a gather:
@@ -245,14 +245,11 @@ __global__ void __launch_bounds__(128) k_pairs(SheetDev G, const PointParams *__
   }
 }
 
-// Z[m, n] (m = test / match basis function, n = source).  Row-major, leading dimension ld.
-__global__ void __launch_bounds__(256) k_assemble(SheetDev G, const PointParams *__restrict__ Pp,
-                                                  const cd *__restrict__ zb, cd *__restrict__ z64,
-                                                  float *__restrict__ zr, float *__restrict__ zi, long long ld) {
-  int n = blockIdx.x * blockDim.x + threadIdx.x;
-  int m = blockIdx.y * blockDim.y + threadIdx.y;
-  if (m >= G.nbf || n >= G.nbf) return;
-  const PointParams &P = *Pp;
+// Z[m, n] (m = test / match basis function, n = source) from the pair terms zb: the <= 4 x 4
+// face incidences of the two basis functions in a fixed order, with the Floquet / sign flags
+// and the surface-resistance terms of Eqs. 7-34/7-35 (FillZY.jl:221-230).
+__device__ __forceinline__ cd assemble_entry(const SheetDev &G, const PointParams &P, const cd *__restrict__ zb,
+                                             int m, int n) {
   cd acc = mkcd(0, 0);
   const int cm = G.inc_cnt[m], cn = G.inc_cnt[n];
   for (int a = 0; a < cm; ++a) {
@@ -283,6 +280,17 @@ __global__ void __launch_bounds__(256) k_assemble(SheetDev G, const PointParams 
       }
     }
   }
+  return acc;
+}
+
+// Z[m, n], row-major, leading dimension ld.
+__global__ void __launch_bounds__(256) k_assemble(SheetDev G, const PointParams *__restrict__ Pp,
+                                                  const cd *__restrict__ zb, cd *__restrict__ z64,
+                                                  float *__restrict__ zr, float *__restrict__ zi, long long ld) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  int m = blockIdx.y * blockDim.y + threadIdx.y;
+  if (m >= G.nbf || n >= G.nbf) return;
+  const cd acc = assemble_entry(G, *Pp, zb, m, n);
   size_t o = (size_t)m * ld + n;
   if (z64) z64[o] = acc;
   if (zr) {
@@ -291,7 +299,93 @@ __global__ void __launch_bounds__(256) k_assemble(SheetDev G, const PointParams 
   }
 }
 
+// Adjoint contraction of one perturbed input set, without its matrix.  CTA x takes the 4
+// rows m = 4x .. 4x+3 (one per threadIdx.y, 64 lanes across the columns), assembles Z_k[m, n]
+// on the fly from the set's pair terms (recomputed Green's-function values, never stored),
+// forms the row's residual  y[m, b] = R_k[m, b] - sum_n Z_k[m, n] X[n, b]  for the
+// right-hand sides b0 .. b0+NB-1, and writes the CTA's share of
+//     G[a + b*nm] = sum_m Lam[m, a] y[m, b]
+// to part[x] (rows in a fixed order; no atomics, so the result is deterministic).
+// Vectors are nbf x nm column-major.
+constexpr int kAdjNB = 8;
+__global__ void __launch_bounds__(256) k_adj_contract(SheetDev G, const PointParams *__restrict__ Pp,
+                                                      const cd *__restrict__ zb, const cd *__restrict__ X,
+                                                      const cd *__restrict__ R, const cd *__restrict__ Lam, int nm,
+                                                      int b0, cd *__restrict__ part) {
+  const int tx = threadIdx.x, ty = threadIdx.y, lane = tx & 31, half = tx >> 5;
+  const int m = blockIdx.x * 4 + ty;
+  const int nb = min(kAdjNB, nm - b0);
+  const int nbf = G.nbf;
+  __shared__ cd red[4][2][kAdjNB];
+  __shared__ cd yrow[4][kAdjNB];
+  cd acc[kAdjNB];
+#pragma unroll
+  for (int b = 0; b < kAdjNB; ++b) acc[b] = mkcd(0, 0);
+  if (m < nbf) {
+    const PointParams &P = *Pp;
+    for (int n = tx; n < nbf; n += 64) {
+      const cd z = assemble_entry(G, P, zb, m, n);
+#pragma unroll
+      for (int b = 0; b < kAdjNB; ++b)
+        if (b < nb) acc[b] = acc[b] + z * X[(size_t)(b0 + b) * nbf + n];
+    }
+  }
+#pragma unroll
+  for (int b = 0; b < kAdjNB; ++b)
+    for (int o = 16; o > 0; o >>= 1) {
+      acc[b].x += __shfl_xor_sync(0xffffffffu, acc[b].x, o);
+      acc[b].y += __shfl_xor_sync(0xffffffffu, acc[b].y, o);
+    }
+  if (lane == 0)
+    for (int b = 0; b < kAdjNB; ++b) red[ty][half][b] = acc[b];
+  __syncthreads();
+  if (tx < kAdjNB) {
+    const int b = tx;
+    yrow[ty][b] = (m < nbf && b < nb) ? R[(size_t)(b0 + b) * nbf + m] - (red[ty][0][b] + red[ty][1][b]) : mkcd(0, 0);
+  }
+  __syncthreads();
+  // this CTA's share of G: thread e of the 256 covers entries e, e + 256, ...
+  const int tid = ty * 64 + tx;
+  for (int e = tid; e < nm * nb; e += 256) {
+    const int a = e % nm, b = e / nm;
+    cd s = mkcd(0, 0);
+    for (int r = 0; r < 4; ++r) {
+      const int mr = blockIdx.x * 4 + r;
+      if (mr < nbf) s = s + Lam[(size_t)a * nbf + mr] * yrow[r][b];
+    }
+    part[(size_t)blockIdx.x * nm * nm + a + (size_t)(b0 + b) * nm] = s;
+  }
+}
+
+// G[e] = sum over the CTAs' shares, in a fixed order (strided partial sums, then a tree).
+__global__ void __launch_bounds__(256) k_adj_reduce(int nparts, int ne, const cd *__restrict__ part, cd *__restrict__ G) {
+  const int e = blockIdx.x;
+  __shared__ cd red[256];
+  cd s = mkcd(0, 0);
+  for (int q = threadIdx.x; q < nparts; q += 256) s = s + part[(size_t)q * ne + e];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] = red[threadIdx.x] + red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) G[e] = red[0];
+}
+
 }  // namespace
+
+size_t pss_adj_part_bytes(int nbf, int nm) { return (size_t)cdiv_u(nbf, 4) * nm * nm * sizeof(cd); }
+
+void pss_adj_contract(const SheetDev &G, const PointParams *dP1, const cd *zb, const cd *X, const cd *R,
+                      const cd *Lam, int nm, cd *part, cd *Gout, cudaStream_t st) {
+  const int nblk = cdiv_u(G.nbf, 4);
+  for (int b0 = 0; b0 < nm; b0 += kAdjNB) {
+    pss_count_launch();
+    k_adj_contract<<<nblk, dim3(64, 4), 0, st>>>(G, dP1, zb, X, R, Lam, nm, b0, part);
+  }
+  pss_count_launch();
+  k_adj_reduce<<<nm * nm, 256, 0, st>>>(nblk, nm * nm, part, Gout);
+}
 
 void pss_filljk(const SheetDev &G, double ulocal, double psi1, double psi2, const double s1[2], const double s2[2],
                 JKDev jk, int *nonconv, cudaStream_t st) {

@@ -66,7 +66,7 @@ struct SheetDev {
   const int *inc_eci;    // 4*nbf edge boundary code 0..4
 };
 
-// J/K cache (Zint.jl:117-242), SoA over unique face pairs.
+// J/K cache (Zint.jl:54-179), SoA over unique face pairs.
 struct JKDev {
   cd *J, *Jxi, *Jeta, *K, *Kxi, *Keta;
   double *rho_r;  // 2*nufp
@@ -145,6 +145,14 @@ void pss_bfft(const SheetDev &G, int nmodes, const double *kvec, double psi1, do
 void pss_rhs(int nbf, int nmodes, const cd *bf, const cd *src, cd *rhs, cudaStream_t st);
 void pss_project(int nbf, int nmodes, const cd *bf, const double *tobs, const cd *wobs, const cd *X, cd *dS,
                  cudaStream_t st);
+// PT (nbf x nmodes, column-major): row i of the projection, t_i · F_i[n], for the adjoint solve.
+void pss_proj_rows(int nbf, int nmodes, const cd *bf, const double *tobs, cd *PT, cudaStream_t st);
+// Adjoint contraction of a perturbed set from its pair terms zb (no matrix stored):
+//   Gout[a + b*nm] = sum_m Lam[m, a] (R[m, b] - sum_n Z[m, n] X[n, b]);
+// part: scratch of pss_adj_part_bytes(nbf, nm).
+size_t pss_adj_part_bytes(int nbf, int nm);
+void pss_adj_contract(const SheetDev &G, const PointParams *dP1, const cd *zb, const cd *X, const cd *R,
+                      const cd *Lam, int nm, cd *part, cd *Gout, cudaStream_t st);
 
 // Dense complex LU and solves (pss_lu.cu); matrices row-major with leading dimension ld.
 // Batched forms factor nb matrices of order n at A + b*ms (elements), pivots at ipiv + b*n,
@@ -190,3 +198,12 @@ int pss_solve_lu(SolveWS &ws, int nb, const cd *LU64, const float *Lr, const flo
 int pss_refine(SolveWS &ws, int nb, const cd *A, long long ld, long long ms, const float *Lr, const float *Li,
                int nrhs, const cd *B, cd *X, cd *R, cd *D, long long vs, int maxit, int *status, cudaStream_t st);
 void pss_solve_status(SolveWS &ws, int nb, int *status, cudaStream_t st);
+// Adjoint (transposed) solves on the same factors: Y = Z^-T B (W: scratch like B), and their
+// FP64 refinement against A (FP32 factors) with a scratch of pss_refine_trans_ws_bytes.
+int pss_solve_lu_trans(SolveWS &ws, int nb, const cd *LU64, const float *Lr, const float *Li, long long ld,
+                       long long ms, int nrhs, const cd *B, cd *Y, cd *W, long long vs, int use_done,
+                       cudaStream_t st);
+size_t pss_refine_trans_ws_bytes(int n, int nrhs, int nb);
+int pss_refine_trans(SolveWS &ws, int nb, const cd *A, long long ld, long long ms, const float *Lr, const float *Li,
+                     int nrhs, const cd *B, cd *Y, cd *R, cd *D, cd *W, void *scratch, size_t scratch_bytes,
+                     long long vs, int maxit, int *status, cudaStream_t st);

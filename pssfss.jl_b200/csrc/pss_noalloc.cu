@@ -23,7 +23,12 @@
 //     kernel;
 //   * the first call on each device resolves the scratch array's address with
 //     cudaGetSymbolAddress (a one-time set-up, done with that device current); make that
-//     first call before any stream capture on the device.
+//     first call before any stream capture on the device.  The address belongs to the
+//     device's current CUDA context: it is cached together with that context's handle and
+//     resolved again when a call finds another context current (after cudaDeviceReset, or
+//     a context the caller created itself), so a stale address is never used.
+#include <cuda.h>
+
 #include <mutex>
 
 #include "pss_internal.cuh"
@@ -39,9 +44,13 @@ static __device__ __align__(256) unsigned char g_lu_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
 void *g_scratch_ptr[kMaxDevices] = {};
+CUcontext g_scratch_ctx[kMaxDevices] = {};  // the context each cached address belongs to
 std::mutex g_setup_mu;
 
-// One-time set-up per device (the caller's current device): the array's device address.
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+CtxGetCurrentFn g_ctx_get_current = nullptr;  // cuCtxGetCurrent, resolved once under g_setup_mu
+
+// Set-up per device (the caller's current device) and context: the array's device address.
 int scratch_for_current_device(void **out) {
   int dev = -1;
   PSS_CUDA_TRY(cudaGetDevice(&dev));
@@ -50,7 +59,22 @@ int scratch_for_current_device(void **out) {
     return -3;
   }
   std::lock_guard<std::mutex> lk(g_setup_mu);
-  if (!g_scratch_ptr[dev]) {
+  if (!g_ctx_get_current) {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn) {
+      pss_set_error("cuCtxGetCurrent unavailable");
+      return -3;
+    }
+    g_ctx_get_current = (CtxGetCurrentFn)fn;
+  }
+  CUcontext ctx = nullptr;
+  if (g_ctx_get_current(&ctx) != CUDA_SUCCESS || !ctx) {
+    pss_set_error("no current CUDA context on device %d", dev);
+    return -3;
+  }
+  if (!g_scratch_ptr[dev] || g_scratch_ctx[dev] != ctx) {
     void *p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_lu_scratch);
     if (e != cudaSuccess || !p) {
@@ -59,6 +83,7 @@ int scratch_for_current_device(void **out) {
       return -3;
     }
     g_scratch_ptr[dev] = p;
+    g_scratch_ctx[dev] = ctx;
   }
   *out = g_scratch_ptr[dev];
   return 0;
@@ -81,9 +106,11 @@ extern "C" int pss_lu_factor_noalloc(int n, double *A, int64_t ld, int *ipiv, in
                   pss_lu_ws_bytes(n, PSS_FP64), n);
     return -1;
   }
+  cudaStream_t st = (cudaStream_t)stream;
+  // first runtime call on the caller's memory: it also makes the device's context current on
+  // this host thread, which the scratch look-up below reads
+  PSS_CUDA_TRY(cudaMemsetAsync(info, 0, sizeof(int), st));
   void *scratch = nullptr;
   if (int rc = scratch_for_current_device(&scratch)) return rc;
-  cudaStream_t st = (cudaStream_t)stream;
-  PSS_CUDA_TRY(cudaMemsetAsync(info, 0, sizeof(int), st));
   return pss_lu64(n, (cd *)A, (long long)ld, ipiv, info, scratch, kScratchBytes, st);
 }

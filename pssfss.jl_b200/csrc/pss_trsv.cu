@@ -148,12 +148,16 @@ __device__ __forceinline__ C czero() { return C{0, 0}; }
 // One chained substitution pass over right-hand sides j0 .. j0+nj-1 (nj <= NJ):
 //   lower: X[rows_b] = Linv_b (B[perm[rows_b]] - sum_{c<b} L[b,c] X[c])
 //   upper: X[rows_b] = Uinv_b (X[rows_b] - sum_{c>b} U[b,c] X[c])   (in place)
+// TRANS (the adjoint system Z^T y = b, Z = P^T L U, so U^T L^T (P y) = b): the lower pass
+// runs with U^T (block (b, c) read as the transpose of block (c, b) of the factor, the
+// diagonal inverse transposed) on B unpermuted, the upper pass with L^T in place; the
+// caller applies P^T to the result (pss_solve_lu_trans).
 // One CTA per 64-row block b (ticket order), 256 threads: row i = tid/4 of the block,
 // quarter p = tid%4 covers 16 columns of each 64-column tile.  Each tile of the factor is
 // loaded into registers BEFORE the wait for the CTA that produces x_c, so the wait hides
 // the load; Dinv_b (dynamic shared memory) and the block's right-hand side are staged at
 // the start.  Blocks of X written by other CTAs are read with L1-bypassing loads.
-template <bool LOWER, bool F32, int NJ>
+template <bool LOWER, bool F32, int NJ, bool TRANS = false>
 __global__ void __launch_bounds__(256, F32 ? 4 : 1) k_trsv(Fac F0, int n, const int *__restrict__ perm0, const cd *__restrict__ B0,
                                               cd *__restrict__ X0, long long vs, int nrhs, int j0,
                                               const cd *__restrict__ Dinv0, long long dstride, Ctrl ctrl, int epoch,
@@ -183,13 +187,15 @@ __global__ void __launch_bounds__(256, F32 ? 4 : 1) k_trsv(Fac F0, int n, const 
   const int tk = s_b;
   const int b = LOWER ? tk : nblk - 1 - tk;
   const int r0 = b * BS, nr = min(BS, n - r0);
-  const cd *D = Dinv + (size_t)(2 * b + (LOWER ? 0 : 1)) * BS * BS;
-  for (int e = tid; e < BS * BS; e += 256) Ds[e] = T::from(D[e]);
+  // diagonal block: L_bb^-1 (lower pass) or U_bb^-1 (upper pass); transposed, U_bb^-T for the
+  // lower pass of the adjoint system and L_bb^-T for its upper pass
+  const cd *D = Dinv + (size_t)(2 * b + ((LOWER != TRANS) ? 0 : 1)) * BS * BS;
+  for (int e = tid; e < BS * BS; e += 256) Ds[e] = T::from(TRANS ? D[(e % BS) * BS + e / BS] : D[e]);
   for (int e = tid; e < BS * NJ; e += 256) {
     const int r = e / NJ, j = e % NJ;
     cd v = mkcd(0, 0);
     if (r < nr && j < nj)
-      v = LOWER ? B[(size_t)(j0 + j) * n + perm[r0 + r]] : ldcg(&X[(size_t)(j0 + j) * n + r0 + r]);
+      v = LOWER ? B[(size_t)(j0 + j) * n + (TRANS ? r0 + r : perm[r0 + r])] : ldcg(&X[(size_t)(j0 + j) * n + r0 + r]);
     y[r][j] = T::from(v);
   }
   C acc[NJ];
@@ -203,7 +209,7 @@ __global__ void __launch_bounds__(256, F32 ? 4 : 1) k_trsv(Fac F0, int n, const 
 #pragma unroll
     for (int q = 0; q < 16; ++q) {
       const int t = p * 16 + q;
-      lv[q] = (i < nr && t < nt) ? T::fac(F, r0 + i, t0 + t) : czero<C>();
+      lv[q] = (i < nr && t < nt) ? (TRANS ? T::fac(F, t0 + t, r0 + i) : T::fac(F, r0 + i, t0 + t)) : czero<C>();
     }
     if (tid == 0) {
       wait_flag(flags, c, epoch, err);
@@ -425,12 +431,97 @@ __global__ void k_axpy(long long total, cd *X0, const cd *D0, long long vs, Ctrl
   if (i < total) X[i] = X[i] + D[i];
 }
 
+// y[perm[r]] = w[r] for every right-hand side: applies P^T after the adjoint passes.
+__global__ void k_unpermute(int n, int nrhs, const int *__restrict__ perm0, const cd *__restrict__ W0,
+                            cd *__restrict__ Y0, long long vs, Ctrl ctrl, int use_done) {
+  const int bm = blockIdx.y;
+  if (use_done && ctrl.of(bm)[2]) return;
+  const int *perm = perm0 + (long long)bm * n;
+  const cd *W = W0 + bm * vs;
+  cd *Y = Y0 + bm * vs;
+  const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (e >= (long long)n * nrhs) return;
+  const int r = (int)(e % n), j = (int)(e / n);
+  Y[(size_t)j * n + perm[r]] = W[e];
+}
+
+// Adjoint residual R = B - A^T Y, first stage: CTA (column block cb of 128, row chunk q of
+// kTrRows) sums its rows for each column j and right-hand side, and the column's |a| sums
+// (the infinity norm of A^T is the largest column sum of A), into part[q] (fixed order, no
+// atomics; the second stage adds the chunks in order).  A thread owns a column, so every row
+// of the chunk is read coalesced across the CTA.
+constexpr int kTrRows = 256, kTrCols = 128;
+__global__ void __launch_bounds__(kTrCols) k_resid_t1(int n, const cd *__restrict__ A0, long long ld, long long ms,
+                                                      int nrhs, const cd *__restrict__ Y0, long long vs,
+                                                      cd *__restrict__ part0, double *__restrict__ cabs0,
+                                                      long long pstride, Ctrl ctrl) {
+  const int bm = blockIdx.z;
+  if (ctrl.of(bm)[2]) return;
+  const cd *A = A0 + bm * ms, *Y = Y0 + bm * vs;
+  const int j = blockIdx.x * kTrCols + threadIdx.x, q = blockIdx.y;
+  const int i0 = q * kTrRows, i1 = min(n, i0 + kTrRows);
+  const int nch = (int)gridDim.y;
+  cd *part = part0 + (long long)bm * pstride;
+  double *cabs = cabs0 + (long long)bm * nch * n;
+  if (j >= n) return;
+  for (int j0 = 0; j0 < nrhs; j0 += kMaxRhs) {
+    const int nj = min(kMaxRhs, nrhs - j0);
+    cd acc[kMaxRhs];
+#pragma unroll
+    for (int t = 0; t < kMaxRhs; ++t) acc[t] = mkcd(0, 0);
+    double cs = 0.0;
+    for (int i = i0; i < i1; ++i) {
+      const cd a = A[(long long)i * ld + j];
+      if (j0 == 0) cs += cabs1(a);
+#pragma unroll
+      for (int t = 0; t < kMaxRhs; ++t)
+        if (t < nj) acc[t] = acc[t] + a * Y[(size_t)(j0 + t) * n + i];
+    }
+    if (j0 == 0) cabs[(long long)q * n + j] = cs;
+#pragma unroll
+    for (int t = 0; t < kMaxRhs; ++t)
+      if (t < nj) part[((long long)q * nrhs + j0 + t) * n + j] = acc[t];
+  }
+}
+
+// Second stage: R = B - sum of the chunks (in chunk order), with the refinement norms of
+// k_resid: max|r_j| (norms[j]), max|y_j| (norms[kNX + j]) and ||A^T||_inf (norms[kNA]).
+__global__ void k_resid_t2(int n, int nch, int nrhs, const cd *__restrict__ part0, const double *__restrict__ cabs0,
+                           long long pstride, const cd *__restrict__ Y0, const cd *__restrict__ B0, cd *__restrict__ R0,
+                           long long vs, double *norms0, Ctrl ctrl) {
+  const int bm = blockIdx.y;
+  if (ctrl.of(bm)[2]) return;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const cd *part = part0 + (long long)bm * pstride;
+  const double *cabs = cabs0 + (long long)bm * nch * n;
+  const cd *Y = Y0 + bm * vs, *B = B0 + bm * vs;
+  cd *R = R0 + bm * vs;
+  double *norms = norms0 + (long long)bm * kNormCount;
+  double cs = 0.0;
+  for (int q = 0; q < nch; ++q) cs += cabs[(long long)q * n + j];
+  atomicMax((unsigned long long *)&norms[kNA], (unsigned long long)__double_as_longlong(cs));
+  for (int t = 0; t < nrhs; ++t) {
+    cd s = mkcd(0, 0);
+    for (int q = 0; q < nch; ++q) s = s + part[((long long)q * nrhs + t) * n + j];
+    const cd r = B[(size_t)t * n + j] - s;
+    R[(size_t)t * n + j] = r;
+    atomicMax((unsigned long long *)&norms[t], (unsigned long long)__double_as_longlong(cabs1(r)));
+    atomicMax((unsigned long long *)&norms[kNX + t],
+              (unsigned long long)__double_as_longlong(cabs1(Y[(size_t)t * n + j])));
+  }
+}
+
 template <bool LOWER>
 cudaError_t set_trsv_smem() {
   const int s64 = BS * BS * (int)sizeof(cd);
   cudaError_t e = cudaFuncSetAttribute(k_trsv<LOWER, false, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, s64);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_trsv<LOWER, false, kMaxRhs>, cudaFuncAttributeMaxDynamicSharedMemorySize, s64);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_trsv<LOWER, false, 4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s64);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_trsv<LOWER, false, kMaxRhs, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s64);
   return e;  // the FP32 forms stage 32 KB, under the default limit
 }
 
@@ -558,6 +649,93 @@ int pss_refine(SolveWS &ws, int nb, const cd *A, long long ld, long long ms, con
     if (rc) return rc;
     pss_count_launch();
     k_axpy<<<dim3(cdiv_u(total, 256), nb), 256, 0, st>>>(total, X, D, vs, ctrl);
+  }
+  PSS_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+// Adjoint solves Y = Z^-T B with the factors of P Z = L U (the same factors as pss_solve_lu,
+// after pss_solve_prepare): U^T V = B, L^T W = V (both chained passes into W), Y = P^T W.
+// W: scratch of the size of B.  use_done: skip matrices whose refinement has converged.
+int pss_solve_lu_trans(SolveWS &ws, int nb, const cd *LU64, const float *Lr, const float *Li, long long ld,
+                       long long ms, int nrhs, const cd *B, cd *Y, cd *W, long long vs, int use_done,
+                       cudaStream_t st) {
+  Fac F{LU64, Lr, Li, ld, ms};
+  const Ctrl ctrl{ws.ctrl, ws.cstride};
+  static DeviceOnce once;
+  if (int rc = device_once(once, [] {
+        PSS_CUDA_TRY(set_trsv_smem<true>());
+        PSS_CUDA_TRY(set_trsv_smem<false>());
+        return 0;
+      }))
+    return rc;
+  const bool f32 = LU64 == nullptr;
+  for (int pass = 0; pass < 2; ++pass)
+    for (int j0 = 0; j0 < nrhs; j0 += kMaxRhs) {
+      ++ws.epoch;
+      PSS_CUDA_TRY(cudaMemset2DAsync(ws.ctrl, ws.cstride * sizeof(int), 0, sizeof(int), nb, st));
+      pss_count_launch();
+      const bool small = nrhs - j0 <= 4;
+      const dim3 grid(ws.nblk, nb);
+      auto go = [&](auto kern, size_t smem) {
+        kern<<<grid, 256, smem, st>>>(F, ws.n, ws.perm, B, W, vs, nrhs, j0, ws.Dinv, ws.dstride, ctrl, ws.epoch,
+                                      use_done);
+      };
+      const size_t s64 = BS * BS * sizeof(cd), s32 = BS * BS * sizeof(cf);
+      if (pass == 0) {
+        if (f32) small ? go(k_trsv<true, true, 4, true>, s32) : go(k_trsv<true, true, kMaxRhs, true>, s32);
+        else small ? go(k_trsv<true, false, 4, true>, s64) : go(k_trsv<true, false, kMaxRhs, true>, s64);
+      } else {
+        if (f32) small ? go(k_trsv<false, true, 4, true>, s32) : go(k_trsv<false, true, kMaxRhs, true>, s32);
+        else small ? go(k_trsv<false, false, 4, true>, s64) : go(k_trsv<false, false, kMaxRhs, true>, s64);
+      }
+    }
+  pss_count_launch();
+  k_unpermute<<<dim3(cdiv_u((long long)ws.n * nrhs, 256), nb), 256, 0, st>>>(ws.n, nrhs, ws.perm, W, Y, vs, ctrl,
+                                                                          use_done);
+  PSS_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+// Scratch of the adjoint residual for nb matrices and nrhs right-hand sides (row-chunk partial
+// sums and column sums).
+size_t pss_refine_trans_ws_bytes(int n, int nrhs, int nb) {
+  const size_t nch = (size_t)(n + kTrRows - 1) / kTrRows;
+  return (size_t)nb * nch * ((size_t)nrhs * n * sizeof(cd) + (size_t)n * sizeof(double)) + 256;
+}
+
+// Iterative refinement of the adjoint solutions Y_b (Z_b^T Y_b = B_b) against the FP64
+// matrices, as pss_refine: r = B - Z^T Y in FP64 (two-stage, fixed order), correction from the
+// FP32 factors (pss_solve_lu_trans), the same stopping rule with ||Z^T||_inf.
+int pss_refine_trans(SolveWS &ws, int nb, const cd *A, long long ld, long long ms, const float *Lr, const float *Li,
+                     int nrhs, const cd *B, cd *Y, cd *R, cd *D, cd *W, void *scratch, size_t scratch_bytes,
+                     long long vs, int maxit, int *status, cudaStream_t st) {
+  if (nrhs > kMaxRefRhs) { pss_set_error("refinement supports at most %d right-hand sides", kMaxRefRhs); return -1; }
+  if (scratch_bytes < pss_refine_trans_ws_bytes(ws.n, nrhs, nb)) {
+    pss_set_error("adjoint refinement scratch too small");
+    return -4;
+  }
+  const Ctrl ctrl{ws.ctrl, ws.cstride};
+  const int nch = (ws.n + kTrRows - 1) / kTrRows;
+  const long long pstride = (long long)nch * nrhs * ws.n;
+  cd *part = (cd *)scratch;
+  double *cabs = (double *)(part + (size_t)nb * pstride);
+  PSS_CUDA_TRY(cudaMemset2DAsync(ws.ctrl + 2, ws.cstride * sizeof(int), 0, sizeof(int), nb, st));
+  const long long total = (long long)ws.n * nrhs;
+  for (int it = 0; it <= maxit; ++it) {
+    pss_count_launch();
+    k_resid_t1<<<dim3(cdiv_u(ws.n, kTrCols), nch, nb), kTrCols, 0, st>>>(ws.n, A, ld, ms, nrhs, Y, vs, part, cabs,
+                                                                        pstride, ctrl);
+    pss_count_launch();
+    k_resid_t2<<<dim3(cdiv_u(ws.n, 256), nb), 256, 0, st>>>(ws.n, nch, nrhs, part, cabs, pstride, Y, B, R, vs,
+                                                            ws.norms, ctrl);
+    pss_count_launch();
+    k_ir_check<<<nb, 1, 0, st>>>(ws.n, nrhs, ws.norms, ctrl, status, it == maxit);
+    if (it == maxit) break;
+    int rc = pss_solve_lu_trans(ws, nb, nullptr, Lr, Li, ld, ms, nrhs, R, D, W, vs, 1, st);
+    if (rc) return rc;
+    pss_count_launch();
+    k_axpy<<<dim3(cdiv_u(total, 256), nb), 256, 0, st>>>(total, Y, D, vs, ctrl);
   }
   PSS_CUDA_TRY(cudaGetLastError());
   return 0;

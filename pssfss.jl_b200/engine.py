@@ -48,6 +48,8 @@ SIGNATURES = {
     "pss_partial_gsms": (_I, [_P, _I, _P, _P, _P, _I, _D, _I, _P, _P, _I, _P, _P, _P, _P, _I, _P, _P]),
     "pss_partial_gsms_lin": (_I, [_P, _I, _P, _P, _P, _I, _D, _I, _P, _P, _I, _P, _P, _P, _P, _I, _P, _P, _P,
                                   _P, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P]),
+    "pss_partial_gsms_adj": (_I, [_P, _I, _P, _P, _P, _I, _D, _I, _P, _P, _I, _P, _P, _P, _P, _I, _P, _P, _P,
+                                  _P, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P]),
     "pss_fill_matrix": (_I, [_P, _I, _P, _P, _P, _I, _D, _D, _D, _D, _P, _P]),
     "pss_modal_tables": (_I, [_P, _I, _I, _P, _P, _P, _I, _D, _D, _D, _D, _P, _P, _D, _L, _P, _P, _P, _P]),
     "pss_face_integrals": (_I, [_P, _D, _D, _D, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
@@ -224,11 +226,20 @@ def partial_gsms(sheet, rwg, points, region_rng, s, u, ios, precision="fp64", de
     return [d.T.copy() for d in dS]
 
 
-def partial_gsms_linearized(sheet, rwg, points, region_rng, s, u, ios, perturbed, precision="fp64", device=0):
+def partial_gsms_adjoint(sheet, rwg, points, region_rng, s, u, ios, perturbed, precision="fp64", device=0):
+    """``partial_gsms_linearized`` in its adjoint form (``pss_partial_gsms_adj``): one
+    factorisation, forward and transposed solves on it, and per perturbed set a fused
+    assemble-and-contract pass instead of a stored matrix and further solves."""
+    return partial_gsms_linearized(sheet, rwg, points, region_rng, s, u, ios, perturbed, precision, device,
+                                   entry="pss_partial_gsms_adj")
+
+
+def partial_gsms_linearized(sheet, rwg, points, region_rng, s, u, ios, perturbed, precision="fp64", device=0,
+                            entry="pss_partial_gsms_lin"):
     """Scattered partial GSMs of one sheet Gblock and their first-order values at each
-    perturbed input set (``pss_partial_gsms_lin``), the ``partial_lin`` form that
-    ``gradient.linearized_gradient`` takes.  ``perturbed``: (sheet_k, rwg_k, points_k, u_k,
-    ios_k) per set, with the topology of ``sheet``."""
+    perturbed input set (``pss_partial_gsms_lin``, or ``entry``), the ``partial_lin`` form
+    that ``gradient.linearized_gradient`` takes.  ``perturbed``: (sheet_k, rwg_k, points_k,
+    u_k, ios_k) per set, with the topology of ``sheet``."""
     i1, i2 = region_rng
     region = points[0].layers[i1 - 1:i2]
     eps, mu, w = region_arrays(region)
@@ -264,10 +275,10 @@ def partial_gsms_linearized(sheet, rwg, points, region_rng, s, u, ios, perturbed
     dS = np.zeros((npts, nm, nm), complex)
     dSp = np.zeros((max(K, 1), npts, nm, nm), complex)
     status = np.zeros(npts, np.int32)
-    _check(lib().pss_partial_gsms_lin(ds.h, len(region), _p(eps), _p(mu), _p(w), s, float(u), npts, _p(k0), _p(psi),
-                                      nm, _p(kvec), _p(src), _p(tobs), _p(wobs), K, psh, _p(peps), _p(pmu),
-                                      _p(pwidth), _p(pu_), _p(ppsi), _p(pkvec), _p(psrc), _p(ptobs), _p(pwobs),
-                                      PRECISIONS[precision], _p(dS), _p(dSp), _p(status)), "pss_partial_gsms_lin")
+    _check(getattr(lib(), entry)(ds.h, len(region), _p(eps), _p(mu), _p(w), s, float(u), npts, _p(k0), _p(psi),
+                                 nm, _p(kvec), _p(src), _p(tobs), _p(wobs), K, psh, _p(peps), _p(pmu),
+                                 _p(pwidth), _p(pu_), _p(ppsi), _p(pkvec), _p(psrc), _p(ptobs), _p(pwobs),
+                                 PRECISIONS[precision], _p(dS), _p(dSp), _p(status)), entry)
     if (status & FATAL_STATUS).any():
         raise RuntimeError(f"solver status {status.tolist()} (singular, non-finite or device timeout)")
     del held

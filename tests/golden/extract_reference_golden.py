@@ -79,4 +79,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: extract_reference_golden.py <checkout of PSSFSS.jl v0.1.4>")
+    main(sys.argv[1])

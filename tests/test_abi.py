@@ -150,3 +150,81 @@ def test_linearized_binding_packs_the_header_layout(monkeypatch):
             assert tuple(seen["ppsi"][k, i]) == (pert[k][4][i].psi1, pert[k][4][i].psi2)
     assert seen["peps"].shape == (K, nl) and seen["peps"][0, 1] == layers[1].epsr
     assert np.array_equal(dS[1], seen["dS"][1].T) and np.array_equal(lin[1][2], seen["dSp"][1, 2].T)
+
+
+def _julia_stub_sheet_arrays(sheet, rwg):
+    """The arguments INTEGRATION.md's Julia stub hands to pss_sheet_create, built from
+    RWGSheet/RWGData-shaped fields the way the stub builds them: every index array passes
+    unchanged (Int64, 1-based, column-major), ufp_rep = first.(rwgdat.ufp2fp)."""
+    import numpy as np
+    jl = {"fv": np.asarray(sheet.fv, np.int64), "fe": np.asarray(sheet.fe, np.int64),
+          "bff": np.asarray(rwg.bff, np.int64), "ebf": np.asarray(rwg.ebf, np.int64),
+          "eci": np.asarray(rwg.eci, np.int64), "ufpm": np.asarray(rwg.ufpm, np.int64),
+          "ufp2fp": rwg.ufp2fp}
+    col = (lambda a: np.ascontiguousarray(a.ravel(order="F")))  # Julia's memory order
+    return {"fv": col(jl["fv"]), "fe": col(jl["fe"]), "bff": col(jl["bff"]), "ebf": col(jl["ebf"]),
+            "eci": col(jl["eci"]), "ufpm": col(jl["ufpm"]),
+            "ufp_rep": np.array([int(v[0]) for v in jl["ufp2fp"]], np.int64)}
+
+
+def test_julia_stub_arrays_are_one_based_and_match_the_binding(pkg):
+    # No device needed: the stub's arrays are exactly the 1-based arrays the Python binding
+    # uploads (engine.DeviceSheet), so the library's 1-based checks accept both.
+    import numpy as np
+    from pssfss_b200.rwg import setup_rwg
+    sheet = pkg.rectstrip(Lx=8, Ly=8, Px=10, Py=10, Nx=4, Ny=4, units=pkg.mm)
+    rwg = setup_rwg(sheet)
+    a = _julia_stub_sheet_arrays(sheet, rwg)
+    assert a["fv"].min() == 1 and a["fv"].max() == sheet.nnode
+    assert a["fe"].min() == 1 and a["fe"].max() == sheet.nedge
+    assert a["ufpm"].min() == 1 and a["ufpm"].max() == rwg.nufp
+    assert a["ebf"].min() == 0 and a["ebf"].max() == rwg.nbf  # 0: edge without a basis function
+    assert np.array_equal(a["ufp_rep"], rwg.ufp_rep)
+    assert np.array_equal(a["fv"], sheet.fv.ravel(order="F"))
+    assert np.array_equal(a["bff"], rwg.bff.ravel(order="F"))
+
+
+@pytest.mark.gpu
+def test_julia_stub_arrays_upload_and_fill_like_the_binding(pkg):
+    # The library accepts the stub's 1-based arrays, and the sheet they make fills the same
+    # matrix as the binding's upload; the same arrays made 0-based (the old stub) are refused.
+    import ctypes
+    import numpy as np
+    from pssfss_b200.layers import Layer
+    from pssfss_b200.rwg import setup_rwg
+    sheet = pkg.rectstrip(Lx=8, Ly=8, Px=10, Py=10, Nx=4, Ny=4, units=pkg.mm)
+    rwg = setup_rwg(sheet)
+    a = _julia_stub_sheet_arrays(sheet, rwg)
+    L = engine.lib()
+    ctx = engine.context(0)
+    f64 = engine._f64
+
+    def create(arr):
+        h = ctypes.c_void_p()
+        rc = L.pss_sheet_create(ctx, b"J", sheet.units.units_per_meter, engine._p(f64(sheet.s1)),
+                                engine._p(f64(sheet.s2)), engine._p(f64(sheet.beta1)), engine._p(f64(sheet.beta2)),
+                                sheet.nnode, engine._p(f64(sheet.rho)), sheet.nface, engine._p(arr["fv"]),
+                                engine._p(arr["fe"]), engine._p(f64(sheet.fr)), sheet.nedge, rwg.nbf,
+                                engine._p(arr["bff"]), engine._p(arr["ebf"]), engine._p(arr["eci"]), rwg.nufp,
+                                engine._p(arr["ufpm"]), engine._p(arr["ufp_rep"]), ctypes.byref(h))
+        return rc, h
+
+    zero_based = {k: (v - 1 if k != "eci" else v) for k, v in a.items()}
+    rc, _ = create(zero_based)
+    assert rc == -1 and "out of range" in L.pss_last_error().decode()
+    rc, h = create(a)
+    assert rc == 0, L.pss_last_error().decode()
+    try:
+        layers = [Layer(), Layer()]
+        eps, mu, w = engine.region_arrays(layers)
+        n = rwg.nbf
+        Z = np.zeros((n, n), complex, order="F")
+        mm = ctypes.c_int()
+        k0 = 2 * np.pi * 15e9 / 299792458.0
+        u = 2 * np.pi / 0.01
+        assert L.pss_fill_matrix(h, 2, engine._p(eps), engine._p(mu), engine._p(w), 1, u, k0, 0.0, 0.0,
+                                 Z.ctypes.data_as(ctypes.c_void_p), ctypes.byref(mm)) == 0
+        Zb, _ = engine.fill_matrix(sheet, rwg, layers, 1, u, k0, 0.0, 0.0)
+        assert np.array_equal(Z, Zb)
+    finally:
+        L.pss_sheet_destroy(h)

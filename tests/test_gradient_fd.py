@@ -57,3 +57,16 @@ def test_tangent_form_equals_adjoint_form():
                                                                         tangent=True), ntri=NTRI)
     for k in P0:
         assert abs(g_tan[k] - g_adj[k]) <= 1e-9 * abs(g_adj[k]), (k, g_tan[k], g_adj[k])
+
+
+def test_fully_adjoint_form_matches_full_central_differences():
+    # dS_k = wobs_k (P_k X + Lam^T (R_k - Z_k X)): no solve per perturbed set, only the adjoint
+    # solve per point; its central differences match two full sweeps per parameter to 1e-5
+    import functools
+    from pssfss_b200.gradient import meander_linearized_gradient
+    f_fd, g_fd = meander_gradient(P0, FREQS, ntri=NTRI, rel_step=1e-4, analyze_fn=oracle.analyze)
+    f_adj, g_adj = meander_linearized_gradient(P0, FREQS, functools.partial(oracle.partial_gsms_linearized,
+                                                                            form="adjoint"), ntri=NTRI)
+    assert abs(f_adj - f_fd) <= 1e-12 * abs(f_fd)
+    for k in P0:
+        assert abs(g_adj[k] - g_fd[k]) <= 1e-5 * abs(g_fd[k]), (k, g_adj[k], g_fd[k])
