@@ -13,6 +13,14 @@ e2e    = the same through the C ABI call with host buffers (per-point inputs cop
          dS copied out), CUDA events on the caller's stream around the call.
 The FP64 form is timed too (fp64_value) and its results give max|dS| of the FP32 form.
 
+Both arms compute the sheet's face-pair integrals (filljk!) once per 101-point sweep: the
+GPU arm drops its cached integrals before every step, the CPU arm adds one J/K pass per
+101 points.
+
+At one GPU the line also carries the 6000-unknown targets (target_sweep: the meanderline at
+ntri = 4000, N = 5610, 201 frequencies, FP32 + refinement against the FP64 form; grads: the
+adjoint gradient of that sweep's objective in trace width, pitch and eps_r, grads/s).
+
 --impl reference: the CPU oracle (C restatement + LAPACK) on the host cores, one point
 per step with the sweep's J/K pass amortised over the 101 points.
 
@@ -58,6 +66,35 @@ TRAFFIC = {
 }
 
 
+CONFIG = {"workload": WORKLOAD, "points_per_sweep": NFREQ, "face_integrals": "once per sweep",
+          "l2": "working set > L2 (Z is 253 MB FP64 + 126 MB FP32 per point)"}
+
+
+def cpu_info():
+    """Host CPU model and the thread counts the CPU legs run with (OpenMP of the oracle,
+    BLAS of LAPACK's LU)."""
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    model = ln.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    omp = blas = None
+    try:
+        from threadpoolctl import threadpool_info
+        for t in threadpool_info():
+            if t.get("user_api") == "openmp":
+                omp = max(omp or 0, t["num_threads"])
+            elif t.get("user_api") == "blas":
+                blas = max(blas or 0, t["num_threads"])
+    except Exception:
+        pass
+    return {"cpu_model": model, "nproc": os.cpu_count(), "omp_threads": omp, "blas_threads": blas}
+
+
 def load_package():
     import importlib.util
     if "pssfss_b200" in sys.modules:
@@ -71,13 +108,13 @@ def load_package():
     return mod
 
 
-def build_case(rank=0, npts=NFREQ):
+def build_case(rank=0, npts=NFREQ, ntri=3000, nfreq=NFREQ):
     pkg = load_package()
     from pssfss_b200.analyze import make_plan, sheet_gblocks, sheet_io
-    sheet = pkg.meander(a=5, b=10, h=6, w1=0.3, w2=0.3, ntri=3000, units=pkg.mm)
+    sheet = pkg.meander(a=5, b=10, h=6, w1=0.3, w2=0.3, ntri=ntri, units=pkg.mm)
     strata = [pkg.Layer(), sheet, pkg.Layer(epsr=2.2, width=pkg.Length(1, pkg.mm)), pkg.Layer()]
     shift = 0.01 * rank
-    freqs = np.linspace(8.0 + shift, 18.0 + shift, NFREQ)[:npts]
+    freqs = np.linspace(8.0 + shift, 18.0 + shift, nfreq)[:npts]
     plan = make_plan(strata, freqs, {"θ": 0.0, "ϕ": 0.0})
     (ig, (i1, i2), isht, s), = sheet_gblocks(plan)
     rwg = plan.rwgdat[isht - 1]
@@ -172,16 +209,16 @@ def run_reference(args, rank, world):
             times.append(dt)
     per_point = statistics.mean(times) + t_jk / NFREQ
     value = 1.0 / per_point
-    cores = os.cpu_count()
+    ci = cpu_info()
+    cores = max(ci["omp_threads"] or 0, ci["blas_threads"] or 0) or os.cpu_count()
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "freq-points/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_point * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
             "data": "synthetic (structured meander mesh built from the reference's element recipe)",
-            "config": {"workload": WORKLOAD, "sample": "1 sweep point per step (fill+LU+solve+projection), "
-                                                       "J/K pass amortised over 101 points",
-                       "l2": "working set > L2 (host run)"},
+            "config": dict(CONFIG),
             "cpu_baseline": {"value": value, "unit": "freq-points/s", "cores": cores, "kind": "port",
-                             "sample": f"{args.steps} points of the sweep + one J/K pass ({t_jk:.1f} s)"},
+                             "sample": f"1 sweep point per step (fill+LU+solve+projection), {args.steps} points, "
+                                       f"+ one J/K pass ({t_jk:.1f} s) amortised over {NFREQ} points", **ci},
             "e2e": {"value": value, "unit": "freq-points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -198,11 +235,13 @@ def cpu_baseline_sample(case):
     t_jk = time.perf_counter() - t0
     oracle.prime_jk_cache(sheet, jk)
     t1 = time.perf_counter()
-    oracle.partial_dS(sheet, rwg, pt.layers[i1 - 1:i2], s, pt.k0, u, io)
+    dS_ref, _, _ = oracle.partial_dS(sheet, rwg, pt.layers[i1 - 1:i2], s, pt.k0, u, io)
     t_pt = time.perf_counter() - t1
-    return {"value": 1.0 / (t_pt + t_jk / NFREQ), "unit": "freq-points/s", "cores": os.cpu_count(),
+    ci = cpu_info()
+    cores = max(ci["omp_threads"] or 0, ci["blas_threads"] or 0) or os.cpu_count()
+    return {"value": 1.0 / (t_pt + t_jk / NFREQ), "unit": "freq-points/s", "cores": cores,
             "kind": "port", "sample": f"1 sweep point (fill+LU+solve+projection {t_pt:.2f} s) + J/K pass "
-                                      f"({t_jk:.1f} s) amortised over {NFREQ} points"}
+                                      f"({t_jk:.1f} s) amortised over {NFREQ} points", **ci}, NFREQ // 2, dS_ref
 
 
 def run_rings(args, rank):
@@ -242,41 +281,78 @@ def run_rings(args, rank):
     print(json.dumps(line), flush=True)
 
 
-def run_grads(args, rank):
-    """Gradients/s of Σ_f (|S21_TE|² − |S21_TM|²) in trace width, pitch and substrate eps_r of
-    the meanderline at ntri = 4000 (N ≈ 6000) over 201 frequencies 8-18 GHz: one FP32 +
-    refinement factorisation per point, the six perturbed sets through the same factors
-    (pss_partial_gsms_lin).  Wall-clock per gradient, device synchronised on both sides."""
-    if rank != 0:
-        return
-    import torch
-    torch.cuda.set_device(0)
-    load_package()
+def grads_sample(npts=None, warmup=1, steps=1, precision="fp32r"):
+    """Adjoint gradient of Σ_f (|S21_TE|² − |S21_TM|²) in trace width, pitch and substrate
+    eps_r of the meanderline at ntri = 4000 (3960 faces, N = 5610) over 201 frequencies
+    8-18 GHz: per point one FP32 + refinement factorisation, forward and transposed solves on
+    it, and per perturbed set (+/- step of each parameter) a fused assemble-and-contract pass
+    (pss_partial_gsms_adj).  Wall clock per gradient, host planning included, device
+    synchronised on both sides.  Returns (seconds per gradient, objective, gradient)."""
     import functools
+    import torch
+    load_package()
     from pssfss_b200 import engine, workloads
     from pssfss_b200.gradient import meander_linearized_gradient
     params, flist, ntri = workloads.meander_gradient_workload()
-    if args.grad_npts:
-        flist = flist[:args.grad_npts]
-    part = functools.partial(engine.partial_gsms_linearized, precision="fp32r")
-    for _ in range(args.warmup):
+    if npts:
+        flist = flist[:npts]
+    part = functools.partial(engine.partial_gsms_adjoint, precision=precision)
+    for _ in range(warmup):
         meander_linearized_gradient(params, flist, part, ntri=ntri)
     times = []
-    for _ in range(args.steps):
+    for _ in range(steps):
         torch.cuda.synchronize()
         t = time.perf_counter()
         f, g = meander_linearized_gradient(params, flist, part, ntri=ntri)
         torch.cuda.synchronize()
         times.append(time.perf_counter() - t)
-    sec = statistics.mean(times)
-    line = {"metric": "grads/s (one-factorisation central-difference gradient)", "value": 1.0 / sec,
+    return statistics.mean(times), float(f), {k: float(v) for k, v in g.items()}, len(flist), ntri
+
+
+def run_grads(args, rank):
+    """The adjoint gradient alone (grads/s), one line."""
+    if rank != 0:
+        return
+    import torch
+    torch.cuda.set_device(0)
+    sec, f, g, nf, ntri = grads_sample(args.grad_npts or None, args.warmup, args.steps)
+    line = {"metric": "grads/s (adjoint gradient of the meanderline sweep objective)", "value": 1.0 / sec,
             "unit": "grads/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64+c128-refine",
             "data": "synthetic (structured meander mesh built from the reference's element recipe)",
-            "config": {"workload": f"meanderline w=0.3 a=5 mm ntri={ntri} on 1 mm eps_r=2.2, "
-                                   f"{len(flist)} freqs 8-18 GHz, d/d(w, a, eps_r)", "objective": float(f),
-                       "gradient": {k: float(v) for k, v in g.items()}}}
+            "config": {"workload": f"meanderline w=0.3 a=5 mm ntri={ntri} on 1 mm eps_r=2.2, {nf} freqs 8-18 GHz, "
+                                   "d/d(w, a, eps_r)", "objective": f, "gradient": g}}
     print(json.dumps(line), flush=True)
+
+
+def target_sweep(fp64_steps=1):
+    """The 6000-unknown sweep (meanderline ntri = 4000, N = 5610, 201 frequencies, normal
+    incidence): points/s of the FP32 + refinement form and of the plain FP64 form (device span
+    of the library, face integrals once per sweep), their ratio and max|dS| between them."""
+    from pssfss_b200 import engine
+    case = build_case(0, ntri=4000, nfreq=201)
+    call = (case["sheet"], case["rwg"], case["plan"].points, case["rng"], case["s"], case["u"], case["ios"])
+    npts = len(case["plan"].points)
+
+    def sweep(prec):
+        engine.clear_face_integrals(case["sheet"], case["rwg"])
+        st = {}
+        dS = engine.partial_gsms(*call, precision=prec, stats=st)
+        return dS, st["timings_ms"]["total"], st["status"]
+
+    sweep("fp32r")  # warm-up: buffers sized, kernels loaded
+    d32, t32, s32 = sweep("fp32r")
+    t64s = []
+    for _ in range(max(1, fp64_steps)):
+        d64, t64, _ = sweep("fp64")
+        t64s.append(t64)
+    t64 = statistics.mean(t64s)
+    return {"workload": "meanderline a=5 b=10 h=6 w1=w2=0.3 mm ntri=4000 (3960 faces, N=%d) on 1 mm eps_r=2.2, "
+                        "normal incidence, 201 freqs 8-18 GHz" % case["rwg"].nbf,
+            "fp32r_value": npts / (t32 / 1e3), "fp64_value": npts / (t64 / 1e3), "unit": "freq-points/s",
+            "fp32r_speedup_vs_fp64": t64 / t32,
+            "max_abs_dS_fp32r_vs_fp64": float(max(np.max(np.abs(a - b)) for a, b in zip(d32, d64))),
+            "refine_fallbacks": int(sum(1 for x in s32 if x & 32))}
 
 
 def main():
@@ -295,6 +371,8 @@ def main():
                     help="frequencies of the gradient workload (default: all 201)")
     ap.add_argument("--rings", action="store_true",
                     help="time the seeded batch of 64 ring problems of differing size instead")
+    ap.add_argument("--no-targets", action="store_true",
+                    help="skip the 6000-unknown target sweep and the gradient (profiling runs)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -322,6 +400,8 @@ def main():
     call_args = (case["sheet"], case["rwg"], case["plan"].points, case["rng"], case["s"], case["u"], case["ios"])
 
     def step(precision):
+        # face-pair integrals once per sweep, as the CPU arm pays them
+        engine.clear_face_integrals(case["sheet"], case["rwg"], dev)
         st = {}
         dS = engine.partial_gsms(*call_args, precision=precision, device=dev, stats=st)
         return dS, st
@@ -388,9 +468,8 @@ def main():
                 "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "c64+c128-refine",
                 "data": "synthetic (structured meander mesh built from the reference's element recipe)",
-                "config": {"workload": WORKLOAD, "points_per_step": npts, "precision": "fp32r",
-                           "l2": "working set > L2 (Z is 253 MB FP64 + 126 MB FP32 per point)",
-                           "parallelism": f"weak x{world}: independent sweeps per GPU"},
+                "config": dict(CONFIG, points_per_sweep=npts),
+                "precision": "fp32r", "parallelism": f"weak x{world}: independent sweeps per GPU",
                 "fp64_value": fp64_value, "fp32r_speedup_vs_fp64": value / fp64_value / world * world,
                 "max_abs_dS_fp32r_vs_fp64": max_dS,
                 "refine_fallbacks": int(sum(1 for s in statuses if s & 32)),
@@ -430,9 +509,29 @@ def main():
             line["roofline"] = None
         if not args.no_cpu_baseline:
             try:
-                line["cpu_baseline"] = cpu_baseline_sample(case)
+                cb, ip, dref = cpu_baseline_sample(case)
+                line["cpu_baseline"] = cb
+                if ip < len(dS32):
+                    # the FP64 oracle's dS at that point against both device forms
+                    line["max_abs_dS_fp32r_vs_oracle"] = float(np.max(np.abs(dS32[ip] - dref)))
+                    line["max_rel_dS_fp64_vs_oracle"] = float(np.max(np.abs(dS64[ip] - dref)) / np.max(np.abs(dref)))
+                    line["oracle_check_point_ghz"] = float(case["plan"].points[ip].fghz)
             except Exception as e:  # report, never fake
                 line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+        if world == 1 and not args.no_targets:
+            try:
+                line["target_sweep"] = target_sweep(args.fp64_steps)
+            except Exception as e:
+                line["target_sweep"] = {"error": str(e)[:200]}
+            try:
+                sec, f, g, nf, ntri = grads_sample()
+                line["grads"] = {"value": 1.0 / sec, "unit": "grads/s", "ms_per_grad": sec * 1e3,
+                                 "workload": f"meanderline ntri={ntri} (N=5610), {nf} freqs, adjoint "
+                                             "d/d(w, a, eps_r) of sum_f |S21_TE|^2 - |S21_TM|^2, FP32 + refinement",
+                                 "objective": f, "gradient": g, "timed": "1 gradient after 1 warm-up, host "
+                                 "planning included"}
+            except Exception as e:
+                line["grads"] = {"error": str(e)[:200]}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

@@ -71,6 +71,10 @@ int pss_sheet_create(pss_ctx *ctx, char cls, double units_per_meter, const doubl
                      int64_t nbf, const int64_t *bff, const int64_t *ebf, const int64_t *eci, int64_t nufp,
                      const int64_t *ufpm, const int64_t *ufp_rep, pss_sheet **out);
 int pss_sheet_destroy(pss_sheet *sheet);
+/* Drop the sheet's cached face-pair integrals (the RWGSheet J/K fields, Sheets.jl:35-47), so
+ * the next call recomputes them as the reference does when its cache key changes
+ * (FillZY.jl:97-99); for a caller that edits geometry in place, or times whole sweeps. */
+int pss_sheet_clear_cache(pss_sheet *sheet);
 
 /* Scattered part of the sheet's partial GSM at npts points.
  * Region layers: nl layers, eps/mu complex (2*nl doubles), width in metres; s = 1-based

@@ -585,6 +585,12 @@ int pss_sheet_destroy(pss_sheet *sh) {
   return 0;
 }
 
+int pss_sheet_clear_cache(pss_sheet *sh) {
+  if (!sh) { pss_set_error("null argument"); return -1; }
+  sh->jk_valid = false;
+  return 0;
+}
+
 int pss_partial_gsms(pss_sheet *sh, int nl, const double *eps, const double *mu, const double *width, int s,
                      double u, int npts, const double *k0, const double *psi, int nmodes, const double *kvec,
                      const double *src, const double *tobs, const double *wobs, int precision, double *dS,

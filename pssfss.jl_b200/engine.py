@@ -45,6 +45,7 @@ SIGNATURES = {
     "pss_sheet_create": (_I, [_P, _C, _D, _P, _P, _P, _P, _L, _P, _L, _P, _P, _P, _L, _L, _P, _P, _P, _L,
                               _P, _P, _P]),
     "pss_sheet_destroy": (_I, [_P]),
+    "pss_sheet_clear_cache": (_I, [_P]),
     "pss_partial_gsms": (_I, [_P, _I, _P, _P, _P, _I, _D, _I, _P, _P, _I, _P, _P, _P, _P, _I, _P, _P]),
     "pss_partial_gsms_lin": (_I, [_P, _I, _P, _P, _P, _I, _D, _I, _P, _P, _I, _P, _P, _P, _P, _I, _P, _P, _P,
                                   _P, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P]),
@@ -191,6 +192,11 @@ def device_sheet(sheet, rwg, device=0, nworkers=None):
             evicted.append(_sheets.popitem(last=False)[1])
     del evicted  # pss_sheet_destroy runs here, outside the lock
     return ds
+
+
+def clear_face_integrals(sheet, rwg, device=0, nworkers=None):
+    """Drop the uploaded sheet's cached face-pair integrals (``pss_sheet_clear_cache``)."""
+    _check(lib().pss_sheet_clear_cache(device_sheet(sheet, rwg, device, nworkers).h), "pss_sheet_clear_cache")
 
 
 def partial_gsms(sheet, rwg, points, region_rng, s, u, ios, precision="fp64", device=0, stats=None,

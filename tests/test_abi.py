@@ -55,6 +55,9 @@ def test_entry_points_reject_bad_arguments_before_any_device_use():
         return L.pss_last_error().decode()
 
     assert L.pss_ctx_destroy(nul) == 0 and L.pss_sheet_destroy(nul) == 0
+    assert L.pss_sheet_clear_cache(nul) == -1 and "null" in err()
+    assert L.pss_partial_gsms_adj(nul, 1, buf, buf, buf, 1, 1.0, 1, buf, buf, 1, buf, buf, buf, buf, 0, nul,
+                                  *([nul] * 9), 0, buf, nul, ibuf) == -1 and "null" in err()
     assert L.pss_partial_gsms(nul, 1, buf, buf, buf, 1, 1.0, 1, buf, buf, 1, buf, buf, buf, buf, 0,
                               buf, ibuf) == -1 and "null" in err()
     assert L.pss_partial_gsms_lin(nul, 1, buf, buf, buf, 1, 1.0, 1, buf, buf, 1, buf, buf, buf, buf, 0, nul,
