@@ -246,39 +246,63 @@ def cpu_baseline_sample(case):
 
 def run_rings(args, rank):
     """Freq-points/s over the seeded batch of 64 ring problems (period 6-12 mm, 300-3000
-    triangles, theta in {0, 15, 30, 45}, 21 frequencies each), FP32 + refinement through
-    ``analyze``, one sweep call per problem.  Wall-clock per pass over the batch, device
-    synchronised on both sides."""
+    triangles, so unknown counts 480-4080; theta in {0, 15, 30, 45}; 21 frequencies each;
+    1344 points), FP32 + refinement, all 64 problems in ONE library call
+    (analyze.analyze_many -> pss_partial_gsms_multi: a shared work list of like-N batches,
+    largest first) with the batch size and LU tile shape of the stored autotuning table.
+    value = points / device span of that call; e2e = points / wall clock of analyze_many
+    (host planning, transfers and the cascade included), device synchronised on both sides."""
     if rank != 0:
         return
     import torch
     torch.cuda.set_device(0)
     load_package()
-    from pssfss_b200 import workloads
-    from pssfss_b200.analyze import analyze
+    from pssfss_b200 import autotune, workloads
+    from pssfss_b200.analyze import analyze_many
     batch = workloads.ring_batch()
     npts = sum(len(f) for _, f, _ in batch)
-
-    def one_pass():
-        for strata, flist, steer in batch:
-            analyze(strata, flist, steer, precision="fp32r")
+    tuned = os.path.exists(autotune.TABLE) and not args.no_tuning
+    tuning = autotune.lookup if tuned else None
     for _ in range(args.warmup):
-        one_pass()
-    times = []
+        analyze_many(batch, precision="fp32r", tuning=tuning)
+    walls, spans = [], []
     for _ in range(args.steps):
+        st = {}
         torch.cuda.synchronize()
         t = time.perf_counter()
-        one_pass()
+        analyze_many(batch, precision="fp32r", tuning=tuning, stats=st)
         torch.cuda.synchronize()
-        times.append(time.perf_counter() - t)
-    sec = statistics.mean(times)
-    line = {"metric": "freq-points/sec over a batch of ring problems of differing size", "value": npts / sec,
-            "unit": "freq-points/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64+c128-refine",
-            "data": "synthetic (seeded ring problems, structured meshes)",
-            "config": {"workload": f"64 ring problems, {npts} points, N {min(b[0][1].nface for b in batch)}.."
-                                   f"{max(b[0][1].nface for b in batch)} faces, host time included"}}
+        walls.append(time.perf_counter() - t)
+        spans.append(st["timings_ms"]["total"] / 1e3)
+    line = {"metric": "freq-points/sec over a batch of ring problems of differing size", "value": npts / statistics.mean(spans),
+            "unit": "freq-points/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": statistics.mean(spans) * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c64+c128-refine",
+            "data": "synthetic (seeded ring problems, own structured meshes)",
+            "e2e": {"value": npts / statistics.mean(walls), "unit": "freq-points/s",
+                    "note": "wall clock of analyze_many: host planning, transfers, cascade included"},
+            "config": {"workload": f"64 ring problems (seed 0), {npts} points, N "
+                                   f"{min(b[0][1].nface for b in batch)}..{max(b[0][1].nface for b in batch)} faces, "
+                                   "one pss_partial_gsms_multi call",
+                       "tuning": autotune.TABLE.split(os.sep + "pssfss.jl_b200" + os.sep)[-1] if tuned else "defaults",
+                       "table": [{k: b[k] for k in ("nmax", "n", "batch", "panel_w", "outer_nb")}
+                                 for b in (json.load(open(autotune.TABLE))["buckets"] if tuned else [])]}}
     print(json.dumps(line), flush=True)
+
+
+def run_autotune(args, rank):
+    """Search the batch size and LU tile shape per unknown-count bucket and store the table."""
+    if rank != 0:
+        return
+    import torch
+    torch.cuda.set_device(0)
+    load_package()
+    from pssfss_b200 import autotune
+    tab = autotune.tune()
+    print(json.dumps({"autotune": autotune.TABLE, "buckets": [{k: b[k] for k in ("nmax", "n", "batch", "panel_w",
+                                                                                   "outer_nb", "ms_per_point",
+                                                                                   "default_ms_per_point")}
+                                                               for b in tab["buckets"]]}), flush=True)
 
 
 def grads_sample(npts=None, warmup=1, steps=1, precision="fp32r"):
@@ -373,6 +397,9 @@ def main():
                     help="time the seeded batch of 64 ring problems of differing size instead")
     ap.add_argument("--no-targets", action="store_true",
                     help="skip the 6000-unknown target sweep and the gradient (profiling runs)")
+    ap.add_argument("--no-tuning", action="store_true", help="--rings with the library defaults")
+    ap.add_argument("--autotune", action="store_true",
+                    help="search batch size and LU tile shape per unknown count; write the table")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -383,6 +410,8 @@ def main():
         return run_grads(args, rank)
     if args.rings:
         return run_rings(args, rank)
+    if args.autotune:
+        return run_autotune(args, rank)
 
     import torch
     dist = None

@@ -91,6 +91,35 @@ int pss_partial_gsms(pss_sheet *sheet, int nl, const double *eps, const double *
                      const double *kvec, const double *src, const double *tobs, const double *wobs,
                      int precision, double *dS, int *status);
 
+/* One problem of pss_partial_gsms_multi: the arguments of pss_partial_gsms for one sheet,
+ * plus the batch size (points factored together; 0: the context's default, PSS_BATCH) and
+ * the FP32 LU tile shape (panel_w 8, 16 or 32 columns per cluster panel, outer_nb 64 or 128
+ * columns per outer block = the tensor-core update's depth; 0: 32 and 128), as an
+ * autotuner picks them per unknown count. */
+typedef struct pss_problem {
+  pss_sheet *sheet;
+  int nl;
+  const double *eps, *mu, *width;
+  int s;
+  double u;
+  int npts;
+  const double *k0, *psi;
+  int nmodes;
+  const double *kvec, *src, *tobs, *wobs;
+  int batch, panel_w, outer_nb;
+  double *dS;
+  int *status;
+} pss_problem;
+
+/* Many sweeps in one call - problems on sheets of different unknown counts (and layers,
+ * steering, modes), all of one context.  The scattered partial GSMs of every point of every
+ * problem, as pss_partial_gsms gives them, computed from one shared work list: every point's
+ * modal tables first, then batches of like-N points (one problem each, the largest matrices
+ * first) taken by the context's worker streams, so no stream idles between problems.
+ * Replaces the loop of _analyze over sheets and steering (src/PSSFSS.jl:230-329) when many
+ * problems are swept together. */
+int pss_partial_gsms_multi(int nprob, const pss_problem *problems, int precision);
+
 /* Linearised partial GSMs for gradients with one factorisation per point (no counterpart in
  * the reference, which has no gradients).  The unperturbed inputs are those of
  * pss_partial_gsms.  For each of npert perturbed input sets k (a sheet psheets[k] of the same

@@ -435,3 +435,33 @@ def analyze(strata, flist, steering, *, precision="fp64", device=0, outlist=(),
     write_outlist(results, outlist, resultfile)
     log.finish()
     return results
+
+
+def analyze_many(cases, *, precision="fp32r", device=0, tuning=None, stats=None):
+    """Many independent analyses in one device call (``pss_partial_gsms_multi``).
+
+    ``cases``: list of ``(strata, flist, steering)`` as ``analyze`` takes them.  Every sheet
+    sweep of every case goes into one shared work list on the device - batches of like-N
+    points, largest matrices first - instead of one library call per sheet and case.
+    ``tuning``: a callable ``n -> dict(batch=, panel_w=, outer_nb=)`` choosing the batch size
+    and the FP32 LU tile shape per unknown count (``autotune.lookup`` reads the stored
+    table); ``None`` keeps the library defaults.  Returns one list of ``Result`` per case."""
+    from . import engine
+    plans, jobs, problems = [], [], []
+    for strata, flist, steering in cases:
+        plan = make_plan(strata, flist, steering)
+        plans.append(plan)
+        for ig, (i1, i2), isht, s in sheet_gblocks(plan):
+            sheet, rwg = plan.sheets[isht - 1], plan.rwgdat[isht - 1]
+            ios = [sheet_io(pt.layers[i1 - 1:i2], sheet, s, pt.k0, pt.beta00) for pt in plan.points]
+            pr = dict(sheet=sheet, rwg=rwg, points=plan.points, region_rng=(i1, i2), s=s, u=plan.uvec[isht - 1],
+                      ios=ios)
+            if tuning is not None:
+                pr.update(tuning(rwg.nbf))
+            jobs.append((len(plans) - 1, ig, ios))
+            problems.append(pr)
+    out = engine.partial_gsms_multi(problems, precision=precision, device=device, stats=stats) if problems else []
+    partial = [dict() for _ in plans]
+    for (c, ig, ios), dS in zip(jobs, out):
+        partial[c][ig] = [add_scattered(io, d) for io, d in zip(ios, dS)]
+    return [assemble(plan, partial[c]) for c, plan in enumerate(plans)]

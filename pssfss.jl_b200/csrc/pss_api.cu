@@ -137,14 +137,14 @@ struct Worker {
   }
   // LU of the worker's first nb matrices (FP64 in z64, or FP32 planes zr/zi) and solves
   // rhs -> X, refined against z64 in FP32 mode.  Status bits go to status[0..nb) (device).
-  int factor_solve(int n, int nb, int prec, int nrhs, int maxit, int *status) {
+  int factor_solve(int n, int nb, int prec, int nrhs, int maxit, int *status, int panel_w = 0, int outer_nb = 0) {
     int rc;
     const long long ld = n, ms = (long long)n * n, vs = (long long)n * nrhs;
     if (prec == PSS_FP64)
       rc = pss_lu64_batched(n, nb, z64.as<cd>(), ld, ms, ipiv.as<int>(), info.as<int>(), luws.p, luws.n, st);
     else
       rc = pss_lu32_batched(n, nb, zr.as<float>(), zi.as<float>(), ld, ms, ipiv.as<int>(), info.as<int>(), luws.p,
-                            luws.n, st);
+                            luws.n, st, panel_w, outer_nb);
     if (rc) return rc;
     pss_count_launch();
     k_info_to_status<<<1, 32, 0, st>>>(nb, info.as<int>(), status);
@@ -309,7 +309,7 @@ void make_params(int magnetic, const StackParams &S, const double b1m[2], const 
 // Tables of npts points (params already on the device at dP).  Fills tabs[i] and ORs
 // PSS_ST_TABLE_NOCONV into hstatus[i].  Synchronises the ctx's first stream.
 int build_tables(pss_ctx *c, const StackParams &S, const PointParams *dP, int npts, double convtest,
-                 std::vector<TableDev> &tabs, std::vector<int> &hstatus) {
+                 std::vector<TableDev> &tabs, std::vector<int> &hstatus, int base = 0) {
   cudaStream_t st = c->w[0].st;
   const int R0 = kRing0;
   const size_t W0 = 2 * (size_t)R0 + 1;
@@ -320,9 +320,12 @@ int build_tables(pss_ctx *c, const StackParams &S, const PointParams *dP, int np
   if (c->conv.ensure((size_t)chunk * (R0 + 1) + 64)) return -3;
   if (c->mm.ensure(2 * sizeof(int) * (size_t)chunk + 64)) return -3;
   if (c->stage.ensure(2 * (size_t)(2 * R0) * (2 * R0) * sizeof(cd))) return -3;
-  if (c->tables.ensure((size_t)npts * 2 * cap0 * sizeof(cd))) return -3;
-  c->bigtables.resize(npts);
-  tabs.assign(npts, TableDev{});
+  // points base .. base+npts-1 of the call; a multi-problem call sizes the table store for
+  // all its points before the first problem, so this never reallocates under earlier tables
+  if (c->tables.ensure((size_t)(base + npts) * 2 * cap0 * sizeof(cd))) return -3;
+  if ((int)c->bigtables.size() < base + npts) c->bigtables.resize(base + npts);
+  if ((int)tabs.size() < base + npts) tabs.resize(base + npts, TableDev{});
+  if ((int)hstatus.size() < base + npts) hstatus.resize(base + npts, 0);
   std::vector<int> hm(2 * chunk);
   for (int c0 = 0; c0 < npts; c0 += chunk) {
     const int nc = std::min(chunk, npts - c0);
@@ -333,7 +336,7 @@ int build_tables(pss_ctx *c, const StackParams &S, const PointParams *dP, int np
     PSS_CUDA_TRY(cudaMemcpyAsync(hm.data(), dmm, 2 * chunk * sizeof(int), cudaMemcpyDeviceToHost, st));
     PSS_CUDA_TRY(cudaStreamSynchronize(st));
     for (int q = 0; q < nc; ++q) {
-      const int i = c0 + q;
+      const int il = c0 + q, i = base + il;  // local (params) and global (storage) index
       int mmax = hm[q], flag = hm[chunk + q];
       if (flag == 2) {
         // rings beyond the first budget: full-size pass for this point only
@@ -341,8 +344,8 @@ int build_tables(pss_ctx *c, const StackParams &S, const PointParams *dP, int np
         const size_t W1 = 2 * (size_t)R1 + 1;
         if (c->bigdense.ensure(2 * W1 * W1 * sizeof(cd))) return -3;
         if (c->conv.ensure((size_t)(R1 + 1) + 64)) return -3;
-        pss_tables_ring_fill(S, dP + i, 1, R1, c->bigdense.as<cd>(), 0, st);
-        pss_tables_ring_sums(dP + i, 1, R1, c->bigdense.as<cd>(), 0, convtest, c->conv.as<unsigned char>(), st);
+        pss_tables_ring_fill(S, dP + il, 1, R1, c->bigdense.as<cd>(), 0, st);
+        pss_tables_ring_sums(dP + il, 1, R1, c->bigdense.as<cd>(), 0, convtest, c->conv.as<unsigned char>(), st);
         pss_tables_find_mmax(1, R1, c->conv.as<unsigned char>(), dmm, dmm + 1, st);
         int h2[2];
         PSS_CUDA_TRY(cudaMemcpyAsync(h2, dmm, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -355,7 +358,7 @@ int build_tables(pss_ctx *c, const StackParams &S, const PointParams *dP, int np
         tabs[i].t1 = c->bigtables[i].as<cd>();
         tabs[i].t2 = tabs[i].t1 + cap;
         tabs[i].mmax = mmax;
-        int rc = pss_tables_finish(c->bigdense.as<cd>(), R1, mmax, dP + i, c->stage.as<cd>(), tabs[i].t1,
+        int rc = pss_tables_finish(c->bigdense.as<cd>(), R1, mmax, dP + il, c->stage.as<cd>(), tabs[i].t1,
                                    tabs[i].t2, st);
         if (rc) return rc;
         continue;
@@ -364,7 +367,7 @@ int build_tables(pss_ctx *c, const StackParams &S, const PointParams *dP, int np
       tabs[i].t1 = c->tables.as<cd>() + (size_t)i * 2 * cap0;
       tabs[i].t2 = tabs[i].t1 + cap0;
       tabs[i].mmax = mmax;
-      int rc = pss_tables_finish(c->dense.as<cd>() + (size_t)q * pstride, R0, mmax, dP + i, c->stage.as<cd>(),
+      int rc = pss_tables_finish(c->dense.as<cd>() + (size_t)q * pstride, R0, mmax, dP + il, c->stage.as<cd>(),
                                  tabs[i].t1, tabs[i].t2, st);
       if (rc) return rc;
     }
@@ -397,9 +400,9 @@ int refresh_jk_cache(pss_sheet *sh, double psi1, double psi2, double ulocal, cud
   return 0;
 }
 
-int ensure_worker(Worker &w, const pss_sheet *sh, int nm, int precision, bool own_jk, int nb) {
-  const size_t n = sh->nbf;
-  if (w.zb.ensure((size_t)sh->nufp * 9 * sizeof(cd))) return -3;
+int ensure_worker_dims(Worker &w, int nufp, int nbf, int nm, int precision, bool own_jk, int nb) {
+  const size_t n = nbf;
+  if (w.zb.ensure((size_t)nufp * 9 * sizeof(cd))) return -3;
   if (w.z64.ensure((size_t)nb * n * n * sizeof(cd))) return -3;
   if (precision == PSS_FP32_REFINE) {
     if (w.zr.ensure((size_t)nb * n * n * sizeof(float)) || w.zi.ensure((size_t)nb * n * n * sizeof(float))) return -3;
@@ -407,10 +410,14 @@ int ensure_worker(Worker &w, const pss_sheet *sh, int nm, int precision, bool ow
   if (w.nonconv.ensure(sizeof(int))) return -3;
   if (w.bf.ensure((size_t)nb * nm * n * 2 * sizeof(cd))) return -3;
   if (w.ensure_solver((int)n, nm, nb)) return -3;
-  if (own_jk && w.jk.ensure(sh->nufp)) return -3;
+  if (own_jk && w.jk.ensure(nufp)) return -3;
   PSS_CUDA_TRY(cudaMemsetAsync(w.info.p, 0, (size_t)nb * sizeof(int), w.st));
   PSS_CUDA_TRY(cudaMemsetAsync(w.nonconv.p, 0, sizeof(int), w.st));
   return 0;
+}
+
+int ensure_worker(Worker &w, const pss_sheet *sh, int nm, int precision, bool own_jk, int nb) {
+  return ensure_worker_dims(w, sh->nufp, sh->nbf, nm, precision, own_jk, nb);
 }
 
 }  // namespace
@@ -591,40 +598,97 @@ int pss_sheet_clear_cache(pss_sheet *sh) {
   return 0;
 }
 
-int pss_partial_gsms(pss_sheet *sh, int nl, const double *eps, const double *mu, const double *width, int s,
-                     double u, int npts, const double *k0, const double *psi, int nmodes, const double *kvec,
-                     const double *src, const double *tobs, const double *wobs, int precision, double *dS,
-                     int *status) {
-  if (!sh || !k0 || !psi || !dS || !status) { pss_set_error("null argument"); return -1; }
-  if (npts <= 0 || nmodes <= 0 || nmodes > 4096) { pss_set_error("invalid npts/nmodes"); return -1; }
+}  // extern "C"
+
+namespace {
+
+// One problem of a (multi-problem) sweep call: a sheet, its layer region and its points, with
+// the FP32 tile shape and batch size to use (0: defaults), plus what the call derives for it.
+struct Problem {
+  pss_sheet *sh = nullptr;
+  StackParams S{};
+  double u = 0;
+  int npts = 0, nm = 0;
+  const double *k0 = nullptr, *psi = nullptr, *kvec = nullptr, *src = nullptr, *tobs = nullptr, *wobs = nullptr;
+  double *dS = nullptr;
+  int *status = nullptr;
+  int batch = 0, panel_w = 0, outer_nb = 0;
+  // derived
+  int p0 = 0;                       // first global point index
+  size_t kb = 0, sb = 0, tb = 0, wb = 0, db = 0;  // bases in the mode and dS arrays (elements)
+  bool own_jk = false;              // face integrals per point (else the sheet's cache)
+};
+
+// Validate one problem's arguments and fill its StackParams.
+int check_problem(const pss_problem &q, int precision, Problem &P) {
+  if (!q.sheet || !q.k0 || !q.psi || !q.dS || !q.status || !q.kvec || !q.src || !q.tobs || !q.wobs || !q.eps ||
+      !q.mu || !q.width) {
+    pss_set_error("null argument");
+    return -1;
+  }
+  if (q.npts <= 0 || q.nmodes <= 0 || q.nmodes > 4096) { pss_set_error("invalid npts/nmodes"); return -1; }
   if (precision != PSS_FP64 && precision != PSS_FP32_REFINE) { pss_set_error("unknown precision %d", precision); return -1; }
-  if (!(u > 0)) { pss_set_error("smoothing parameter u must be positive"); return -1; }
-  pss_ctx *c = sh->ctx;
-  if (set_device(c)) return -3;
-  StackParams S;
-  if (make_stack(nl, eps, mu, width, s, S)) return -1;
-  const int magnetic = sh->cls == 'M';
-  const double b1m[2] = {sh->b1[0] * sh->upm, sh->b1[1] * sh->upm};
-  const double b2m[2] = {sh->b2[0] * sh->upm, sh->b2[1] * sh->upm};
-  std::vector<PointParams> hP(npts);
-  for (int i = 0; i < npts; ++i) {
-    if (!(k0[i] > 0) || !std::isfinite(psi[2 * i]) || !std::isfinite(psi[2 * i + 1])) {
+  if (!(q.u > 0)) { pss_set_error("smoothing parameter u must be positive"); return -1; }
+  if (q.batch < 0 || q.batch > kMaxBatch) { pss_set_error("batch %d outside 0..%d", q.batch, kMaxBatch); return -1; }
+  if (!(q.panel_w == 0 || q.panel_w == 8 || q.panel_w == 16 || q.panel_w == 32) ||
+      !(q.outer_nb == 0 || q.outer_nb == 64 || q.outer_nb == 128)) {
+    pss_set_error("tile shape: panel_w must be 0, 8, 16 or 32 and outer_nb 0, 64 or 128");
+    return -1;
+  }
+  if (make_stack(q.nl, q.eps, q.mu, q.width, q.s, P.S)) return -1;
+  for (int i = 0; i < q.npts; ++i)
+    if (!(q.k0[i] > 0) || !std::isfinite(q.psi[2 * i]) || !std::isfinite(q.psi[2 * i + 1])) {
       pss_set_error("invalid k0/psi at point %d", i);
       return -1;
     }
-    make_params(magnetic, S, b1m, b2m, u, k0[i], psi[2 * i], psi[2 * i + 1], hP[i]);
+  P.sh = q.sheet; P.u = q.u; P.npts = q.npts; P.nm = q.nmodes;
+  P.k0 = q.k0; P.psi = q.psi; P.kvec = q.kvec; P.src = q.src; P.tobs = q.tobs; P.wobs = q.wobs;
+  P.dS = q.dS; P.status = q.status;
+  P.batch = q.batch; P.panel_w = q.panel_w; P.outer_nb = q.outer_nb;
+  return 0;
+}
+
+// The sweep of every problem on one context: tables of all points, then a shared work list of
+// (problem, batch of like-N points) items, largest matrices first, taken by one host thread
+// per worker stream; each item runs fill -> batched LU -> solves (+ refinement) -> projection
+// on its worker.  FP32 points whose refinement stalls are redone in FP64; then dS and status
+// go back to each problem's caller arrays.
+int sweep_impl(pss_ctx *c, std::vector<Problem> &PR, int precision) {
+  if (set_device(c)) return -3;
+  // global point numbering, mode-array bases, parameters
+  int total = 0;
+  size_t nk = 0, ns = 0, nt = 0, nw = 0, nd = 0;
+  for (auto &P : PR) {
+    if (P.sh->ctx != c) { pss_set_error("every sheet of a call must belong to the same context"); return -1; }
+    P.p0 = total;
+    P.kb = nk; P.sb = ns; P.tb = nt; P.wb = nw; P.db = nd;
+    const size_t nmp = (size_t)P.npts * P.nm;
+    nk += nmp * 2; ns += nmp * 2; nt += nmp * 2; nw += nmp; nd += (size_t)P.npts * P.nm * P.nm;
+    total += P.npts;
+  }
+  std::vector<PointParams> hP(total);
+  for (auto &P : PR) {
+    const pss_sheet *sh = P.sh;
+    const double b1m[2] = {sh->b1[0] * sh->upm, sh->b1[1] * sh->upm};
+    const double b2m[2] = {sh->b2[0] * sh->upm, sh->b2[1] * sh->upm};
+    for (int i = 0; i < P.npts; ++i)
+      make_params(sh->cls == 'M', P.S, b1m, b2m, P.u, P.k0[i], P.psi[2 * i], P.psi[2 * i + 1], hP[P.p0 + i]);
   }
   if (upload(c->params, hP.data(), hP.size())) return -3;
   const PointParams *dP = c->params.as<PointParams>();
-  // device-time span of the whole batch (start on worker 0; every worker joins it at the end)
   cudaEvent_t span0, span1;
   PSS_CUDA_TRY(cudaEventCreate(&span0));
   PSS_CUDA_TRY(cudaEventCreate(&span1));
   PSS_CUDA_TRY(cudaEventRecord(span0, c->w[0].st));
-  std::vector<int> hstatus(npts, 0);
-  std::vector<TableDev> tabs;
-  int rc = build_tables(c, S, dP, npts, 1e-7, tabs, hstatus);
-  if (rc) return rc;
+  // modal tables of every point (the table store is sized for all points first)
+  std::vector<int> hstatus(total, 0);
+  std::vector<TableDev> tabs(total);
+  {
+    const size_t cap0 = (size_t)(2 * kRing0 + 2) * (2 * kRing0 + 2);
+    if (c->tables.ensure((size_t)total * 2 * cap0 * sizeof(cd))) return -3;
+    for (auto &P : PR)
+      if (int rc = build_tables(c, P.S, dP + P.p0, P.npts, 1e-7, tabs, hstatus, P.p0)) return rc;
+  }
   float tables_ms = 0;
   {
     cudaEvent_t t;
@@ -634,46 +698,109 @@ int pss_partial_gsms(pss_sheet *sh, int nl, const double *eps, const double *mu,
     cudaEventElapsedTime(&tables_ms, span0, t);
     cudaEventDestroy(t);
   }
-
-  // mode data for all points
-  const size_t nmp = (size_t)npts * nmodes;
-  size_t off_k = 0, off_s = off_k + nmp * 2 * sizeof(double), off_t = off_s + nmp * 2 * sizeof(cd),
-         off_w = off_t + nmp * 2 * sizeof(double), tot = off_w + nmp * sizeof(cd);
+  // mode data of every point of every problem
+  const size_t off_k = 0, off_s = off_k + nk * sizeof(double), off_t = off_s + ns * sizeof(cd),
+               off_w = off_t + nt * sizeof(double), tot = off_w + nw * sizeof(cd);
   if (c->modes.ensure(tot)) return -3;
   char *mb = c->modes.as<char>();
-  PSS_CUDA_TRY(cudaMemcpy(mb + off_k, kvec, nmp * 2 * sizeof(double), cudaMemcpyHostToDevice));
-  PSS_CUDA_TRY(cudaMemcpy(mb + off_s, src, nmp * 2 * sizeof(cd), cudaMemcpyHostToDevice));
-  PSS_CUDA_TRY(cudaMemcpy(mb + off_t, tobs, nmp * 2 * sizeof(double), cudaMemcpyHostToDevice));
-  PSS_CUDA_TRY(cudaMemcpy(mb + off_w, wobs, nmp * sizeof(cd), cudaMemcpyHostToDevice));
-  const size_t nm2 = (size_t)nmodes * nmodes;
-  if (c->dS.ensure((size_t)npts * nm2 * sizeof(cd)) || c->status.ensure((size_t)npts * sizeof(int))) return -3;
-  PSS_CUDA_TRY(cudaMemset(c->status.p, 0, (size_t)npts * sizeof(int)));
+  const double *dkv = (const double *)(mb + off_k), *dtob = (const double *)(mb + off_t);
+  const cd *dsrc = (const cd *)(mb + off_s), *dwob = (const cd *)(mb + off_w);
+  for (auto &P : PR) {
+    const size_t nmp = (size_t)P.npts * P.nm;
+    PSS_CUDA_TRY(cudaMemcpy(mb + off_k + P.kb * sizeof(double), P.kvec, nmp * 2 * sizeof(double), cudaMemcpyHostToDevice));
+    PSS_CUDA_TRY(cudaMemcpy(mb + off_s + P.sb * sizeof(cd), P.src, nmp * 2 * sizeof(cd), cudaMemcpyHostToDevice));
+    PSS_CUDA_TRY(cudaMemcpy(mb + off_t + P.tb * sizeof(double), P.tobs, nmp * 2 * sizeof(double), cudaMemcpyHostToDevice));
+    PSS_CUDA_TRY(cudaMemcpy(mb + off_w + P.wb * sizeof(cd), P.wobs, nmp * sizeof(cd), cudaMemcpyHostToDevice));
+  }
+  if (c->dS.ensure(std::max<size_t>(nd, 1) * sizeof(cd)) || c->status.ensure((size_t)total * sizeof(int))) return -3;
+  PSS_CUDA_TRY(cudaMemset(c->status.p, 0, (size_t)total * sizeof(int)));
   int *dstatus = c->status.as<int>();
 
-  // J/K face-pair integrals: shared cache when every point has the same (ψ1, ψ2)
-  const double ulocal = u / sh->upm;
-  bool same_psi = true;
-  for (int i = 1; i < npts; ++i)
-    same_psi = same_psi && psi[2 * i] == psi[0] && psi[2 * i + 1] == psi[1];
-  if (same_psi) {
-    if ((rc = refresh_jk_cache(sh, psi[0], psi[1], ulocal, c->w[0].st))) return rc;
-    if (sh->jk_nonconv)
-      for (int i = 0; i < npts; ++i) hstatus[i] |= PSS_ST_JK_NOCONV;
+  // Face-pair integrals: a problem whose points share (ψ1, ψ2) uses its sheet's cache,
+  // refreshed here, unless another problem of the call needs the same sheet at another key
+  // (then both compute per point, like problems whose ψ varies).
+  {
+    std::vector<bool> same(PR.size());
+    for (size_t p = 0; p < PR.size(); ++p) {
+      const Problem &P = PR[p];
+      bool sp = true;
+      for (int i = 1; i < P.npts; ++i) sp = sp && P.psi[2 * i] == P.psi[0] && P.psi[2 * i + 1] == P.psi[1];
+      same[p] = sp;
+      PR[p].own_jk = !sp;
+    }
+    for (size_t p = 0; p < PR.size(); ++p)
+      for (size_t q = 0; q < PR.size(); ++q)
+        if (p != q && PR[p].sh == PR[q].sh && same[p] && same[q] &&
+            (PR[p].psi[0] != PR[q].psi[0] || PR[p].psi[1] != PR[q].psi[1] || PR[p].u != PR[q].u))
+          PR[p].own_jk = true;
+    for (auto &P : PR) {
+      if (P.own_jk) continue;
+      if (int rc = refresh_jk_cache(P.sh, P.psi[0], P.psi[1], P.u / P.sh->upm, c->w[0].st)) return rc;
+      if (P.sh->jk_nonconv)
+        for (int i = 0; i < P.npts; ++i) hstatus[P.p0 + i] |= PSS_ST_JK_NOCONV;
+    }
   }
-  const int nw = c->nworkers;
-  const int B = std::max(1, std::min(c->batch, npts));  // points factored together per worker
-  for (int k = 0; k < nw; ++k)
-    if ((rc = ensure_worker(c->w[k], sh, nmodes, precision, !same_psi, B))) return rc;
-
-  const int n = sh->nbf;
-  const long long ld = n, msz = (long long)n * n, vsz = (long long)n * nmodes;
+  // work list: batches of up to B points with the same unknown and mode counts - points of one
+  // problem, or of several problems whose sheets have the same N - largest matrices first
+  struct Item { int cnt; int p[kMaxBatch]; int i[kMaxBatch]; };
+  std::vector<Item> items;
+  {
+    std::vector<std::pair<int, int>> pts;  // (problem, point)
+    for (size_t p = 0; p < PR.size(); ++p)
+      for (int i = 0; i < PR[p].npts; ++i) pts.push_back({(int)p, i});
+    std::stable_sort(pts.begin(), pts.end(), [&](const std::pair<int, int> &a, const std::pair<int, int> &b) {
+      const Problem &A = PR[a.first], &Bq = PR[b.first];
+      if (A.sh->nbf != Bq.sh->nbf) return A.sh->nbf > Bq.sh->nbf;
+      return A.nm < Bq.nm;
+    });
+    for (size_t k = 0; k < pts.size();) {
+      const Problem &P = PR[pts[k].first];
+      const int B = std::max(1, std::min(P.batch > 0 ? P.batch : c->batch, kMaxBatch));
+      Item it{};
+      while (k < pts.size() && it.cnt < B && PR[pts[k].first].sh->nbf == P.sh->nbf && PR[pts[k].first].nm == P.nm &&
+             PR[pts[k].first].panel_w == P.panel_w && PR[pts[k].first].outer_nb == P.outer_nb) {
+        it.p[it.cnt] = pts[k].first;
+        it.i[it.cnt] = pts[k].second;
+        ++it.cnt;
+        ++k;
+      }
+      items.push_back(it);
+    }
+  }
+  // every worker sized once for the largest item of the call
+  const int nwk = c->nworkers;
+  {
+    int mufp = 0, mn = 0, mnm = 0, mB = 1;
+    bool ojk = false;
+    for (auto &it : items) {
+      for (int b = 0; b < it.cnt; ++b) {
+        const Problem &P = PR[it.p[b]];
+        mufp = std::max(mufp, P.sh->nufp); mn = std::max(mn, P.sh->nbf); mnm = std::max(mnm, P.nm);
+        ojk = ojk || P.own_jk;
+      }
+      mB = std::max(mB, it.cnt);
+    }
+    for (int k = 0; k < nwk; ++k)
+      if (int rc = ensure_worker_dims(c->w[k], mufp, mn, mnm, precision, ojk, mB)) return rc;
+  }
   std::vector<cudaEvent_t> ev;  // phase events of worker 0's batches (pushed by its thread only)
-  std::vector<KProf> kprofs(nw);
-  // A batch of cnt points (indices idx[0..cnt)) on worker w: per point face integrals (when
-  // ψ varies), fill into matrix slot b, basis transforms and right-hand sides; then one
-  // batched LU + solve (+ refinement) of all cnt matrices; then per point the projection.
-  auto run_batch = [&](const int *idx, int cnt, int prec, Worker &w, bool rec) -> int {
+  std::vector<KProf> kprofs(nwk);
+  // One batch: per point its problem's fill, transforms and right-hand sides into matrix slot
+  // b; one batched LU + solve (+ refinement) of all cnt matrices; per point the projection.
+  auto run_batch = [&](const Item &it, int prec, Worker &w, bool rec) -> int {
     cudaStream_t st = w.st;
+    const int cnt = it.cnt;
+    const Problem &P0 = PR[it.p[0]];
+    const int n = P0.sh->nbf, nm = P0.nm;
+    const long long ld = n, msz = (long long)n * n, vsz = (long long)n * nm;
+    const size_t nm2 = (size_t)nm * nm;
+    int mufp = 0;
+    bool ojk = false;
+    for (int b = 0; b < cnt; ++b) {
+      mufp = std::max(mufp, PR[it.p[b]].sh->nufp);
+      ojk = ojk || PR[it.p[b]].own_jk;
+    }
+    if (int rc = ensure_worker_dims(w, mufp, n, nm, prec, ojk, cnt)) return rc;
     cudaEvent_t e[8];
     if (rec) {
       for (int q = 0; q < 8; ++q) { cudaEventCreate(&e[q]); ev.push_back(e[q]); }
@@ -683,57 +810,60 @@ int pss_partial_gsms(pss_sheet *sh, int nl, const double *eps, const double *mu,
     float *zr = prec == PSS_FP32_REFINE ? w.zr.as<float>() : nullptr;
     float *zi = prec == PSS_FP32_REFINE ? w.zi.as<float>() : nullptr;
     for (int b = 0; b < cnt; ++b) {
-      const int i = idx[b];
-      const PointParams *Pi = dP + i;
+      const Problem &P = PR[it.p[b]];
+      pss_sheet *sh = P.sh;
+      const int i = it.i[b], g = P.p0 + i;
+      const PointParams *Pi = dP + g;
       JKDev jk;
-      if (same_psi) {
+      if (!P.own_jk) {
         jk = sh->cache.jk;
       } else {
         jk = w.jk.jk;
-        pss_filljk(sh->G, ulocal, psi[2 * i], psi[2 * i + 1], sh->s1, sh->s2, jk, w.nonconv.as<int>(), st);
+        pss_filljk(sh->G, P.u / sh->upm, P.psi[2 * i], P.psi[2 * i + 1], sh->s1, sh->s2, jk, w.nonconv.as<int>(), st);
         pss_count_launch();
-        k_nonconv_to_status<<<1, 1, 0, st>>>(w.nonconv.as<int>(), dstatus + i);
+        k_nonconv_to_status<<<1, 1, 0, st>>>(w.nonconv.as<int>(), dstatus + g);
       }
-      pss_fill_pairs(sh->G, Pi, jk, tabs[i].t1, tabs[i].t2, tabs[i].mmax, w.zb.as<cd>(), st);
+      pss_fill_pairs(sh->G, Pi, jk, tabs[g].t1, tabs[g].t2, tabs[g].mmax, w.zb.as<cd>(), st);
       pss_fill_assemble(sh->G, Pi, w.zb.as<cd>(), w.z64.as<cd>() + b * msz, zr ? zr + b * msz : nullptr,
                         zi ? zi + b * msz : nullptr, ld, st);
     }
     if (rec) cudaEventRecord(e[2], st);
     for (int b = 0; b < cnt; ++b) {
-      const int i = idx[b];
-      const double *kv = (const double *)(mb + off_k) + (size_t)i * nmodes * 2;
-      const cd *sv = (const cd *)(mb + off_s) + (size_t)i * nmodes * 2;
-      cd *bf = w.bf.as<cd>() + (size_t)b * nmodes * n * 2;
-      pss_bfft(sh->G, nmodes, kv, psi[2 * i], psi[2 * i + 1], bf, st);
-      pss_rhs(n, nmodes, bf, sv, w.rhs.as<cd>() + b * vsz, st);
+      const Problem &P = PR[it.p[b]];
+      const int i = it.i[b];
+      const double *kv = dkv + P.kb + (size_t)i * nm * 2;
+      const cd *sv = dsrc + P.sb + (size_t)i * nm * 2;
+      cd *bf = w.bf.as<cd>() + (size_t)b * nm * n * 2;
+      pss_bfft(P.sh->G, nm, kv, P.psi[2 * i], P.psi[2 * i + 1], bf, st);
+      pss_rhs(n, nm, bf, sv, w.rhs.as<cd>() + b * vsz, st);
     }
     if (rec) { cudaEventRecord(e[3], st); cudaEventRecord(e[4], st); }
     PSS_CUDA_TRY(cudaMemsetAsync(w.bstat.p, 0, (size_t)cnt * sizeof(int), st));
-    int rc2 = w.factor_solve(n, cnt, prec, nmodes, kMaxRefine, w.bstat.as<int>());
+    int rc2 = w.factor_solve(n, cnt, prec, nm, kMaxRefine, w.bstat.as<int>(), P0.panel_w, P0.outer_nb);
     if (rc2) return rc2;
     StatusMap sm{};
-    for (int b = 0; b < cnt; ++b) sm.idx[b] = idx[b];
+    for (int b = 0; b < cnt; ++b) sm.idx[b] = PR[it.p[b]].p0 + it.i[b];
     pss_count_launch();
     k_status_scatter<<<1, 32, 0, st>>>(cnt, w.bstat.as<int>(), dstatus, sm);
     if (rec) cudaEventRecord(e[5], st);
     for (int b = 0; b < cnt; ++b) {
-      const int i = idx[b];
-      const double *tv = (const double *)(mb + off_t) + (size_t)i * nmodes * 2;
-      const cd *wv = (const cd *)(mb + off_w) + (size_t)i * nmodes;
-      pss_project(n, nmodes, w.bf.as<cd>() + (size_t)b * nmodes * n * 2, tv, wv, w.X.as<cd>() + b * vsz,
-                  c->dS.as<cd>() + (size_t)i * nm2, st);
+      const Problem &P = PR[it.p[b]];
+      const int i = it.i[b];
+      const double *tv = dtob + P.tb + (size_t)i * nm * 2;
+      const cd *wv = dwob + P.wb + (size_t)i * nm;
+      pss_project(n, nm, w.bf.as<cd>() + (size_t)b * nm * n * 2, tv, wv, w.X.as<cd>() + b * vsz,
+                  c->dS.as<cd>() + P.db + (size_t)i * nm2, st);
     }
     if (rec) { cudaEventRecord(e[6], st); cudaEventRecord(e[7], st); }
     PSS_CUDA_TRY(cudaGetLastError());
     return 0;
   };
-  // One host thread per worker stream: each enqueues its own batches (batch q holds points
-  // [q*B, q*B + B), worker k takes q = k, k + nw, ...), so a stream whose launch queue is full
-  // blocks only its own thread, not the other streams.
+  // One host thread per worker stream, each taking the next item of the shared list, so a
+  // stream whose launch queue is full blocks only its own thread.
   {
-    const int nbat = (npts + B - 1) / B;
-    std::vector<int> wrc(nw, 0);
-    std::vector<std::string> werr(nw);
+    std::atomic<int> next{0};
+    std::vector<int> wrc(nwk, 0);
+    std::vector<std::string> werr(nwk);
     auto feed = [&](int k) {
       if (cudaSetDevice(c->device) != cudaSuccess) {
         wrc[k] = -3;
@@ -741,44 +871,56 @@ int pss_partial_gsms(pss_sheet *sh, int nl, const double *eps, const double *mu,
         return;
       }
       g_kprof = c->prof_on ? &kprofs[k] : nullptr;
-      int idx[kMaxBatch];
-      for (int q = k; q < nbat && !wrc[k]; q += nw) {
-        const int i0 = q * B, cnt = std::min(B, npts - i0);
-        for (int b = 0; b < cnt; ++b) idx[b] = i0 + b;
-        wrc[k] = run_batch(idx, cnt, precision, c->w[k], k == 0);
-      }
+      for (int q = next.fetch_add(1); q < (int)items.size() && !wrc[k]; q = next.fetch_add(1))
+        wrc[k] = run_batch(items[q], precision, c->w[k], k == 0);
       g_kprof = nullptr;
       if (wrc[k]) werr[k] = pss_last_error();
     };
     std::vector<std::thread> th;
-    for (int k = 1; k < nw; ++k) th.emplace_back(feed, k);
+    for (int k = 1; k < nwk; ++k) th.emplace_back(feed, k);
     feed(0);
     for (auto &t : th) t.join();
-    for (int k = 0; k < nw; ++k)
+    for (int k = 0; k < nwk; ++k)
       if (wrc[k]) {
         pss_set_error("%s", werr[k].c_str());
         return wrc[k];
       }
   }
   for (auto &w : c->w) PSS_CUDA_TRY(cudaStreamSynchronize(w.st));
-  PSS_CUDA_TRY(cudaMemcpy(status, c->status.p, (size_t)npts * sizeof(int), cudaMemcpyDeviceToHost));
+  std::vector<int> hst(total);
+  PSS_CUDA_TRY(cudaMemcpy(hst.data(), c->status.p, (size_t)total * sizeof(int), cudaMemcpyDeviceToHost));
   // FP32 points whose refinement stalled (cond(Z) * eps32 too close to 1) or went
   // non-finite are recomputed with the FP64 LU; the status keeps a record of it.
   if (precision == PSS_FP32_REFINE) {
     std::vector<int> redo;
-    for (int i = 0; i < npts; ++i)
-      if (status[i] & (PSS_ST_REFINE_NOCONV | PSS_ST_NONFINITE)) redo.push_back(i);
+    for (int g = 0; g < total; ++g)
+      if (hst[g] & (PSS_ST_REFINE_NOCONV | PSS_ST_NONFINITE)) redo.push_back(g);
     if (!redo.empty()) {
-      std::vector<int> cleared(npts);
-      for (int i = 0; i < npts; ++i) cleared[i] = status[i] & ~(PSS_ST_REFINE_NOCONV | PSS_ST_NONFINITE);
-      PSS_CUDA_TRY(cudaMemcpy(c->status.p, cleared.data(), (size_t)npts * sizeof(int), cudaMemcpyHostToDevice));
-      for (size_t q0 = 0, k = 0; q0 < redo.size(); q0 += B, ++k) {
-        const int cnt = (int)std::min<size_t>(B, redo.size() - q0);
-        if ((rc = run_batch(redo.data() + q0, cnt, PSS_FP64, c->w[k % nw], false))) return rc;
+      std::vector<int> cleared(total);
+      for (int g = 0; g < total; ++g) cleared[g] = hst[g] & ~(PSS_ST_REFINE_NOCONV | PSS_ST_NONFINITE);
+      PSS_CUDA_TRY(cudaMemcpy(c->status.p, cleared.data(), (size_t)total * sizeof(int), cudaMemcpyHostToDevice));
+      size_t k = 0;
+      for (size_t p = 0; p < PR.size(); ++p) {
+        Item it{};
+        auto flush = [&]() -> int {
+          if (!it.cnt) return 0;
+          const int rc = run_batch(it, PSS_FP64, c->w[k++ % nwk], false);
+          it.cnt = 0;
+          return rc;
+        };
+        const int B = std::max(1, std::min(PR[p].batch > 0 ? PR[p].batch : c->batch, kMaxBatch));
+        for (int g : redo) {
+          if (g < PR[p].p0 || g >= PR[p].p0 + PR[p].npts) continue;
+          it.p[it.cnt] = (int)p;
+          it.i[it.cnt] = g - PR[p].p0;
+          if (++it.cnt == B)
+            if (int rc = flush()) return rc;
+        }
+        if (int rc = flush()) return rc;
       }
       for (auto &w : c->w) PSS_CUDA_TRY(cudaStreamSynchronize(w.st));
-      PSS_CUDA_TRY(cudaMemcpy(status, c->status.p, (size_t)npts * sizeof(int), cudaMemcpyDeviceToHost));
-      for (int i : redo) status[i] |= PSS_ST_FP64_FALLBACK;
+      PSS_CUDA_TRY(cudaMemcpy(hst.data(), c->status.p, (size_t)total * sizeof(int), cudaMemcpyDeviceToHost));
+      for (int g : redo) hst[g] |= PSS_ST_FP64_FALLBACK;
     }
   }
   for (size_t k = 1; k < c->w.size(); ++k) {
@@ -794,8 +936,11 @@ int pss_partial_gsms(pss_sheet *sh, int nl, const double *eps, const double *mu,
   cudaEventElapsedTime(&span_ms, span0, span1);
   cudaEventDestroy(span0);
   cudaEventDestroy(span1);
-  PSS_CUDA_TRY(cudaMemcpy(dS, c->dS.p, (size_t)npts * nm2 * sizeof(cd), cudaMemcpyDeviceToHost));
-  for (int i = 0; i < npts; ++i) status[i] |= hstatus[i];
+  for (auto &P : PR) {
+    const size_t nm2 = (size_t)P.nm * P.nm;
+    PSS_CUDA_TRY(cudaMemcpy(P.dS, c->dS.as<cd>() + P.db, (size_t)P.npts * nm2 * sizeof(cd), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < P.npts; ++i) P.status[i] = hst[P.p0 + i] | hstatus[P.p0 + i];
+  }
   for (int q = 0; q < 8; ++q) c->last_ms[q] = 0;
   for (size_t b = 0; b + 8 <= ev.size(); b += 8) {
     float ms;
@@ -823,6 +968,33 @@ int pss_partial_gsms(pss_sheet *sh, int nl, const double *eps, const double *mu,
   c->last_ms[7] = span_ms;
   for (auto e : ev) cudaEventDestroy(e);
   return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pss_partial_gsms(pss_sheet *sh, int nl, const double *eps, const double *mu, const double *width, int s,
+                     double u, int npts, const double *k0, const double *psi, int nmodes, const double *kvec,
+                     const double *src, const double *tobs, const double *wobs, int precision, double *dS,
+                     int *status) {
+  if (!sh) { pss_set_error("null argument"); return -1; }
+  pss_problem q{sh, nl, eps, mu, width, s, u, npts, k0, psi, nmodes, kvec, src, tobs, wobs, 0, 0, 0, dS, status};
+  std::vector<Problem> PR(1);
+  if (int rc = check_problem(q, precision, PR[0])) return rc;
+  return sweep_impl(sh->ctx, PR, precision);
+}
+
+int pss_partial_gsms_multi(int nprob, const pss_problem *probs, int precision) {
+  if (nprob <= 0 || !probs) { pss_set_error("null or empty problem list"); return -1; }
+  std::vector<Problem> PR(nprob);
+  for (int p = 0; p < nprob; ++p)
+    if (int rc = check_problem(probs[p], precision, PR[p])) {
+      const std::string m = pss_last_error();
+      pss_set_error("problem %d: %s", p, m.c_str());
+      return rc;
+    }
+  return sweep_impl(probs[0].sheet->ctx, PR, precision);
 }
 
 int pss_last_timings(pss_ctx *c, double *ms8) {

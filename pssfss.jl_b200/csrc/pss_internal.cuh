@@ -162,8 +162,10 @@ int pss_lu32(int n, float *Ar, float *Ai, long long ld, int *ipiv, int *info, vo
              cudaStream_t st);
 int pss_lu64_batched(int n, int nb, cd *A, long long ld, long long ms, int *ipiv, int *info, void *ws,
                      size_t ws_bytes, cudaStream_t st);
+// FP32 tile shape: panel_w in {8, 16, 32} columns per cluster panel, outer_nb in {64, 128}
+// columns per outer block (the tensor-core update's K); 0 picks 32 / 128.
 int pss_lu32_batched(int n, int nb, float *Ar, float *Ai, long long ld, long long ms, int *ipiv, int *info,
-                     void *ws, size_t ws_bytes, cudaStream_t st);
+                     void *ws, size_t ws_bytes, cudaStream_t st, int panel_w = 0, int outer_nb = 0);
 size_t pss_lu_ws_bytes(int n, int precision, int nb = 1);
 
 // Tensor-core (tcgen05, 3xTF32) complex Schur update on FP32 planes (pss_gemm_tc.cu), for

@@ -632,15 +632,23 @@ int pss_lu64_batched(int n, int nb, cd *A, long long ld, long long ms, int *ipiv
 }
 
 int pss_lu32_batched(int n, int nb, float *Ar, float *Ai, long long ld, long long ms, int *ipiv, int *info,
-                     void *ws, size_t ws_bytes, cudaStream_t st) {
+                     void *ws, size_t ws_bytes, cudaStream_t st, int panel_w, int outer_nb) {
   if (nb <= 0) return 0;
   if (ws_bytes < pss_lu_ws_bytes(n, 1, nb)) { pss_set_error("LU workspace too small"); return -4; }
+  if (panel_w == 0) panel_w = 32;
+  if (outer_nb == 0) outer_nb = kNB32;
+  if ((panel_w != 8 && panel_w != 16 && panel_w != 32) || (outer_nb != 64 && outer_nb != 128) ||
+      outer_nb % panel_w) {
+    pss_set_error("FP32 LU tile shape (panel %d, outer block %d) not one of panel 8/16/32, outer 64/128",
+                  panel_w, outer_nb);
+    return -1;
+  }
   Mat<true> M{Ar, Ai, ld};
-  int W = pick_panel_width<true>(n, 32);
+  int W = pick_panel_width<true>(n, panel_w);
   if (W < 0) { pss_set_error("matrix order %d too large for the cluster panel", n); return -6; }
   const size_t lb = list_bytes(nb);
   const LuBatch bt{ms, n, ipiv, info, (int *)ws};
-  return lu_blocked<true>(n, nb, M, bt, kNB32, W, TcWs{(char *)ws + lb, ws_bytes - lb}, st);
+  return lu_blocked<true>(n, nb, M, bt, outer_nb, W, TcWs{(char *)ws + lb, ws_bytes - lb}, st);
 }
 
 int pss_lu64(int n, cd *A, long long ld, int *ipiv, int *info, void *ws, size_t ws_bytes, cudaStream_t st) {
@@ -649,5 +657,5 @@ int pss_lu64(int n, cd *A, long long ld, int *ipiv, int *info, void *ws, size_t 
 
 int pss_lu32(int n, float *Ar, float *Ai, long long ld, int *ipiv, int *info, void *ws, size_t ws_bytes,
              cudaStream_t st) {
-  return pss_lu32_batched(n, 1, Ar, Ai, ld, 0, ipiv, info, ws, ws_bytes, st);
+  return pss_lu32_batched(n, 1, Ar, Ai, ld, 0, ipiv, info, ws, ws_bytes, st, 0, 0);
 }

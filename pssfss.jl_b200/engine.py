@@ -47,6 +47,7 @@ SIGNATURES = {
     "pss_sheet_destroy": (_I, [_P]),
     "pss_sheet_clear_cache": (_I, [_P]),
     "pss_partial_gsms": (_I, [_P, _I, _P, _P, _P, _I, _D, _I, _P, _P, _I, _P, _P, _P, _P, _I, _P, _P]),
+    "pss_partial_gsms_multi": (_I, [_I, _P, _I]),
     "pss_partial_gsms_lin": (_I, [_P, _I, _P, _P, _P, _I, _D, _I, _P, _P, _I, _P, _P, _P, _P, _I, _P, _P, _P,
                                   _P, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P]),
     "pss_partial_gsms_adj": (_I, [_P, _I, _P, _P, _P, _I, _D, _I, _P, _P, _I, _P, _P, _P, _P, _I, _P, _P, _P,
@@ -230,6 +231,53 @@ def partial_gsms(sheet, rwg, points, region_rng, s, u, ios, precision="fp64", de
     if bad.any():
         raise RuntimeError(f"solver status {status.tolist()} (singular, non-finite or device timeout)")
     return [d.T.copy() for d in dS]
+
+
+class Problem(ctypes.Structure):
+    """``pss_problem`` of include/pssfss_b200.h."""
+    _fields_ = [("sheet", _P), ("nl", _I), ("eps", _P), ("mu", _P), ("width", _P), ("s", _I), ("u", _D),
+                ("npts", _I), ("k0", _P), ("psi", _P), ("nmodes", _I), ("kvec", _P), ("src", _P), ("tobs", _P),
+                ("wobs", _P), ("batch", _I), ("panel_w", _I), ("outer_nb", _I), ("dS", _P), ("status", _P)]
+
+
+def partial_gsms_multi(problems, precision="fp64", device=0, nworkers=None, stats=None):
+    """Scattered partial GSMs of many sheet sweeps in one ``pss_partial_gsms_multi`` call.
+
+    ``problems``: list of dicts with the arguments of ``partial_gsms`` (``sheet``, ``rwg``,
+    ``points``, ``region_rng``, ``s``, ``u``, ``ios``) and optionally ``batch``, ``panel_w``,
+    ``outer_nb`` (0: defaults).  Returns one list of per-point dS matrices per problem."""
+    keep, arr, outs = [], (Problem * len(problems))(), []
+    for k, pr in enumerate(problems):
+        i1, i2 = pr["region_rng"]
+        pts, ios = pr["points"], pr["ios"]
+        region = pts[0].layers[i1 - 1:i2]
+        eps, mu, w = region_arrays(region)
+        npts, nm = len(pts), len(ios[0].wobs)
+        bufs = dict(eps=eps, mu=mu, w=w, k0=_f64([pt.k0 for pt in pts]),
+                    psi=_f64([[io.psi1, io.psi2] for io in ios]), kvec=_f64(np.stack([io.kvec for io in ios])),
+                    src=_c2d(np.stack([io.src for io in ios])), tobs=_f64(np.stack([io.tobs for io in ios])),
+                    wobs=_c2d(np.stack([io.wobs for io in ios])), dS=np.zeros((npts, nm, nm), complex),
+                    status=np.zeros(npts, np.int32),
+                    ds=device_sheet(pr["sheet"], pr["rwg"], device, nworkers))
+        keep.append(bufs)
+        arr[k] = Problem(bufs["ds"].h, len(region), _p(eps), _p(mu), _p(w), int(pr["s"]), float(pr["u"]), npts,
+                         _p(bufs["k0"]), _p(bufs["psi"]), nm, _p(bufs["kvec"]), _p(bufs["src"]), _p(bufs["tobs"]),
+                         _p(bufs["wobs"]), int(pr.get("batch", 0)), int(pr.get("panel_w", 0)),
+                         int(pr.get("outer_nb", 0)), _p(bufs["dS"]), _p(bufs["status"]))
+    _check(lib().pss_partial_gsms_multi(len(problems), ctypes.cast(arr, ctypes.c_void_p), PRECISIONS[precision]),
+           "pss_partial_gsms_multi")
+    if stats is not None:
+        t = np.zeros(8)
+        lib().pss_last_timings(context(device, nworkers), _p(t))
+        stats["status"] = [b["status"].tolist() for b in keep]
+        stats["timings_ms"] = dict(zip(["tables", "face_integrals", "fill", "transforms", "unused",
+                                        "factor_solve", "project", "total"], t.tolist()))
+        stats["timings_ms"].pop("unused")
+    for b in keep:
+        if (b["status"] & FATAL_STATUS).any():
+            raise RuntimeError(f"solver status {b['status'].tolist()} (singular, non-finite or device timeout)")
+        outs.append([d.T.copy() for d in b["dS"]])
+    return outs
 
 
 def partial_gsms_adjoint(sheet, rwg, points, region_rng, s, u, ios, perturbed, precision="fp64", device=0):
