@@ -1,8 +1,9 @@
 // K2 + K3: face-pair integrals and the MoM matrix fill.
 //
 // K2 k_filljk   restates Zint.jl:54-179 (filljk!) with PGF.jl:67-106 (jksums):
-//               one thread per unique face pair, the 7-point rule and each lattice
-//               ring summed in the reference's order, FP64.
+//               one warp per unique face pair, the 7-point rule in the reference's order,
+//               each lattice ring's summands spread over the lanes and reduced with warp
+//               shuffles, the rings and their convergence test in the reference's order, FP64.
 // K3a k_pairs   restates Zint.jl:218-245 (zint) and the per-edge algebra of
 //               FillZY.jl:141-197 / 362-419: one thread per unique face pair computes
 //               the 3x3 unflagged edge-pair terms  zA*(ρc2[iml]·a_isl) - zP*φ.
@@ -15,8 +16,23 @@
 
 namespace {
 
-__device__ __forceinline__ int jksums_dev(double urx, double ury, double psi1, double psi2, double us1x,
-                                          double us1y, double us2x, double us2y, cd &jout, cd &kout) {
+// jksums (PGF.jl:67-106) with one warp per lattice sum: ring r's 8r summands are spread over the lanes
+// (lane t takes t, t + 32, ...), each lane adds its share in order, and the ring's partial
+// sums are reduced with xor shuffles (every lane ends with the same bits: each butterfly
+// step adds the same two operands on both partner lanes).  The convergence test and the
+// ring loop are uniform over the warp.  Same rules as jksums (PGF.jl:67-106): rmin = 5,
+// at most 65 rings, relative change 1e-8 in both sums.
+__device__ __forceinline__ cd warp_sum(cd v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+    v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+  }
+  return v;
+}
+
+__device__ __forceinline__ int jksums_warp(double urx, double ury, double psi1, double psi2, double us1x,
+                                           double us1y, double us2x, double us2y, int lane, cd &jout, cd &kout) {
   const int rmin = 5;
   const double small = 1e-5, convtest = 1e-8;
   double arg = sqrt(urx * urx + ury * ury);
@@ -29,7 +45,7 @@ __device__ __forceinline__ int jksums_dev(double urx, double ury, double psi1, d
   for (int r = 1; r <= PSS_JKRINGMAX; ++r) {
     cd jring = mkcd(0, 0), kring = mkcd(0, 0);
     const int len = 8 * r;
-    for (int t = 0; t < len; ++t) {
+    for (int t = lane; t < len; t += 32) {
       int m, n;
       ring_mn(r, t, m, n);
       double dx = urx - ((double)m * us1x + (double)n * us2x);
@@ -43,14 +59,16 @@ __device__ __forceinline__ int jksums_dev(double urx, double ury, double psi1, d
         double ph = (double)m * psi1 + (double)n * psi2;
         if (ph == 0.0) term = mkcd(er, -ph);
         else {
-          double s, c;
-          sincos(-ph, &s, &c);
-          term = mkcd(er * c, er * s);
+          double sn, cs;
+          sincos(-ph, &sn, &cs);
+          term = mkcd(er * cs, er * sn);
         }
       }
       jring = jring + term / a;
       kring = kring + term;
     }
+    jring = warp_sum(jring);
+    kring = warp_sum(kring);
     jsum = jsum + jring;
     ksum = ksum + kring;
     if (r > rmin) {
@@ -71,10 +89,24 @@ __device__ __forceinline__ void face_vtx(const SheetDev &G, int f, double r[3][2
   }
 }
 
-__global__ void k_filljk(SheetDev G, double ul, double psi1, double psi2, double us1x, double us1y,
-                         double us2x, double us2y, JKDev jk, int *nonconv) {
-  int iu = blockIdx.x * blockDim.x + threadIdx.x;
-  if (iu >= G.nufp) return;
+__device__ __forceinline__ void filljk_pair(const SheetDev &G, double ul, double psi1, double psi2, double us1x,
+                                            double us1y, double us2x, double us2y, const JKDev &jk, int *nonconv,
+                                            int iu, int lane);
+
+// One warp per unique face pair (grid-stride over pairs): the 7 lattice sums of the pair one
+// after another, each spread over the lanes (jksums_warp); every lane then holds the same
+// sums and lane 0 writes the pair's integrals.
+__global__ void __launch_bounds__(256) k_filljk(SheetDev G, double ul, double psi1, double psi2, double us1x,
+                                                double us1y, double us2x, double us2y, JKDev jk, int *nonconv) {
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (int)((gridDim.x * (long long)blockDim.x) >> 5);
+  for (int iu = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5); iu < G.nufp; iu += nwarps)
+    filljk_pair(G, ul, psi1, psi2, us1x, us1y, us2x, us2y, jk, nonconv, iu, lane);
+}
+
+__device__ __forceinline__ void filljk_pair(const SheetDev &G, double ul, double psi1, double psi2, double us1x,
+                                            double us1y, double us2x, double us2y, const JKDev &jk, int *nonconv,
+                                            int iu, int lane) {
   int fp = G.ufp_rep[iu];
   int ifm = fp % G.nface, ifs = fp / G.nface;
   double rs[3][2], rm[3][2];
@@ -94,7 +126,7 @@ __global__ void k_filljk(SheetDev G, double ul, double psi1, double psi2, double
     double rtx = (rs[0][0] + rs21[0] * c_qxi[i]) + rs31[0] * c_qeta[i];
     double rty = (rs[0][1] + rs21[1] * c_qxi[i]) + rs31[1] * c_qeta[i];
     cd js, ks;
-    if (!jksums_dev(ul * (rmc[0] - rtx), ul * (rmc[1] - rty), psi1, psi2, us1x, us1y, us2x, us2y, js, ks))
+    if (!jksums_warp(ul * (rmc[0] - rtx), ul * (rmc[1] - rty), psi1, psi2, us1x, us1y, us2x, us2y, lane, js, ks))
       bad = 1;
     cd jw = c_qw[i] * js;
     aJx = aJx + c_qxi[i] * jw;
@@ -139,6 +171,7 @@ __global__ void k_filljk(SheetDev G, double ul, double psi1, double psi2, double
   rr0 /= area2;
   rr1 /= area2;
   ri /= (area2 * ul);
+  if (lane) return;
   jk.J[iu] = aJ; jk.Jxi[iu] = aJx; jk.Jeta[iu] = aJe;
   jk.K[iu] = aK; jk.Kxi[iu] = aKx; jk.Keta[iu] = aKe;
   jk.rho_r[2 * iu] = rr0;
@@ -223,7 +256,7 @@ __global__ void __launch_bounds__(128) k_pairs(SheetDev G, const PointParams *__
     rc2[i][0] = 0.5 * (rmc[0] - rm[i][0]);
     rc2[i][1] = 0.5 * (rmc[1] - rm[i][1]);
   }
-  cd *out = zb + (size_t)iu * 9;
+  cd *out = zb + iu;  // plane q at out[q * nufp]: consecutive classes, coalesced stores
 #pragma unroll
   for (int isl = 0; isl < 3; ++isl) {
     double sing0 = rr0 + (u * rinv) * (rmc[0] - rs[isl][0]);
@@ -240,7 +273,7 @@ __global__ void __launch_bounds__(128) k_pairs(SheetDev G, const PointParams *__
 #pragma unroll
     for (int iml = 0; iml < 3; ++iml) {
       cd dp = rc2[iml][0] * av[0] + rc2[iml][1] * av[1];
-      out[3 * isl + iml] = C.zA * dp - zphi;
+      out[(size_t)(3 * isl + iml) * G.nufp] = C.zA * dp - zphi;
     }
   }
 }
@@ -260,8 +293,8 @@ __device__ __forceinline__ cd assemble_entry(const SheetDev &G, const PointParam
       const int fb = G.inc_face[4 * n + b], kb = G.inc_loc[4 * n + b];
       const cd ffb = P.ff[G.inc_eci[4 * n + b]];
       const cd sflag = G.inc_sgn[4 * n + b] > 0 ? ffb : -ffb;
-      const int iu = G.ufpm[(size_t)fa + (size_t)fb * G.nface];
-      const cd v = zb[(size_t)iu * 9 + 3 * kb + ka];
+      const int iu = G.ufpm[(size_t)fb + (size_t)fa * G.nface];
+      const cd v = zb[(size_t)(3 * kb + ka) * G.nufp + iu];
       acc = acc + (mflag * sflag) * v;
       if (!P.magnetic && fa == fb) {
         const double fr = G.fr[fa];
@@ -391,8 +424,14 @@ void pss_filljk(const SheetDev &G, double ulocal, double psi1, double psi2, cons
                 JKDev jk, int *nonconv, cudaStream_t st) {
   if (G.nufp == 0) return;
   pss_count_launch();
-  k_filljk<<<cdiv_u(G.nufp, 128), 128, 0, st>>>(G, ulocal, psi1, psi2, ulocal * s1[0], ulocal * s1[1],
-                                                 ulocal * s2[0], ulocal * s2[1], jk, nonconv);
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  // a warp per pair, grid-strided: at most 8 resident 256-thread CTAs per SM are useful
+  const long long want = cdiv_u((long long)G.nufp * 32, 256);
+  const int grid = (int)std::min<long long>(want, (long long)nsm * 8);
+  k_filljk<<<grid, 256, 0, st>>>(G, ulocal, psi1, psi2, ulocal * s1[0], ulocal * s1[1], ulocal * s2[0],
+                                 ulocal * s2[1], jk, nonconv);
 }
 
 void pss_fill_pairs(const SheetDev &G, const PointParams *dP1, const JKDev &jk, const cd *t1, const cd *t2,

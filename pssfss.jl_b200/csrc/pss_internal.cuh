@@ -54,8 +54,10 @@ struct SheetDev {
   double upm;  // sheet units per metre
   const double *rho;     // 2*nnode, sheet units
   const int *fv;         // 3*nface
-  const int *ufpm;       // nface*nface, column-major (match fastest), 0-based class
+  const int *ufpm;       // nface*nface, 0-based class of (match fa, source fb) at fb + fa*nface
   const int *ufp_rep;    // nufp, 0-based column-major face pair of the class representative
+  // pair terms zb (pss_fill_pairs): 9 planes of nufp complex, term 3*isl + iml of class iu at
+  // zb[(3*isl + iml)*nufp + iu]
   const double *fr;      // nface
   const double *face_ls; // 3*nface edge lengths (m): |r3-r2|, |r1-r3|, |r1-r2|
   const double *face_a48;// nface: 48*|area| (m²)
