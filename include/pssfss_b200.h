@@ -210,6 +210,14 @@ int pss_profile_result(pss_ctx *ctx, double *out);
 int pss_schur_update(pss_ctx *ctx, int m, int n, int k, const float *Lr, const float *Li, const float *Ur,
                      const float *Ui, float *Cr, float *Ci, int *status);
 
+/* Poll limit of the bounded hand-off waits inside the tensor-core update (TMA producer, MMA
+ * issuer and epilogue waiting on each other); 0 restores the default of 2^24 polls.  A wait
+ * that runs out marks the update's matrices with PSS_STATUS_DEVICE_TIMEOUT, and the kernel
+ * waits (at the default limit) for its copies and MMAs in flight, frees its tensor memory
+ * and returns, leaving the context usable.  A test hook: a limit of a few polls makes the
+ * waits run out.  No counterpart in the reference.  Applies to launches made after the call. */
+int pss_set_wait_limit(int64_t iterations);
+
 /* FP64 complex LU factorisation, in place, on caller-owned device memory, allocating no
  * device memory at all (no cudaMalloc, cudaFree or allocating library routine).  It has
  * no counterpart in the reference.  It serves callers that cannot let a library allocate

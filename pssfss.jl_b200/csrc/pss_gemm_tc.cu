@@ -50,10 +50,10 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
-// Bounded wait for the phase with parity `par` to complete.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t par) {
+// Bounded wait for the phase with parity `par` to complete: at most `cap` polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t par, long long cap = kWaitCap) {
   const uint32_t a = smem_u32(bar);
-  for (long long it = 0; it < kWaitCap; ++it) {
+  for (long long it = 0; it < cap; ++it) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -132,6 +132,7 @@ struct GemmArgs {
   int nb;             // matrices in the batch
   int *err;           // one error word per matrix
   int tma_epi;        // C -= D by TMA reduce-add (mapCr / mapCi), else by loads and stores
+  long long wait_cap; // polls of a pipeline hand-off wait (the final drain waits use kWaitCap)
 };
 
 // OR / AND of a predicate over the 128 epilogue threads (named barrier 1).
@@ -208,7 +209,7 @@ __global__ void __launch_bounds__(192, 1) k_cgemm_tf32x3(const __grid_constant__
         const int b = t / per, tt = t % per;
         const int mt = tt / tiles_n, nt = tt % tiles_n;
         for (int kb = 0; kb < g.nk; ++kb) {
-          if (!mbar_wait(&empty[s], ph ^ 1)) { fail_all(g); *(volatile int *)abort_flag = 1; break; }
+          if (!mbar_wait(&empty[s], ph ^ 1, g.wait_cap)) { fail_all(g); *(volatile int *)abort_flag = 1; break; }
           mbar_expect_tx(&full[s], STAGE_BYTES);
           unsigned char *st = base + s * STAGE_BYTES;
           for (int p = 0; p < 4; ++p) tma_load_3d(st + p * TILE_BYTES, &mapA, &full[s], kb * BK, mt * BM, 4 * b + p);
@@ -231,12 +232,12 @@ __global__ void __launch_bounds__(192, 1) k_cgemm_tf32x3(const __grid_constant__
       for (int t = blockIdx.x; t < ntiles && !*(volatile int *)abort_flag; t += gridDim.x, ++local) {
         const int ab = local & 1;
         const uint32_t aph = (local >> 1) & 1;
-        if (!mbar_wait(&acce[ab], aph ^ 1)) { fail_all(g); *(volatile int *)abort_flag = 1; break; }
+        if (!mbar_wait(&acce[ab], aph ^ 1, g.wait_cap)) { fail_all(g); *(volatile int *)abort_flag = 1; break; }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t dr = tmem + ab * 256, di = dr + 128;
         bool ok = true;
         for (int kb = 0; kb < g.nk; ++kb) {
-          if (!mbar_wait(&full[s], ph)) { ok = false; break; }
+          if (!mbar_wait(&full[s], ph, g.wait_cap)) { ok = false; break; }
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           unsigned char *st = base + s * STAGE_BYTES;
           for (int ks = 0; ks < BK / KSUB; ++ks) {
@@ -279,7 +280,7 @@ __global__ void __launch_bounds__(192, 1) k_cgemm_tf32x3(const __grid_constant__
       // decisions uniform over the 4 epilogue warps: tcgen05.ld needs whole warps and the
       // staging tile's named barrier needs all 128 threads
       if (epi_any(*(volatile int *)abort_flag != 0)) break;
-      if (!epi_all(mbar_wait(&accf[ab], aph))) {
+      if (!epi_all(mbar_wait(&accf[ab], aph, g.wait_cap))) {
         if (threadIdx.x == 64) { fail_all(g); *(volatile int *)abort_flag = 1; }
         break;
       }
@@ -462,8 +463,15 @@ int make_map(CUtensorMap *m, const float *planes, int rows, int KP, int nplanes)
 constexpr int kMaxDevices = 64;
 int g_num_sms[kMaxDevices] = {};  // per device, written once under g_setup
 DeviceOnce g_setup;
+std::atomic<long long> g_wait_cap{kWaitCap};  // pss_set_wait_limit
 
 }  // namespace
+
+extern "C" int pss_set_wait_limit(int64_t iterations) {
+  if (iterations < 0) { pss_set_error("wait limit must be >= 0"); return -1; }
+  g_wait_cap.store(iterations == 0 ? kWaitCap : (long long)iterations, std::memory_order_relaxed);
+  return 0;
+}
 
 // Workspace for the split operands of a batch of nb updates with up to Mmax rows / Nmax
 // columns, K <= KP.
@@ -507,7 +515,8 @@ int pss_cgemm_tc(float *Ar, float *Ai, long long ld, long long ms, int nb, int m
   } else {
     mcr = mci = ma;  // not read
   }
-  GemmArgs g{Ar, Ai, ld, ms, m0, n0, M, N, KP / BK, nb, err, tma_epi ? 1 : 0};
+  GemmArgs g{Ar, Ai, ld, ms, m0, n0, M, N, KP / BK, nb, err, tma_epi ? 1 : 0,
+             g_wait_cap.load(std::memory_order_relaxed)};
   const int tiles = ((M + BM - 1) / BM) * ((N + BN - 1) / BN) * nb;
   const int grid = std::min(tiles, g_num_sms[dev]);
   const int tok = pss_prof_begin(st);

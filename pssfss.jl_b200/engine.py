@@ -62,6 +62,7 @@ SIGNATURES = {
     "pss_profile_result": (_I, [_P, _P]),
     "pss_schur_update": (_I, [_P, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P]),
     "pss_lu_factor_noalloc": (_I, [_I, _P, _L, _P, _P, _P]),
+    "pss_set_wait_limit": (_I, [_L]),
 }
 
 

@@ -338,3 +338,27 @@ def test_linearised_partial_gsms_and_gradient(precision):
                                            ntri=120)
     for k in P0:
         assert abs(g_dev[k] - g_ref[k]) <= 1e-6 * abs(g_ref[k]), (k, g_dev[k], g_ref[k])
+
+
+def test_pipeline_wait_timeout_reports_status_and_context_survives():
+    """Bounded waits of the tensor-core update: with a limit of one poll the TMA / MMA /
+    epilogue hand-offs run out (the epilogue's first wait spans a whole 128 x 128 x 1024 tile
+    of MMAs, far longer than one poll), the call returns PSS_STATUS_DEVICE_TIMEOUT (64) instead of
+    hanging, the kernel drains its copies and MMAs at the default limit before it frees its
+    tensor memory, and the context stays usable: with the default limit restored the same
+    update is exact to FP32 level again."""
+    lib = engine.lib()
+    rng = np.random.default_rng(5)
+    cplx = lambda *s: (rng.standard_normal(s) + 1j * rng.standard_normal(s)).astype(np.complex64)
+    L, U, C = cplx(256, 1024), cplx(1024, 256), cplx(256, 256)
+    try:
+        assert lib.pss_set_wait_limit(1) == 0
+        _, st = engine.schur_update(L, U, C)
+        assert st == 64
+    finally:
+        assert lib.pss_set_wait_limit(0) == 0
+    out, st = engine.schur_update(L, U, C)
+    ref = C.astype(np.complex128) - L.astype(np.complex128) @ U.astype(np.complex128)
+    scale = np.abs(L).astype(np.float64) @ np.abs(U).astype(np.float64) + np.abs(C)
+    assert st == 0 and float(np.max(np.abs(out - ref) / scale)) < 4e-6
+    assert lib.pss_set_wait_limit(-1) == -1
