@@ -39,7 +39,7 @@ def rel(a, b):
 
 
 def test_multi_equals_single_calls_and_oracle():
-    shared = ring(8.0, 0.40, 200)
+    shared = ring(8.0, 0.40, 300)
     probs = [problem(ring(6.0, 0.40, 160), [10.0, 14.0, 19.0], 0.0),
              problem(ring(12.0, 0.44, 360), [11.0, 17.0], 15.0, batch=1),
              problem(ring(6.0, 0.40, 160), [12.0, 16.0], 0.0),     # same N as the first: shared batches
