@@ -135,15 +135,20 @@ struct Worker {
     if (rhs.ensure(v) || X.ensure(v) || R.ensure(v) || D.ensure(v)) return -3;
     return 0;
   }
+  // Leading dimension of the FP32 planes: rows padded to 32 floats (128 bytes), so every row
+  // starts on a 16-byte boundary - the tensor-core update's TMA reduce-add epilogue needs
+  // that - and the panel and interchange kernels move whole 128-byte lines.
+  static long long ld32(int n) { return ((long long)n + 31) & ~31LL; }
   // LU of the worker's first nb matrices (FP64 in z64, or FP32 planes zr/zi) and solves
   // rhs -> X, refined against z64 in FP32 mode.  Status bits go to status[0..nb) (device).
   int factor_solve(int n, int nb, int prec, int nrhs, int maxit, int *status, int panel_w = 0, int outer_nb = 0) {
     int rc;
     const long long ld = n, ms = (long long)n * n, vs = (long long)n * nrhs;
+    const long long ldf = ld32(n), msf = (long long)n * ldf;
     if (prec == PSS_FP64)
       rc = pss_lu64_batched(n, nb, z64.as<cd>(), ld, ms, ipiv.as<int>(), info.as<int>(), luws.p, luws.n, st);
     else
-      rc = pss_lu32_batched(n, nb, zr.as<float>(), zi.as<float>(), ld, ms, ipiv.as<int>(), info.as<int>(), luws.p,
+      rc = pss_lu32_batched(n, nb, zr.as<float>(), zi.as<float>(), ldf, msf, ipiv.as<int>(), info.as<int>(), luws.p,
                             luws.n, st, panel_w, outer_nb);
     if (rc) return rc;
     pss_count_launch();
@@ -151,10 +156,11 @@ struct Worker {
     const cd *L64 = prec == PSS_FP64 ? z64.as<cd>() : nullptr;
     const float *Lr = prec == PSS_FP64 ? nullptr : zr.as<float>();
     const float *Li = prec == PSS_FP64 ? nullptr : zi.as<float>();
-    if ((rc = pss_solve_prepare(sws, nb, L64, Lr, Li, ld, ms, ipiv.as<int>(), st))) return rc;
-    if ((rc = pss_solve_lu(sws, nb, L64, Lr, Li, ld, ms, nrhs, rhs.as<cd>(), X.as<cd>(), vs, 0, st))) return rc;
+    const long long fld = L64 ? ld : ldf, fms = L64 ? ms : msf;  // the factor's layout
+    if ((rc = pss_solve_prepare(sws, nb, L64, Lr, Li, fld, fms, ipiv.as<int>(), st))) return rc;
+    if ((rc = pss_solve_lu(sws, nb, L64, Lr, Li, fld, fms, nrhs, rhs.as<cd>(), X.as<cd>(), vs, 0, st))) return rc;
     if (prec == PSS_FP32_REFINE &&
-        (rc = pss_refine(sws, nb, z64.as<cd>(), ld, ms, Lr, Li, nrhs, rhs.as<cd>(), X.as<cd>(), R.as<cd>(),
+        (rc = pss_refine(sws, nb, z64.as<cd>(), ld, ms, Lr, Li, ldf, msf, nrhs, rhs.as<cd>(), X.as<cd>(), R.as<cd>(),
                          D.as<cd>(), vs, maxit, status, st)))
       return rc;
     pss_solve_status(sws, nb, status, st);
@@ -405,7 +411,8 @@ int ensure_worker_dims(Worker &w, int nufp, int nbf, int nm, int precision, bool
   if (w.zb.ensure((size_t)nufp * 9 * sizeof(cd))) return -3;
   if (w.z64.ensure((size_t)nb * n * n * sizeof(cd))) return -3;
   if (precision == PSS_FP32_REFINE) {
-    if (w.zr.ensure((size_t)nb * n * n * sizeof(float)) || w.zi.ensure((size_t)nb * n * n * sizeof(float))) return -3;
+    const size_t pl = (size_t)nb * n * (size_t)Worker::ld32((int)n) * sizeof(float);
+    if (w.zr.ensure(pl) || w.zi.ensure(pl)) return -3;
   }
   if (w.nonconv.ensure(sizeof(int))) return -3;
   if (w.bf.ensure((size_t)nb * nm * n * 2 * sizeof(cd))) return -3;
@@ -797,6 +804,7 @@ int sweep_impl(pss_ctx *c, std::vector<Problem> &PR, int precision) {
     const Problem &P0 = PR[it.p[0]];
     const int n = P0.sh->nbf, nm = P0.nm;
     const long long ld = n, msz = (long long)n * n, vsz = (long long)n * nm;
+    const long long ldf = Worker::ld32(n), msf = (long long)n * ldf;
     const size_t nm2 = (size_t)nm * nm;
     int mufp = 0;
     bool ojk = false;
@@ -828,8 +836,8 @@ int sweep_impl(pss_ctx *c, std::vector<Problem> &PR, int precision) {
         k_nonconv_to_status<<<1, 1, 0, st>>>(w.nonconv.as<int>(), dstatus + g);
       }
       pss_fill_pairs(sh->G, Pi, jk, tabs[g].t1, tabs[g].t2, tabs[g].mmax, w.zb.as<cd>(), st);
-      pss_fill_assemble(sh->G, Pi, w.zb.as<cd>(), w.z64.as<cd>() + b * msz, zr ? zr + b * msz : nullptr,
-                        zi ? zi + b * msz : nullptr, ld, st);
+      pss_fill_assemble(sh->G, Pi, w.zb.as<cd>(), w.z64.as<cd>() + b * msz, zr ? zr + b * msf : nullptr,
+                        zi ? zi + b * msf : nullptr, ld, ldf, st);
     }
     if (rec) cudaEventRecord(e[2], st);
     for (int b = 0; b < cnt; ++b) {
@@ -1040,7 +1048,7 @@ int pss_fill_matrix(pss_sheet *sh, int nl, const double *eps, const double *mu, 
   if ((rc = ensure_worker(w, sh, 1, PSS_FP64, false, 1))) return rc;
   pss_fill_pairs(sh->G, c->params.as<PointParams>(), sh->cache.jk, tabs[0].t1, tabs[0].t2, tabs[0].mmax,
                  w.zb.as<cd>(), w.st);
-  pss_fill_assemble(sh->G, c->params.as<PointParams>(), w.zb.as<cd>(), w.z64.as<cd>(), nullptr, nullptr, sh->nbf,
+  pss_fill_assemble(sh->G, c->params.as<PointParams>(), w.zb.as<cd>(), w.z64.as<cd>(), nullptr, nullptr, sh->nbf, sh->nbf,
                     w.st);
   PSS_CUDA_TRY(cudaStreamSynchronize(w.st));
   const size_t n = sh->nbf;
@@ -1134,11 +1142,16 @@ int pss_lu_solve(pss_ctx *c, int n, const double *Z, int nrhs, const double *B, 
   PSS_CUDA_TRY(cudaMemcpy(w.rhs.p, B, (size_t)n * nrhs * sizeof(cd), cudaMemcpyHostToDevice));
   int rc;
   if (precision == PSS_FP32_REFINE) {
-    if (w.zr.ensure(nn * sizeof(float)) || w.zi.ensure(nn * sizeof(float))) return -3;
-    std::vector<float> hr(nn), hi(nn);
-    for (size_t i = 0; i < nn; ++i) { hr[i] = (float)h[i].x; hi[i] = (float)h[i].y; }
-    PSS_CUDA_TRY(cudaMemcpy(w.zr.p, hr.data(), nn * sizeof(float), cudaMemcpyHostToDevice));
-    PSS_CUDA_TRY(cudaMemcpy(w.zi.p, hi.data(), nn * sizeof(float), cudaMemcpyHostToDevice));
+    const size_t ldf = (size_t)Worker::ld32(n), nf = (size_t)n * ldf;
+    if (w.zr.ensure(nf * sizeof(float)) || w.zi.ensure(nf * sizeof(float))) return -3;
+    std::vector<float> hr(nf, 0.f), hi(nf, 0.f);
+    for (size_t m = 0; m < (size_t)n; ++m)
+      for (size_t q = 0; q < (size_t)n; ++q) {
+        hr[m * ldf + q] = (float)h[m * n + q].x;
+        hi[m * ldf + q] = (float)h[m * n + q].y;
+      }
+    PSS_CUDA_TRY(cudaMemcpy(w.zr.p, hr.data(), nf * sizeof(float), cudaMemcpyHostToDevice));
+    PSS_CUDA_TRY(cudaMemcpy(w.zi.p, hi.data(), nf * sizeof(float), cudaMemcpyHostToDevice));
   }
   if ((rc = w.factor_solve(n, 1, precision, nrhs, kMaxRefine, st_buf.as<int>()))) return rc;
   PSS_CUDA_TRY(cudaStreamSynchronize(st));
@@ -1372,7 +1385,7 @@ extern "C" int pss_partial_gsms_lin(pss_sheet *sh, int nl, const double *eps, co
     if (sh->jk_nonconv) hst |= PSS_ST_JK_NOCONV;
     // Z into slot 0 (and the FP32 planes), fills and transforms of every set
     pss_fill_pairs(sh->G, dP, sh->cache.jk, t0.t1, t0.t2, t0.mmax, w.zb.as<cd>(), st);
-    pss_fill_assemble(sh->G, dP, w.zb.as<cd>(), w.z64.as<cd>(), zr, zi, ld, st);
+    pss_fill_assemble(sh->G, dP, w.zb.as<cd>(), w.z64.as<cd>(), zr, zi, ld, Worker::ld32(n), st);
     cd *bf = w.bf.as<cd>();
     const size_t bfs = (size_t)nm * n * 2;
     pss_bfft(sh->G, nm, kv_of(0), psi[2 * i], psi[2 * i + 1], bf, st);
@@ -1383,7 +1396,8 @@ extern "C" int pss_partial_gsms_lin(pss_sheet *sh, int nl, const double *eps, co
       if ((rc = refresh_jk_cache(q, pp[0], pp[1], pu[k] / q->upm, st))) return rc;
       if (q->jk_nonconv) hst |= PSS_ST_JK_NOCONV;
       pss_fill_pairs(q->G, dP + 1 + k, q->cache.jk, tk[k].t1, tk[k].t2, tk[k].mmax, w.zb.as<cd>(), st);
-      pss_fill_assemble(q->G, dP + 1 + k, w.zb.as<cd>(), w.z64.as<cd>() + (1 + k) * msz, nullptr, nullptr, ld, st);
+      pss_fill_assemble(q->G, dP + 1 + k, w.zb.as<cd>(), w.z64.as<cd>() + (1 + k) * msz, nullptr, nullptr, ld, ld,
+                        st);
       pss_bfft(q->G, nm, kv_of(1 + k), pp[0], pp[1], bf + (1 + k) * bfs, st);
       pss_rhs(n, nm, bf + (1 + k) * bfs, src_of(1 + k), w.rhs.as<cd>() + (size_t)(1 + k) * nm * n, st);
     }
@@ -1399,10 +1413,11 @@ extern "C" int pss_partial_gsms_lin(pss_sheet *sh, int nl, const double *eps, co
     }
     if (K > 0) {
       const long long vs2 = (long long)n * nrhs2;
-      if ((rc = pss_solve_lu(w.sws, 1, L64, zr, zi, ld, msz, nrhs2, Ybuf.as<cd>(), Wbuf.as<cd>(), vs2, 0, st)))
+      const long long fld = L64 ? ld : Worker::ld32(n), fms = (long long)n * fld;
+      if ((rc = pss_solve_lu(w.sws, 1, L64, zr, zi, fld, fms, nrhs2, Ybuf.as<cd>(), Wbuf.as<cd>(), vs2, 0, st)))
         return rc;
       if (precision == PSS_FP32_REFINE &&
-          (rc = pss_refine(w.sws, 1, w.z64.as<cd>(), ld, msz, zr, zi, nrhs2, Ybuf.as<cd>(), Wbuf.as<cd>(),
+          (rc = pss_refine(w.sws, 1, w.z64.as<cd>(), ld, msz, zr, zi, fld, fms, nrhs2, Ybuf.as<cd>(), Wbuf.as<cd>(),
                            w.R.as<cd>(), w.D.as<cd>(), vs2, kMaxRefine, w.bstat.as<int>(), st)))
         return rc;
       pss_solve_status(w.sws, 1, w.bstat.as<int>(), st);
@@ -1558,7 +1573,7 @@ extern "C" int pss_partial_gsms_adj(pss_sheet *sh, int nl, const double *eps, co
     if ((rc = refresh_jk_cache(sh, psi[2 * i], psi[2 * i + 1], u / sh->upm, st))) return rc;
     if (sh->jk_nonconv) hst |= PSS_ST_JK_NOCONV;
     pss_fill_pairs(sh->G, dP, sh->cache.jk, t0.t1, t0.t2, t0.mmax, w.zb.as<cd>(), st);
-    pss_fill_assemble(sh->G, dP, w.zb.as<cd>(), w.z64.as<cd>(), zr, zi, ld, st);
+    pss_fill_assemble(sh->G, dP, w.zb.as<cd>(), w.z64.as<cd>(), zr, zi, ld, Worker::ld32(n), st);
     cd *bf = w.bf.as<cd>();
     pss_bfft(sh->G, nm, kv_of(0), psi[2 * i], psi[2 * i + 1], bf, st);
     pss_rhs(n, nm, bf, src_of(0), w.rhs.as<cd>(), st);
@@ -1567,9 +1582,10 @@ extern "C" int pss_partial_gsms_adj(pss_sheet *sh, int nl, const double *eps, co
     // against the FP64 Z in the FP32 form
     PSS_CUDA_TRY(cudaMemsetAsync(w.bstat.p, 0, sizeof(int), st));
     if ((rc = w.factor_solve(n, 1, precision, nm, kMaxRefine, w.bstat.as<int>()))) return rc;
-    if ((rc = pss_solve_lu_trans(w.sws, 1, L64, zr, zi, ld, msz, nm, PT, Lam, Wt, vsz, 0, st))) return rc;
+    const long long fld = L64 ? ld : Worker::ld32(n), fms = (long long)n * fld;
+    if ((rc = pss_solve_lu_trans(w.sws, 1, L64, zr, zi, fld, fms, nm, PT, Lam, Wt, vsz, 0, st))) return rc;
     if (precision == PSS_FP32_REFINE &&
-        (rc = pss_refine_trans(w.sws, 1, w.z64.as<cd>(), ld, msz, zr, zi, nm, PT, Lam, w.R.as<cd>(), w.D.as<cd>(),
+        (rc = pss_refine_trans(w.sws, 1, w.z64.as<cd>(), ld, msz, zr, zi, fld, fms, nm, PT, Lam, w.R.as<cd>(), w.D.as<cd>(),
                                Wt, rtw.p, rtw.n, vsz, kMaxRefine, w.bstat.as<int>(), st)))
       return rc;
     pss_solve_status(w.sws, 1, w.bstat.as<int>(), st);

@@ -1,9 +1,9 @@
 // K2 + K3: face-pair integrals and the MoM matrix fill.
 //
-// K2 k_filljk   restates Zint.jl:54-179 (filljk!) with PGF.jl:67-106 (jksums):
-//               one warp per unique face pair, the 7-point rule in the reference's order,
-//               each lattice ring's summands spread over the lanes and reduced with warp
-//               shuffles, the rings and their convergence test in the reference's order, FP64.
+// K2 k_filljk   restates Zint.jl:54-179 (filljk!) with PGF.jl:67-106 (jksums): eight
+//               lanes per unique face pair, one lattice sum (quadrature point) per lane in
+//               the reference's ring order, the seven sums gathered by warp shuffles and
+//               accumulated in the 7-point rule's order, FP64.
 // K3a k_pairs   restates Zint.jl:218-245 (zint) and the per-edge algebra of
 //               FillZY.jl:141-197 / 362-419: one thread per unique face pair computes
 //               the 3x3 unflagged edge-pair terms  zA*(ρc2[iml]·a_isl) - zP*φ.
@@ -16,23 +16,10 @@
 
 namespace {
 
-// jksums (PGF.jl:67-106) with one warp per lattice sum: ring r's 8r summands are spread over the lanes
-// (lane t takes t, t + 32, ...), each lane adds its share in order, and the ring's partial
-// sums are reduced with xor shuffles (every lane ends with the same bits: each butterfly
-// step adds the same two operands on both partner lanes).  The convergence test and the
-// ring loop are uniform over the warp.  Same rules as jksums (PGF.jl:67-106): rmin = 5,
-// at most 65 rings, relative change 1e-8 in both sums.
-__device__ __forceinline__ cd warp_sum(cd v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
-    v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
-  }
-  return v;
-}
-
-__device__ __forceinline__ int jksums_warp(double urx, double ury, double psi1, double psi2, double us1x,
-                                           double us1y, double us2x, double us2y, int lane, cd &jout, cd &kout) {
+// jksums (PGF.jl:67-106): the spatial lattice sums J and K at one observation offset, ring by
+// ring in the reference's order (rmin = 5, at most 65 rings, relative change 1e-8).
+__device__ __forceinline__ int jksums_dev(double urx, double ury, double psi1, double psi2, double us1x,
+                                          double us1y, double us2x, double us2y, cd &jout, cd &kout) {
   const int rmin = 5;
   const double small = 1e-5, convtest = 1e-8;
   double arg = sqrt(urx * urx + ury * ury);
@@ -45,7 +32,7 @@ __device__ __forceinline__ int jksums_warp(double urx, double ury, double psi1, 
   for (int r = 1; r <= PSS_JKRINGMAX; ++r) {
     cd jring = mkcd(0, 0), kring = mkcd(0, 0);
     const int len = 8 * r;
-    for (int t = lane; t < len; t += 32) {
+    for (int t = 0; t < len; ++t) {
       int m, n;
       ring_mn(r, t, m, n);
       double dx = urx - ((double)m * us1x + (double)n * us2x);
@@ -59,16 +46,14 @@ __device__ __forceinline__ int jksums_warp(double urx, double ury, double psi1, 
         double ph = (double)m * psi1 + (double)n * psi2;
         if (ph == 0.0) term = mkcd(er, -ph);
         else {
-          double sn, cs;
-          sincos(-ph, &sn, &cs);
-          term = mkcd(er * cs, er * sn);
+          double s, c;
+          sincos(-ph, &s, &c);
+          term = mkcd(er * c, er * s);
         }
       }
       jring = jring + term / a;
       kring = kring + term;
     }
-    jring = warp_sum(jring);
-    kring = warp_sum(kring);
     jsum = jsum + jring;
     ksum = ksum + kring;
     if (r > rmin) {
@@ -89,26 +74,19 @@ __device__ __forceinline__ void face_vtx(const SheetDev &G, int f, double r[3][2
   }
 }
 
-__device__ __forceinline__ void filljk_pair(const SheetDev &G, double ul, double psi1, double psi2, double us1x,
-                                            double us1y, double us2x, double us2y, const JKDev &jk, int *nonconv,
-                                            int iu, int lane);
-
-// One warp per unique face pair (grid-stride over pairs): the 7 lattice sums of the pair one
-// after another, each spread over the lanes (jksums_warp); every lane then holds the same
-// sums and lane 0 writes the pair's integrals.
+// Eight lanes per unique face pair (four pairs per warp): lane q < 7 computes the lattice
+// sums of quadrature point q (jksums, serial in the reference's ring order); the group's
+// first lane gathers the seven results with warp shuffles and accumulates them in the
+// 7-point rule's order, so each pair's integrals are those of a serial evaluation bit for bit.
+// Seven times the parallelism of a thread per pair, each thread one lattice sum.
 __global__ void __launch_bounds__(256) k_filljk(SheetDev G, double ul, double psi1, double psi2, double us1x,
                                                 double us1y, double us2x, double us2y, JKDev jk, int *nonconv) {
-  const int lane = threadIdx.x & 31;
-  const int nwarps = (int)((gridDim.x * (long long)blockDim.x) >> 5);
-  for (int iu = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5); iu < G.nufp; iu += nwarps)
-    filljk_pair(G, ul, psi1, psi2, us1x, us1y, us2x, us2y, jk, nonconv, iu, lane);
-}
-
-__device__ __forceinline__ void filljk_pair(const SheetDev &G, double ul, double psi1, double psi2, double us1x,
-                                            double us1y, double us2x, double us2y, const JKDev &jk, int *nonconv,
-                                            int iu, int lane) {
-  int fp = G.ufp_rep[iu];
-  int ifm = fp % G.nface, ifs = fp / G.nface;
+  const int lane = threadIdx.x & 31, q = lane & 7, grp = lane & ~7;
+  const long long gid = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 3;  // pair of this group
+  const bool live = gid < G.nufp;
+  const int iu = live ? (int)gid : G.nufp - 1;  // idle groups mirror the last pair, write nothing
+  const int fp = G.ufp_rep[iu];
+  const int ifm = fp % G.nface, ifs = fp / G.nface;
   double rs[3][2], rm[3][2];
   face_vtx(G, ifs, rs, 1.0);
   face_vtx(G, ifm, rm, 1.0);
@@ -120,23 +98,33 @@ __device__ __forceinline__ void filljk_pair(const SheetDev &G, double ul, double
   double rs31[2] = {rs[2][0] - rs[0][0], rs[2][1] - rs[0][1]};
   double rs21[2] = {-rs12[0], -rs12[1]};
   double rmc[2] = {((rm[0][0] + rm[1][0]) + rm[2][0]) / 3, ((rm[0][1] + rm[1][1]) + rm[2][1]) / 3};
+  cd js = mkcd(0, 0), ks = mkcd(0, 0);
+  int ok = 1;
+  if (q < 7) {
+    double rtx = (rs[0][0] + rs21[0] * c_qxi[q]) + rs31[0] * c_qeta[q];
+    double rty = (rs[0][1] + rs21[1] * c_qxi[q]) + rs31[1] * c_qeta[q];
+    ok = jksums_dev(ul * (rmc[0] - rtx), ul * (rmc[1] - rty), psi1, psi2, us1x, us1y, us2x, us2y, js, ks);
+  }
   cd aJ = mkcd(0, 0), aJx = aJ, aJe = aJ, aK = aJ, aKx = aJ, aKe = aJ;
   int bad = 0;
-  for (int i = 0; i < 7; ++i) {
-    double rtx = (rs[0][0] + rs21[0] * c_qxi[i]) + rs31[0] * c_qeta[i];
-    double rty = (rs[0][1] + rs21[1] * c_qxi[i]) + rs31[1] * c_qeta[i];
-    cd js, ks;
-    if (!jksums_warp(ul * (rmc[0] - rtx), ul * (rmc[1] - rty), psi1, psi2, us1x, us1y, us2x, us2y, lane, js, ks))
-      bad = 1;
-    cd jw = c_qw[i] * js;
+#pragma unroll
+  for (int i = 0; i < 7; ++i) {  // every lane takes part in the shuffles; the group's lane 0 keeps the sums
+    cd jv, kv;
+    jv.x = __shfl_sync(0xffffffffu, js.x, grp + i);
+    jv.y = __shfl_sync(0xffffffffu, js.y, grp + i);
+    kv.x = __shfl_sync(0xffffffffu, ks.x, grp + i);
+    kv.y = __shfl_sync(0xffffffffu, ks.y, grp + i);
+    bad |= !__shfl_sync(0xffffffffu, ok, grp + i);
+    cd jw = c_qw[i] * jv;
     aJx = aJx + c_qxi[i] * jw;
     aJe = aJe + c_qeta[i] * jw;
     aJ = aJ + jw;
-    cd kw = c_qw[i] * ks;
+    cd kw = c_qw[i] * kv;
     aKx = aKx + c_qxi[i] * kw;
     aKe = aKe + c_qeta[i] * kw;
     aK = aK + kw;
   }
+  if (q != 0 || !live) return;
   const int nxt[3] = {1, 2, 0};
   double rr0 = 0, rr1 = 0, ri = 0;
   for (int i = 0; i < 3; ++i) {
@@ -171,7 +159,6 @@ __device__ __forceinline__ void filljk_pair(const SheetDev &G, double ul, double
   rr0 /= area2;
   rr1 /= area2;
   ri /= (area2 * ul);
-  if (lane) return;
   jk.J[iu] = aJ; jk.Jxi[iu] = aJx; jk.Jeta[iu] = aJe;
   jk.K[iu] = aK; jk.Kxi[iu] = aKx; jk.Keta[iu] = aKe;
   jk.rho_r[2 * iu] = rr0;
@@ -319,14 +306,15 @@ __device__ __forceinline__ cd assemble_entry(const SheetDev &G, const PointParam
 // Z[m, n], row-major, leading dimension ld.
 __global__ void __launch_bounds__(256) k_assemble(SheetDev G, const PointParams *__restrict__ Pp,
                                                   const cd *__restrict__ zb, cd *__restrict__ z64,
-                                                  float *__restrict__ zr, float *__restrict__ zi, long long ld) {
+                                                  float *__restrict__ zr, float *__restrict__ zi, long long ld,
+                                                  long long ldf) {
   int n = blockIdx.x * blockDim.x + threadIdx.x;
   int m = blockIdx.y * blockDim.y + threadIdx.y;
   if (m >= G.nbf || n >= G.nbf) return;
   const cd acc = assemble_entry(G, *Pp, zb, m, n);
-  size_t o = (size_t)m * ld + n;
-  if (z64) z64[o] = acc;
+  if (z64) z64[(size_t)m * ld + n] = acc;
   if (zr) {
+    const size_t o = (size_t)m * ldf + n;
     zr[o] = (float)acc.x;
     zi[o] = (float)acc.y;
   }
@@ -424,14 +412,9 @@ void pss_filljk(const SheetDev &G, double ulocal, double psi1, double psi2, cons
                 JKDev jk, int *nonconv, cudaStream_t st) {
   if (G.nufp == 0) return;
   pss_count_launch();
-  int dev = 0, nsm = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  // a warp per pair, grid-strided: at most 8 resident 256-thread CTAs per SM are useful
-  const long long want = cdiv_u((long long)G.nufp * 32, 256);
-  const int grid = (int)std::min<long long>(want, (long long)nsm * 8);
-  k_filljk<<<grid, 256, 0, st>>>(G, ulocal, psi1, psi2, ulocal * s1[0], ulocal * s1[1], ulocal * s2[0],
-                                 ulocal * s2[1], jk, nonconv);
+  k_filljk<<<cdiv_u((long long)G.nufp * 8, 256), 256, 0, st>>>(G, ulocal, psi1, psi2, ulocal * s1[0],
+                                                                 ulocal * s1[1], ulocal * s2[0], ulocal * s2[1], jk,
+                                                                 nonconv);
 }
 
 void pss_fill_pairs(const SheetDev &G, const PointParams *dP1, const JKDev &jk, const cd *t1, const cd *t2,
@@ -442,9 +425,9 @@ void pss_fill_pairs(const SheetDev &G, const PointParams *dP1, const JKDev &jk, 
 }
 
 void pss_fill_assemble(const SheetDev &G, const PointParams *dP1, const cd *zb, cd *z64, float *zr, float *zi,
-                       long long ld, cudaStream_t st) {
+                       long long ld, long long ldf, cudaStream_t st) {
   dim3 blk(64, 4);
   dim3 grd(cdiv_u(G.nbf, 64), cdiv_u(G.nbf, 4));
   pss_count_launch();
-  k_assemble<<<grd, blk, 0, st>>>(G, dP1, zb, z64, zr, zi, ld);
+  k_assemble<<<grd, blk, 0, st>>>(G, dP1, zb, z64, zr, zi, ld, ldf);
 }

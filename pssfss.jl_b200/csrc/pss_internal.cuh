@@ -137,9 +137,10 @@ void pss_filljk(const SheetDev &G, double ulocal, double psi1, double psi2, cons
                 const double s2[2], JKDev jk, int *nonconv, cudaStream_t st);
 void pss_fill_pairs(const SheetDev &G, const PointParams *dP1, const JKDev &jk, const cd *t1, const cd *t2,
                     int mmax, cd *zb, cudaStream_t st);
-// Assemble Z (row-major, ld columns).  z64 and/or (zr, zi) may be null.
+// Assemble Z (row-major): z64 with leading dimension ld, the FP32 planes (zr, zi) with ldf.
+// z64 and/or (zr, zi) may be null.
 void pss_fill_assemble(const SheetDev &G, const PointParams *dP1, const cd *zb, cd *z64, float *zr, float *zi,
-                       long long ld, cudaStream_t st);
+                       long long ld, long long ldf, cudaStream_t st);
 
 // Basis-function transforms, right-hand sides, projection (pss_bfft.cu)
 void pss_bfft(const SheetDev &G, int nmodes, const double *kvec, double psi1, double psi2, cd *bf,
@@ -200,7 +201,7 @@ int pss_solve_prepare(SolveWS &ws, int nb, const cd *LU64, const float *Lr, cons
 int pss_solve_lu(SolveWS &ws, int nb, const cd *LU64, const float *Lr, const float *Li, long long ld, long long ms,
                  int nrhs, const cd *B, cd *X, long long vs, int use_done, cudaStream_t st);
 int pss_refine(SolveWS &ws, int nb, const cd *A, long long ld, long long ms, const float *Lr, const float *Li,
-               int nrhs, const cd *B, cd *X, cd *R, cd *D, long long vs, int maxit, int *status, cudaStream_t st);
+               long long ldf, long long msf, int nrhs, const cd *B, cd *X, cd *R, cd *D, long long vs, int maxit, int *status, cudaStream_t st);
 void pss_solve_status(SolveWS &ws, int nb, int *status, cudaStream_t st);
 // Adjoint (transposed) solves on the same factors: Y = Z^-T B (W: scratch like B), and their
 // FP64 refinement against A (FP32 factors) with a scratch of pss_refine_trans_ws_bytes.
@@ -209,5 +210,5 @@ int pss_solve_lu_trans(SolveWS &ws, int nb, const cd *LU64, const float *Lr, con
                        cudaStream_t st);
 size_t pss_refine_trans_ws_bytes(int n, int nrhs, int nb);
 int pss_refine_trans(SolveWS &ws, int nb, const cd *A, long long ld, long long ms, const float *Lr, const float *Li,
-                     int nrhs, const cd *B, cd *Y, cd *R, cd *D, cd *W, void *scratch, size_t scratch_bytes,
+                     long long ldf, long long msf, int nrhs, const cd *B, cd *Y, cd *R, cd *D, cd *W, void *scratch, size_t scratch_bytes,
                      long long vs, int maxit, int *status, cudaStream_t st);

@@ -623,7 +623,7 @@ void pss_solve_status(SolveWS &ws, int nb, int *status, cudaStream_t st) {
 // Iterative refinement of each X_b against its FP64 matrix A_b (FP32 factors), up to
 // maxit steps; matrices that converge drop out (their converged word).
 int pss_refine(SolveWS &ws, int nb, const cd *A, long long ld, long long ms, const float *Lr, const float *Li,
-               int nrhs, const cd *B, cd *X, cd *R, cd *D, long long vs, int maxit, int *status, cudaStream_t st) {
+               long long ldf, long long msf, int nrhs, const cd *B, cd *X, cd *R, cd *D, long long vs, int maxit, int *status, cudaStream_t st) {
   if (nrhs > kMaxRefRhs) { pss_set_error("refinement supports at most %d right-hand sides", kMaxRefRhs); return -1; }
   const Ctrl ctrl{ws.ctrl, ws.cstride};
   static DeviceOnce once;
@@ -645,7 +645,7 @@ int pss_refine(SolveWS &ws, int nb, const cd *A, long long ld, long long ms, con
     pss_count_launch();
     k_ir_check<<<nb, 1, 0, st>>>(ws.n, nrhs, ws.norms, ctrl, status, it == maxit);
     if (it == maxit) break;
-    int rc = pss_solve_lu(ws, nb, nullptr, Lr, Li, ld, ms, nrhs, R, D, vs, 1, st);
+    int rc = pss_solve_lu(ws, nb, nullptr, Lr, Li, ldf, msf, nrhs, R, D, vs, 1, st);
     if (rc) return rc;
     pss_count_launch();
     k_axpy<<<dim3(cdiv_u(total, 256), nb), 256, 0, st>>>(total, X, D, vs, ctrl);
@@ -708,7 +708,7 @@ size_t pss_refine_trans_ws_bytes(int n, int nrhs, int nb) {
 // matrices, as pss_refine: r = B - Z^T Y in FP64 (two-stage, fixed order), correction from the
 // FP32 factors (pss_solve_lu_trans), the same stopping rule with ||Z^T||_inf.
 int pss_refine_trans(SolveWS &ws, int nb, const cd *A, long long ld, long long ms, const float *Lr, const float *Li,
-                     int nrhs, const cd *B, cd *Y, cd *R, cd *D, cd *W, void *scratch, size_t scratch_bytes,
+                     long long ldf, long long msf, int nrhs, const cd *B, cd *Y, cd *R, cd *D, cd *W, void *scratch, size_t scratch_bytes,
                      long long vs, int maxit, int *status, cudaStream_t st) {
   if (nrhs > kMaxRefRhs) { pss_set_error("refinement supports at most %d right-hand sides", kMaxRefRhs); return -1; }
   if (scratch_bytes < pss_refine_trans_ws_bytes(ws.n, nrhs, nb)) {
@@ -732,7 +732,7 @@ int pss_refine_trans(SolveWS &ws, int nb, const cd *A, long long ld, long long m
     pss_count_launch();
     k_ir_check<<<nb, 1, 0, st>>>(ws.n, nrhs, ws.norms, ctrl, status, it == maxit);
     if (it == maxit) break;
-    int rc = pss_solve_lu_trans(ws, nb, nullptr, Lr, Li, ld, ms, nrhs, R, D, W, vs, 1, st);
+    int rc = pss_solve_lu_trans(ws, nb, nullptr, Lr, Li, ldf, msf, nrhs, R, D, W, vs, 1, st);
     if (rc) return rc;
     pss_count_launch();
     k_axpy<<<dim3(cdiv_u(total, 256), nb), 256, 0, st>>>(total, Y, D, vs, ctrl);
