@@ -98,6 +98,21 @@ struct DevBuf {
   T *as() const { return (T *)p; }
 };
 
+// A DevBuf owned by one scope: freed when it goes out of scope (DevBuf itself is a plain
+// handle, copied into containers, and never frees on its own).
+struct LocalBuf : DevBuf {
+  LocalBuf() = default;
+  LocalBuf(const LocalBuf &) = delete;
+  LocalBuf &operator=(const LocalBuf &) = delete;
+  LocalBuf(LocalBuf &&o) noexcept {
+    p = o.p;
+    n = o.n;
+    o.p = nullptr;
+    o.n = 0;
+  }
+  ~LocalBuf() { release(); }
+};
+
 struct JKBufs {
   DevBuf buf;
   JKDev jk{};
@@ -659,12 +674,23 @@ int check_problem(const pss_problem &q, int precision, Problem &P) {
   return 0;
 }
 
+// The adjoint stage of a sweep (pss_partial_gsms_adj): problems 1..K of the call are the
+// perturbed input sets of problem 0 - their tables, face integrals and mode data are prepared
+// with the sweep, but they take no factorisation; after each batched factorisation of problem
+// 0's points the adjoint solves Lam = Z^-T P^T run on the same factors, and every set k gets
+//   dSp[k][i] = wobs_k o (P_k X)   and   G[k][i] = Lam^T (R_k - Z_k X)   (device, nm^2 each).
+struct AdjSpec {
+  int K = 0;
+  cd *dSp = nullptr;
+  cd *G = nullptr;
+};
+
 // The sweep of every problem on one context: tables of all points, then a shared work list of
 // (problem, batch of like-N points) items, largest matrices first, taken by one host thread
 // per worker stream; each item runs fill -> batched LU -> solves (+ refinement) -> projection
 // on its worker.  FP32 points whose refinement stalls are redone in FP64; then dS and status
 // go back to each problem's caller arrays.
-int sweep_impl(pss_ctx *c, std::vector<Problem> &PR, int precision) {
+int sweep_impl(pss_ctx *c, std::vector<Problem> &PR, int precision, const AdjSpec *adj = nullptr) {
   if (set_device(c)) return -3;
   // global point numbering, mode-array bases, parameters
   int total = 0;
@@ -756,8 +782,8 @@ int sweep_impl(pss_ctx *c, std::vector<Problem> &PR, int precision) {
   struct Item { int cnt; int p[kMaxBatch]; int i[kMaxBatch]; };
   std::vector<Item> items;
   {
-    std::vector<std::pair<int, int>> pts;  // (problem, point)
-    for (size_t p = 0; p < PR.size(); ++p)
+    std::vector<std::pair<int, int>> pts;  // (problem, point); with an adjoint stage only problem 0
+    for (size_t p = 0; p < (adj ? 1 : PR.size()); ++p)
       for (int i = 0; i < PR[p].npts; ++i) pts.push_back({(int)p, i});
     std::stable_sort(pts.begin(), pts.end(), [&](const std::pair<int, int> &a, const std::pair<int, int> &b) {
       const Problem &A = PR[a.first], &Bq = PR[b.first];
@@ -791,8 +817,27 @@ int sweep_impl(pss_ctx *c, std::vector<Problem> &PR, int precision) {
       }
       mB = std::max(mB, it.cnt);
     }
+    for (auto &P : PR) {  // the perturbed sets' pair terms go through the same buffers
+      mufp = std::max(mufp, P.sh->nufp);
+      ojk = ojk || P.own_jk;
+    }
     for (int k = 0; k < nwk; ++k)
       if (int rc = ensure_worker_dims(c->w[k], mufp, mn, mnm, precision, ojk, mB)) return rc;
+  }
+  // adjoint-stage buffers of every worker: PT, Lam, scratch W (a batch each), R_k and the
+  // set's transforms (one point each), the contraction's CTA shares, refinement scratch
+  struct AdjBufs { LocalBuf v, rtw, part; };
+  std::vector<AdjBufs> ab(adj ? nwk : 0);
+  long long adj_mB = 0;
+  if (adj) {
+    const int n0 = PR[0].sh->nbf, nm0 = PR[0].nm;
+    const size_t vs0 = (size_t)n0 * nm0;
+    for (auto &it : items) adj_mB = std::max<long long>(adj_mB, it.cnt);
+    for (auto &A : ab)
+      if (A.v.ensure((3 * (size_t)adj_mB + 3) * vs0 * sizeof(cd)) ||
+          A.rtw.ensure(precision == PSS_FP32_REFINE ? pss_refine_trans_ws_bytes(n0, nm0, (int)adj_mB) : 0) ||
+          A.part.ensure(pss_adj_part_bytes(n0, nm0)))
+        return -3;
   }
   std::vector<cudaEvent_t> ev;  // phase events of worker 0's batches (pushed by its thread only)
   std::vector<KProf> kprofs(nwk);
@@ -853,6 +898,51 @@ int sweep_impl(pss_ctx *c, std::vector<Problem> &PR, int precision) {
     PSS_CUDA_TRY(cudaMemsetAsync(w.bstat.p, 0, (size_t)cnt * sizeof(int), st));
     int rc2 = w.factor_solve(n, cnt, prec, nm, kMaxRefine, w.bstat.as<int>(), P0.panel_w, P0.outer_nb);
     if (rc2) return rc2;
+    if (adj) {
+      AdjBufs &A = ab[&w - c->w.data()];
+      cd *PT = A.v.as<cd>(), *Lam = PT + adj_mB * vsz, *Wt = Lam + adj_mB * vsz, *Rk = Wt + adj_mB * vsz;
+      cd *bfk = Rk + vsz;
+      for (int b = 0; b < cnt; ++b) {
+        const Problem &P = PR[it.p[b]];
+        pss_proj_rows(n, nm, w.bf.as<cd>() + (size_t)b * nm * n * 2, dtob + P.tb + (size_t)it.i[b] * nm * 2,
+                      PT + b * vsz, st);
+      }
+      const cd *L64 = prec == PSS_FP64 ? w.z64.as<cd>() : nullptr;
+      const long long fld = L64 ? ld : ldf, fms = L64 ? msz : msf;
+      if ((rc2 = pss_solve_lu_trans(w.sws, cnt, L64, zr, zi, fld, fms, nm, PT, Lam, Wt, vsz, 0, st))) return rc2;
+      if (prec == PSS_FP32_REFINE &&
+          (rc2 = pss_refine_trans(w.sws, cnt, w.z64.as<cd>(), ld, msz, zr, zi, ldf, msf, nm, PT, Lam, w.R.as<cd>(),
+                                  w.D.as<cd>(), Wt, A.rtw.p, A.rtw.n, vsz, kMaxRefine, w.bstat.as<int>(), st)))
+        return rc2;
+      pss_solve_status(w.sws, cnt, w.bstat.as<int>(), st);
+      const int np0 = PR[0].npts;
+      for (int b = 0; b < cnt; ++b) {
+        const int i = it.i[b];
+        const cd *Xb = w.X.as<cd>() + b * vsz;
+        for (int k = 0; k < adj->K; ++k) {
+          const Problem &Q = PR[1 + k];
+          const int gq = Q.p0 + i;
+          JKDev jq;
+          if (!Q.own_jk) {
+            jq = Q.sh->cache.jk;
+          } else {
+            jq = w.jk.jk;
+            pss_filljk(Q.sh->G, Q.u / Q.sh->upm, Q.psi[2 * i], Q.psi[2 * i + 1], Q.sh->s1, Q.sh->s2, jq,
+                       w.nonconv.as<int>(), st);
+            pss_count_launch();
+            k_nonconv_to_status<<<1, 1, 0, st>>>(w.nonconv.as<int>(), dstatus + PR[0].p0 + i);
+          }
+          pss_fill_pairs(Q.sh->G, dP + gq, jq, tabs[gq].t1, tabs[gq].t2, tabs[gq].mmax, w.zb.as<cd>(), st);
+          pss_bfft(Q.sh->G, nm, dkv + Q.kb + (size_t)i * nm * 2, Q.psi[2 * i], Q.psi[2 * i + 1], bfk, st);
+          pss_rhs(n, nm, bfk, dsrc + Q.sb + (size_t)i * nm * 2, Rk, st);
+          const size_t o = ((size_t)k * np0 + i) * nm2;
+          pss_project(n, nm, bfk, dtob + Q.tb + (size_t)i * nm * 2, dwob + Q.wb + (size_t)i * nm, Xb, adj->dSp + o,
+                      st);
+          pss_adj_contract(Q.sh->G, dP + gq, w.zb.as<cd>(), Xb, Rk, Lam + b * vsz, nm, A.part.as<cd>(), adj->G + o,
+                           st);
+        }
+      }
+    }
     StatusMap sm{};
     for (int b = 0; b < cnt; ++b) sm.idx[b] = PR[it.p[b]].p0 + it.i[b];
     pss_count_launch();
@@ -1113,7 +1203,7 @@ int pss_basis_transforms(pss_sheet *sh, int nmodes, const double *kvec, double p
   pss_ctx *c = sh->ctx;
   if (set_device(c)) return -3;
   Worker &w = c->w[0];
-  DevBuf kb;
+  LocalBuf kb;
   if (upload(kb, kvec, 2 * (size_t)nmodes)) return -3;
   if (w.bf.ensure((size_t)nmodes * sh->nbf * 2 * sizeof(cd))) return -3;
   pss_bfft(sh->G, nmodes, kb.as<double>(), psi1, psi2, w.bf.as<cd>(), w.st);
@@ -1196,7 +1286,7 @@ int pss_schur_update(pss_ctx *c, int m, int n, int k, const float *Lr, const flo
     }
   }
   const size_t tcb = pss_tc_ws_bytes(m, n, (k + 15) / 16 * 16);
-  DevBuf ar, ai, ws, err;
+  LocalBuf ar, ai, ws, err;
   if (ar.ensure(total * sizeof(float)) || ai.ensure(total * sizeof(float)) || ws.ensure(tcb) ||
       err.ensure(sizeof(int)))
     return -3;
@@ -1320,8 +1410,8 @@ extern "C" int pss_partial_gsms_lin(pss_sheet *sh, int nl, const double *eps, co
   int maxufp = sh->nufp;
   for (int k = 0; k < K; ++k) maxufp = std::max(maxufp, psh[k]->nufp);
   if (w.zb.ensure((size_t)maxufp * 9 * sizeof(cd))) return -3;
-  DevBuf pbuf, tb0, mbuf, Ybuf, Wbuf, out;
-  std::vector<DevBuf> tbk(K);
+  LocalBuf pbuf, tb0, mbuf, Ybuf, Wbuf, out;
+  std::vector<LocalBuf> tbk(K);
   if (pbuf.ensure((size_t)(1 + K) * sizeof(PointParams)) ||
       mbuf.ensure((size_t)(1 + K) * nm * (2 * sizeof(double) + 2 * sizeof(cd) + 2 * sizeof(double) + sizeof(cd))) ||
       Ybuf.ensure((size_t)n * std::max(nrhs2, 1) * sizeof(cd)) || Wbuf.ensure((size_t)n * std::max(nrhs2, 1) * sizeof(cd)) ||
@@ -1453,11 +1543,13 @@ extern "C" int pss_partial_gsms_lin(pss_sheet *sh, int nl, const double *eps, co
 
 // Adjoint form of the linearised partial GSMs (same inputs and outputs as
 // pss_partial_gsms_lin):  dSp[k] = wobs_k o (P_k X + Lam^T (R_k - Z_k X)),  X = Z^-1 R,
-// Lam = Z^-T P^T.  Per point: one fill of Z, one factorisation, nm forward and nm adjoint
-// solves on the same factors; each perturbed set then costs its pair terms (Green's-function
-// table interpolations recomputed for the set), its basis transforms and one fused
-// assemble-and-contract pass (pss_adj_contract) - no perturbed matrix is stored and no
-// further solve is taken.
+// Lam = Z^-T P^T.  The points are swept as pss_partial_gsms sweeps them (batched fills and
+// factorisations on the worker streams), the perturbed sets riding along as extra problems
+// whose tables, face integrals and mode data are prepared with the sweep; after each batched
+// factorisation the adjoint solves run on the same factors, and each perturbed set costs its
+// pair terms (Green's-function table interpolations recomputed for the set), its basis
+// transforms and one fused assemble-and-contract pass (pss_adj_contract) - no perturbed
+// matrix is stored and no further solve is taken.
 extern "C" int pss_partial_gsms_adj(pss_sheet *sh, int nl, const double *eps, const double *mu, const double *width,
                                     int s, double u, int npts, const double *k0, const double *psi, int nmodes,
                                     const double *kvec, const double *src, const double *tobs, const double *wobs,
@@ -1477,152 +1569,50 @@ extern "C" int pss_partial_gsms_adj(pss_sheet *sh, int nl, const double *eps, co
     pss_set_error("null perturbation argument");
     return -1;
   }
-  if (precision != PSS_FP64 && precision != PSS_FP32_REFINE) { pss_set_error("unknown precision %d", precision); return -1; }
   for (int k = 0; k < npert; ++k)
     if (!psh[k] || psh[k]->ctx != sh->ctx || psh[k]->nbf != sh->nbf || psh[k]->cls != sh->cls) {
       pss_set_error("perturbed sheet %d is not a sheet of the same context, class and basis count", k);
       return -1;
     }
-  if (!(u > 0)) { pss_set_error("smoothing parameter u must be positive"); return -1; }
+  const int K = npert, nm = nmodes;
+  const size_t nm2 = (size_t)nm * nm, per = (size_t)npts * nm;
+  std::vector<Problem> PR(1 + K);
+  pss_problem q0{sh, nl, eps, mu, width, s, u, npts, k0, psi, nmodes, kvec, src, tobs, wobs, 0, 0, 0, dS, status};
+  if (int rc = check_problem(q0, precision, PR[0])) return rc;
+  // the perturbed sets' own dS and status are not produced (they take no solve): scratch
+  std::vector<double> kdS((size_t)std::max(K, 1) * npts * nm2 * 2);
+  std::vector<int> kst((size_t)std::max(K, 1) * npts);
+  for (int k = 0; k < K; ++k) {
+    pss_problem qk{psh[k], nl, peps + 2 * (size_t)k * nl, pmu + 2 * (size_t)k * nl, pwidth + (size_t)k * nl, s,
+                   pu[k], npts, k0, ppsi + 2 * (size_t)k * npts, nmodes, pkvec + 2 * k * per, psrc + 4 * k * per,
+                   ptobs + 2 * k * per, pwobs + 2 * k * per, 0, 0, 0, kdS.data() + (size_t)k * npts * nm2 * 2,
+                   kst.data() + (size_t)k * npts};
+    if (int rc = check_problem(qk, precision, PR[1 + k])) {
+      const std::string m = pss_last_error();
+      pss_set_error("perturbed set %d: %s", k, m.c_str());
+      return rc;
+    }
+  }
   pss_ctx *c = sh->ctx;
   if (set_device(c)) return -3;
-  const int magnetic = sh->cls == 'M';
-  const int n = sh->nbf, nm = nmodes, K = npert;
-  const long long ld = n, msz = (long long)n * n, vsz = (long long)n * nm;
-  StackParams S;
-  if (make_stack(nl, eps, mu, width, s, S)) return -1;
-  std::vector<StackParams> Sk(K);
-  for (int k = 0; k < K; ++k) {
-    if (make_stack(nl, peps + 2 * (size_t)k * nl, pmu + 2 * (size_t)k * nl, pwidth + (size_t)k * nl, s, Sk[k]))
-      return -1;
-    if (!(pu[k] > 0)) { pss_set_error("perturbed smoothing parameter %d must be positive", k); return -1; }
-  }
-  Worker &w = c->w[0];
-  cudaStream_t st = w.st;
-  int rc = ensure_worker(w, sh, nm, precision, false, 1);
-  if (rc) return rc;
-  int maxufp = sh->nufp;
-  for (int k = 0; k < K; ++k) maxufp = std::max(maxufp, psh[k]->nufp);
-  if (w.zb.ensure((size_t)maxufp * 9 * sizeof(cd))) return -3;
-  DevBuf pbuf, tb0, mbuf, vbuf, rtw, part, gout, out;
-  std::vector<DevBuf> tbk(K);
-  const size_t nvec = (size_t)vsz;  // one n x nm block
-  // vectors: PT, Lam, W (adjoint scratch), Rk, bfk (nm x n x 2)
-  if (pbuf.ensure((size_t)(1 + K) * sizeof(PointParams)) ||
-      mbuf.ensure((size_t)(1 + K) * nm * (2 * sizeof(double) + 2 * sizeof(cd) + 2 * sizeof(double) + sizeof(cd))) ||
-      vbuf.ensure((4 * nvec + 2 * nvec) * sizeof(cd)) ||
-      rtw.ensure(precision == PSS_FP32_REFINE ? pss_refine_trans_ws_bytes(n, nm, 1) : 0) ||
-      part.ensure(pss_adj_part_bytes(n, nm)) || gout.ensure((size_t)std::max(K, 1) * nm * nm * sizeof(cd)) ||
-      out.ensure((size_t)(1 + K) * nm * nm * sizeof(cd)))
-    return -3;
-  cd *PT = vbuf.as<cd>(), *Lam = PT + nvec, *Wt = Lam + nvec, *Rk = Wt + nvec, *bfk = Rk + nvec;
-  const size_t nmk = (size_t)nm * 2;
-  char *mb = mbuf.as<char>();
-  auto kv_of = [&](int q) { return (double *)mb + (size_t)q * nmk; };
-  auto src_of = [&](int q) { return (cd *)(mb + (size_t)(1 + K) * nmk * sizeof(double)) + (size_t)q * nmk; };
-  auto tob_of = [&](int q) {
-    return (double *)(mb + (size_t)(1 + K) * nmk * (sizeof(double) + sizeof(cd))) + (size_t)q * nmk;
-  };
-  auto wob_of = [&](int q) {
-    return (cd *)(mb + (size_t)(1 + K) * nmk * (2 * sizeof(double) + sizeof(cd))) + (size_t)q * nm;
-  };
-  const size_t nm2 = (size_t)nm * nm;
-  std::vector<cd> hout((1 + K) * nm2), hG(std::max(K, 1) * nm2), hw((1 + K) * (size_t)nm);
-  float *zr = precision == PSS_FP32_REFINE ? w.zr.as<float>() : nullptr;
-  float *zi = precision == PSS_FP32_REFINE ? w.zi.as<float>() : nullptr;
-  const cd *L64 = precision == PSS_FP64 ? w.z64.as<cd>() : nullptr;
-  for (int i = 0; i < npts; ++i) {
-    if (!(k0[i] > 0) || !std::isfinite(psi[2 * i]) || !std::isfinite(psi[2 * i + 1])) {
-      pss_set_error("invalid k0/psi at point %d", i);
-      return -1;
-    }
-    int hst = 0;
-    std::vector<PointParams> hP(1 + K);
-    {
-      const double b1m[2] = {sh->b1[0] * sh->upm, sh->b1[1] * sh->upm};
-      const double b2m[2] = {sh->b2[0] * sh->upm, sh->b2[1] * sh->upm};
-      make_params(magnetic, S, b1m, b2m, u, k0[i], psi[2 * i], psi[2 * i + 1], hP[0]);
-    }
-    for (int k = 0; k < K; ++k) {
-      const pss_sheet *q = psh[k];
-      const double b1m[2] = {q->b1[0] * q->upm, q->b1[1] * q->upm};
-      const double b2m[2] = {q->b2[0] * q->upm, q->b2[1] * q->upm};
-      const double *pp = ppsi + 2 * ((size_t)k * npts + i);
-      make_params(magnetic, Sk[k], b1m, b2m, pu[k], k0[i], pp[0], pp[1], hP[1 + k]);
-    }
-    PSS_CUDA_TRY(cudaMemcpyAsync(pbuf.p, hP.data(), hP.size() * sizeof(PointParams), cudaMemcpyHostToDevice, st));
-    const PointParams *dP = pbuf.as<PointParams>();
-    for (int q = 0; q <= K; ++q) {
-      const size_t off = q == 0 ? (size_t)i * nm : ((size_t)(q - 1) * npts + i) * nm;
-      const double *kv = q == 0 ? kvec : pkvec;
-      const double *sv = q == 0 ? src : psrc;
-      const double *tv = q == 0 ? tobs : ptobs;
-      const double *wv = q == 0 ? wobs : pwobs;
-      PSS_CUDA_TRY(cudaMemcpyAsync(kv_of(q), kv + 2 * off, nm * 2 * sizeof(double), cudaMemcpyHostToDevice, st));
-      PSS_CUDA_TRY(cudaMemcpyAsync(src_of(q), sv + 4 * off, nm * 2 * sizeof(cd), cudaMemcpyHostToDevice, st));
-      PSS_CUDA_TRY(cudaMemcpyAsync(tob_of(q), tv + 2 * off, nm * 2 * sizeof(double), cudaMemcpyHostToDevice, st));
-      PSS_CUDA_TRY(cudaMemcpyAsync(wob_of(q), wv + 2 * off, nm * sizeof(cd), cudaMemcpyHostToDevice, st));
-      for (int a = 0; a < nm; ++a) hw[(size_t)q * nm + a] = mkcd(wv[2 * (off + a)], wv[2 * (off + a) + 1]);
-    }
-    // the unperturbed point: tables, face integrals, Z (+ FP32 planes), transforms, R
-    TableDev t0;
-    std::vector<TableDev> tk(K);
-    if ((rc = point_tables(c, S, dP, tb0, t0, hst))) return rc;
+  LocalBuf dbuf;
+  if (dbuf.ensure(2 * std::max<size_t>((size_t)K * npts * nm2, 1) * sizeof(cd))) return -3;
+  AdjSpec adj{K, dbuf.as<cd>(), dbuf.as<cd>() + std::max<size_t>((size_t)K * npts * nm2, 1)};
+  if (int rc = sweep_impl(c, PR, precision, &adj)) return rc;
+  if (K > 0) {
+    std::vector<cd> hP((size_t)K * npts * nm2), hG((size_t)K * npts * nm2);
+    PSS_CUDA_TRY(cudaMemcpy(hP.data(), adj.dSp, hP.size() * sizeof(cd), cudaMemcpyDeviceToHost));
+    PSS_CUDA_TRY(cudaMemcpy(hG.data(), adj.G, hG.size() * sizeof(cd), cudaMemcpyDeviceToHost));
     for (int k = 0; k < K; ++k)
-      if ((rc = point_tables(c, Sk[k], dP + 1 + k, tbk[k], tk[k], hst))) return rc;
-    if ((rc = refresh_jk_cache(sh, psi[2 * i], psi[2 * i + 1], u / sh->upm, st))) return rc;
-    if (sh->jk_nonconv) hst |= PSS_ST_JK_NOCONV;
-    pss_fill_pairs(sh->G, dP, sh->cache.jk, t0.t1, t0.t2, t0.mmax, w.zb.as<cd>(), st);
-    pss_fill_assemble(sh->G, dP, w.zb.as<cd>(), w.z64.as<cd>(), zr, zi, ld, Worker::ld32(n), st);
-    cd *bf = w.bf.as<cd>();
-    pss_bfft(sh->G, nm, kv_of(0), psi[2 * i], psi[2 * i + 1], bf, st);
-    pss_rhs(n, nm, bf, src_of(0), w.rhs.as<cd>(), st);
-    pss_proj_rows(n, nm, bf, tob_of(0), PT, st);
-    // one factorisation; X = Z^-1 R (forward) and Lam = Z^-T P^T (adjoint), both refined
-    // against the FP64 Z in the FP32 form
-    PSS_CUDA_TRY(cudaMemsetAsync(w.bstat.p, 0, sizeof(int), st));
-    if ((rc = w.factor_solve(n, 1, precision, nm, kMaxRefine, w.bstat.as<int>()))) return rc;
-    const long long fld = L64 ? ld : Worker::ld32(n), fms = (long long)n * fld;
-    if ((rc = pss_solve_lu_trans(w.sws, 1, L64, zr, zi, fld, fms, nm, PT, Lam, Wt, vsz, 0, st))) return rc;
-    if (precision == PSS_FP32_REFINE &&
-        (rc = pss_refine_trans(w.sws, 1, w.z64.as<cd>(), ld, msz, zr, zi, fld, fms, nm, PT, Lam, w.R.as<cd>(), w.D.as<cd>(),
-                               Wt, rtw.p, rtw.n, vsz, kMaxRefine, w.bstat.as<int>(), st)))
-      return rc;
-    pss_solve_status(w.sws, 1, w.bstat.as<int>(), st);
-    cd *X = w.X.as<cd>();
-    cd *o = out.as<cd>();
-    pss_project(n, nm, bf, tob_of(0), wob_of(0), X, o, st);
-    // every perturbed set: its pair terms, transforms and right-hand sides, P_k X, and the
-    // contraction Lam^T (R_k - Z_k X) assembled on the fly
-    for (int k = 0; k < K; ++k) {
-      pss_sheet *q = psh[k];
-      const double *pp = ppsi + 2 * ((size_t)k * npts + i);
-      if ((rc = refresh_jk_cache(q, pp[0], pp[1], pu[k] / q->upm, st))) return rc;
-      if (q->jk_nonconv) hst |= PSS_ST_JK_NOCONV;
-      pss_fill_pairs(q->G, dP + 1 + k, q->cache.jk, tk[k].t1, tk[k].t2, tk[k].mmax, w.zb.as<cd>(), st);
-      pss_bfft(q->G, nm, kv_of(1 + k), pp[0], pp[1], bfk, st);
-      pss_rhs(n, nm, bfk, src_of(1 + k), Rk, st);
-      pss_project(n, nm, bfk, tob_of(1 + k), wob_of(1 + k), X, o + (1 + k) * nm2, st);
-      pss_adj_contract(q->G, dP + 1 + k, w.zb.as<cd>(), X, Rk, Lam, nm, part.as<cd>(), gout.as<cd>() + k * nm2, st);
-    }
-    int bst = 0;
-    PSS_CUDA_TRY(cudaMemcpyAsync(hout.data(), o, hout.size() * sizeof(cd), cudaMemcpyDeviceToHost, st));
-    if (K > 0)
-      PSS_CUDA_TRY(cudaMemcpyAsync(hG.data(), gout.p, (size_t)K * nm2 * sizeof(cd), cudaMemcpyDeviceToHost, st));
-    PSS_CUDA_TRY(cudaMemcpyAsync(&bst, w.bstat.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-    PSS_CUDA_TRY(cudaStreamSynchronize(st));
-    status[i] = hst | bst;
-    for (size_t e = 0; e < nm2; ++e) {
-      dS[2 * ((size_t)i * nm2 + e)] = hout[e].x;
-      dS[2 * ((size_t)i * nm2 + e) + 1] = hout[e].y;
-    }
-    for (int k = 0; k < K; ++k)
-      for (size_t e = 0; e < nm2; ++e) {
-        const size_t a = e % nm;  // row (observation mode) of entry e, column-major
-        const cd v = hout[(1 + k) * nm2 + e] + hw[(size_t)(1 + k) * nm + a] * hG[k * nm2 + e];
-        const size_t d = ((size_t)k * npts + i) * nm2 + e;
-        dSp[2 * d] = v.x;
-        dSp[2 * d + 1] = v.y;
+      for (int i = 0; i < npts; ++i) {
+        const double *wk = pwobs + 2 * (k * per + (size_t)i * nm);
+        for (size_t e = 0; e < nm2; ++e) {
+          const size_t a = e % nm, d = ((size_t)k * npts + i) * nm2 + e;  // a: observation mode (row)
+          const cd v = hP[d] + mkcd(wk[2 * a], wk[2 * a + 1]) * hG[d];
+          dSp[2 * d] = v.x;
+          dSp[2 * d + 1] = v.y;
+        }
+        status[i] |= kst[(size_t)k * npts + i];  // the sets' table / face-integral flags
       }
   }
   return 0;

@@ -107,8 +107,11 @@ def linearized_gradient(build, params, flist, steering, objective, partial_lin=N
                 raise ValueError(f"step changes the mesh topology: {topology(p)} != {key0} at {p}")
             steps.append((name, h, p))
     cache = {}  # steps of layer parameters keep the sheet's geometry: one RWG setup serves them
-    plan0 = make_plan(build(p0), flist, steering, plan_flist, rwg_cache=cache)
-    plans = [make_plan(build(p), flist, steering, plan_flist, rwg_cache=cache) for _, _, p in steps]
+    strata0 = build(p0)
+    stratas = [build(p) for _, _, p in steps]
+    _prefill_rwg(cache, [strata0] + stratas)
+    plan0 = make_plan(strata0, flist, steering, plan_flist, rwg_cache=cache)
+    plans = [make_plan(st, flist, steering, plan_flist, rwg_cache=cache) for st in stratas]
     blocks = sheet_gblocks(plan0)
     for pl in plans:
         if (sheet_gblocks(pl) != blocks or len(pl.points) != len(plan0.points)
@@ -137,6 +140,27 @@ def linearized_gradient(build, params, flist, steering, objective, partial_lin=N
         name, h, _ = steps[k]
         grad[name] = (fs[k] - fs[k + 1]) / (2 * h)
     return f0, grad
+
+
+def _prefill_rwg(cache, stratas):
+    """Basis-function setup (``setup_rwg``) of every distinct sheet geometry of the steps,
+    concurrently: the face-pair classing is a few large numpy sorts that release the GIL."""
+    from concurrent.futures import ThreadPoolExecutor
+    from .analyze import _geometry_key
+    from .rwg import setup_rwg
+    from .sheets import RWGSheet
+    todo = {}
+    for st in stratas:
+        for sh in st:
+            if isinstance(sh, RWGSheet) and sh.style != "NULL":
+                key = _geometry_key(sh)
+                if key not in cache and key not in todo:
+                    todo[key] = sh
+    if not todo:
+        return
+    with ThreadPoolExecutor(max_workers=min(len(todo), 8)) as ex:
+        for key, rwg in zip(todo, ex.map(setup_rwg, todo.values())):
+            cache[key] = rwg
 
 
 def meander_linearized_gradient(params, flist, partial_lin=None, *, ntri=4000, rel_step=1e-4):
