@@ -37,7 +37,11 @@ __device__ __forceinline__ int jksums_dev(double urx, double ury, double psi1, d
       ring_mn(r, t, m, n);
       double dx = urx - ((double)m * us1x + (double)n * us2x);
       double dy = ury - ((double)m * us1y + (double)n * us2y);
-      double a = sqrt(dx * dx + dy * dy);
+      // one reciprocal square root gives both the distance and the 1/r weight (two FP64
+      // divisions fewer per summand than sqrt then term / r)
+      const double d2 = dx * dx + dy * dy;
+      const double ra = rsqrt(d2);
+      const double a = d2 * ra;
       double er = exp(-a);
       cd term;
       if (nophase) {
@@ -51,7 +55,7 @@ __device__ __forceinline__ int jksums_dev(double urx, double ury, double psi1, d
           term = mkcd(er * c, er * s);
         }
       }
-      jring = jring + term / a;
+      jring = jring + mkcd(term.x * ra, term.y * ra);
       kring = kring + term;
     }
     jsum = jsum + jring;

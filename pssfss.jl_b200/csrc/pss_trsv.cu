@@ -158,7 +158,7 @@ __device__ __forceinline__ C czero() { return C{0, 0}; }
 // the load; Dinv_b (dynamic shared memory) and the block's right-hand side are staged at
 // the start.  Blocks of X written by other CTAs are read with L1-bypassing loads.
 template <bool LOWER, bool F32, int NJ, bool TRANS = false>
-__global__ void __launch_bounds__(256, F32 ? 4 : 1) k_trsv(Fac F0, int n, const int *__restrict__ perm0, const cd *__restrict__ B0,
+__global__ void __launch_bounds__(256, F32 ? 2 : 1) k_trsv(Fac F0, int n, const int *__restrict__ perm0, const cd *__restrict__ B0,
                                               cd *__restrict__ X0, long long vs, int nrhs, int j0,
                                               const cd *__restrict__ Dinv0, long long dstride, Ctrl ctrl, int epoch,
                                               int use_done) {
@@ -198,10 +198,72 @@ __global__ void __launch_bounds__(256, F32 ? 4 : 1) k_trsv(Fac F0, int n, const 
       v = LOWER ? B[(size_t)(j0 + j) * n + (TRANS ? r0 + r : perm[r0 + r])] : ldcg(&X[(size_t)(j0 + j) * n + r0 + r]);
     y[r][j] = T::from(v);
   }
+  const int c_lo = LOWER ? 0 : b + 1, c_hi = LOWER ? b : nblk;
+  if constexpr (F32 && !TRANS && NJ == 4) {
+    // Coalesced form for the FP32 factors of the sweep: warp w owns rows 8w .. 8w+7 of the
+    // block, lane l columns l and l + 32 of every 64-column tile, so each load instruction of
+    // a warp reads one contiguous 128-byte row segment; the lane's partial sums run over all
+    // tiles and are reduced across the warp once at the end.  Each warp waits for x_c on its
+    // own (lane 0 polls the flag), so no block barrier sits in the tile loop.
+    const int warp = tid >> 5, lane = tid & 31;
+    C a8[8][NJ];
+#pragma unroll
+    for (int rr = 0; rr < 8; ++rr)
+#pragma unroll
+      for (int j = 0; j < NJ; ++j) a8[rr][j] = czero<C>();
+    for (int cc = c_lo; cc < c_hi; ++cc) {
+      const int c = LOWER ? cc : c_hi - 1 - (cc - c_lo);
+      const int t0 = c * BS, nt = min(BS, n - t0);
+      C lv[8][2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int col = lane + 32 * h;
+#pragma unroll
+        for (int rr = 0; rr < 8; ++rr) {
+          const int row = warp * 8 + rr;
+          lv[rr][h] = (row < nr && col < nt) ? T::fac(F, r0 + row, t0 + col) : czero<C>();
+        }
+      }
+      if (lane == 0) {
+        wait_flag(flags, c, epoch, err);
+        __threadfence();
+      }
+      __syncwarp();
+      C xv[2][NJ];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int col = lane + 32 * h;
+#pragma unroll
+        for (int j = 0; j < NJ; ++j)
+          xv[h][j] = (col < nt && j < nj) ? T::from(ldcg(&X[(size_t)(j0 + j) * n + t0 + col])) : czero<C>();
+      }
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int rr = 0; rr < 8; ++rr)
+#pragma unroll
+          for (int j = 0; j < NJ; ++j) a8[rr][j] = a8[rr][j] + lv[rr][h] * xv[h][j];
+    }
+#pragma unroll
+    for (int rr = 0; rr < 8; ++rr)
+#pragma unroll
+      for (int j = 0; j < NJ; ++j) {
+        for (int o = 16; o > 0; o >>= 1) {
+          a8[rr][j].x += __shfl_xor_sync(0xffffffff, a8[rr][j].x, o);
+          a8[rr][j].y += __shfl_xor_sync(0xffffffff, a8[rr][j].y, o);
+        }
+        if (lane == 0) xs[warp * 8 + rr][j] = a8[rr][j];
+      }
+    __syncthreads();
+    for (int e = tid; e < BS * NJ; e += 256) {
+      const int r = e / NJ, j = e % NJ;
+      if (r < nr && j < nj) y[r][j] = y[r][j] - xs[r][j];
+    }
+    __syncthreads();
+  } else {
   C acc[NJ];
 #pragma unroll
   for (int j = 0; j < NJ; ++j) acc[j] = czero<C>();
-  const int c_lo = LOWER ? 0 : b + 1, c_hi = LOWER ? b : nblk;
   for (int cc = c_lo; cc < c_hi; ++cc) {
     const int c = LOWER ? cc : c_hi - 1 - (cc - c_lo);  // upper: the last block is ready first
     const int t0 = c * BS, nt = min(BS, n - t0);
@@ -239,6 +301,7 @@ __global__ void __launch_bounds__(256, F32 ? 4 : 1) k_trsv(Fac F0, int n, const 
     for (int j = 0; j < NJ; ++j) y[i][j] = y[i][j] - acc[j];
   }
   __syncthreads();
+  }
   // X[rows] = Dinv_b * y: 4 threads per output, 16 terms each, combined by shuffles
   for (int e0 = 0; e0 < nr * nj; e0 += 64) {
     const int e = e0 + (tid >> 2), part = tid & 3;
