@@ -58,6 +58,8 @@ int64_t pss_kernel_launches(void);
 /* One context per device; nworkers CUDA streams process frequency points concurrently. */
 int pss_ctx_create(int device, int nworkers, pss_ctx **out);
 int pss_ctx_destroy(pss_ctx *ctx);
+/* The device a context runs on. */
+int pss_ctx_device(const pss_ctx *ctx, int *device);
 
 /* Upload a triangulated sheet and its basis-function topology.
  * cls: 'J' (conductor, fillz) or 'M' (aperture, filly).  s1, s2, beta1, beta2 in sheet
@@ -158,6 +160,21 @@ int pss_partial_gsms_adj(pss_sheet *sheet, int nl, const double *eps, const doub
                          const double *pwidth, const double *pu, const double *ppsi, const double *pkvec,
                          const double *psrc, const double *ptobs, const double *pwobs, int precision,
                          double *dS, double *dSp, int *status);
+
+/* GSM cascade of npts frequency points on the device: the Gblock walk of _analyze
+ * (src/PSSFSS.jl:256-305) - cascade (the star product of Eq. 3.35, src/GSMs.jl:125-141) and
+ * cascade! (propagation through a layer, src/GSMs.jl:154-176) - for every point at once.
+ * Per point the chain starts from the identity GSM of region 0 propagated through layer 0,
+ * then for each Gblock k = 0..nblk-1: A <- cascade(A, B_k), and A's region-2 ports are
+ * propagated through the layer behind the block.  dims: nblk + 1 mode counts (block k joins
+ * region k, dims[k] modes, to region k + 1), each 1..64, the same for every point.
+ * gsm: per point, per block: s11 (dims[k]^2), s12 (dims[k] x dims[k+1]), s21, s22, each
+ * column-major complex, in that order.  prop: per point, exp(-gamma d) of every mode of
+ * layer 0 (dims[0] values), then of the layer behind each block (dims[k+1]); 1 where the
+ * width is zero.  out: per point s11 (d0 x d0), s12 (d0 x dK), s21 (dK x d0), s22 (dK x dK).
+ * status: npts, PSS_STATUS_SINGULAR where a star-product system had a zero pivot. */
+int pss_cascade(pss_ctx *ctx, int npts, int nblk, const int *dims, const double *gsm, const double *prop,
+                double *out, int *status);
 
 /* The MoM matrix of one point: Z (nbf x nbf complex, column-major like zorymat). */
 int pss_fill_matrix(pss_sheet *sheet, int nl, const double *eps, const double *mu, const double *width, int s,

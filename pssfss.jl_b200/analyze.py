@@ -16,6 +16,7 @@ cascade (``PSSFSS.jl:256-305``).
 ``getsttuple`` (PSSFSS.jl:607-617) reads an undefined global for ψ steering in
 reference v0.1.4; here ψ steering works as its docstring describes.
 """
+import cmath
 import copy
 import math
 from dataclasses import dataclass, field
@@ -287,45 +288,82 @@ def sheet_gblocks(plan):
     return out
 
 
-def assemble(plan, partial):
-    """Cascade each point's Gblock GSMs (PSSFSS.jl:256-312).  ``partial[ig][p]`` is the
-    partial GSM of sheet Gblock ``ig`` at point ``p``."""
-    results = []
-    for p, pt in enumerate(plan.points):
-        L = pt.layers
-        n1 = len(L[0].P)
-        gsma = cascade_layer(GSM.identity(n1, n1), L[0])
-        gsm_save = {}
-        gsmc = gsma
-        for ig, g in enumerate(plan.gbls):
-            i1, i2 = g.first, g.last + 1
-            if g.j != 0:
-                isht = plan.junc[g.j - 1]
-                sheet = plan.sheets[isht - 1]
-                if plan.gbldup[ig] > 0:
-                    gsmb = gsm_save[plan.gbldup[ig] - 1].copy()
-                else:
-                    if sheet.cls in ("J", "M") and sheet.style != "NULL":
-                        gsmb = partial[ig][p].copy()
-                    elif sheet.cls == "E":
-                        gsmb = pecgsm(len(L[i1 - 1].P), len(L[i2 - 1].P))
-                    elif sheet.cls == "H":
-                        gsmb = pmcgsm(len(L[i1 - 1].P), len(L[i2 - 1].P))
-                    else:
-                        raise ValueError(f"Illegal sheet class: {sheet.cls}")
-                    if plan.gbldup[ig] < 0:
-                        gsm_save[ig] = gsmb.copy()
-                if sheet.dx != 0 or sheet.dy != 0:
-                    upm = sheet.units.units_per_meter
-                    translate_gsm(gsmb, sheet.dx / upm, sheet.dy / upm, L[i1 - 1], L[i2 - 1])
+def _propagation(layer):
+    """exp(-γ d) of every mode of ``layer`` (``cascade!``, GSMs.jl:154-176); ones when d = 0."""
+    if layer.width == 0:
+        return np.ones(len(layer.gamma), complex)
+    return np.array([cmath.exp(-g * layer.width) for g in layer.gamma], complex)
+
+
+def _gblock_chain(plan, partial, p, gsm_save):
+    """The GSM of every Gblock at point ``p`` (sheet partial GSMs, PEC/PMC, or bare slab
+    interfaces; translations applied), each with the propagation factors of the layer
+    behind it (PSSFSS.jl:256-305)."""
+    pt = plan.points[p]
+    L = pt.layers
+    chain = [_propagation(L[0])]
+    for ig, g in enumerate(plan.gbls):
+        i1, i2 = g.first, g.last + 1
+        if g.j != 0:
+            isht = plan.junc[g.j - 1]
+            sheet = plan.sheets[isht - 1]
+            if plan.gbldup[ig] > 0:
+                gsmb = gsm_save[plan.gbldup[ig] - 1].copy()
             else:
-                gsmb = gsm_slab_interface(L[i1 - 1], L[i2 - 1], pt.k0)
+                if sheet.cls in ("J", "M") and sheet.style != "NULL":
+                    gsmb = partial[ig][p].copy()
+                elif sheet.cls == "E":
+                    gsmb = pecgsm(len(L[i1 - 1].P), len(L[i2 - 1].P))
+                elif sheet.cls == "H":
+                    gsmb = pmcgsm(len(L[i1 - 1].P), len(L[i2 - 1].P))
+                else:
+                    raise ValueError(f"Illegal sheet class: {sheet.cls}")
+                if plan.gbldup[ig] < 0:
+                    gsm_save[ig] = gsmb.copy()
+            if sheet.dx != 0 or sheet.dy != 0:
+                upm = sheet.units.units_per_meter
+                translate_gsm(gsmb, sheet.dx / upm, sheet.dy / upm, L[i1 - 1], L[i2 - 1])
+        else:
+            gsmb = gsm_slab_interface(L[i1 - 1], L[i2 - 1], pt.k0)
+        chain.append((gsmb, _propagation(L[i2 - 1])))
+    return chain
+
+
+def _result(pt, gsmc):
+    L = pt.layers
+    return Result(gsmc, pt.steer, pt.beta00, pt.fghz, L[0].epsr, L[0].mur, L[0].beta1.copy(), L[0].beta2.copy(),
+                  L[-1].epsr, L[-1].mur, L[-1].beta1.copy(), L[-1].beta2.copy())
+
+
+def assemble(plan, partial, where="auto", device=0):
+    """Cascade each point's Gblock GSMs (PSSFSS.jl:256-312).  ``partial[ig][p]`` is the
+    partial GSM of sheet Gblock ``ig`` at point ``p``.  ``where``: ``"device"`` runs the
+    star products of every point in one ``pss_cascade`` call, ``"host"`` in numpy,
+    ``"auto"`` (default) the device when a GPU is there and every region has at most 64
+    modes."""
+    if not plan.points:
+        return []
+    gsm_save = {}
+    chains = [_gblock_chain(plan, partial, p, gsm_save) for p in range(len(plan.points))]
+    use_device = where == "device"
+    if where == "auto":
+        from . import engine
+        dims = [len(chains[0][0])] + [len(pv) for _, pv in chains[0][1:]]
+        use_device = max(dims) <= engine.CASCADE_MAX_MODES and engine.device_available()
+    if use_device:
+        from . import engine
+        out = engine.cascade_points(chains, device=device)
+        return [_result(pt, GSM(*o)) for pt, o in zip(plan.points, out)]
+    results = []
+    for pt, chain in zip(plan.points, chains):
+        n1 = len(pt.layers[0].P)
+        gsma = cascade_layer(GSM.identity(n1, n1), pt.layers[0])
+        gsmc = gsma
+        for (gsmb, _), g in zip(chain[1:], plan.gbls):
             gsmc = cascade(gsma, gsmb)
-            cascade_layer(gsmc, L[i2 - 1])
+            cascade_layer(gsmc, pt.layers[g.last])
             gsma = gsmc
-        results.append(Result(gsmc, pt.steer, pt.beta00, pt.fghz, L[0].epsr, L[0].mur,
-                              L[0].beta1.copy(), L[0].beta2.copy(), L[-1].epsr, L[-1].mur,
-                              L[-1].beta1.copy(), L[-1].beta2.copy()))
+        results.append(_result(pt, gsmc))
     return results
 
 

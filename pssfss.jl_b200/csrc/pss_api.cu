@@ -618,6 +618,12 @@ int pss_sheet_destroy(pss_sheet *sh) {
   return 0;
 }
 
+int pss_ctx_device(const pss_ctx *c, int *dev) {
+  if (!c) { pss_set_error("null context"); return -1; }
+  *dev = c->device;
+  return 0;
+}
+
 int pss_sheet_clear_cache(pss_sheet *sh) {
   if (!sh) { pss_set_error("null argument"); return -1; }
   sh->jk_valid = false;

@@ -114,6 +114,9 @@ __device__ __forceinline__ cd sigma_interp(const cd *__restrict__ T, int mmax, c
   return s;
 }
 
+// The device a context runs on (0, or -1 for a null context with a message).
+extern "C" int pss_ctx_device(const pss_ctx *c, int *dev);
+
 // Counts every kernel the library launches (reported by pss_kernel_launches()).
 void pss_count_launch();
 // Optional CUDA-event timing of the Schur-complement GEMM launches (pss_profile): returns

@@ -42,6 +42,8 @@ SIGNATURES = {
     "pss_kernel_launches": (_L, []),
     "pss_ctx_create": (_I, [_I, _I, _P]),
     "pss_ctx_destroy": (_I, [_P]),
+    "pss_ctx_device": (_I, [_P, _P]),
+    "pss_cascade": (_I, [_P, _I, _I, _P, _P, _P, _P, _P]),
     "pss_sheet_create": (_I, [_P, _C, _D, _P, _P, _P, _P, _L, _P, _L, _P, _P, _P, _L, _L, _P, _P, _P, _L,
                               _P, _P, _P]),
     "pss_sheet_destroy": (_I, [_P]),
@@ -80,6 +82,19 @@ def profile_result(device=0, nworkers=None):
     _check(lib().pss_profile_result(context(device, nworkers), _p(out)), "pss_profile_result")
     return {k: {"launches": int(out[3 * i]), "ms": float(out[3 * i + 1]), "work": float(out[3 * i + 2])}
             for i, k in enumerate(PROFILE_KINDS)}
+
+
+def device_available():
+    """True when the library loads and a CUDA device is present (no context is created)."""
+    try:
+        L = lib()
+    except RuntimeError:
+        return False
+    try:
+        import torch
+        return bool(torch.cuda.is_available())
+    except Exception:
+        return False
 
 
 def lib():
@@ -338,6 +353,49 @@ def partial_gsms_linearized(sheet, rwg, points, region_rng, s, u, ios, perturbed
         raise RuntimeError(f"solver status {status.tolist()} (singular, non-finite or device timeout)")
     del held
     return [d.T.copy() for d in dS], [[d.T.copy() for d in dSp[k]] for k in range(K)]
+
+
+CASCADE_MAX_MODES = 64
+
+
+def cascade_points(chains, device=0):
+    """GSM cascade of many points on the device (``pss_cascade``).  ``chains``: per point a
+    list ``[p0, (B_0, p_1), (B_1, p_2), ...]`` - p0 the propagation factors of layer 0, then
+    per Gblock its GSM (``.s11 .. .s22``) and the factors of the layer behind it.  Every point
+    must have the same mode counts.  Returns per point (s11, s12, s21, s22)."""
+    npts = len(chains)
+    p0 = np.asarray(chains[0][0])
+    blocks = chains[0][1:]
+    dims = [len(p0)] + [len(p) for _, p in blocks]
+    nblk = len(blocks)
+    recs, props = [], []
+    for ch in chains:
+        pr = [np.asarray(ch[0], complex)]
+        rec = []
+        for B, p in ch[1:]:
+            rec += [np.asarray(B.s11, complex).ravel(order="F"), np.asarray(B.s12, complex).ravel(order="F"),
+                    np.asarray(B.s21, complex).ravel(order="F"), np.asarray(B.s22, complex).ravel(order="F")]
+            pr.append(np.asarray(p, complex))
+        recs.append(np.concatenate(rec))
+        props.append(np.concatenate(pr))
+    gsm = _c2d(np.concatenate(recs))
+    prop = _c2d(np.concatenate(props))
+    n0, nK = dims[0], dims[-1]
+    per = n0 * n0 + 2 * n0 * nK + nK * nK
+    out = np.zeros(npts * per, complex)
+    status = np.zeros(npts, np.int32)
+    d = np.ascontiguousarray(np.asarray(dims, np.int32))
+    _check(lib().pss_cascade(context(device), npts, nblk, _p(d), _p(gsm), _p(prop), _p(out), _p(status)),
+           "pss_cascade")
+    if (status & 4).any():
+        raise RuntimeError(f"pss_cascade: singular star-product system at points {np.flatnonzero(status).tolist()}")
+    res = []
+    for i in range(npts):
+        o = out[i * per:(i + 1) * per]
+        a, b, c = n0 * n0, n0 * n0 + n0 * nK, n0 * n0 + 2 * n0 * nK
+        res.append((o[:a].reshape((n0, n0), order="F"), o[a:b].reshape((n0, nK), order="F"),
+                    o[b:c].reshape((nK, n0), order="F"), o[c:].reshape((nK, nK), order="F")))
+    return res
 
 
 def fill_matrix(sheet, rwg, layers, s, u, k0, psi1, psi2, device=0):
