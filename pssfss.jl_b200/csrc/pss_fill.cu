@@ -16,10 +16,16 @@
 
 namespace {
 
+// Phase factors of the lattice terms, cis(-m psi1) and cis(-n psi2) for |m|, |n| <= 65 (the
+// ring budget): kPhase entries each, index m + 65.  A term's factor cis(-(m psi1 + n psi2)) is
+// their product, one complex multiply in place of a sincos per summand.
+constexpr int kPhase = 2 * PSS_JKRINGMAX + 1;
+
 // jksums (PGF.jl:67-106): the spatial lattice sums J and K at one observation offset, ring by
 // ring in the reference's order (rmin = 5, at most 65 rings, relative change 1e-8).
 __device__ __forceinline__ int jksums_dev(double urx, double ury, double psi1, double psi2, double us1x,
-                                          double us1y, double us2x, double us2y, cd &jout, cd &kout) {
+                                          double us1y, double us2x, double us2y, const cd *__restrict__ ph1,
+                                          const cd *__restrict__ ph2, cd &jout, cd &kout) {
   const int rmin = 5;
   const double small = 1e-5, convtest = 1e-8;
   double arg = sqrt(urx * urx + ury * ury);
@@ -47,13 +53,8 @@ __device__ __forceinline__ int jksums_dev(double urx, double ury, double psi1, d
       if (nophase) {
         term = mkcd(er, 0.0);
       } else {
-        double ph = (double)m * psi1 + (double)n * psi2;
-        if (ph == 0.0) term = mkcd(er, -ph);
-        else {
-          double s, c;
-          sincos(-ph, &s, &c);
-          term = mkcd(er * c, er * s);
-        }
+        const cd f = ph1[m + PSS_JKRINGMAX] * ph2[n + PSS_JKRINGMAX];
+        term = mkcd(er * f.x, er * f.y);
       }
       jring = jring + mkcd(term.x * ra, term.y * ra);
       kring = kring + term;
@@ -85,6 +86,16 @@ __device__ __forceinline__ void face_vtx(const SheetDev &G, int f, double r[3][2
 // Seven times the parallelism of a thread per pair, each thread one lattice sum.
 __global__ void __launch_bounds__(256) k_filljk(SheetDev G, double ul, double psi1, double psi2, double us1x,
                                                 double us1y, double us2x, double us2y, JKDev jk, int *nonconv) {
+  __shared__ cd ph1[kPhase], ph2[kPhase];
+  for (int t = threadIdx.x; t < kPhase; t += blockDim.x) {
+    const double k = (double)(t - PSS_JKRINGMAX);
+    double s1, c1, s2, c2;
+    sincos(-(k * psi1), &s1, &c1);
+    sincos(-(k * psi2), &s2, &c2);
+    ph1[t] = mkcd(c1, s1);
+    ph2[t] = mkcd(c2, s2);
+  }
+  __syncthreads();
   const int lane = threadIdx.x & 31, q = lane & 7, grp = lane & ~7;
   const long long gid = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 3;  // pair of this group
   const bool live = gid < G.nufp;
@@ -107,7 +118,7 @@ __global__ void __launch_bounds__(256) k_filljk(SheetDev G, double ul, double ps
   if (q < 7) {
     double rtx = (rs[0][0] + rs21[0] * c_qxi[q]) + rs31[0] * c_qeta[q];
     double rty = (rs[0][1] + rs21[1] * c_qxi[q]) + rs31[1] * c_qeta[q];
-    ok = jksums_dev(ul * (rmc[0] - rtx), ul * (rmc[1] - rty), psi1, psi2, us1x, us1y, us2x, us2y, js, ks);
+    ok = jksums_dev(ul * (rmc[0] - rtx), ul * (rmc[1] - rty), psi1, psi2, us1x, us1y, us2x, us2y, ph1, ph2, js, ks);
   }
   cd aJ = mkcd(0, 0), aJx = aJ, aJe = aJ, aK = aJ, aKx = aJ, aKe = aJ;
   int bad = 0;
