@@ -528,15 +528,14 @@ int pss_sheet_create(pss_ctx *ctx, char cls, double units_per_meter, const doubl
     hfv[i] = (int)(fv[i] - 1);
     if (fe[i] < 1 || fe[i] > nedge) { pss_set_error("fe[%lld] out of range", (long long)i); delete sh; return -1; }
   }
-  // device copy transposed (source face fastest): the assembly reads a row of Z, one match
-  // face against consecutive source faces, so its class look-ups become contiguous
+  // device copy in the reference's order (match face fastest): the assembly gathers a column
+  // of a Z tile - consecutive match faces against one source face - whose classes are then
+  // consecutive entries of this map
   std::vector<int> hufpm((size_t)nface * nface);
-  for (int64_t fb = 0; fb < nface; ++fb)
-    for (int64_t fa = 0; fa < nface; ++fa) {
-      const int64_t v = ufpm[fa + fb * nface];
-      if (v < 1 || v > nufp) { pss_set_error("ufpm entry out of range"); delete sh; return -1; }
-      hufpm[fb + fa * nface] = (int)(v - 1);
-    }
+  for (size_t i = 0; i < hufpm.size(); ++i) {
+    if (ufpm[i] < 1 || ufpm[i] > nufp) { pss_set_error("ufpm entry out of range"); delete sh; return -1; }
+    hufpm[i] = (int)(ufpm[i] - 1);
+  }
   std::vector<int> hrep(nufp);
   for (int64_t i = 0; i < nufp; ++i) {
     if (ufp_rep[i] < 1 || ufp_rep[i] > nface * nface) { pss_set_error("ufp_rep out of range"); delete sh; return -1; }

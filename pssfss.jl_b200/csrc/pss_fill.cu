@@ -295,7 +295,7 @@ __device__ __forceinline__ cd assemble_entry(const SheetDev &G, const PointParam
       const int fb = G.inc_face[4 * n + b], kb = G.inc_loc[4 * n + b];
       const cd ffb = P.ff[G.inc_eci[4 * n + b]];
       const cd sflag = G.inc_sgn[4 * n + b] > 0 ? ffb : -ffb;
-      const int iu = G.ufpm[(size_t)fb + (size_t)fa * G.nface];
+      const int iu = G.ufpm[(size_t)fa + (size_t)fb * G.nface];
       const cd v = zb[(size_t)(3 * kb + ka) * G.nufp + iu];
       acc = acc + (mflag * sflag) * v;
       if (!P.magnetic && fa == fb) {
@@ -318,48 +318,75 @@ __device__ __forceinline__ cd assemble_entry(const SheetDev &G, const PointParam
   return acc;
 }
 
-// Z[m, n], row-major, leading dimension ld.
+// Z[m, n], row-major (z64 with leading dimension ld, the FP32 planes with ldf), one 32 x 64
+// tile per CTA of 32 x 8 threads.  The gathers run with a warp along the 32 rows of a tile
+// column (consecutive match basis functions against one source basis function: consecutive
+// match faces, so the class look-ups and most pair-term loads of a warp are contiguous); each
+// thread takes 8 columns (independent gathers in flight); the tile then goes out through
+// shared memory row by row, 64 consecutive entries per row.
 __global__ void __launch_bounds__(256) k_assemble(SheetDev G, const PointParams *__restrict__ Pp,
                                                   const cd *__restrict__ zb, cd *__restrict__ z64,
                                                   float *__restrict__ zr, float *__restrict__ zi, long long ld,
                                                   long long ldf) {
-  int n = blockIdx.x * blockDim.x + threadIdx.x;
-  int m = blockIdx.y * blockDim.y + threadIdx.y;
-  if (m >= G.nbf || n >= G.nbf) return;
-  const cd acc = assemble_entry(G, *Pp, zb, m, n);
-  if (z64) z64[(size_t)m * ld + n] = acc;
-  if (zr) {
-    const size_t o = (size_t)m * ldf + n;
-    zr[o] = (float)acc.x;
-    zi[o] = (float)acc.y;
+  __shared__ cd tile[32][65];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int m0 = blockIdx.y * 32, n0 = blockIdx.x * 64;
+  const int m = m0 + tx;
+  const PointParams &P = *Pp;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int c = ty + 8 * k, n = n0 + c;
+    tile[tx][c] = (m < G.nbf && n < G.nbf) ? assemble_entry(G, P, zb, m, n) : mkcd(0, 0);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int rr = 0; rr < 4; ++rr) {
+    const int r = ty * 4 + rr, mm = m0 + r;
+    if (mm >= G.nbf) break;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int c = tx + 32 * h, n = n0 + c;
+      if (n >= G.nbf) continue;
+      const cd v = tile[r][c];
+      if (z64) z64[(size_t)mm * ld + n] = v;
+      if (zr) {
+        zr[(size_t)mm * ldf + n] = (float)v.x;
+        zi[(size_t)mm * ldf + n] = (float)v.y;
+      }
+    }
   }
 }
 
-// Adjoint contraction of one perturbed input set, without its matrix.  CTA x takes the 4
-// rows m = 4x .. 4x+3 (one per threadIdx.y, 64 lanes across the columns), assembles Z_k[m, n]
-// on the fly from the set's pair terms (recomputed Green's-function values, never stored),
-// forms the row's residual  y[m, b] = R_k[m, b] - sum_n Z_k[m, n] X[n, b]  for the
-// right-hand sides b0 .. b0+NB-1, and writes the CTA's share of
-//     G[a + b*nm] = sum_m Lam[m, a] y[m, b]
-// to part[x] (rows in a fixed order; no atomics, so the result is deterministic).
+// Adjoint contraction of one perturbed input set, without its matrix.  CTA (x, y) takes the 32
+// rows m = 32x .. 32x+31 (threadIdx.x) and column chunk y of gridDim.y; its 8 warps split the
+// chunk's columns (n = chunk start + threadIdx.y + 8j);
+// each thread assembles Z_k[m, n] on the fly from the set's pair terms (recomputed
+// Green's-function values, never stored) - a warp gathers one column's 32 rows, consecutive
+// match faces, so its class look-ups are contiguous - and accumulates Z_k[m, n] X[n, b].  The
+// 8 column shares of a row are added in a fixed order to form the chunk's part of
+//     y[m, b] = R_k[m, b] - sum_n Z_k[m, n] X[n, b]
+// (R_k in chunk 0's part) for the right-hand sides b0 .. b0+NB-1, and the CTA writes its share
+// of G[a + b*nm] = sum_m Lam[m, a] y[m, b] to part[x + y*gridDim.x] (rows in a fixed order, no
+// atomics: the shares are added in a fixed order by k_adj_reduce, so the result is deterministic).
 // Vectors are nbf x nm column-major.
 constexpr int kAdjNB = 8;
 __global__ void __launch_bounds__(256) k_adj_contract(SheetDev G, const PointParams *__restrict__ Pp,
                                                       const cd *__restrict__ zb, const cd *__restrict__ X,
                                                       const cd *__restrict__ R, const cd *__restrict__ Lam, int nm,
                                                       int b0, cd *__restrict__ part) {
-  const int tx = threadIdx.x, ty = threadIdx.y, lane = tx & 31, half = tx >> 5;
-  const int m = blockIdx.x * 4 + ty;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int m = blockIdx.x * 32 + tx;
   const int nb = min(kAdjNB, nm - b0);
   const int nbf = G.nbf;
-  __shared__ cd red[4][2][kAdjNB];
-  __shared__ cd yrow[4][kAdjNB];
+  const int csz = (nbf + gridDim.y - 1) / gridDim.y, c0 = blockIdx.y * csz, c1 = min(nbf, c0 + csz);
+  __shared__ cd red[8][32][kAdjNB];
+  __shared__ cd yrow[32][kAdjNB];
   cd acc[kAdjNB];
 #pragma unroll
   for (int b = 0; b < kAdjNB; ++b) acc[b] = mkcd(0, 0);
   if (m < nbf) {
     const PointParams &P = *Pp;
-    for (int n = tx; n < nbf; n += 64) {
+    for (int n = c0 + ty; n < c1; n += 8) {
       const cd z = assemble_entry(G, P, zb, m, n);
 #pragma unroll
       for (int b = 0; b < kAdjNB; ++b)
@@ -367,29 +394,27 @@ __global__ void __launch_bounds__(256) k_adj_contract(SheetDev G, const PointPar
     }
   }
 #pragma unroll
-  for (int b = 0; b < kAdjNB; ++b)
-    for (int o = 16; o > 0; o >>= 1) {
-      acc[b].x += __shfl_xor_sync(0xffffffffu, acc[b].x, o);
-      acc[b].y += __shfl_xor_sync(0xffffffffu, acc[b].y, o);
-    }
-  if (lane == 0)
-    for (int b = 0; b < kAdjNB; ++b) red[ty][half][b] = acc[b];
+  for (int b = 0; b < kAdjNB; ++b) red[ty][tx][b] = acc[b];
   __syncthreads();
-  if (tx < kAdjNB) {
-    const int b = tx;
-    yrow[ty][b] = (m < nbf && b < nb) ? R[(size_t)(b0 + b) * nbf + m] - (red[ty][0][b] + red[ty][1][b]) : mkcd(0, 0);
+  if (ty == 0) {
+    for (int b = 0; b < kAdjNB; ++b) {
+      cd sdot = mkcd(0, 0);
+      for (int w = 0; w < 8; ++w) sdot = sdot + red[w][tx][b];
+      const cd rb = blockIdx.y == 0 ? R[(size_t)(b0 + b) * nbf + m] : mkcd(0, 0);
+      yrow[tx][b] = (m < nbf && b < nb) ? rb - sdot : mkcd(0, 0);
+    }
   }
   __syncthreads();
   // this CTA's share of G: thread e of the 256 covers entries e, e + 256, ...
-  const int tid = ty * 64 + tx;
+  const int tid = ty * 32 + tx;
   for (int e = tid; e < nm * nb; e += 256) {
     const int a = e % nm, b = e / nm;
-    cd s = mkcd(0, 0);
-    for (int r = 0; r < 4; ++r) {
-      const int mr = blockIdx.x * 4 + r;
-      if (mr < nbf) s = s + Lam[(size_t)a * nbf + mr] * yrow[r][b];
+    cd sum = mkcd(0, 0);
+    for (int r = 0; r < 32; ++r) {
+      const int mr = blockIdx.x * 32 + r;
+      if (mr < nbf) sum = sum + Lam[(size_t)a * nbf + mr] * yrow[r][b];
     }
-    part[(size_t)blockIdx.x * nm * nm + a + (size_t)(b0 + b) * nm] = s;
+    part[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * nm * nm + a + (size_t)(b0 + b) * nm] = sum;
   }
 }
 
@@ -410,17 +435,18 @@ __global__ void __launch_bounds__(256) k_adj_reduce(int nparts, int ne, const cd
 
 }  // namespace
 
-size_t pss_adj_part_bytes(int nbf, int nm) { return (size_t)cdiv_u(nbf, 4) * nm * nm * sizeof(cd); }
+constexpr int kAdjChunks = 8;  // column chunks of the contraction grid
+size_t pss_adj_part_bytes(int nbf, int nm) { return (size_t)cdiv_u(nbf, 32) * kAdjChunks * nm * nm * sizeof(cd); }
 
 void pss_adj_contract(const SheetDev &G, const PointParams *dP1, const cd *zb, const cd *X, const cd *R,
                       const cd *Lam, int nm, cd *part, cd *Gout, cudaStream_t st) {
-  const int nblk = cdiv_u(G.nbf, 4);
+  const int nblk = cdiv_u(G.nbf, 32);
   for (int b0 = 0; b0 < nm; b0 += kAdjNB) {
     pss_count_launch();
-    k_adj_contract<<<nblk, dim3(64, 4), 0, st>>>(G, dP1, zb, X, R, Lam, nm, b0, part);
+    k_adj_contract<<<dim3(nblk, kAdjChunks), dim3(32, 8), 0, st>>>(G, dP1, zb, X, R, Lam, nm, b0, part);
   }
   pss_count_launch();
-  k_adj_reduce<<<nm * nm, 256, 0, st>>>(nblk, nm * nm, part, Gout);
+  k_adj_reduce<<<nm * nm, 256, 0, st>>>(nblk * kAdjChunks, nm * nm, part, Gout);
 }
 
 void pss_filljk(const SheetDev &G, double ulocal, double psi1, double psi2, const double s1[2], const double s2[2],
@@ -441,8 +467,8 @@ void pss_fill_pairs(const SheetDev &G, const PointParams *dP1, const JKDev &jk, 
 
 void pss_fill_assemble(const SheetDev &G, const PointParams *dP1, const cd *zb, cd *z64, float *zr, float *zi,
                        long long ld, long long ldf, cudaStream_t st) {
-  dim3 blk(64, 4);
-  dim3 grd(cdiv_u(G.nbf, 64), cdiv_u(G.nbf, 4));
+  dim3 blk(32, 8);
+  dim3 grd(cdiv_u(G.nbf, 64), cdiv_u(G.nbf, 32));
   pss_count_launch();
   k_assemble<<<grd, blk, 0, st>>>(G, dP1, zb, z64, zr, zi, ld, ldf);
 }

@@ -54,7 +54,7 @@ struct SheetDev {
   double upm;  // sheet units per metre
   const double *rho;     // 2*nnode, sheet units
   const int *fv;         // 3*nface
-  const int *ufpm;       // nface*nface, 0-based class of (match fa, source fb) at fb + fa*nface
+  const int *ufpm;       // nface*nface, 0-based class of (match fa, source fb) at fa + fb*nface
   const int *ufp_rep;    // nufp, 0-based column-major face pair of the class representative
   // pair terms zb (pss_fill_pairs): 9 planes of nufp complex, term 3*isl + iml of class iu at
   // zb[(3*isl + iml)*nufp + iu]
