@@ -211,7 +211,7 @@ __device__ __forceinline__ PairCoef pair_coef(const PointParams &P) {
   return c;
 }
 
-__global__ void __launch_bounds__(128) k_pairs(SheetDev G, const PointParams *__restrict__ Pp, JKDev jk,
+__global__ void __launch_bounds__(128, 5) k_pairs(SheetDev G, const PointParams *__restrict__ Pp, JKDev jk,
                                                const cd *__restrict__ t1, const cd *__restrict__ t2, int mmax,
                                                cd *__restrict__ zb) {
   int iu = blockIdx.x * blockDim.x + threadIdx.x;
