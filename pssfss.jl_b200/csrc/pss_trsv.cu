@@ -164,7 +164,9 @@ __global__ void __launch_bounds__(256, F32 ? 2 : 1) k_trsv(Fac F0, int n, const 
                                               int use_done) {
   using T = SolveT<F32>;
   using C = typename T::C;
-  const int bm = blockIdx.y;  // matrix of the batch
+  // matrix of the batch: the grid runs matrix-fastest, so the CTAs start block row by block
+  // row across all matrices and every matrix's chain advances in the same waves
+  const int bm = blockIdx.x;
   int *cw = ctrl.of(bm);
   if (use_done && cw[2]) return;
   const Fac F = F0.of(bm);
@@ -659,7 +661,7 @@ int pss_solve_lu(SolveWS &ws, int nb, const cd *LU64, const float *Lr, const flo
       PSS_CUDA_TRY(cudaMemset2DAsync(ws.ctrl, ws.cstride * sizeof(int), 0, sizeof(int), nb, st));
       pss_count_launch();
       const bool small = nrhs - j0 <= 4;
-      const dim3 grid(ws.nblk, nb);
+      const dim3 grid(nb, ws.nblk);
       auto go = [&](auto kern, size_t smem) {
         kern<<<grid, 256, smem, st>>>(F, ws.n, ws.perm, B, X, vs, nrhs, j0, ws.Dinv, ws.dstride, ctrl, ws.epoch,
                                       use_done);
@@ -739,7 +741,7 @@ int pss_solve_lu_trans(SolveWS &ws, int nb, const cd *LU64, const float *Lr, con
       PSS_CUDA_TRY(cudaMemset2DAsync(ws.ctrl, ws.cstride * sizeof(int), 0, sizeof(int), nb, st));
       pss_count_launch();
       const bool small = nrhs - j0 <= 4;
-      const dim3 grid(ws.nblk, nb);
+      const dim3 grid(nb, ws.nblk);
       auto go = [&](auto kern, size_t smem) {
         kern<<<grid, 256, smem, st>>>(F, ws.n, ws.perm, B, W, vs, nrhs, j0, ws.Dinv, ws.dstride, ctrl, ws.epoch,
                                       use_done);
