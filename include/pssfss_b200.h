@@ -176,6 +176,18 @@ int pss_partial_gsms_adj(pss_sheet *sheet, int nl, const double *eps, const doub
 int pss_cascade(pss_ctx *ctx, int npts, int nblk, const int *dims, const double *gsm, const double *prop,
                 double *out, int *status);
 
+/* Unique face-pair classes of a sheet on the device (the O(nface^2) classing of setup_rwg,
+ * src/RWG.jl:287-319): pair (match m, source n) is keyed by the source face's shape class
+ * shape[n] (0-based ids, < 2^31) and the offset of match centroid cen[m] from the source's first
+ * vertex r1[n], quantised on the grid g (round half to even; offsets within 2^31 grid steps);
+ * equal keys share a class.  Classes are numbered from 1 in the order of their first member in
+ * column-major (match fastest) order.  cen, r1: nface x 2 interleaved (sheet units).
+ * ufpm: nface x nface int32 out, column-major; rep: rep_cap int64 out, the 1-based column-major
+ * pair index of each class's first member; nufp_out: the number of classes (also when it
+ * exceeds rep_cap, which returns -5).  nface <= 16384. */
+int pss_face_pair_classes(pss_ctx *ctx, int64_t nface, const double *cen, const double *r1, const int64_t *shape,
+                          double g, int32_t *ufpm, int64_t *rep, int64_t rep_cap, int64_t *nufp_out);
+
 /* The MoM matrix of one point: Z (nbf x nbf complex, column-major like zorymat). */
 int pss_fill_matrix(pss_sheet *sheet, int nl, const double *eps, const double *mu, const double *width, int s,
                     double u, double k0, double psi1, double psi2, double *Z, int *mmax_out);

@@ -44,6 +44,7 @@ SIGNATURES = {
     "pss_ctx_destroy": (_I, [_P]),
     "pss_ctx_device": (_I, [_P, _P]),
     "pss_cascade": (_I, [_P, _I, _I, _P, _P, _P, _P, _P]),
+    "pss_face_pair_classes": (_I, [_P, _L, _P, _P, _P, _D, _P, _P, _L, _P]),
     "pss_sheet_create": (_I, [_P, _C, _D, _P, _P, _P, _P, _L, _P, _L, _P, _P, _P, _L, _L, _P, _P, _P, _L,
                               _P, _P, _P]),
     "pss_sheet_destroy": (_I, [_P]),
@@ -353,6 +354,32 @@ def partial_gsms_linearized(sheet, rwg, points, region_rng, s, u, ios, perturbed
         raise RuntimeError(f"solver status {status.tolist()} (singular, non-finite or device timeout)")
     del held
     return [d.T.copy() for d in dS], [[d.T.copy() for d in dSp[k]] for k in range(K)]
+
+
+CLASSING_MAX_FACES = 16384
+
+
+def face_pair_classes(cen, r1, shape_id, g, device=0):
+    """Unique face-pair classes on the device (``pss_face_pair_classes``): returns (ufpm
+    (nface x nface int64, 1-based, column-major), rep (1-based pair indices), nufp)."""
+    nface = len(shape_id)
+    cen = _f64(cen)
+    r1 = _f64(r1)
+    shape = _i64(shape_id)
+    ufpm = np.zeros((nface, nface), np.int32, order="F")
+    cap = max(1024, nface * nface // 8)
+    nufp = ctypes.c_int64()
+    for _ in range(2):
+        rep = np.zeros(cap, np.int64)
+        rc = lib().pss_face_pair_classes(context(device), nface, _p(cen), _p(r1), _p(shape), float(g),
+                                         ufpm.ctypes.data_as(ctypes.c_void_p), _p(rep), cap, ctypes.byref(nufp))
+        if rc == -5:
+            cap = int(nufp.value)
+            continue
+        _check(rc, "pss_face_pair_classes")
+        break
+    n = int(nufp.value)
+    return ufpm.astype(np.int64), rep[:n].copy(), n
 
 
 CASCADE_MAX_MODES = 64

@@ -164,6 +164,14 @@ def _ufp_keys(sheet):
     """Per face pair (match m, source n): the source triangle's shape class and the offset of
     the match centroid from the source's first vertex, quantised on a grid of 1e-6 of the
     first two centroids' distance (the KD-tree radius of ``RWG.jl:305-315``)."""
+    cen, r1, shape_id, g = _ufp_geometry(sheet)
+    dx = np.round((cen[:, None, 0] - r1[None, :, 0]) / g).astype(np.int64)  # [m, n]
+    dy = np.round((cen[:, None, 1] - r1[None, :, 1]) / g).astype(np.int64)
+    return shape_id, dx, dy
+
+
+def _ufp_geometry(sheet):
+    """Centroids, first vertices, source-shape ids and the quantisation grid of the classing."""
     rho = sheet.rho
     r1 = rho[sheet.fv[0] - 1]
     r2 = rho[sheet.fv[1] - 1]
@@ -173,17 +181,27 @@ def _ufp_keys(sheet):
     g = 1e-6 * math.sqrt(d[0] * d[0] + d[1] * d[1])
     shape_key = np.round(np.hstack([r2 - r1, r3 - r1]) / g).astype(np.int64)
     _, shape_id = np.unique(shape_key, axis=0, return_inverse=True)
-    shape_id = shape_id.ravel().astype(np.int64)
-    dx = np.round((cen[:, None, 0] - r1[None, :, 0]) / g).astype(np.int64)  # [m, n]
-    dy = np.round((cen[:, None, 1] - r1[None, :, 1]) / g).astype(np.int64)
-    return shape_id, dx, dy
+    return cen, r1, shape_id.ravel().astype(np.int64), g
 
 
-def unique_face_pairs(sheet):
+def unique_face_pairs(sheet, where="auto"):
     """Translation-equivalence classes of face pairs (``RWG.jl:287-319``), numbered in the
-    order of their first member in column-major (match fastest) order.  The three keys are
-    packed into one integer when they fit in 62 bits (one sort), else sorted together."""
+    order of their first member in column-major (match fastest) order.
+
+    ``where="auto"`` classes on the GPU when one is present (``pss_face_pair_classes``: a hash
+    table keyed on the same quantised keys, one thread per pair) and the sheet fits its limits;
+    else on the host, where the three keys are packed into one integer when they fit in 62 bits
+    (one sort) or sorted together."""
     nface = sheet.nface
+    if where != "host":
+        from . import engine
+        if where == "device" or (nface <= engine.CLASSING_MAX_FACES and engine.device_available()):
+            cen, r1, shape_id, g = _ufp_geometry(sheet)
+            span = float(np.ptp(np.vstack([cen, r1]), axis=0).max())  # bounds every |offset|
+            if span / g < 2.0 ** 30:
+                return engine.face_pair_classes(cen, r1, shape_id, g)
+            if where == "device":
+                raise ValueError("face-pair offsets exceed the device classing's key range")
     shape_id, dx, dy = _ufp_keys(sheet)
     dx -= dx.min()
     dy -= dy.min()
