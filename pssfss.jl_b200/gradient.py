@@ -143,9 +143,11 @@ def linearized_gradient(build, params, flist, steering, objective, partial_lin=N
 
 
 def _prefill_rwg(cache, stratas):
-    """Basis-function setup (``setup_rwg``) of every distinct sheet geometry of the steps,
-    concurrently: the face-pair classing is a few large numpy sorts that release the GIL."""
+    """Basis-function setup (``setup_rwg``) of every distinct sheet geometry of the steps: one
+    after another when the face-pair classing runs on the GPU (a fraction of a second each),
+    else concurrently, the host classing being a few large numpy sorts that release the GIL."""
     from concurrent.futures import ThreadPoolExecutor
+    from . import engine
     from .analyze import _geometry_key
     from .rwg import setup_rwg
     from .sheets import RWGSheet
@@ -157,6 +159,10 @@ def _prefill_rwg(cache, stratas):
                 if key not in cache and key not in todo:
                     todo[key] = sh
     if not todo:
+        return
+    if engine.device_available():
+        for key, sh in todo.items():
+            cache[key] = setup_rwg(sh)
         return
     with ThreadPoolExecutor(max_workers=min(len(todo), 8)) as ex:
         for key, rwg in zip(todo, ex.map(setup_rwg, todo.values())):
