@@ -25,6 +25,7 @@ namespace {
 
 constexpr int kScanBlock = 1024;  // flags per CTA of the scan (256 threads x 4)
 constexpr int kSpin = 1 << 20;
+constexpr int kMaxProbe = 4096;  // a longer probe sequence means the table is (nearly) full
 
 __device__ __forceinline__ unsigned long long mix64(unsigned long long x) {
   x ^= x >> 33;
@@ -55,7 +56,7 @@ __global__ void k_ufp_insert(long long nface, const double *__restrict__ cen, co
     const unsigned long long k1 = ((unsigned long long)(unsigned int)shape[n] << 32) | (unsigned int)dy;
     unsigned long long s = mix64(k0 ^ mix64(k1)) & T.mask;
     bool done = false;
-    for (unsigned long long probe = 0; probe <= T.mask && !done; ++probe, s = (s + 1) & T.mask) {
+    for (int probe = 0; probe < kMaxProbe && !done; ++probe, s = (s + 1) & T.mask) {
       const int st = atomicCAS(&T.state[s], 0, 1);
       if (st == 0) {  // claimed an empty slot: write the key, then publish it
         T.w0[s] = k0;
@@ -212,9 +213,13 @@ extern "C" int pss_face_pair_classes(pss_ctx *ctx, int64_t nface, const double *
   PSS_CUDA_TRY(cudaMemcpy(dcen.p, cen, 2 * nface * sizeof(double), cudaMemcpyHostToDevice));
   PSS_CUDA_TRY(cudaMemcpy(dr1.p, r1, 2 * nface * sizeof(double), cudaMemcpyHostToDevice));
   PSS_CUDA_TRY(cudaMemcpy(dshape.p, shape, nface * sizeof(long long), cudaMemcpyHostToDevice));
-  // the table: start at twice the pairs / 8 (structured sheets have few classes), grow on overflow
+  // the table: first sized for a structured sheet's few classes (a quarter of the pairs); when
+  // that fills (a sheet whose symmetry is broken, say a perturbed one), once more at twice the
+  // pairs, so every key fits at a load of at most one half
   unsigned long long cap = 1ull << 20;
   while (cap < (unsigned long long)npairs / 4) cap <<= 1;
+  unsigned long long cap_full = 1ull << 20;
+  while (cap_full < 2ull * (unsigned long long)npairs) cap_full <<= 1;
   for (int attempt = 0;; ++attempt) {
     Buf w0, w1, state, first;
     PSS_CUDA_TRY(cudaMalloc(&w0.p, cap * sizeof(unsigned long long)));
@@ -231,8 +236,8 @@ extern "C" int pss_face_pair_classes(pss_ctx *ctx, int64_t nface, const double *
                                 T, (int *)dslot.p, (int *)derr.p);
     int herr = 0;
     PSS_CUDA_TRY(cudaMemcpy(&herr, derr.p, sizeof(int), cudaMemcpyDeviceToHost));
-    if (herr == 1 && cap < 2ull * (unsigned long long)npairs && cap < (1ull << 28) && attempt < 4) {  // full: grow
-      cap <<= 2;
+    if (herr == 1 && cap < cap_full && cap_full <= (1ull << 28)) {  // full: once more, large enough
+      cap = cap_full;
       continue;
     }
     if (herr) {

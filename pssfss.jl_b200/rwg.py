@@ -199,7 +199,11 @@ def unique_face_pairs(sheet, where="auto"):
             cen, r1, shape_id, g = _ufp_geometry(sheet)
             span = float(np.ptp(np.vstack([cen, r1]), axis=0).max())  # bounds every |offset|
             if span / g < 2.0 ** 30:
-                return engine.face_pair_classes(cen, r1, shape_id, g)
+                try:
+                    return engine.face_pair_classes(cen, r1, shape_id, g)
+                except RuntimeError:
+                    if where == "device":
+                        raise  # asked for the device explicitly; "auto" classes on the host
             if where == "device":
                 raise ValueError("face-pair offsets exceed the device classing's key range")
     shape_id, dx, dy = _ufp_keys(sheet)
