@@ -137,8 +137,9 @@ struct Worker {
   cudaStream_t st = nullptr;
   int cap = 1;  // batch capacity (points)
   DevBuf zb, z64, zr, zi, ipiv, info, bstat, bf, rhs, X, R, D, nonconv, luws, solvews;
-  JKBufs jk;
+  JKBufs jk, jkx[kJKGroup - 1];  // face integrals of the points whose phasing varies: slots 0..kJKGroup
   SolveWS sws;
+  JKDev jk_slot(int q) const { return q == 0 ? jk.jk : jkx[q - 1].jk; }
   int ensure_solver(int n, int nrhs, int nb) {
     if (ipiv.ensure((size_t)nb * n * sizeof(int)) || info.ensure((size_t)nb * sizeof(int)) ||
         bstat.ensure((size_t)nb * sizeof(int)))
@@ -429,12 +430,16 @@ int ensure_worker_dims(Worker &w, int nufp, int nbf, int nm, int precision, bool
     const size_t pl = (size_t)nb * n * (size_t)Worker::ld32((int)n) * sizeof(float);
     if (w.zr.ensure(pl) || w.zi.ensure(pl)) return -3;
   }
-  if (w.nonconv.ensure(sizeof(int))) return -3;
+  if (w.nonconv.ensure(kJKGroup * sizeof(int))) return -3;
   if (w.bf.ensure((size_t)nb * nm * n * 2 * sizeof(cd))) return -3;
   if (w.ensure_solver((int)n, nm, nb)) return -3;
-  if (own_jk && w.jk.ensure(nufp)) return -3;
+  if (own_jk) {
+    if (w.jk.ensure(nufp)) return -3;
+    for (auto &x : w.jkx)
+      if (x.ensure(nufp)) return -3;
+  }
   PSS_CUDA_TRY(cudaMemsetAsync(w.info.p, 0, (size_t)nb * sizeof(int), w.st));
-  PSS_CUDA_TRY(cudaMemsetAsync(w.nonconv.p, 0, sizeof(int), w.st));
+  PSS_CUDA_TRY(cudaMemsetAsync(w.nonconv.p, 0, kJKGroup * sizeof(int), w.st));
   return 0;
 }
 
@@ -488,6 +493,7 @@ int pss_ctx_destroy(pss_ctx *c) {
                       &w.luws, &w.solvews})
       b->release();
     w.jk.buf.release();
+    for (auto &x : w.jkx) x.buf.release();
     if (w.st) cudaStreamDestroy(w.st);
   }
   for (DevBuf *b : {&c->params, &c->dense, &c->conv, &c->mm, &c->stage, &c->tables, &c->bigdense, &c->modes,
@@ -871,23 +877,39 @@ int sweep_impl(pss_ctx *c, std::vector<Problem> &PR, int precision, const AdjSpe
     }
     float *zr = prec == PSS_FP32_REFINE ? w.zr.as<float>() : nullptr;
     float *zi = prec == PSS_FP32_REFINE ? w.zi.as<float>() : nullptr;
-    for (int b = 0; b < cnt; ++b) {
+    for (int b = 0; b < cnt;) {
+      // points whose phasing varies take their face integrals in groups of up to kJKGroup
+      // points of one sheet (one launch per group), the others read their sheet's cache
       const Problem &P = PR[it.p[b]];
       pss_sheet *sh = P.sh;
-      const int i = it.i[b], g = P.p0 + i;
-      const PointParams *Pi = dP + g;
-      JKDev jk;
-      if (!P.own_jk) {
-        jk = sh->cache.jk;
+      int gsz = 1;
+      JKDev jks[kJKGroup];
+      if (P.own_jk) {
+        while (gsz < kJKGroup && b + gsz < cnt && PR[it.p[b + gsz]].own_jk && PR[it.p[b + gsz]].sh == sh &&
+               PR[it.p[b + gsz]].u == P.u)
+          ++gsz;
+        double p1[kJKGroup], p2[kJKGroup];
+        for (int q = 0; q < gsz; ++q) {
+          const Problem &Q = PR[it.p[b + q]];
+          p1[q] = Q.psi[2 * it.i[b + q]];
+          p2[q] = Q.psi[2 * it.i[b + q] + 1];
+          jks[q] = w.jk_slot(q);
+        }
+        pss_filljk_group(sh->G, P.u / sh->upm, gsz, p1, p2, sh->s1, sh->s2, jks, w.nonconv.as<int>(), st);
+        for (int q = 0; q < gsz; ++q) {
+          pss_count_launch();
+          k_nonconv_to_status<<<1, 1, 0, st>>>(w.nonconv.as<int>() + q, dstatus + PR[it.p[b + q]].p0 + it.i[b + q]);
+        }
       } else {
-        jk = w.jk.jk;
-        pss_filljk(sh->G, P.u / sh->upm, P.psi[2 * i], P.psi[2 * i + 1], sh->s1, sh->s2, jk, w.nonconv.as<int>(), st);
-        pss_count_launch();
-        k_nonconv_to_status<<<1, 1, 0, st>>>(w.nonconv.as<int>(), dstatus + g);
+        jks[0] = sh->cache.jk;
       }
-      pss_fill_pairs(sh->G, Pi, jk, tabs[g].t1, tabs[g].t2, tabs[g].mmax, w.zb.as<cd>(), st);
-      pss_fill_assemble(sh->G, Pi, w.zb.as<cd>(), w.z64.as<cd>() + b * msz, zr ? zr + b * msf : nullptr,
-                        zi ? zi + b * msf : nullptr, ld, ldf, st);
+      for (int q = 0; q < gsz; ++q, ++b) {
+        const int g = PR[it.p[b]].p0 + it.i[b];
+        const PointParams *Pi = dP + g;
+        pss_fill_pairs(sh->G, Pi, jks[q], tabs[g].t1, tabs[g].t2, tabs[g].mmax, w.zb.as<cd>(), st);
+        pss_fill_assemble(sh->G, Pi, w.zb.as<cd>(), w.z64.as<cd>() + b * msz, zr ? zr + b * msf : nullptr,
+                          zi ? zi + b * msf : nullptr, ld, ldf, st);
+      }
     }
     if (rec) cudaEventRecord(e[2], st);
     for (int b = 0; b < cnt; ++b) {

@@ -12,6 +12,8 @@
 //               test and source basis functions, applying the Floquet/sign flags and the
 //               surface-resistance terms of Eqs. 7-34/7-35 (FillZY.jl:221-230).
 //               Deterministic, atomic-free; writes FP64 and/or split FP32 planes.
+#include <algorithm>
+
 #include "pss_internal.cuh"
 
 namespace {
@@ -22,21 +24,31 @@ namespace {
 constexpr int kPhase = 2 * PSS_JKRINGMAX + 1;
 
 // jksums (PGF.jl:67-106): the spatial lattice sums J and K at one observation offset, ring by
-// ring in the reference's order (rmin = 5, at most 65 rings, relative change 1e-8).
-__device__ __forceinline__ int jksums_dev(double urx, double ury, double psi1, double psi2, double us1x,
-                                          double us1y, double us2x, double us2y, const cd *__restrict__ ph1,
-                                          const cd *__restrict__ ph2, cd &jout, cd &kout) {
+// ring in the reference's order (rmin = 5, at most 65 rings, relative change 1e-8), for NP
+// phasings at once.  A summand's distance, exp(-u r) and 1/r do not depend on the phasing, so
+// they are evaluated once and weighted by each phasing's factor; every phasing keeps its own
+// ring partials and stops accumulating at its own convergence ring, so its sums are those of
+// a serial evaluation at that phasing alone, bit for bit.  Slots p >= np are idle.  Returns the
+// mask of converged phasings.
+template <int NP>
+__device__ __forceinline__ unsigned jksums_group(double urx, double ury, int np, bool nophase, double us1x,
+                                                 double us1y, double us2x, double us2y,
+                                                 const cd (*__restrict__ ph1)[kPhase],
+                                                 const cd (*__restrict__ ph2)[kPhase], cd *jout, cd *kout) {
   const int rmin = 5;
   const double small = 1e-5, convtest = 1e-8;
   double arg = sqrt(urx * urx + ury * ury);
   double rterm = exp(-arg);
-  cd ksum = mkcd(rterm, 0.0), jsum;
-  if (arg <= small) jsum = mkcd((-arg / 6 + 0.5) * arg - 1, 0.0);
-  else jsum = mkcd((rterm - 1) / arg, 0.0);
-  const bool nophase = (psi1 == 0.0 && psi2 == 0.0);
-  int converged = 0;
-  for (int r = 1; r <= PSS_JKRINGMAX; ++r) {
-    cd jring = mkcd(0, 0), kring = mkcd(0, 0);
+  const cd k0 = mkcd(rterm, 0.0);
+  const cd j0 = arg <= small ? mkcd((-arg / 6 + 0.5) * arg - 1, 0.0) : mkcd((rterm - 1) / arg, 0.0);
+  cd jsum[NP], ksum[NP];
+#pragma unroll
+  for (int p = 0; p < NP; ++p) { jsum[p] = j0; ksum[p] = k0; }
+  unsigned live = (1u << np) - 1u, conv = 0;
+  for (int r = 1; r <= PSS_JKRINGMAX && live; ++r) {
+    cd jring[NP], kring[NP];
+#pragma unroll
+    for (int p = 0; p < NP; ++p) { jring[p] = mkcd(0, 0); kring[p] = mkcd(0, 0); }
     const int len = 8 * r;
     for (int t = 0; t < len; ++t) {
       int m, n;
@@ -49,26 +61,33 @@ __device__ __forceinline__ int jksums_dev(double urx, double ury, double psi1, d
       const double ra = rsqrt(d2);
       const double a = d2 * ra;
       double er = exp(-a);
-      cd term;
-      if (nophase) {
-        term = mkcd(er, 0.0);
+      if (NP == 1 && nophase) {
+        jring[0] = jring[0] + mkcd(er * ra, 0.0 * ra);
+        kring[0] = kring[0] + mkcd(er, 0.0);
       } else {
-        const cd f = ph1[m + PSS_JKRINGMAX] * ph2[n + PSS_JKRINGMAX];
-        term = mkcd(er * f.x, er * f.y);
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+          const cd f = ph1[p][m + PSS_JKRINGMAX] * ph2[p][n + PSS_JKRINGMAX];
+          const cd term = mkcd(er * f.x, er * f.y);
+          jring[p] = jring[p] + mkcd(term.x * ra, term.y * ra);
+          kring[p] = kring[p] + term;
+        }
       }
-      jring = jring + mkcd(term.x * ra, term.y * ra);
-      kring = kring + term;
     }
-    jsum = jsum + jring;
-    ksum = ksum + kring;
-    if (r > rmin) {
-      double c1 = cabsd(jring / jsum), c2 = cabsd(kring / ksum);
-      if (fmax(c1, c2) < convtest) { converged = 1; break; }
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+      if (!((live >> p) & 1u)) continue;
+      jsum[p] = jsum[p] + jring[p];
+      ksum[p] = ksum[p] + kring[p];
+      if (r > rmin) {
+        double c1 = cabsd(jring[p] / jsum[p]), c2 = cabsd(kring[p] / ksum[p]);
+        if (fmax(c1, c2) < convtest) { live &= ~(1u << p); conv |= 1u << p; }
+      }
     }
   }
-  jout = jsum;
-  kout = ksum;
-  return converged;
+#pragma unroll
+  for (int p = 0; p < NP; ++p) { jout[p] = jsum[p]; kout[p] = ksum[p]; }
+  return conv;
 }
 
 __device__ __forceinline__ void face_vtx(const SheetDev &G, int f, double r[3][2], double scale) {
@@ -80,22 +99,31 @@ __device__ __forceinline__ void face_vtx(const SheetDev &G, int f, double r[3][2
 }
 
 // Eight lanes per unique face pair (four pairs per warp): lane q < 7 computes the lattice
-// sums of quadrature point q (jksums, serial in the reference's ring order); the group's
-// first lane gathers the seven results with warp shuffles and accumulates them in the
-// 7-point rule's order, so each pair's integrals are those of a serial evaluation bit for bit.
-// Seven times the parallelism of a thread per pair, each thread one lattice sum.
-__global__ void __launch_bounds__(256) k_filljk(SheetDev G, double ul, double psi1, double psi2, double us1x,
-                                                double us1y, double us2x, double us2y, JKDev jk, int *nonconv) {
-  __shared__ cd ph1[kPhase], ph2[kPhase];
-  for (int t = threadIdx.x; t < kPhase; t += blockDim.x) {
-    const double k = (double)(t - PSS_JKRINGMAX);
+// sums of quadrature point q (jksums, serial in the reference's ring order) for the group's
+// np <= NP phasings; the pair's first lane gathers the seven results with warp shuffles and
+// accumulates them in the 7-point rule's order, so each pair's integrals are those of a
+// serial evaluation bit for bit.  The phasing-free parts (the smooth-term geometry, rho_r and
+// the 1/R integral) are computed once and written to every phasing's slot.
+template <int NP>
+constexpr int jk_threads() { return NP == 1 ? 256 : 128; }
+
+template <int NP>
+__global__ void __launch_bounds__(jk_threads<NP>(), NP == 1 ? 1 : 4) k_filljk(SheetDev G, double ul, PsiGroup pg, double us1x, double us1y,
+                                                double us2x, double us2y, JKGroup jk, int *nonconv) {
+  __shared__ cd ph1[NP][kPhase], ph2[NP][kPhase];
+  const int np = NP == 1 ? 1 : pg.n;
+  for (int t = threadIdx.x; t < NP * kPhase; t += blockDim.x) {
+    const int p = t / kPhase;
+    const double k = (double)(t % kPhase - PSS_JKRINGMAX);
+    const double a1 = p < np ? pg.psi1[p] : 0.0, a2 = p < np ? pg.psi2[p] : 0.0;
     double s1, c1, s2, c2;
-    sincos(-(k * psi1), &s1, &c1);
-    sincos(-(k * psi2), &s2, &c2);
-    ph1[t] = mkcd(c1, s1);
-    ph2[t] = mkcd(c2, s2);
+    sincos(-(k * a1), &s1, &c1);
+    sincos(-(k * a2), &s2, &c2);
+    ph1[p][t % kPhase] = mkcd(c1, s1);
+    ph2[p][t % kPhase] = mkcd(c2, s2);
   }
   __syncthreads();
+  const bool nophase = NP == 1 && pg.psi1[0] == 0.0 && pg.psi2[0] == 0.0;
   const int lane = threadIdx.x & 31, q = lane & 7, grp = lane & ~7;
   const long long gid = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 3;  // pair of this group
   const bool live = gid < G.nufp;
@@ -113,73 +141,83 @@ __global__ void __launch_bounds__(256) k_filljk(SheetDev G, double ul, double ps
   double rs31[2] = {rs[2][0] - rs[0][0], rs[2][1] - rs[0][1]};
   double rs21[2] = {-rs12[0], -rs12[1]};
   double rmc[2] = {((rm[0][0] + rm[1][0]) + rm[2][0]) / 3, ((rm[0][1] + rm[1][1]) + rm[2][1]) / 3};
-  cd js = mkcd(0, 0), ks = mkcd(0, 0);
-  int ok = 1;
+  cd js[NP], ks[NP];
+#pragma unroll
+  for (int p = 0; p < NP; ++p) { js[p] = mkcd(0, 0); ks[p] = mkcd(0, 0); }
+  unsigned ok = (1u << np) - 1u;
   if (q < 7) {
     double rtx = (rs[0][0] + rs21[0] * c_qxi[q]) + rs31[0] * c_qeta[q];
     double rty = (rs[0][1] + rs21[1] * c_qxi[q]) + rs31[1] * c_qeta[q];
-    ok = jksums_dev(ul * (rmc[0] - rtx), ul * (rmc[1] - rty), psi1, psi2, us1x, us1y, us2x, us2y, ph1, ph2, js, ks);
+    ok = jksums_group<NP>(ul * (rmc[0] - rtx), ul * (rmc[1] - rty), np, nophase, us1x, us1y, us2x, us2y, ph1, ph2,
+                          js, ks);
   }
-  cd aJ = mkcd(0, 0), aJx = aJ, aJe = aJ, aK = aJ, aKx = aJ, aKe = aJ;
-  int bad = 0;
-#pragma unroll
-  for (int i = 0; i < 7; ++i) {  // every lane takes part in the shuffles; the group's lane 0 keeps the sums
-    cd jv, kv;
-    jv.x = __shfl_sync(0xffffffffu, js.x, grp + i);
-    jv.y = __shfl_sync(0xffffffffu, js.y, grp + i);
-    kv.x = __shfl_sync(0xffffffffu, ks.x, grp + i);
-    kv.y = __shfl_sync(0xffffffffu, ks.y, grp + i);
-    bad |= !__shfl_sync(0xffffffffu, ok, grp + i);
-    cd jw = c_qw[i] * jv;
-    aJx = aJx + c_qxi[i] * jw;
-    aJe = aJe + c_qeta[i] * jw;
-    aJ = aJ + jw;
-    cd kw = c_qw[i] * kv;
-    aKx = aKx + c_qxi[i] * kw;
-    aKe = aKe + c_qeta[i] * kw;
-    aK = aK + kw;
-  }
-  if (q != 0 || !live) return;
-  const int nxt[3] = {1, 2, 0};
+  // phasing-free terms (the pair's first lane only)
   double rr0 = 0, rr1 = 0, ri = 0;
-  for (int i = 0; i < 3; ++i) {
-    int ip1 = nxt[i];
-    double lx = rs[ip1][0] - rs[i][0], ly = rs[ip1][1] - rs[i][1];
-    double ln = sqrt(lx * lx + ly * ly);
-    lx /= ln;
-    ly /= ln;
-    double ux = (-unz) * (-ly), uy = (-unz) * lx;
-    double d0x = rs[i][0] - rmc[0], d0y = rs[i][1] - rmc[1];
-    double d1x = rs[ip1][0] - rmc[0], d1y = rs[ip1][1] - rmc[1];
-    double p0 = ux * d0x + uy * d0y;
-    double p0sq = p0 * p0;
-    double lp = lx * d1x + ly * d1y;
-    double lm = lx * d0x + ly * d0y;
-    double ledge = lp - lm;
-    double pplus = sqrt(p0sq + lp * lp);
-    double pminus = sqrt(p0sq + lm * lm);
-    double factor;
-    if (fabs(p0 / ledge) < 1e-4) {
-      factor = lp * pplus - lm * pminus;
-    } else {
-      factor = p0 * log((pplus + lp) / (pminus + lm));
-      ri += factor;
-      factor = (factor * p0 + pplus * lp) - pminus * lm;
+  if (q == 0) {
+    const int nxt[3] = {1, 2, 0};
+    for (int i = 0; i < 3; ++i) {
+      int ip1 = nxt[i];
+      double lx = rs[ip1][0] - rs[i][0], ly = rs[ip1][1] - rs[i][1];
+      double ln = sqrt(lx * lx + ly * ly);
+      lx /= ln;
+      ly /= ln;
+      double ux = (-unz) * (-ly), uy = (-unz) * lx;
+      double d0x = rs[i][0] - rmc[0], d0y = rs[i][1] - rmc[1];
+      double d1x = rs[ip1][0] - rmc[0], d1y = rs[ip1][1] - rmc[1];
+      double p0 = ux * d0x + uy * d0y;
+      double p0sq = p0 * p0;
+      double lp = lx * d1x + ly * d1y;
+      double lm = lx * d0x + ly * d0y;
+      double ledge = lp - lm;
+      double pplus = sqrt(p0sq + lp * lp);
+      double pminus = sqrt(p0sq + lm * lm);
+      double factor;
+      if (fabs(p0 / ledge) < 1e-4) {
+        factor = lp * pplus - lm * pminus;
+      } else {
+        factor = p0 * log((pplus + lp) / (pminus + lm));
+        ri += factor;
+        factor = (factor * p0 + pplus * lp) - pminus * lm;
+      }
+      rr0 += ux * factor;
+      rr1 += uy * factor;
     }
-    rr0 += ux * factor;
-    rr1 += uy * factor;
+    rr0 *= 0.5;
+    rr1 *= 0.5;
+    rr0 /= area2;
+    rr1 /= area2;
+    ri /= (area2 * ul);
   }
-  rr0 *= 0.5;
-  rr1 *= 0.5;
-  rr0 /= area2;
-  rr1 /= area2;
-  ri /= (area2 * ul);
-  jk.J[iu] = aJ; jk.Jxi[iu] = aJx; jk.Jeta[iu] = aJe;
-  jk.K[iu] = aK; jk.Kxi[iu] = aKx; jk.Keta[iu] = aKe;
-  jk.rho_r[2 * iu] = rr0;
-  jk.rho_r[2 * iu + 1] = rr1;
-  jk.rinv[iu] = ri;
-  if (bad) atomicAdd(nonconv, 1);
+#pragma unroll
+  for (int p = 0; p < NP; ++p) {
+    cd aJ = mkcd(0, 0), aJx = aJ, aJe = aJ, aK = aJ, aKx = aJ, aKe = aJ;
+    int bad = 0;
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {  // every lane takes part in the shuffles; the group's lane 0 keeps the sums
+      cd jv, kv;
+      jv.x = __shfl_sync(0xffffffffu, js[p].x, grp + i);
+      jv.y = __shfl_sync(0xffffffffu, js[p].y, grp + i);
+      kv.x = __shfl_sync(0xffffffffu, ks[p].x, grp + i);
+      kv.y = __shfl_sync(0xffffffffu, ks[p].y, grp + i);
+      bad |= !((__shfl_sync(0xffffffffu, ok, grp + i) >> p) & 1u);
+      cd jw = c_qw[i] * jv;
+      aJx = aJx + c_qxi[i] * jw;
+      aJe = aJe + c_qeta[i] * jw;
+      aJ = aJ + jw;
+      cd kw = c_qw[i] * kv;
+      aKx = aKx + c_qxi[i] * kw;
+      aKe = aKe + c_qeta[i] * kw;
+      aK = aK + kw;
+    }
+    if (q != 0 || !live || p >= np) continue;
+    const JKDev &o = jk.s[p];
+    o.J[iu] = aJ; o.Jxi[iu] = aJx; o.Jeta[iu] = aJe;
+    o.K[iu] = aK; o.Kxi[iu] = aKx; o.Keta[iu] = aKe;
+    o.rho_r[2 * iu] = rr0;
+    o.rho_r[2 * iu + 1] = rr1;
+    o.rinv[iu] = ri;
+    if (bad) atomicAdd(nonconv + p, 1);
+  }
 }
 
 // Per-point coefficients that turn the face-pair integrals into Z terms:
@@ -449,13 +487,32 @@ void pss_adj_contract(const SheetDev &G, const PointParams *dP1, const cd *zb, c
   k_adj_reduce<<<nm * nm, 256, 0, st>>>(nblk * kAdjChunks, nm * nm, part, Gout);
 }
 
+void pss_filljk_group(const SheetDev &G, double ulocal, int np, const double *psi1, const double *psi2,
+                      const double s1[2], const double s2[2], const JKDev *jk, int *nonconv, cudaStream_t st) {
+  if (G.nufp == 0 || np <= 0) return;
+  PsiGroup pg{};
+  JKGroup jg{};
+  pg.n = std::min(np, kJKGroup);
+  for (int p = 0; p < pg.n; ++p) {
+    pg.psi1[p] = psi1[p];
+    pg.psi2[p] = psi2[p];
+    jg.s[p] = jk[p];
+  }
+  const double a = ulocal * s1[0], b = ulocal * s1[1], c = ulocal * s2[0], d = ulocal * s2[1];
+  const long long lanes = (long long)G.nufp * 8;
+  pss_count_launch();
+  if (pg.n == 1)
+    k_filljk<1><<<cdiv_u(lanes, jk_threads<1>()), jk_threads<1>(), 0, st>>>(G, ulocal, pg, a, b, c, d, jg, nonconv);
+  else if (pg.n == 2)
+    k_filljk<2><<<cdiv_u(lanes, jk_threads<2>()), jk_threads<2>(), 0, st>>>(G, ulocal, pg, a, b, c, d, jg, nonconv);
+  else
+    k_filljk<kJKGroup><<<cdiv_u(lanes, jk_threads<kJKGroup>()), jk_threads<kJKGroup>(), 0, st>>>(G, ulocal, pg, a, b,
+                                                                                             c, d, jg, nonconv);
+}
+
 void pss_filljk(const SheetDev &G, double ulocal, double psi1, double psi2, const double s1[2], const double s2[2],
                 JKDev jk, int *nonconv, cudaStream_t st) {
-  if (G.nufp == 0) return;
-  pss_count_launch();
-  k_filljk<<<cdiv_u((long long)G.nufp * 8, 256), 256, 0, st>>>(G, ulocal, psi1, psi2, ulocal * s1[0],
-                                                                 ulocal * s1[1], ulocal * s2[0], ulocal * s2[1], jk,
-                                                                 nonconv);
+  pss_filljk_group(G, ulocal, 1, &psi1, &psi2, s1, s2, &jk, nonconv, st);
 }
 
 void pss_fill_pairs(const SheetDev &G, const PointParams *dP1, const JKDev &jk, const cd *t1, const cd *t2,

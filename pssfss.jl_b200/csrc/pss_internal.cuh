@@ -75,6 +75,17 @@ struct JKDev {
   double *rinv;   // nufp
 };
 
+// Face-pair integrals of up to kJKGroup phasings (psi1, psi2) of one sheet in one launch: the
+// phasing-free part of every lattice summand is shared, each phasing keeps its own sums.
+constexpr int kJKGroup = 4;
+struct PsiGroup {
+  double psi1[kJKGroup], psi2[kJKGroup];
+  int n;
+};
+struct JKGroup {
+  JKDev s[kJKGroup];
+};
+
 // Modal tables of one point: padded (mmax+2)^2 column-major, index (m,n) in -1..mmax.
 struct TableDev {
   cd *t1, *t2;
@@ -138,6 +149,9 @@ size_t pss_table_cap(int mmax);  // (mmax+2)^2 entries per padded table
 // Face-pair integrals and matrix fill (pss_fill.cu)
 void pss_filljk(const SheetDev &G, double ulocal, double psi1, double psi2, const double s1[2],
                 const double s2[2], JKDev jk, int *nonconv, cudaStream_t st);
+// np <= kJKGroup phasings at once into jk[0..np), non-convergence counts into nonconv[0..np)
+void pss_filljk_group(const SheetDev &G, double ulocal, int np, const double *psi1, const double *psi2,
+                      const double s1[2], const double s2[2], const JKDev *jk, int *nonconv, cudaStream_t st);
 void pss_fill_pairs(const SheetDev &G, const PointParams *dP1, const JKDev &jk, const cd *t1, const cd *t2,
                     int mmax, cd *zb, cudaStream_t st);
 // Assemble Z (row-major): z64 with leading dimension ld, the FP32 planes (zr, zi) with ldf.

@@ -26,8 +26,8 @@ def ring(period, ro, ntri):
     return polyring(s1=[period, 0], s2=[0, period], a=[r - 0.05 * period], b=[r], sides=24, ntri=ntri, units=mm)
 
 
-def problem(sheet, freqs, theta, **kw):
-    plan = make_plan([Layer(), sheet, Layer()], freqs, {"θ": theta, "ϕ": 0.0})
+def problem(sheet, freqs, theta, phi=0.0, **kw):
+    plan = make_plan([Layer(), sheet, Layer()], freqs, {"θ": theta, "ϕ": phi})
     (ig, (i1, i2), isht, s), = sheet_gblocks(plan)
     ios = [sheet_io(pt.layers[i1 - 1:i2], sheet, s, pt.k0, pt.beta00) for pt in plan.points]
     return dict(sheet=sheet, rwg=plan.rwgdat[isht - 1], points=plan.points, region_rng=(i1, i2), s=s,
@@ -56,6 +56,29 @@ def test_multi_equals_single_calls_and_oracle():
             assert rel(g, s1) < 1e-12
             ref, _, _ = oracle.partial_dS(pr["sheet"], pr["rwg"], pt.layers[i1 - 1:i2], pr["s"], pt.k0, pr["u"], io)
             assert rel(g, ref) < 1e-9
+
+
+def test_grouped_face_integrals_at_oblique_incidence():
+    # the phasing varies with frequency, so every point takes its own face integrals, computed
+    # for up to four points of a batch in one launch: batches of 1 (one phasing per launch),
+    # 3 (a group with an idle slot) and 6 (a group of four, then two) give the same dS, and
+    # that dS matches the oracle
+    sheet = ring(8.0, 0.42, 300)
+    freqs = [10.0, 11.5, 13.0, 14.5, 16.0, 17.5]
+    res = {}
+    for batch in (1, 3, 6):
+        pr = problem(sheet, freqs, 30.0, 20.0, batch=batch)
+        assert len({(io.psi1, io.psi2) for io in pr["ios"]}) == len(freqs)
+        res[batch] = engine.partial_gsms_multi([pr], precision="fp64")[0]
+    for b in (3, 6):
+        for g, r in zip(res[b], res[1]):
+            assert rel(g, r) < 1e-12
+    i1, i2 = pr["region_rng"]
+    for k in (0, 3, 5):
+        pt, io = pr["points"][k], pr["ios"][k]
+        assert abs(io.psi1) > 0 and abs(io.psi2) > 0
+        ref, _, _ = oracle.partial_dS(sheet, pr["rwg"], pt.layers[i1 - 1:i2], pr["s"], pt.k0, pr["u"], io)
+        assert rel(res[6][k], ref) < 1e-9
 
 
 @pytest.mark.parametrize("panel_w,outer_nb,batch", [(32, 128, 12), (16, 128, 5), (32, 64, 3), (16, 64, 32),
