@@ -5,16 +5,18 @@ and ``combine`` exactly as in the reference, so node numbering, edge numbering a
 coordinates are identical.  ``pecsheet``/``pmcsheet`` (``:108-126``) are the null
 sheets.
 
-``polyring`` (``:368-558``) and ``jerusalemcross`` (``:963-...``) take the reference's
-geometry arguments but are meshed here with structured meshes of their own (a polar grid
-per ring; a rectilinear grid over the union of rectangles), because the reference meshes
-them with Shewchuk's Triangle, which is not available: same shapes, different
-triangulations, so results agree with the reference only to discretisation accuracy.
+``polyring`` (``:368-558``), ``loadedcross`` (``:794-961``) and ``jerusalemcross``
+(``:963-1100``) build a boundary graph (points, segments, hole seeds) and mesh it with
+``meshsub`` as the reference does; the reference's mesher is Shewchuk's Triangle, which is not
+available, so ``meshsub.py`` meshes the graph by its own conforming Delaunay refinement under
+the same switches: same shapes and mesh sizes, different triangulations, so results agree
+with the reference only to discretisation accuracy.
 """
 import math
 
 import numpy as np
 
+from .meshsub import meshsub
 from .sheets import RWGSheet, combine, recttri, rotate, s1s2_to_b1b2, translate
 
 _DEFAULTS = dict(cls="J", dx=0.0, dy=0.0, rot=0.0, Rsheet=0.0, save="", fufp=False)
@@ -311,12 +313,12 @@ def _finish_sheet(sheet, style, units, s1, s2, kwargs):
 def polyring(*, s1, s2, a, b, sides, ntri, units, orient=0.0, **kwarg):
     """Concentric regular-polygon rings (``Elements.jl:368-558``): ring i spans radii
     a[i]..b[i] (a[i] = 0: a solid polygon), centred in the cell, first vertex at angle
-    ``orient`` (degrees).  Structured polar mesh of about ``ntri`` triangles in total,
-    shared among the rings by area.  ``b[-1] < 0`` makes the last ring fill the cell out to
-    its boundary, with ``-b[-1]`` edges along the shorter lattice vector (the longer one in
-    proportion): its polygonal inner edge is joined to the cell boundary by layers blended
-    along rays from the centre, the last of them zipped to the boundary nodes by angle, and
-    the sheet is periodic across the cell edges."""
+    ``orient`` (degrees), about ``ntri`` triangles in total.  ``b[-1] < 0`` makes the last
+    ring fill the cell out to its boundary, with ``-b[-1]`` edges along the shorter lattice
+    vector (the longer one in proportion), and the sheet is periodic across the cell edges.
+    The boundary graph, its hole seeds and the area target are the reference's; the graph is
+    meshed by ``meshsub`` (conforming Delaunay, 30-degree angle bound), the cell boundary of
+    a cell-filling ring without added nodes so opposite edges keep matching nodes."""
     kwargs = dict(kwarg)
     kwargs.setdefault("fufp", False)
     _check_kwargs(kwargs)
@@ -325,14 +327,17 @@ def polyring(*, s1, s2, a, b, sides, ntri, units, orient=0.0, **kwarg):
     b = [float(x) for x in b]
     if len(a) != len(b):
         raise ValueError("length(a) !== length(b)")
+    nring = len(a)
     fillcell = b[-1] < 0
-    for i in range(len(a)):
-        if a[i] >= b[i] and not (fillcell and i == len(a) - 1):
+    for i in range(nring):
+        if a[i] >= b[i] and not (fillcell and i == nring - 1):
             raise ValueError(f"a[{i + 1}] >= b[{i + 1}]")
-        if i + 1 < len(a) and b[i] >= a[i + 1]:
+        if i + 1 < nring and b[i] >= a[i + 1]:
             raise ValueError(f"b[{i + 1}] >= a[{i + 2}]")
     s1 = np.asarray(s1, float)
     s2 = np.asarray(s2, float)
+    if s1.shape != (2,) or s2.shape != (2,):
+        raise ValueError("s1 and s2 must have length 2")
     rho0 = 0.5 * (s1 + s2)
     alpha = 2 * math.pi / sides
     area_factor = 0.5 * sides * math.sin(alpha)
@@ -340,162 +345,145 @@ def polyring(*, s1, s2, a, b, sides, ntri, units, orient=0.0, **kwarg):
     if fillcell:
         if a[-1] <= 0:
             raise ValueError("a cell-filling ring needs a[end] > 0")
+        nshort = int(round(-b[-1]))
+        if nshort < 1:
+            raise ValueError("-b[end] must be a positive number of edges")
+        n1, n2 = np.linalg.norm(s1), np.linalg.norm(s2)
+        ns1, ns2 = (nshort, round(nshort * n2 / n1)) if n1 <= n2 else (round(nshort * n1 / n2), nshort)
         areas[-1] = abs(s1[0] * s2[1] - s1[1] * s2[0]) - area_factor * a[-1] * a[-1]
-    rho, tris = [], []
-    for iring, (aa, bb, ar) in enumerate(zip(a, b, areas)):
-        nt = max(2 * sides, round(ntri * ar / sum(areas)))
-        if fillcell and iring == len(a) - 1:
-            _cell_ring(rho, tris, rho0, s1, s2, int(round(-bb)), aa, sides, orient, nt)
-            continue
-        # ns segments per polygon side, nr radial layers, cells as close to square as the
-        # triangle budget allows: 2 * sides * ns * nr ~ nt with (bb - aa) / nr ~ side(rmid) / ns
-        rmid = 0.5 * (aa + bb)
-        side = 2 * rmid * math.sin(alpha / 2)
-        ratio = (bb - aa) / side  # nr / ns
-        ns = max(1, round(math.sqrt(nt / (2 * sides * ratio))))
-        nr = max(1, round(nt / (2 * sides * ns)))
-        m = sides * ns  # nodes per layer
-        verts = [np.array([math.cos(math.radians(orient) + i * alpha), math.sin(math.radians(orient) + i * alpha)])
-                 for i in range(sides)]
-        dirs = [verts[i] + (verts[(i + 1) % sides] - verts[i]) * (t / ns) for i in range(sides) for t in range(ns)]
-        layers = []
-        r_in = aa if aa > 0 else bb / (nr + 1)
-        nl = nr + 1 if aa > 0 else nr
-        for k in range(nl + (0 if aa > 0 else 1)):
-            r = (aa + (bb - aa) * k / nr) if aa > 0 else bb * (k + 1) / (nr + 1)
-            base = len(rho)
-            rho.extend(rho0 + r * d for d in dirs)
-            layers.append(base)
-        if aa == 0:  # centre node and its fan to the first layer
-            c = len(rho)
-            rho.append(rho0.copy())
-            for i in range(m):
-                tris.append((c, layers[0] + i, layers[0] + (i + 1) % m))
-        for k in range(len(layers) - 1):
-            lo, hi = layers[k], layers[k + 1]
-            for i in range(m):
-                i1 = (i + 1) % m
-                tris.append((lo + i, hi + i, hi + i1))
-                tris.append((lo + i, hi + i1, lo + i1))
-    sheet = _sheet_from_triangles(rho, tris)
+    pts, segs, marks = [], [], []
+
+    def loop(points, marker):
+        base = len(pts)
+        pts.extend(points)
+        k = len(points)
+        segs.extend((base + i, base + (i + 1) % k) for i in range(k))
+        marks.extend([marker] * k)
+
+    def polygon(r):
+        o = math.radians(orient)
+        return [rho0 + r * np.array([math.cos(o + i * alpha), math.sin(o + i * alpha)]) for i in range(sides)]
+    boundary = 0
+    for iring in range(nring):
+        if a[iring] == 0:
+            boundary += 1
+            loop(polygon(b[iring]), boundary)
+        elif fillcell and iring == nring - 1:
+            boundary += 1
+            cell = ([i / ns1 * s1 for i in range(ns1)] + [s1 + i / ns2 * s2 for i in range(ns2)] +
+                    [s1 + s2 - i / ns1 * s1 for i in range(ns1)] + [s2 - i / ns2 * s2 for i in range(ns2)])
+            loop(cell, boundary)
+            cell_marker = boundary
+            boundary += 1
+            loop(polygon(a[iring]), boundary)
+        else:
+            for r in (b[iring], a[iring]):
+                boundary += 1
+                loop(polygon(r), boundary)
+    holes = []
+    if a[0] > 0:
+        holes.append(rho0)
+    u = np.array([math.cos(math.radians(orient)), math.sin(math.radians(orient))])
+    for i in range(nring - 1):
+        holes.append(rho0 + 0.5 * (b[i] + a[i + 1]) * u)
+    sheet = meshsub(points=np.array(pts).T, seglist=np.array(segs).T + 1, segmarkers=marks,
+                    holes=np.array(holes).T if holes else None, area=sum(areas) / ntri, ntri=ntri,
+                    fixed_markers=(cell_marker,) if fillcell else ())
     _finish_sheet(sheet, "polyring", units, s1, s2, kwargs)
     sheet.xi_eta_check = fillcell
     return sheet
 
 
-def _cell_ring(rho, tris, rho0, s1, s2, nshort, a, sides, orient, nt):
-    """Append the mesh of the region between the regular polygon of radius ``a`` (centred at
-    ``rho0``, first vertex at ``orient`` degrees) and the boundary of the cell spanned by
-    ``s1``, ``s2`` from the origin.  Boundary nodes are uniform, ``nshort`` edges along the
-    shorter lattice vector and the longer one in proportion (``Elements.jl:393-403``), so
-    opposite edges match for the periodic basis functions.  The polygon, with about as many
-    nodes as the boundary, is carried outward in layers along the rays through its nodes
-    (quad strips split on a diagonal); the last layer is joined to the boundary nodes by a
-    merge in angle about the centre."""
-    if nshort < 1:
-        raise ValueError("-b[end] must be a positive number of edges")
-    n1, n2 = np.linalg.norm(s1), np.linalg.norm(s2)
-    ns1, ns2 = (nshort, round(nshort * n2 / n1)) if n1 <= n2 else (round(nshort * n1 / n2), nshort)
-    outer = ([i / ns1 * s1 for i in range(ns1)] + [s1 + i / ns2 * s2 for i in range(ns2)] +
-             [s1 + s2 - i / ns1 * s1 for i in range(ns1)] + [s2 - i / ns2 * s2 for i in range(ns2)])
-    M = len(outer)
-    ns = max(1, round(M / sides))
-    m = sides * ns
-    alpha = 2 * math.pi / sides
-    verts = [rho0 + a * np.array([math.cos(math.radians(orient) + i * alpha), math.sin(math.radians(orient) + i * alpha)])
-             for i in range(sides)]
-    poly = [verts[i] + (verts[(i + 1) % sides] - verts[i]) * (t / ns) for i in range(sides) for t in range(ns)]
-    Binv = np.linalg.inv(np.column_stack([s1, s2]))
-
-    def reach(d):  # distance from the centre to the cell boundary along direction d
-        q = Binv @ d
-        return 0.5 / max(abs(q[0]), abs(q[1]))
-    rays = []
-    for p in poly:
-        v = p - rho0
-        r0 = np.linalg.norm(v)
-        rays.append((r0, v / r0, reach(v / r0)))
-    nlayer = max(1, 1 + round((nt - m - M) / (2 * m)))
-    layers = []
-    for k in range(nlayer):
-        base = len(rho)
-        rho.extend(rho0 + (r0 + (R - r0) * k / nlayer) * d for r0, d, R in rays)
-        layers.append(base)
-    for k in range(nlayer - 1):
-        lo, hi = layers[k], layers[k + 1]
-        for i in range(m):
-            i1 = (i + 1) % m
-            tris.append((lo + i, hi + i, hi + i1))
-            tris.append((lo + i, hi + i1, lo + i1))
-    obase = len(rho)
-    rho.extend(outer)
-
-    def ang(p):
-        return math.atan2(p[1] - rho0[1], p[0] - rho0[0])
-    ref = ang(outer[0])
-    inner = [layers[-1] + i for i in range(m)]
-    ai = [(ang(rho[q]) - ref) % (2 * math.pi) for q in inner]
-    s0 = int(np.argmin(ai))
-    inner, ai = inner[s0:] + inner[:s0], ai[s0:] + ai[:s0]
-    ao = [(ang(p) - ref) % (2 * math.pi) for p in outer]
-    ao[0] = 0.0
-    i = j = 0
-    while i < m or j < M:
-        nxt_i = ai[(i + 1) % m] + (2 * math.pi if i + 1 >= m else 0.0)
-        nxt_o = ao[(j + 1) % M] + (2 * math.pi if j + 1 >= M else 0.0)
-        I, O = inner[i % m], obase + j % M
-        if j < M and (i >= m or nxt_o <= nxt_i):
-            tris.append((I, O, obase + (j + 1) % M))
-            j += 1
-        else:
-            tris.append((I, O, inner[(i + 1) % m]))
-            i += 1
-
-
-def _rect_union_mesh(rects, h, holes=()):
-    """Conforming triangulation of a union of axis-aligned rectangles (x0, y0, x1, y1) less
-    the union of the ``holes`` rectangles: grid lines at every rectangle edge, refined to
-    steps <= h, cells inside the region split along the lower-left/upper-right diagonal."""
-    def lines(vals):
-        vals = sorted(set(round(v, 12) for v in vals))
-        out = [vals[0]]
-        for lo, hi in zip(vals, vals[1:]):
-            k = max(1, math.ceil((hi - lo) / h - 1e-9))
-            out.extend(lo + (hi - lo) * (i + 1) / k for i in range(k))
-        return np.array(out)
+def _rect_union_outline(rects, holes=()):
+    """Boundary graph of a union of axis-aligned rectangles (x0, y0, x1, y1) less the union
+    of the ``holes`` rectangles: the boundary loops of the region (corners only, the region
+    on the left of each segment), one marker per loop, and a seed point just outside the
+    region beside every loop (hole seeds for ``meshsub``)."""
     allr = list(rects) + list(holes)
-    xs = lines([r[0] for r in allr] + [r[2] for r in allr])
-    ys = lines([r[1] for r in allr] + [r[3] for r in allr])
-    inside = np.zeros((len(xs) - 1, len(ys) - 1), bool)
-    xc = 0.5 * (xs[:-1] + xs[1:])
-    yc = 0.5 * (ys[:-1] + ys[1:])
+    xs = np.array(sorted(set(round(v, 12) for r in allr for v in (r[0], r[2]))))
+    ys = np.array(sorted(set(round(v, 12) for r in allr for v in (r[1], r[3]))))
+    xc, yc = 0.5 * (xs[:-1] + xs[1:]), 0.5 * (ys[:-1] + ys[1:])
+    inside = np.zeros((len(xc), len(yc)), bool)
     for x0, y0, x1, y1 in rects:
         inside |= ((xc > x0) & (xc < x1))[:, None] & ((yc > y0) & (yc < y1))[None, :]
     for x0, y0, x1, y1 in holes:
         inside &= ~(((xc > x0) & (xc < x1))[:, None] & ((yc > y0) & (yc < y1))[None, :])
-    nid = -np.ones((len(xs), len(ys)), np.int64)
-    rho, tris = [], []
 
-    def node(i, j):
-        if nid[i, j] < 0:
-            nid[i, j] = len(rho)
-            rho.append((xs[i], ys[j]))
-        return nid[i, j]
-    for j in range(len(ys) - 1):
-        for i in range(len(xs) - 1):
-            if inside[i, j]:
-                ll, lr, ur, ul = node(i, j), node(i + 1, j), node(i + 1, j + 1), node(i, j + 1)
-                tris.append((ll, ur, ul))
-                tris.append((ll, lr, ur))
-    return np.array(rho), np.array(tris)
+    def ins(i, j):
+        return 0 <= i < len(xc) and 0 <= j < len(yc) and inside[i, j]
+    nxt = {}  # directed boundary edges, region on the left: start grid node -> end grid node
+    for i in range(len(xc)):
+        for j in range(len(yc)):
+            if not inside[i, j]:
+                continue
+            if not ins(i, j - 1):
+                nxt.setdefault((i, j), []).append((i + 1, j))
+            if not ins(i + 1, j):
+                nxt.setdefault((i + 1, j), []).append((i + 1, j + 1))
+            if not ins(i, j + 1):
+                nxt.setdefault((i + 1, j + 1), []).append((i, j + 1))
+            if not ins(i - 1, j):
+                nxt.setdefault((i, j + 1), []).append((i, j))
+    pts, segs, marks, seeds = [], [], [], []
+    dmin = min(np.diff(xs).min(), np.diff(ys).min())
+    while nxt:
+        start = min(nxt)
+        loop = [start]
+        cur, prev_dir = start, None
+        while True:
+            outs = nxt[cur]
+            if len(outs) > 1 and prev_dir is not None:  # a pinch: turn left first
+                outs.sort(key=lambda q: -((prev_dir[0] * (q[1] - cur[1]) - prev_dir[1] * (q[0] - cur[0]))))
+            q = outs.pop(0)
+            if not outs:
+                del nxt[cur]
+            prev_dir = (q[0] - cur[0], q[1] - cur[1])
+            cur = q
+            if cur == start:
+                break
+            loop.append(cur)
+        # corners only
+        k = len(loop)
+        corner = []
+        for m in range(k):
+            p0, p1, p2 = loop[m - 1], loop[m], loop[(m + 1) % k]
+            if (p1[0] - p0[0]) * (p2[1] - p1[1]) - (p1[1] - p0[1]) * (p2[0] - p1[0]) != 0:
+                corner.append(p1)
+        base = len(pts)
+        pts.extend((xs[i], ys[j]) for i, j in corner)
+        marker = len(seeds) + 1
+        segs.extend((base + m, base + (m + 1) % len(corner)) for m in range(len(corner)))
+        marks.extend([marker] * len(corner))
+        (i0, j0), (i1, j1) = loop[0], loop[1]
+        mx, my = 0.5 * (xs[i0] + xs[i1]), 0.5 * (ys[j0] + ys[j1])
+        dx, dy = np.sign(i1 - i0), np.sign(j1 - j0)
+        seeds.append((mx + 0.25 * dmin * dy, my - 0.25 * dmin * dx))  # right of the edge: outside
+    return np.array(pts), np.array(segs), marks, np.array(seeds)
+
+
+def _outline_area(pts, segs):
+    """Area enclosed by the boundary loops (region on the left of every segment)."""
+    p, q = pts[segs[:, 0]], pts[segs[:, 1]]
+    return 0.5 * float(np.sum(p[:, 0] * q[:, 1] - q[:, 0] * p[:, 1]))
+
+
+def _mesh_outline(rects, holes, ntri, rot=None, shift=(0.0, 0.0)):
+    """``meshsub`` of a rectangle union's outline (about ``ntri`` triangles, maximum area
+    the region's over ``ntri`` as the reference's ``areat / ntri``), optionally rotated by
+    the matrix ``rot`` (row vectors) and shifted."""
+    pts, segs, marks, seeds = _rect_union_outline(rects, holes)
+    if rot is not None:
+        pts, seeds = pts @ rot, seeds @ rot
+    pts, seeds = pts + np.asarray(shift), seeds + np.asarray(shift)
+    return meshsub(points=pts.T, seglist=segs.T + 1, segmarkers=marks, holes=seeds.T,
+                   area=_outline_area(pts, segs) / ntri, ntri=ntri)
 
 
 def loadedcross(*, s1, s2, L1, L2, w, ntri, units, orient=0.0, **kwarg):
     """Loaded cross (``Elements.jl:794-961``): a cross of arm length ``L1`` (tip to tip) and
     arm width ``L2`` centred in the cell, hollowed to a loop of trace width ``w`` when
     2w < L2 (solid otherwise), rotated by ``orient`` degrees about its centre.  The outline
-    is axis-aligned before the rotation, so it is meshed by a conforming grid (cells of
-    about equal area, ~``ntri`` triangles) instead of the reference's Triangle mesh."""
+    (axis-aligned before the rotation) is meshed by ``meshsub`` to about ``ntri`` triangles."""
     kwargs = dict(kwarg)
     kwargs.setdefault("fufp", False)
     _check_kwargs(kwargs)
@@ -508,19 +496,14 @@ def loadedcross(*, s1, s2, L1, L2, w, ntri, units, orient=0.0, **kwarg):
         raise ValueError("L2 must be smaller than L1")
     h1, h2 = L1 / 2, L2 / 2
     rects = [(-h1, -h2, h1, h2), (-h2, -h1, h2, h1)]
-    area = 2 * L1 * L2 - L2 * L2
     holes = []
     if 2 * w < L2:
         holes = [(-h1 + w, -h2 + w, h1 - w, h2 - w), (-h2 + w, -h1 + w, h2 - w, h1 - w)]
-        a1, a2 = L1 - 2 * w, L2 - 2 * w
-        area -= 2 * a1 * a2 - a2 * a2
-    h = math.sqrt(2 * area / ntri)
-    rho, tris = _rect_union_mesh(rects, min(h, w if holes else h), holes)
+    rot = None
     if orient != 0:
         sn, cs = math.sin(math.radians(orient)), math.cos(math.radians(orient))
-        rho = rho @ np.array([[cs, sn], [-sn, cs]])
-    rho = rho + 0.5 * (s1 + s2)
-    sheet = _sheet_from_triangles(rho, tris)
+        rot = np.array([[cs, sn], [-sn, cs]])
+    sheet = _mesh_outline(rects, holes, ntri, rot, 0.5 * (s1 + s2))
     return _finish_sheet(sheet, "loadedcross", units, s1, s2, kwargs)
 
 
@@ -530,8 +513,8 @@ def jerusalemcross(*, P, L1, L2, A, B, w, ntri, units, **kwarg):
     trace width w.  As in the reference, a part whose width is at most 2w is solid: w >= L2/2
     fills the arms, w >= B/2 the caps, both fill the whole cross.  With hollow arms and
     solid caps the arm slot stops a trace width short of the caps; with both hollow the
-    slot runs into the caps' openings.  The outline is axis-aligned, so it is meshed by a
-    conforming grid (about ``ntri`` triangles) instead of the reference's Triangle mesh."""
+    slot runs into the caps' openings.  The outline is meshed by ``meshsub`` to about
+    ``ntri`` triangles."""
     kwargs = dict(kwarg)
     kwargs.setdefault("fufp", False)
     _check_kwargs(kwargs)
@@ -543,7 +526,6 @@ def jerusalemcross(*, P, L1, L2, A, B, w, ntri, units, **kwarg):
     rects = [(c - h1, c - h2, c + h1, c + h2), (c - h2, c - h1, c + h2, c + h1),   # arms
              (c - h1, c - hA, c - h1 + B, c + hA), (c + h1 - B, c - hA, c + h1, c + hA),  # caps
              (c - hA, c - h1, c + hA, c - h1 + B), (c - hA, c + h1 - B, c + hA, c + h1)]
-    area = 2 * L1 * L2 - L2 * L2 + 4 * (A * B - L2 * B)
     hollow_arms, hollow_caps = 2 * w < L2, 2 * w < B
     holes = []
     if hollow_arms:
@@ -554,7 +536,5 @@ def jerusalemcross(*, P, L1, L2, A, B, w, ntri, units, **kwarg):
         a_, b_ = hA - w, h1 - w
         holes += [(c - b_, c - a_, c - h1 + B - w, c + a_), (c + h1 - B + w, c - a_, c + b_, c + a_),
                   (c - a_, c - b_, c + a_, c - h1 + B - w), (c - a_, c + h1 - B + w, c + a_, c + b_)]
-    h = math.sqrt(2 * area / ntri)  # two triangles per h x h cell
-    rho, tris = _rect_union_mesh(rects, min(h, w) if holes else h, holes)
-    sheet = _sheet_from_triangles(rho, tris)
+    sheet = _mesh_outline(rects, holes, ntri)
     return _finish_sheet(sheet, "jerusalemcross", units, [float(P), 0.0], [0.0, float(P)], kwargs)
