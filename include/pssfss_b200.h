@@ -211,6 +211,12 @@ int pss_basis_transforms(pss_sheet *sheet, int nmodes, const double *kvec, doubl
 int pss_lu_solve(pss_ctx *ctx, int n, const double *Z, int nrhs, const double *B, int precision, double *X,
                  int *status);
 
+/* FP32 factorisation of the FP32 + refinement form on its own (no counterpart; the reference's
+ * zgetrf is FP64): Z n x n complex column-major in, rounded to complex64; LU out, the packed
+ * unit-lower L and upper U, n x n complex64 column-major; ipiv out 1-based, LAPACK's
+ * interchange convention (row j swapped with row ipiv[j]); info out, the first zero pivot. */
+int pss_lu32_factor(pss_ctx *ctx, int n, const double *Z, float *LU, int *ipiv, int *info);
+
 /* Device milliseconds of the last pss_partial_gsms call, summed over worker 0's batches:
  * [tables, face_integrals (0: folded into fill), fill, transforms+rhs, 0, factor+solve+refine,
  *  projection, total span of the call over all workers]. */

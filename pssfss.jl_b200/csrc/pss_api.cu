@@ -1290,6 +1290,42 @@ int pss_lu_solve(pss_ctx *c, int n, const double *Z, int nrhs, const double *B, 
   return 0;
 }
 
+int pss_lu32_factor(pss_ctx *c, int n, const double *Z, float *LU, int *ipiv, int *info) {
+  if (!c || !Z || !LU || !ipiv || !info || n <= 0) { pss_set_error("invalid argument"); return -1; }
+  if (set_device(c)) return -3;
+  Worker &w = c->w[0];
+  cudaStream_t st = w.st;
+  const size_t ldf = (size_t)Worker::ld32(n), nf = (size_t)n * ldf;
+  if (w.ensure_solver(n, 1, 1) || w.zr.ensure(nf * sizeof(float)) || w.zi.ensure(nf * sizeof(float))) return -3;
+  std::vector<float> hr(nf, 0.f), hi(nf, 0.f);  // row-major planes, row pitch ldf
+  for (size_t m = 0; m < (size_t)n; ++m)
+    for (size_t q = 0; q < (size_t)n; ++q) {
+      hr[m * ldf + q] = (float)Z[2 * (m + q * n)];
+      hi[m * ldf + q] = (float)Z[2 * (m + q * n) + 1];
+    }
+  PSS_CUDA_TRY(cudaMemcpy(w.zr.p, hr.data(), nf * sizeof(float), cudaMemcpyHostToDevice));
+  PSS_CUDA_TRY(cudaMemcpy(w.zi.p, hi.data(), nf * sizeof(float), cudaMemcpyHostToDevice));
+  PSS_CUDA_TRY(cudaMemsetAsync(w.info.p, 0, sizeof(int), st));
+  if (int rc = pss_lu32_batched(n, 1, w.zr.as<float>(), w.zi.as<float>(), (long long)ldf, (long long)nf,
+                                w.ipiv.as<int>(), w.info.as<int>(), w.luws.p, w.luws.n, st))
+    return rc;
+  PSS_CUDA_TRY(cudaStreamSynchronize(st));
+  PSS_CUDA_TRY(cudaGetLastError());
+  PSS_CUDA_TRY(cudaMemcpy(hr.data(), w.zr.p, nf * sizeof(float), cudaMemcpyDeviceToHost));
+  PSS_CUDA_TRY(cudaMemcpy(hi.data(), w.zi.p, nf * sizeof(float), cudaMemcpyDeviceToHost));
+  std::vector<int> hp(n);
+  PSS_CUDA_TRY(cudaMemcpy(hp.data(), w.ipiv.p, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost));
+  PSS_CUDA_TRY(cudaMemcpy(info, w.info.p, sizeof(int), cudaMemcpyDeviceToHost));
+  PSS_CUDA_TRY(cudaMemset(w.info.p, 0, sizeof(int)));
+  for (size_t m = 0; m < (size_t)n; ++m)
+    for (size_t q = 0; q < (size_t)n; ++q) {
+      LU[2 * (m + q * n)] = hr[m * ldf + q];
+      LU[2 * (m + q * n) + 1] = hi[m * ldf + q];
+    }
+  for (int j = 0; j < n; ++j) ipiv[j] = hp[j] + 1;
+  return 0;
+}
+
 int pss_schur_update(pss_ctx *c, int m, int n, int k, const float *Lr, const float *Li, const float *Ur,
                      const float *Ui, float *Cr, float *Ci, int *status) {
   if (!c || !Lr || !Li || !Ur || !Ui || !Cr || !Ci || m <= 0 || n <= 0 || k <= 0) {

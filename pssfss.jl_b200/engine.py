@@ -66,6 +66,7 @@ SIGNATURES = {
     "pss_schur_update": (_I, [_P, _I, _I, _I, _P, _P, _P, _P, _P, _P, _P]),
     "pss_lu_factor_noalloc": (_I, [_I, _P, _L, _P, _P, _P]),
     "pss_set_wait_limit": (_I, [_L]),
+    "pss_lu32_factor": (_I, [_P, _I, _P, _P, _P, _P]),
 }
 
 
@@ -486,6 +487,20 @@ def lu_solve(Z, B, precision="fp64", device=0):
                               PRECISIONS[precision], X.ctypes.data_as(ctypes.c_void_p), ctypes.byref(st)),
            "pss_lu_solve")
     return X, st.value
+
+
+def lu32_factor(Z, device=0):
+    """FP32 LU of the FP32 + refinement form (``pss_lu32_factor``): returns (LU packed
+    complex64, 1-based ipiv, info)."""
+    ctx = context(device)
+    Z = np.asfortranarray(np.asarray(Z, complex))
+    n = Z.shape[0]
+    LU = np.zeros((n, n), np.complex64, order="F")
+    ipiv = np.zeros(n, np.int32)
+    info = ctypes.c_int()
+    _check(lib().pss_lu32_factor(ctx, n, Z.ctypes.data_as(ctypes.c_void_p), LU.ctypes.data_as(ctypes.c_void_p),
+                                 ipiv.ctypes.data_as(ctypes.c_void_p), ctypes.byref(info)), "pss_lu32_factor")
+    return LU, ipiv, info.value
 
 
 def schur_update(L, U, C, device=0):

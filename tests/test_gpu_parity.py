@@ -132,6 +132,42 @@ def test_lu_solve_matches_lapack(precision, n):
     assert relerr(X, Xr) < 1e-11
 
 
+def _apply_ipiv(A, ipiv):
+    P = np.array(A, copy=True)
+    for j, p in enumerate(ipiv):
+        if p - 1 != j:
+            P[[j, p - 1]] = P[[p - 1, j]]
+    return P
+
+
+@pytest.mark.parametrize("n,dominant", [(700, False), (1300, True), (1300, False), (3000, False)])
+def test_fp32_factor_against_lapack_cgetrf(n, dominant):
+    # The FP32 factorisation of the FP32 + refinement form on its own: P Z = L U with LAPACK's
+    # interchange convention, multipliers bounded by the |re|+|im| pivot rule, and a backward
+    # error within a small factor of LAPACK cgetrf's on the same complex64 matrix (the
+    # trailing updates run as 3xTF32 products on the tensor cores).
+    import scipy.linalg as sl
+    rng = np.random.default_rng(n + dominant)
+    Z = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    if dominant:
+        Z += 3 * np.sqrt(n) * np.eye(n)
+    Z32 = Z.astype(np.complex64).astype(complex)
+    lu_l, piv_l = sl.lu_factor(Z.astype(np.complex64))
+    L_l = np.tril(lu_l.astype(complex), -1) + np.eye(n)
+    back_l = np.linalg.norm(_apply_ipiv(Z32, piv_l + 1) - L_l @ np.triu(lu_l.astype(complex))) / np.linalg.norm(Z32)
+    LU, ipiv, info = engine.lu32_factor(Z)
+    assert info == 0
+    assert ((ipiv >= np.arange(1, n + 1)) & (ipiv <= n)).all()
+    L = np.tril(LU.astype(complex), -1) + np.eye(n)
+    U = np.triu(LU.astype(complex))
+    back = np.linalg.norm(_apply_ipiv(Z32, ipiv) - L @ U) / np.linalg.norm(Z32)
+    assert back < 10 * back_l, (back, back_l)
+    assert np.max(np.abs(L)) <= np.sqrt(2) + 1e-5
+    assert np.max(np.abs(U)) / np.max(np.abs(Z32)) < 100
+    if dominant:  # no interchanges are needed, and none are made
+        assert (ipiv == np.arange(1, n + 1)).all()
+
+
 def test_lu_solve_mom_matrix_fp32_refinement():
     # The FillZY_test matrix (1-mil substrates) has cond(Z) ~ 2.2e6: two FP64 LAPACK
     # drivers already differ by ~1.5e-10 on it, and rounding Z to FP32 alone moves the
