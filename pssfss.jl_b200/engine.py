@@ -22,7 +22,7 @@ STATUS_BITS = {1: "table_noconv", 2: "jk_noconv", 4: "singular", 8: "refine_noco
 FATAL_STATUS = 4 | 16 | 64
 
 _lib = None
-_lock = threading.Lock()
+_lock = threading.RLock()  # context() reports a failed create through lib() while holding it
 _ctx = {}
 # uploaded sheets, most recently used last; a sheet's device arrays (its face-pair integral
 # cache grows as nface^2 for unstructured sheets) are freed when it falls out

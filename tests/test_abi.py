@@ -40,6 +40,20 @@ def test_no_device_error_is_reported_not_raised_in_c():
     rc = engine.lib().pss_ctx_create(0, 1, ctypes.byref(h))
     assert rc != 0
     assert b"device" in engine.lib().pss_last_error().lower() or b"cuda" in engine.lib().pss_last_error().lower()
+    # and the binding raises it (from inside its context cache, without deadlocking on its lock)
+    import threading
+    out = {}
+
+    def make():
+        try:
+            engine.context(0, 1)
+        except RuntimeError as e:
+            out["err"] = str(e)
+    t = threading.Thread(target=make, daemon=True)
+    t.start()
+    t.join(60)
+    assert not t.is_alive(), "engine.context() hung on a failed pss_ctx_create"
+    assert "pss_ctx_create" in out.get("err", "")
 
 
 def test_entry_points_reject_bad_arguments_before_any_device_use():
