@@ -213,14 +213,12 @@ extern "C" int pss_face_pair_classes(pss_ctx *ctx, int64_t nface, const double *
   PSS_CUDA_TRY(cudaMemcpy(dcen.p, cen, 2 * nface * sizeof(double), cudaMemcpyHostToDevice));
   PSS_CUDA_TRY(cudaMemcpy(dr1.p, r1, 2 * nface * sizeof(double), cudaMemcpyHostToDevice));
   PSS_CUDA_TRY(cudaMemcpy(dshape.p, shape, nface * sizeof(long long), cudaMemcpyHostToDevice));
-  // the table: first sized for a structured sheet's few classes (a quarter of the pairs); when
-  // that fills (a sheet whose symmetry is broken, say a perturbed one), once more at twice the
-  // pairs, so every key fits at a load of at most one half
+  // the table: the power of two at or above twice the pairs (every key fits at a load of at
+  // most one half, whatever the sheet's symmetry: a structured meander has a class for
+  // every 2.5 pairs, a perturbed one nearly one per pair), at most 2^28 slots (7.5 GB)
   unsigned long long cap = 1ull << 20;
-  while (cap < (unsigned long long)npairs / 4) cap <<= 1;
-  unsigned long long cap_full = 1ull << 20;
-  while (cap_full < 2ull * (unsigned long long)npairs) cap_full <<= 1;
-  for (int attempt = 0;; ++attempt) {
+  while (cap < 2ull * (unsigned long long)npairs && cap < (1ull << 28)) cap <<= 1;
+  {
     Buf w0, w1, state, first;
     PSS_CUDA_TRY(cudaMalloc(&w0.p, cap * sizeof(unsigned long long)));
     PSS_CUDA_TRY(cudaMalloc(&w1.p, cap * sizeof(unsigned long long)));
@@ -236,10 +234,6 @@ extern "C" int pss_face_pair_classes(pss_ctx *ctx, int64_t nface, const double *
                                 T, (int *)dslot.p, (int *)derr.p);
     int herr = 0;
     PSS_CUDA_TRY(cudaMemcpy(&herr, derr.p, sizeof(int), cudaMemcpyDeviceToHost));
-    if (herr == 1 && cap < cap_full && cap_full <= (1ull << 28)) {  // full: once more, large enough
-      cap = cap_full;
-      continue;
-    }
     if (herr) {
       pss_set_error("face-pair class table %s", herr == 1 ? "overflowed" : "insertion did not settle");
       return -3;
