@@ -23,6 +23,33 @@ namespace {
 // their product, one complex multiply in place of a sincos per summand.
 constexpr int kPhase = 2 * PSS_JKRINGMAX + 1;
 
+// exp(-a), a >= 0, by Tang's table-driven method (P. T. P. Tang, "Table-driven implementation
+// of the exponential function in IEEE floating-point arithmetic", ACM Trans. Math. Softw. 15
+// (1989) 144-157): -a = (256 m + j) ln2/256 + r with |r| <= ln2/512 (k = 256 m + j the nearest
+// integer to -a 256/ln2, found by adding 1.5 * 2^52; ln2/256 in two parts, so r keeps its full
+// precision), exp(-a) = 2^m * 2^(j/256) * p(r) with p the degree-5 Taylor polynomial of e^r
+// (remainder below r^6/720 < 1e-20 relative) and 2^(j/256) from a 256-entry table; 2^m enters
+// through the exponent field.  About ten FP64 operations.  a >= 708 gives 0: such summands are
+// far below the lattice sums' 1e-8 convergence test.
+constexpr double kExpShift = 6755399441055744.0;  // 1.5 * 2^52
+constexpr double kExpInvStep = 0x1.71547652b82fep+8;  // 256 / ln2
+constexpr double kExpStepHi = 0x1.62e42fefa39efp-9;   // ln2 / 256, nearest double
+constexpr double kExpStepLo = 0x1.abc9e3b39803fp-64;  // ln2 / 256 - kExpStepHi
+__device__ __forceinline__ double exp_neg(double a, const double *__restrict__ tab) {
+  if (!(a < 708.0)) return 0.0;
+  const double sh = fma(-a, kExpInvStep, kExpShift);
+  const int k = __double2loint(sh);  // nearest integer to -a 256/ln2, two's complement
+  const double kf = sh - kExpShift;
+  const double r = fma(kf, -kExpStepLo, fma(kf, -kExpStepHi, -a));
+  double p = fma(r, 1.0 / 120, 1.0 / 24);
+  p = fma(p, r, 1.0 / 6);
+  p = fma(p, r, 0.5);
+  p = fma(p, r, 1.0);
+  p = fma(p, r, 1.0);
+  const double t = tab[k & 255] * p;
+  return __hiloint2double(__double2hiint(t) + ((k >> 8) << 20), __double2loint(t));
+}
+
 // jksums (PGF.jl:67-106): the spatial lattice sums J and K at one observation offset, ring by
 // ring in the reference's order (rmin = 5, at most 65 rings, relative change 1e-8), for NP
 // phasings at once.  A summand's distance, exp(-u r) and 1/r do not depend on the phasing, so
@@ -34,11 +61,12 @@ template <int NP>
 __device__ __forceinline__ unsigned jksums_group(double urx, double ury, int np, bool nophase, double us1x,
                                                  double us1y, double us2x, double us2y,
                                                  const cd (*__restrict__ ph1)[kPhase],
-                                                 const cd (*__restrict__ ph2)[kPhase], cd *jout, cd *kout) {
+                                                 const cd (*__restrict__ ph2)[kPhase], const double *__restrict__ etab,
+                                                 cd *jout, cd *kout) {
   const int rmin = 5;
   const double small = 1e-5, convtest = 1e-8;
   double arg = sqrt(urx * urx + ury * ury);
-  double rterm = exp(-arg);
+  double rterm = exp_neg(arg, etab);
   const cd k0 = mkcd(rterm, 0.0);
   const cd j0 = arg <= small ? mkcd((-arg / 6 + 0.5) * arg - 1, 0.0) : mkcd((rterm - 1) / arg, 0.0);
   cd jsum[NP], ksum[NP];
@@ -49,21 +77,18 @@ __device__ __forceinline__ unsigned jksums_group(double urx, double ury, int np,
     cd jring[NP], kring[NP];
 #pragma unroll
     for (int p = 0; p < NP; ++p) { jring[p] = mkcd(0, 0); kring[p] = mkcd(0, 0); }
-    const int len = 8 * r;
-    for (int t = 0; t < len; ++t) {
-      int m, n;
-      ring_mn(r, t, m, n);
-      double dx = urx - ((double)m * us1x + (double)n * us2x);
-      double dy = ury - ((double)m * us1y + (double)n * us2y);
+    auto summand = [&](int m, int n, double dm, double dn) {
+      double dx = urx - (dm * us1x + dn * us2x);
+      double dy = ury - (dm * us1y + dn * us2y);
       // one reciprocal square root gives both the distance and the 1/r weight (two FP64
       // divisions fewer per summand than sqrt then term / r)
       const double d2 = dx * dx + dy * dy;
       const double ra = rsqrt(d2);
       const double a = d2 * ra;
-      double er = exp(-a);
-      if (NP == 1 && nophase) {
-        jring[0] = jring[0] + mkcd(er * ra, 0.0 * ra);
-        kring[0] = kring[0] + mkcd(er, 0.0);
+      double er = exp_neg(a, etab);
+      if (NP == 1 && nophase) {  // real terms: the imaginary parts stay exactly zero
+        jring[0].x = jring[0].x + er * ra;
+        kring[0].x = kring[0].x + er;
       } else {
 #pragma unroll
         for (int p = 0; p < NP; ++p) {
@@ -73,6 +98,27 @@ __device__ __forceinline__ unsigned jksums_group(double urx, double ury, int np,
           kring[p] = kring[p] + term;
         }
       }
+    };
+    // the ring's 8r lattice points in Ring's order (ring_mn): m = r with n = -r..r, m = -r with
+    // n = -r..r, then n = -r and n = r with m = -r+1..r-1; for one phasing the indices are
+    // also counted in FP64 (exact integers), so no summand converts one (with more phasings
+    // the registers go to their sums)
+    if constexpr (NP > 1) {
+      for (int t = 0; t < 8 * r; ++t) {
+        int m, n;
+        ring_mn(r, t, m, n);
+        summand(m, n, (double)m, (double)n);
+      }
+    } else {
+      const double dr = (double)r;
+      double dn = -dr;
+      for (int i = -r; i <= r; ++i, dn += 1.0) summand(r, i, dr, dn);
+      dn = -dr;
+      for (int i = -r; i <= r; ++i, dn += 1.0) summand(-r, i, -dr, dn);
+      double dm = 1.0 - dr;
+      for (int i = 1 - r; i < r; ++i, dm += 1.0) summand(i, -r, dm, -dr);
+      dm = 1.0 - dr;
+      for (int i = 1 - r; i < r; ++i, dm += 1.0) summand(i, r, dm, dr);
     }
 #pragma unroll
     for (int p = 0; p < NP; ++p) {
@@ -111,6 +157,8 @@ template <int NP>
 __global__ void __launch_bounds__(jk_threads<NP>(), NP == 1 ? 1 : 4) k_filljk(SheetDev G, double ul, PsiGroup pg, double us1x, double us1y,
                                                 double us2x, double us2y, JKGroup jk, int *nonconv) {
   __shared__ cd ph1[NP][kPhase], ph2[NP][kPhase];
+  __shared__ double etab[256];  // 2^(j/256) for exp_neg
+  for (int t = threadIdx.x; t < 256; t += blockDim.x) etab[t] = exp2((double)t / 256.0);
   const int np = NP == 1 ? 1 : pg.n;
   for (int t = threadIdx.x; t < NP * kPhase; t += blockDim.x) {
     const int p = t / kPhase;
@@ -149,7 +197,7 @@ __global__ void __launch_bounds__(jk_threads<NP>(), NP == 1 ? 1 : 4) k_filljk(Sh
     double rtx = (rs[0][0] + rs21[0] * c_qxi[q]) + rs31[0] * c_qeta[q];
     double rty = (rs[0][1] + rs21[1] * c_qxi[q]) + rs31[1] * c_qeta[q];
     ok = jksums_group<NP>(ul * (rmc[0] - rtx), ul * (rmc[1] - rty), np, nophase, us1x, us1y, us2x, us2y, ph1, ph2,
-                          js, ks);
+                          etab, js, ks);
   }
   // phasing-free terms (the pair's first lane only)
   double rr0 = 0, rr1 = 0, ri = 0;
