@@ -100,16 +100,9 @@ __device__ __forceinline__ unsigned jksums_group(double urx, double ury, int np,
       }
     };
     // the ring's 8r lattice points in Ring's order (ring_mn): m = r with n = -r..r, m = -r with
-    // n = -r..r, then n = -r and n = r with m = -r+1..r-1; for one phasing the indices are
-    // also counted in FP64 (exact integers), so no summand converts one (with more phasings
-    // the registers go to their sums)
-    if constexpr (NP > 1) {
-      for (int t = 0; t < 8 * r; ++t) {
-        int m, n;
-        ring_mn(r, t, m, n);
-        summand(m, n, (double)m, (double)n);
-      }
-    } else {
+    // n = -r..r, then n = -r and n = r with m = -r+1..r-1; the indices are also counted in
+    // FP64 (exact integers), so no summand converts one
+    {
       const double dr = (double)r;
       double dn = -dr;
       for (int i = -r; i <= r; ++i, dn += 1.0) summand(r, i, dr, dn);
@@ -154,7 +147,7 @@ template <int NP>
 constexpr int jk_threads() { return NP == 1 ? 256 : 128; }
 
 template <int NP>
-__global__ void __launch_bounds__(jk_threads<NP>(), NP == 1 ? 1 : 4) k_filljk(SheetDev G, double ul, PsiGroup pg, double us1x, double us1y,
+__global__ void __launch_bounds__(jk_threads<NP>(), NP == 1 ? 1 : 3) k_filljk(SheetDev G, double ul, PsiGroup pg, double us1x, double us1y,
                                                 double us2x, double us2y, JKGroup jk, int *nonconv) {
   __shared__ cd ph1[NP][kPhase], ph2[NP][kPhase];
   __shared__ double etab[256];  // 2^(j/256) for exp_neg

@@ -6,7 +6,9 @@
 * Jerusalem-cross / aperture cascade at its stated size: cross ntri = 1500, aperture
   ntri = 1200, theta = 30, phi = 45 (face-pair integrals recomputed per point) - 2 of its 51
   frequencies through analyze (both sheets, cascade included);
-* meanderline gradient workload: ntri = 4000 (3960 faces, N = 5610) - one frequency.
+* meanderline gradient workload: ntri = 4000 (3960 faces, N = 5610) - one frequency;
+* batched ring workload (64 seeded problems): its largest normal-incidence ring (3046 faces)
+  and its largest oblique ring (3202 faces, theta = 15) at 15 GHz, in one multi-problem call.
 
 Bars: the FP64 form within 1e-9 relative of the FP64 oracle (max-abs difference over
 max-abs value); the FP32 + FP64-refinement form within |dS| <= 1e-6 absolute of the FP64
@@ -71,3 +73,28 @@ def test_jerusalem_aperture_cascade_at_stated_size():
                     assert d / np.max(np.abs(b.gsm[k])) < 1e-9, (prec, k)
                 else:
                     assert d <= bar, (prec, k, d)
+
+
+def test_ring_batch_members_at_stated_size():
+    # the batched workload (64 seeded ring problems, 21 frequencies each, theta in {0, 15, 30,
+    # 45}): its largest normal-incidence ring and its largest oblique ring, at one frequency
+    # each, through one pss_partial_gsms_multi call, against the FP64 oracle
+    from pssfss_b200.analyze import make_plan, sheet_gblocks, sheet_io
+    batch = workloads.ring_batch()
+    normal = max((c for c in batch if c[2]["θ"] == 0.0), key=lambda c: c[0][1].nface)
+    oblique = max((c for c in batch if c[2]["θ"] != 0.0), key=lambda c: c[0][1].nface)
+    probs, refs = [], []
+    for strata, flist, steer in (normal, oblique):
+        plan = make_plan(strata, [float(flist[10])], steer)
+        (ig, (i1, i2), isht, s), = sheet_gblocks(plan)
+        sheet, rwg, u = plan.sheets[isht - 1], plan.rwgdat[isht - 1], plan.uvec[isht - 1]
+        ios = [sheet_io(pt.layers[i1 - 1:i2], sheet, s, pt.k0, pt.beta00) for pt in plan.points]
+        probs.append(dict(sheet=sheet, rwg=rwg, points=plan.points, region_rng=(i1, i2), s=s, u=u, ios=ios))
+        pt = plan.points[0]
+        refs.append(oracle.partial_dS(sheet, rwg, pt.layers[i1 - 1:i2], s, pt.k0, u, ios[0])[0])
+    assert probs[0]["rwg"].nbf > 4000 and probs[1]["rwg"].nbf > 3000
+    d64 = engine.partial_gsms_multi(probs, precision="fp64")
+    d32 = engine.partial_gsms_multi(probs, precision="fp32r")
+    for g64, g32, r in zip(d64, d32, refs):
+        assert np.max(np.abs(g64[0] - r)) / np.max(np.abs(r)) < 1e-9
+        assert np.max(np.abs(g32[0] - r)) <= 1e-6
