@@ -147,7 +147,7 @@ template <int NP>
 constexpr int jk_threads() { return NP == 1 ? 256 : 128; }
 
 template <int NP>
-__global__ void __launch_bounds__(jk_threads<NP>(), NP == 1 ? 1 : 3) k_filljk(SheetDev G, double ul, PsiGroup pg, double us1x, double us1y,
+__global__ void __launch_bounds__(jk_threads<NP>(), 3) k_filljk(SheetDev G, double ul, PsiGroup pg, double us1x, double us1y,
                                                 double us2x, double us2y, JKGroup jk, int *nonconv) {
   __shared__ cd ph1[NP][kPhase], ph2[NP][kPhase];
   __shared__ double etab[256];  // 2^(j/256) for exp_neg
