@@ -244,46 +244,70 @@ def cpu_baseline_sample(case):
                                       f"({t_jk:.1f} s) amortised over {NFREQ} points", **ci}, NFREQ // 2, dS_ref
 
 
-def run_rings(args, rank):
+def run_rings(args, rank, world=1, local=0):
     """Freq-points/s over the seeded batch of 64 ring problems (period 6-12 mm, 300-3000
-    triangles, so unknown counts 480-4080; theta in {0, 15, 30, 45}; 21 frequencies each;
-    1344 points), FP32 + refinement, all 64 problems in ONE library call
+    triangles, so unknown counts 480-4800; theta in {0, 15, 30, 45}; 21 frequencies each;
+    1344 points), FP32 + refinement, with the batch size and LU tile shape of the stored
+    autotuning table.  On one GPU all 64 problems go into ONE library call
     (analyze.analyze_many -> pss_partial_gsms_multi: a shared work list of like-N batches,
-    largest first) with the batch size and LU tile shape of the stored autotuning table.
-    value = points / device span of that call; e2e = points / wall clock of analyze_many
-    (host planning, transfers and the cascade included), device synchronised on both sides."""
-    if rank != 0:
-        return
+    largest first); under torchrun the problems are split across the ranks by estimated cost
+    (sweep.analyze_many_sharded: one call per rank, one gather of the results), a fixed total
+    workload (strong scaling).  value = points / device span of the ranks' calls (max over
+    ranks); e2e = points / wall clock of analyze_many_sharded (host planning, transfers, the
+    cascade and the gather included, max over ranks), device synchronised on both sides."""
     import torch
-    torch.cuda.set_device(0)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
     load_package()
     from pssfss_b200 import autotune, workloads
-    from pssfss_b200.analyze import analyze_many
+    from pssfss_b200.sweep import analyze_many_sharded
     batch = workloads.ring_batch()
     npts = sum(len(f) for _, f, _ in batch)
     tuned = os.path.exists(autotune.TABLE) and not args.no_tuning
     tuning = autotune.lookup if tuned else None
     for _ in range(args.warmup):
-        analyze_many(batch, precision="fp32r", tuning=tuning)
+        analyze_many_sharded(batch, precision="fp32r", tuning=tuning)
     walls, spans = [], []
     for _ in range(args.steps):
         st = {}
+        if dist:
+            dist.barrier()
         torch.cuda.synchronize()
         t = time.perf_counter()
-        analyze_many(batch, precision="fp32r", tuning=tuning, stats=st)
+        analyze_many_sharded(batch, precision="fp32r", tuning=tuning, stats=st)
         torch.cuda.synchronize()
-        walls.append(time.perf_counter() - t)
-        spans.append(st["timings_ms"]["total"] / 1e3)
+        wall = time.perf_counter() - t
+        span = st["timings_ms"]["total"] / 1e3 if "timings_ms" in st else 0.0
+        if dist:
+            m = torch.tensor([wall, span], dtype=torch.float64, device="cuda")
+            dist.all_reduce(m, op=dist.ReduceOp.MAX)
+            wall, span = float(m[0]), float(m[1])
+        walls.append(wall)
+        spans.append(span)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
     line = {"metric": "freq-points/sec over a batch of ring problems of differing size", "value": npts / statistics.mean(spans),
-            "unit": "freq-points/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": statistics.mean(spans) * 1e3, "higher_is_better": True, "scaling": "weak",
+            "unit": "freq-points/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": statistics.mean(spans) * 1e3, "higher_is_better": True,
+            "scaling": "strong" if world > 1 else "weak",
             "vs_baseline": None, "dtype": "c64+c128-refine",
-            "data": "synthetic (seeded ring problems, own structured meshes)",
+            "data": "synthetic (seeded ring problems, own Delaunay meshes)",
             "e2e": {"value": npts / statistics.mean(walls), "unit": "freq-points/s",
-                    "note": "wall clock of analyze_many: host planning, transfers, cascade included"},
+                    "note": "wall clock of analyze_many_sharded: host planning, transfers, cascade, gather included"},
             "config": {"workload": f"64 ring problems (seed 0), {npts} points, N "
                                    f"{min(b[0][1].nface for b in batch)}..{max(b[0][1].nface for b in batch)} faces, "
-                                   "one pss_partial_gsms_multi call",
+                                   + ("one pss_partial_gsms_multi call" if world == 1 else
+                                      f"problems split over {world} ranks by estimated cost, one call per rank"),
+                       "parallelism": f"problems x{world}",
                        "tuning": autotune.TABLE.split(os.sep + "pssfss.jl_b200" + os.sep)[-1] if tuned else "defaults",
                        "table": [{k: b[k] for k in ("nmax", "n", "batch", "panel_w", "outer_nb")}
                                  for b in (json.load(open(autotune.TABLE))["buckets"] if tuned else [])]}}
@@ -409,7 +433,7 @@ def main():
     if args.grads:
         return run_grads(args, rank)
     if args.rings:
-        return run_rings(args, rank)
+        return run_rings(args, rank, world, local)
     if args.autotune:
         return run_autotune(args, rank)
 

@@ -158,3 +158,74 @@ def test_linearized_gradient_sharded_gloo_matches_single_process():
         assert abs(f - f1) <= 1e-12 * abs(f1)
         for name in GRAD_P0:
             assert abs(g[name] - g1[name]) <= 1e-9 * abs(g1[name]), (name, g[name], g1[name])
+
+
+def test_assign_problems_balances_longest_first():
+    from pssfss_b200.sweep import assign_problems
+    costs = [5.0, 1.0, 4.0, 3.0, 3.0, 2.0, 2.0]
+    parts = assign_problems(costs, 2)
+    assert sorted(i for p in parts for i in p) == list(range(len(costs)))
+    loads = [sum(costs[i] for i in p) for p in parts]
+    assert max(loads) - min(loads) <= max(costs) and loads == [10.0, 10.0]
+    assert assign_problems(costs, 1) == [list(range(len(costs)))]
+    assert assign_problems([], 3) == [[], [], []]
+    with pytest.raises(ValueError):
+        assign_problems(costs, 0)
+
+
+def test_problem_cost_orders_by_size_and_incidence():
+    from pssfss_b200.elements import polyring
+    from pssfss_b200.layers import Layer
+    from pssfss_b200.sweep import problem_cost
+    from pssfss_b200.units import mm
+    small = polyring(s1=[8, 0], s2=[0, 8], a=[2.8], b=[3.2], sides=24, ntri=200, units=mm)
+    big = polyring(s1=[8, 0], s2=[0, 8], a=[2.8], b=[3.2], sides=24, ntri=800, units=mm)
+    c = lambda sh, th, nf=5: problem_cost(([Layer(), sh, Layer()], [10.0 + k for k in range(nf)], {"θ": th, "ϕ": 0.0}))
+    assert c(small, 0.0) < c(big, 0.0) < c(big, 30.0)
+    assert abs(c(big, 0.0, 10) - 2 * c(big, 0.0, 5)) < 1e-12 * c(big, 0.0, 10)
+
+
+def fake_analyze_many(cases, precision="fp32r", device=0):
+    """Stand-in for analyze_many: per case a list of (case tag, frequency) results."""
+    return [[(strata, f) for f in flist] for strata, flist, steering in cases]
+
+
+def _many_worker(rank, world, port, cases, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), LOCAL_RANK=str(rank))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        import pssfss_b200.sweep as sw
+        sw.problem_cost = lambda case: float(case[0])  # the tag is the cost: no sheets needed
+        q.put((rank, sw.analyze_many_sharded(cases, analyze_many_fn=fake_analyze_many)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_analyze_many_sharded_gloo_matches_single_process():
+    world = 2
+    cases = [(c, [10.0 + k for k in range(n)], {"θ": 0.0, "ϕ": 0.0})
+             for c, n in ((7, 3), (1, 2), (4, 1), (9, 2), (2, 4), (3, 1))]
+    single = fake_analyze_many(cases)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_many_worker, args=(k, world, port, cases, q)) for k in range(world)]
+    for p in procs:
+        p.start()
+    got = {}
+    try:
+        for _ in range(240):
+            while not q.empty() and len(got) < world:
+                k, v = q.get()
+                got[k] = v
+            if len(got) == world or any(p.exitcode not in (None, 0) for p in procs):
+                break
+            procs[0].join(timeout=0.5)
+    finally:
+        for p in procs:
+            p.join(timeout=60)
+            if p.is_alive():
+                p.kill()
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    for k in range(world):
+        assert got[k] == single
