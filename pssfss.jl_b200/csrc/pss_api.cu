@@ -801,18 +801,41 @@ int sweep_impl(pss_ctx *c, std::vector<Problem> &PR, int precision, const AdjSpe
       if (A.sh->nbf != Bq.sh->nbf) return A.sh->nbf > Bq.sh->nbf;
       return A.nm < Bq.nm;
     });
+    // runs of points that may share a batch (same unknown and mode counts and LU tile shape),
+    // each cut into near-equal batches of at most B points; a call that is one run (a single
+    // sweep) takes a multiple of the worker count, while its batches stay at least half full,
+    // so the workers' last rounds end together
+    std::vector<std::pair<size_t, size_t>> runs;  // [begin, end) in pts
     for (size_t k = 0; k < pts.size();) {
       const Problem &P = PR[pts[k].first];
+      size_t e = k + 1;
+      while (e < pts.size() && PR[pts[e].first].sh->nbf == P.sh->nbf && PR[pts[e].first].nm == P.nm &&
+             PR[pts[e].first].panel_w == P.panel_w && PR[pts[e].first].outer_nb == P.outer_nb)
+        ++e;
+      runs.push_back({k, e});
+      k = e;
+    }
+    for (const auto &rn : runs) {
+      const Problem &P = PR[pts[rn.first].first];
       const int B = std::max(1, std::min(P.batch > 0 ? P.batch : c->batch, kMaxBatch));
-      Item it{};
-      while (k < pts.size() && it.cnt < B && PR[pts[k].first].sh->nbf == P.sh->nbf && PR[pts[k].first].nm == P.nm &&
-             PR[pts[k].first].panel_w == P.panel_w && PR[pts[k].first].outer_nb == P.outer_nb) {
-        it.p[it.cnt] = pts[k].first;
-        it.i[it.cnt] = pts[k].second;
-        ++it.cnt;
-        ++k;
+      const long long cnt = (long long)(rn.second - rn.first);
+      long long nbat = (cnt + B - 1) / B;
+      const long long nw = c->nworkers;
+      if (runs.size() == 1 && nbat > 1 && nbat % nw) {
+        const long long up = (nbat + nw - 1) / nw * nw;
+        if (2 * cnt >= up * (long long)B) nbat = up;  // batches of at least B/2 points
       }
-      items.push_back(it);
+      size_t k = rn.first;
+      for (long long q = 0; q < nbat; ++q) {
+        const long long sz = cnt / nbat + (q < cnt % nbat ? 1 : 0);
+        Item it{};
+        for (long long t = 0; t < sz; ++t, ++k) {
+          it.p[it.cnt] = pts[k].first;
+          it.i[it.cnt] = pts[k].second;
+          ++it.cnt;
+        }
+        items.push_back(it);
+      }
     }
   }
   // every worker sized once for the largest item of the call
