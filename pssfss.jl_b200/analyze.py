@@ -17,7 +17,6 @@ cascade (``PSSFSS.jl:256-305``).
 reference v0.1.4; here ψ steering works as its docstring describes.
 """
 import cmath
-import copy
 import math
 from dataclasses import dataclass, field
 
@@ -132,7 +131,7 @@ def make_plan(strata, flist, steering, plan_flist=None, rwg_cache=None):
     and layer modes (PSSFSS.jl:215-221) - the whole sweep when ``flist`` is one shard.
     ``rwg_cache``: a dict reused across calls so that sheets of identical geometry share one
     basis-function setup (gradients perturb layers as well as geometry)."""
-    layers = [copy.deepcopy(s) for s in strata if isinstance(s, Layer)]
+    layers = [s.copy() for s in strata if isinstance(s, Layer)]
     sheets = [s for s in strata if isinstance(s, RWGSheet)]
     nl = len(layers)
     junc = [0] * (nl - 1)
@@ -189,7 +188,7 @@ def make_plan(strata, flist, steering, plan_flist=None, rwg_cache=None):
                 if "θ" in steer:
                     k1 = k0 * math.sqrt((layers[0].epsr * layers[0].mur).real)
                     b00 = np.array([k1 * st * cp, k1 * st * sp])
-                pl = copy.deepcopy(layers)
+                pl = [l.copy() for l in layers]
                 for l in pl:
                     setup_modes(l, k0, b00)
                 a0 = np.angle(pl[0].gamma[0])

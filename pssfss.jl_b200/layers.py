@@ -47,8 +47,17 @@ class Layer:
         self.tvec = np.zeros((0, 2))
 
     def copy(self):
-        import copy
-        return copy.deepcopy(self)
+        """An independent copy: the mode lists and modal arrays are copied; the name,
+        constants and width (never changed in place) are shared."""
+        c = Layer.__new__(Layer)
+        d = dict(self.__dict__)
+        for k, v in d.items():
+            if isinstance(v, list):
+                d[k] = list(v)
+            elif isinstance(v, np.ndarray):
+                d[k] = v.copy()
+        c.__dict__.update(d)
+        return c
 
     def same_as(self, other):
         """Field-wise equality (``Layers.jl:123``) used by the Gblock duplicate search."""

@@ -177,97 +177,96 @@ def recttri(rhobl, rhotr, nx, ny):
     return sh
 
 
+def _renumber_after_removal(vals, removed):
+    """Decrement every value by the number of ``removed`` thresholds (sorted, distinct) below
+    it: the effect of the reference's descending ``x[x .> r] .-= 1`` loops on values that are
+    none of the thresholds."""
+    return vals - np.searchsorted(removed, vals, side="left")
+
+
 def combine(sh1, sh2, dup_coor, dup_coor_value):
     """Merge two triangulations that may share a line of nodes and edges
-    (``Sheets.jl:234-389``)."""
+    (``Sheets.jl:234-389``).
+
+    The reference's rules are kept: a node of ``sh2`` within ``tol`` of the line pairs with
+    the first node of ``sh1`` within ``tol`` of it, a shared edge with the first ``sh1`` edge
+    joining the paired nodes, and the shared nodes and edges of ``sh2`` are dropped with the
+    later indices closed up.  The searches and renumberings are array operations."""
     if sh1.units != sh2.units:
         raise ValueError("Inconsistent units for sh1 and sh2")
     nv1, ne1, nf1 = sh1.nnode, sh1.nedge, sh1.nface
-    vcen1, vcen2 = [], []
-    ecen1, ecen2 = [], []
+    vcen1 = vcen2 = ecen1 = ecen2 = np.zeros(0, np.int64)
     if dup_coor != " ":
         d = sh1.rho[sh1.e1[0] - 1] - sh1.rho[sh1.e2[0] - 1]
         tol = 0.5e-4 * math.sqrt(d[0] * d[0] + d[1] * d[1])
-        for i in range(sh2.nnode):
-            test = sh2.rho[i, 0] if dup_coor == "x" else sh2.rho[i, 1]
-            if abs(test - dup_coor_value) < tol:
-                n1match = 0
-                for n1 in range(nv1):
-                    dd = sh1.rho[n1] - sh2.rho[i]
-                    if math.sqrt(dd[0] * dd[0] + dd[1] * dd[1]) < tol:
-                        n1match = n1 + 1
-                        break
-                if n1match != 0:
-                    vcen2.append(i + 1)
-                    vcen1.append(n1match)
-        vset2 = {v: k for k, v in enumerate(vcen2)}
-        for i in range(sh2.nedge):
-            a, b = int(sh2.e1[i]), int(sh2.e2[i])
-            if a in vset2 and b in vset2:
-                ecen2.append(i + 1)
-                va, vb = vcen1[vset2[a]], vcen1[vset2[b]]
-                found = 0
-                for j1 in range(ne1):
-                    if (sh1.e1[j1] == va and sh1.e2[j1] == vb) or (sh1.e2[j1] == va and sh1.e1[j1] == vb):
-                        found = j1 + 1
-                        break
-                if found == 0:
-                    raise RuntimeError("Unable to find matching duplicate edge in combine_sheet")
-                ecen1.append(found)
+        ax = 0 if dup_coor == "x" else 1
+        cand2 = np.flatnonzero(np.abs(sh2.rho[:, ax] - dup_coor_value) < tol)
+        # a matching sh1 node lies within 2 tol of the line; a wider band keeps rounding out
+        near1 = np.flatnonzero(np.abs(sh1.rho[:, ax] - dup_coor_value) < 3 * tol)
+        v1, v2 = [], []
+        if len(cand2) and len(near1):
+            dx = sh1.rho[near1, 0][None, :] - sh2.rho[cand2, 0][:, None]
+            dy = sh1.rho[near1, 1][None, :] - sh2.rho[cand2, 1][:, None]
+            hit = np.sqrt(dx * dx + dy * dy) < tol
+            has = hit.any(axis=1)
+            first = near1[np.argmax(hit, axis=1)]  # near1 ascending: the first sh1 match
+            v2 = cand2[has] + 1
+            v1 = first[has] + 1
+        vcen2 = np.asarray(v2, np.int64)
+        vcen1 = np.asarray(v1, np.int64)
+        if len(vcen2):
+            # sh2 edges with both ends shared, in sh2 order, and the first sh1 edge on the
+            # same (unordered) node pair
+            vpair = np.zeros(sh2.nnode + 1, np.int64)
+            vpair[vcen2] = vcen1
+            a2, b2 = np.asarray(sh2.e1, np.int64), np.asarray(sh2.e2, np.int64)
+            both = (vpair[a2] > 0) & (vpair[b2] > 0)
+            ecen2 = np.flatnonzero(both) + 1
+            va, vb = vpair[a2[both]], vpair[b2[both]]
+            big = np.int64(nv1 + 1)
+            a1, b1 = np.asarray(sh1.e1, np.int64), np.asarray(sh1.e2, np.int64)
+            key1 = np.minimum(a1, b1) * big + np.maximum(a1, b1)
+            ukey, ufirst = np.unique(key1, return_index=True)
+            want = np.minimum(va, vb) * big + np.maximum(va, vb)
+            pos = np.searchsorted(ukey, want)
+            ok = (pos < len(ukey)) & (ukey[np.minimum(pos, len(ukey) - 1)] == want)
+            if not ok.all():
+                raise RuntimeError("Unable to find matching duplicate edge in combine_sheet")
+            ecen1 = ufirst[pos].astype(np.int64) + 1
     Nvcen, Necen = len(vcen2), len(ecen2)
     sh3 = RWGSheet()
     sh3.units = sh1.units
-    # vertices
-    if dup_coor == " ":
-        sh3.rho = np.vstack([sh1.rho, sh2.rho])
-    else:
-        keep = [i for i in range(sh2.nnode) if (i + 1) not in vcen2]
-        sh3.rho = np.vstack([sh1.rho, sh2.rho[keep]])
-    # edges
-    e1 = np.zeros(ne1 + sh2.nedge - Necen, np.int64)
-    e2 = np.zeros_like(e1)
-    e1[:ne1] = sh1.e1
-    e2[:ne1] = sh1.e2
     voffset = nv1
-    if dup_coor == " ":
-        e1[ne1:] = sh2.e1 + voffset
-        e2[ne1:] = sh2.e2 + voffset
-    else:
-        eoffset = ne1
-        ecen2_set = set(ecen2)
-        vmap = {v: vcen1[k] for k, v in enumerate(vcen2)}
-        for i in range(sh2.nedge):
-            if (i + 1) in ecen2_set:
-                eoffset -= 1
-                continue
-            a, b = int(sh2.e1[i]), int(sh2.e2[i])
-            e1[i + eoffset] = vmap[a] if a in vmap else a + voffset
-            e2[i + eoffset] = vmap[b] if b in vmap else b + voffset
-        for i in range(Nvcen - 1, -1, -1):
-            thr = nv1 + vcen2[i]
-            e1[e1 > thr] -= 1
-            e2[e2 > thr] -= 1
+    # sh2 node index (1-based) -> merged index before the shared nodes are closed up
+    vmap2 = np.arange(sh2.nnode + 1, dtype=np.int64) + voffset
+    vmap2[vcen2] = vcen1
+    # vertices
+    keepv = np.ones(sh2.nnode, bool)
+    keepv[vcen2 - 1] = False
+    sh3.rho = np.vstack([sh1.rho, sh2.rho[keepv]])
+    # edges
+    removed_v = voffset + vcen2  # ascending
+    keepe = np.ones(sh2.nedge, bool)
+    keepe[ecen2 - 1] = False
+    e1 = np.concatenate([np.asarray(sh1.e1, np.int64),
+                         _renumber_after_removal(vmap2[np.asarray(sh2.e1, np.int64)[keepe]], removed_v)])
+    e2 = np.concatenate([np.asarray(sh1.e2, np.int64),
+                         _renumber_after_removal(vmap2[np.asarray(sh2.e2, np.int64)[keepe]], removed_v)])
     sh3.e1, sh3.e2 = e1, e2
     # faces / vertices
     fv = np.zeros((3, nf1 + sh2.nface), np.int64)
     fv[:, :nf1] = sh1.fv
-    fv[:, nf1:] = sh2.fv + voffset
-    for n2 in range(Nvcen):
-        fv[fv == vcen2[n2] + voffset] = vcen1[n2]
-    for i in range(Nvcen - 1, -1, -1):
-        fv[fv > voffset + vcen2[i]] -= 1
+    fv[:, nf1:] = _renumber_after_removal(vmap2[np.asarray(sh2.fv, np.int64)], removed_v)
     sh3.fv = fv
     # faces / edges
     eoffset = ne1
+    emap2 = np.arange(sh2.nedge + 1, dtype=np.int64) + eoffset
+    emap2[ecen2] = ecen1
     fe = np.zeros((3, nf1 + sh2.nface), np.int64)
     fe[:, :nf1] = sh1.fe
-    fe[:, nf1:] = sh2.fe + eoffset
-    if dup_coor != " ":
-        for n2 in range(len(ecen2)):
-            fe[fe == ecen2[n2] + eoffset] = ecen1[n2]
-        for i in range(len(ecen2) - 1, -1, -1):
-            fe[fe > eoffset + ecen2[i]] -= 1
+    fe[:, nf1:] = _renumber_after_removal(emap2[np.asarray(sh2.fe, np.int64)], eoffset + ecen2)
     sh3.fe = fe
+    assert Necen == len(ecen1) and Nvcen == len(vcen1)
     return sh3
 
 
