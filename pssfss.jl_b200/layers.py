@@ -49,7 +49,7 @@ class Layer:
     def copy(self):
         """An independent copy: the mode lists and modal arrays are copied; the name,
         constants and width (never changed in place) are shared."""
-        c = Layer.__new__(Layer)
+        c = type(self).__new__(type(self))
         d = dict(self.__dict__)
         for k, v in d.items():
             if isinstance(v, list):
