@@ -500,3 +500,102 @@ def test_meshers_on_seeded_random_shapes():
         A, B = rng.uniform(1.05, 1.6) * L2, rng.uniform(0.1, 0.8) * (L1 - L2) / 2
         if A < P:
             setup_rwg(jerusalemcross(P=P, L1=L1, L2=L2, A=A, B=B, w=w, ntri=int(rng.integers(100, 600)), units=mm))
+
+
+def _combine_loops(sh1, sh2, dup_coor, val):
+    """Sheets.jl:234-389 written as its loops (first-match searches, sequential replacement and
+    descending renumbering), the check on the array form of ``combine``.  Returns
+    (rho, e1, e2, fv, fe)."""
+    nv1, ne1, nf1 = sh1.nnode, sh1.nedge, sh1.nface
+    vcen1, vcen2, ecen1, ecen2 = [], [], [], []
+    if dup_coor != " ":
+        d = sh1.rho[sh1.e1[0] - 1] - sh1.rho[sh1.e2[0] - 1]
+        tol = 0.5e-4 * math.sqrt(d[0] * d[0] + d[1] * d[1])
+        ax = 0 if dup_coor == "x" else 1
+        for i in range(sh2.nnode):
+            if abs(sh2.rho[i, ax] - val) < tol:
+                for n1 in range(nv1):
+                    dd = sh1.rho[n1] - sh2.rho[i]
+                    if math.sqrt(dd[0] * dd[0] + dd[1] * dd[1]) < tol:
+                        vcen2.append(i + 1)
+                        vcen1.append(n1 + 1)
+                        break
+        for i in range(sh2.nedge):
+            a, b = int(sh2.e1[i]), int(sh2.e2[i])
+            if a in vcen2 and b in vcen2:
+                va, vb = vcen1[vcen2.index(a)], vcen1[vcen2.index(b)]
+                found = [j + 1 for j in range(ne1) if {int(sh1.e1[j]), int(sh1.e2[j])} == {va, vb}]
+                if not found:
+                    raise RuntimeError("no matching edge")
+                ecen2.append(i + 1)
+                ecen1.append(found[0])
+    rho = np.vstack([sh1.rho, sh2.rho[[i for i in range(sh2.nnode) if i + 1 not in vcen2]]])
+    e1, e2 = list(sh1.e1), list(sh1.e2)
+    for i in range(sh2.nedge):
+        if i + 1 in ecen2:
+            continue
+        for dst, src in ((e1, sh2.e1), (e2, sh2.e2)):
+            v = int(src[i])
+            dst.append(vcen1[vcen2.index(v)] if v in vcen2 else v + nv1)
+    e1, e2 = np.array(e1, np.int64), np.array(e2, np.int64)
+    fv = np.hstack([sh1.fv, sh2.fv + nv1]).astype(np.int64)
+    fe = np.hstack([sh1.fe, sh2.fe + ne1]).astype(np.int64)
+    for k in range(len(vcen2)):
+        fv[fv == vcen2[k] + nv1] = vcen1[k]
+    for k in range(len(ecen2)):
+        fe[fe == ecen2[k] + ne1] = ecen1[k]
+    for k in range(len(vcen2) - 1, -1, -1):
+        for x in (e1, e2, fv):
+            x[x > nv1 + vcen2[k]] -= 1
+    for k in range(len(ecen2) - 1, -1, -1):
+        fe[fe > ne1 + ecen2[k]] -= 1
+    return rho, e1, e2, fv, fe
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_combine_matches_loop_form(seed):
+    """Seeded strips merged along x, along y and without a shared line, then merged again with a
+    third strip, as the element builders chain them: identical nodes, edges and faces; a shared
+    line whose nodes do not match an edge of the first sheet raises in both forms."""
+    rng = np.random.default_rng(seed)
+    for _ in range(40):
+        mode = ["x", "y", " "][int(rng.integers(3))]
+        n1, n2, m = (int(v) for v in rng.integers(1, 7, 3))
+        m2 = m if rng.random() < 0.8 else int(rng.integers(1, 7))
+        h = float(rng.choice([1.0, 1.5]))
+        if mode == "x":
+            boxes = [([0., 0.], [1., h], n1, m), ([1., 0.], [2.5, h], n2, m2), ([2.5, 0.], [3., h], n1, m2)]
+            vals = [1.0, 2.5]
+        elif mode == "y":
+            boxes = [([0., 0.], [h, 1.], m, n1), ([0., 1.], [h, 2.5], m2, n2), ([0., 2.5], [h, 3.], m2, n1)]
+            vals = [1.0, 2.5]
+        else:
+            boxes = [([0., 0.], [1., 1.], n1, m), ([2., 0.], [3., 1.], n2, m2)]
+            vals = [0.0]
+        sh = recttri(*boxes[0])
+        for box, val in zip(boxes[1:], vals):
+            other = recttri(*box)
+            try:
+                want = _combine_loops(sh, other, mode, val)
+            except RuntimeError:
+                with pytest.raises(RuntimeError):
+                    combine(sh, other, mode, val)
+                break
+            sh = combine(sh, other, mode, val)
+            got = (sh.rho, sh.e1, sh.e2, sh.fv, sh.fe)
+            for g, w in zip(got, want):
+                assert g.shape == w.shape and np.array_equal(g, w)
+
+
+def test_layer_copy_is_independent():
+    """A point's layer copy takes its own mode lists and modal arrays: filling or editing them
+    leaves the planned layer untouched."""
+    lay = Layer(width=Length(1, mm), epsr=2.2, tandel=0.001)
+    lay.P, lay.M, lay.N = [1, 2], [0, 0], [0, 0]
+    lay.beta1 = np.array([1.0, 0.0])
+    c = lay.copy()
+    assert c.same_as(lay) and type(c) is Layer
+    c.P.append(1)
+    c.beta1[0] = 5.0
+    c.gamma = np.ones(2, complex)
+    assert lay.P == [1, 2] and lay.beta1[0] == 1.0 and len(lay.gamma) == 0
