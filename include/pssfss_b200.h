@@ -116,8 +116,9 @@ typedef struct pss_problem {
 /* Many sweeps in one call - problems on sheets of different unknown counts (and layers,
  * steering, modes), all of one context.  The scattered partial GSMs of every point of every
  * problem, as pss_partial_gsms gives them, computed from one shared work list: every point's
- * modal tables first, then batches of like-N points (one problem each, the largest matrices
- * first) taken by the context's worker streams, so no stream idles between problems.
+ * modal tables first, then batches of points with the same unknown and mode counts (from one
+ * problem, or from several whose sheets have the same N; the largest matrices first) taken
+ * by the context's worker streams, so no stream idles between problems.
  * Replaces the loop of _analyze over sheets and steering (src/PSSFSS.jl:230-329) when many
  * problems are swept together. */
 int pss_partial_gsms_multi(int nprob, const pss_problem *problems, int precision);
@@ -151,8 +152,9 @@ int pss_partial_gsms_lin(pss_sheet *sheet, int nl, const double *eps, const doub
  * and the adjoint (transposed) solves of P^T on the same factors; each perturbed set then
  * recomputes its pair terms (the Green's-function values of its sheet and layers) and
  * contracts Lam^T Z_k X while assembling Z_k entry by entry - no perturbed matrix is stored
- * and no further solve is taken.  Points run one at a time on the context's first stream;
- * calls on one context must not overlap.  nmodes <= 1024. */
+ * and no further solve is taken.  The points are swept as pss_partial_gsms sweeps them
+ * (batched fills and factorisations on the context's worker streams); calls on one context
+ * must not overlap.  nmodes <= 1024, npert <= 64. */
 int pss_partial_gsms_adj(pss_sheet *sheet, int nl, const double *eps, const double *mu, const double *width,
                          int s, double u, int npts, const double *k0, const double *psi, int nmodes,
                          const double *kvec, const double *src, const double *tobs, const double *wobs,

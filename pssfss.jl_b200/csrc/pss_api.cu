@@ -697,7 +697,7 @@ struct AdjSpec {
 };
 
 // The sweep of every problem on one context: tables of all points, then a shared work list of
-// (problem, batch of like-N points) items, largest matrices first, taken by one host thread
+// batches of like-N points (of one or several problems), largest first, taken by one host thread
 // per worker stream; each item runs fill -> batched LU -> solves (+ refinement) -> projection
 // on its worker.  FP32 points whose refinement stalls are redone in FP64; then dS and status
 // go back to each problem's caller arrays.
