@@ -266,38 +266,49 @@ def partial_dS(sheet, rwg, region, s, k0, u, io):
 
 
 def analyze(strata, flist, steering):
-    """Oracle ``analyze`` (PSSFSS.jl:114-334), independent of the package's host numerics.
+    """Oracle ``analyze`` (PSSFSS.jl:114-334), independent of the package's host code.
 
-    Only the *selection* steps come from the package's planner: the Gblocks, the layer mode
-    lists and the duplicate-Gblock map (``choose_gblocks``, ``choose_layer_modes!``,
-    ``get_gbldup``, pinned to the reference's golden values of test/GSMs_test.jl and
-    test/Modes_test.jl) and the basis-function topology (``setup_rwg``, pinned by
-    test/RWGData_test.jl).  Everything numeric is the oracle's own: modal constants,
-    incident GSMs and transmission-line Green's functions, source and projection factors
-    (``host.py``), the fill and basis transforms (``pssfss_oracle.c``), LAPACK's LU, the
-    cascade.  Returns the package's ``Result`` containers so outputs can be taken from them."""
+    The selection steps - Gblocks, layer mode lists, duplicate-Gblock map - are the oracle's
+    own (``select.py``: ``choose_gblocks``, ``choose_layer_modes!``, ``get_gbldup``, pinned to
+    the reference's golden values of test/GSMs_test.jl and test/Modes_test.jl), and so is
+    everything numeric: modal constants, incident GSMs and transmission-line Green's
+    functions, source and projection factors (``host.py``), the fill and basis transforms
+    (``pssfss_oracle.c``), LAPACK's LU, the cascade.  Only the basis-function topology comes
+    from the package (``setup_rwg`` through its planner, pinned by test/RWGData_test.jl).
+    Returns the package's ``Result`` containers so outputs can be taken from them."""
     import importlib
     from . import host
+    from . import select as S
     A = importlib.import_module("pssfss_b200.analyze")
     O = importlib.import_module("pssfss_b200.outputs")
     Gm = importlib.import_module("pssfss_b200.gsms")
-    plan = A.make_plan(strata, flist, steering)  # selection only: its points are not used
+    plan = A.make_plan(strata, flist, steering)  # basis topology only (plan.rwgdat)
     freqs = [float(f) for f in np.atleast_1d(np.asarray(flist, float))]
-    base = [host.ModalLayer(l.epsr, l.mur, l.width, list(l.P), list(l.M), list(l.N),
-                            np.array(l.beta1, float), np.array(l.beta2, float)) for l in plan.layers]
-    sh0 = plan.sheets[0]
+    junc1, gbls, modes, gbldup = S.select(strata, freqs, lambda x: not hasattr(x, "style"))
+    junc = junc1[1:]
+    layers = [x for x in strata if not hasattr(x, "style")]
+    sheets = [x for x in strata if hasattr(x, "style")]
+    assert all(a is b for a, b in zip(sheets, plan.sheets)) and len(sheets) == len(plan.sheets)
+    none = {"modes": [], "b1": np.zeros(2), "b2": np.zeros(2)}
+    base = []
+    for l, m in zip(layers, modes[1:]):
+        m = none if m is None else m
+        base.append(host.ModalLayer(l.epsr, l.mur, l.width, [p for p, _, _ in m["modes"]],
+                                    [a for _, a, _ in m["modes"]], [b for _, _, b in m["modes"]],
+                                    np.array(m["b1"], float), np.array(m["b2"], float)))
+    sh0 = sheets[0]
     upm0 = sh0.units.units_per_meter
     points = host.steering_points(base, freqs, steering, (sh0.beta1 * upm0, sh0.beta2 * upm0))
     uvec = [0.0 if sh.style == "NULL" else
             0.5 * sh.units.units_per_meter * max(np.linalg.norm(sh.beta1), np.linalg.norm(sh.beta2))
-            for sh in plan.sheets]
+            for sh in sheets]
     saved = {}
 
     def sheet_gsm(ig, p, region, s, k0):
-        g = plan.gbls[ig]
-        sheet = plan.sheets[plan.junc[g.j - 1] - 1]
-        if plan.gbldup[ig] > 0:
-            gb = {k: v.copy() for k, v in saved[(plan.gbldup[ig] - 1, p)].items()}
+        gj = gbls[ig][2]
+        sheet = sheets[junc[gj - 1] - 1]
+        if gbldup[ig] > 0:
+            gb = {k: v.copy() for k, v in saved[(gbldup[ig] - 1, p)].items()}
         else:
             if sheet.cls == "E":
                 gb = host.pec(region[0].nmodes, region[-1].nmodes)
@@ -307,11 +318,11 @@ def analyze(strata, flist, steering):
                 gb = (host.electric_gblock if sheet.cls == "J" else host.magnetic_gblock)(region, s, k0)[0]
             else:
                 upm = sheet.units.units_per_meter
-                rwg = plan.rwgdat[plan.junc[g.j - 1] - 1]
+                rwg = plan.rwgdat[junc[gj - 1] - 1]
                 b00 = points[p][3]
                 psi1 = float(b00 @ np.asarray(sheet.s1, float)) / upm
                 psi2 = float(b00 @ np.asarray(sheet.s2, float)) / upm
-                Z, _ = fill(k0, uvec[plan.junc[g.j - 1] - 1], region, s, psi1, psi2, sheet, rwg)
+                Z, _ = fill(k0, uvec[junc[gj - 1] - 1], region, s, psi1, psi2, sheet, rwg)
                 import scipy.linalg as sl
                 lu = sl.lu_factor(Z, check_finite=False)
                 ends = (region[0], region[-1])
@@ -319,16 +330,15 @@ def analyze(strata, flist, steering):
                 gb = host.sheet_partial_gsm(
                     sheet.cls, region, s, k0, area, lambda b: sl.lu_solve(lu, b, check_finite=False),
                     lambda r, q: rwgbfft(rwg, sheet, ends[r].beta[q], psi1, psi2))
-            if plan.gbldup[ig] < 0:
+            if gbldup[ig] < 0:
                 saved[(ig, p)] = {k: v.copy() for k, v in gb.items()}
         if sheet.dx != 0 or sheet.dy != 0:
             upm = sheet.units.units_per_meter
             host.translate(gb, sheet.dx / upm, sheet.dy / upm, region[0], region[-1])
         return gb
 
-    gbls = [(g.first, g.last, g.j) for g in plan.gbls]
     out = []
-    for steer, f, b00, g, L in host.cascade_points(points, gbls, plan.junc, sheet_gsm):
+    for steer, f, b00, g, L in host.cascade_points(points, gbls, junc, sheet_gsm):
         gsm = Gm.GSM(g["s11"], g["s12"], g["s21"], g["s22"])
         out.append(O.Result(gsm, steer, np.array(b00, float), f, L[0].epsr, L[0].mur, L[0].beta1.copy(),
                             L[0].beta2.copy(), L[-1].epsr, L[-1].mur, L[-1].beta1.copy(), L[-1].beta2.copy()))
