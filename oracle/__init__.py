@@ -5,6 +5,11 @@ ctypes front end of ``pssfss_oracle.c`` (a plain-C FP64 restatement of PSSFSS.jl
 and the modal projection of ``PSSFSS.jl:362-587``.  Only tests, ``__graft_entry__.smoke``
 and the CPU-baseline leg of ``bench.py`` import this package; the product never does.
 
+``analyze`` runs the whole reference analysis with the oracle's own host restatements
+(``host.py``: modal and GSM algebra; ``select.py``: Gblocks, layer modes, duplicate Gblocks;
+``rwg.py``: basis topology) around this fill and solve, so no code of the package under test
+takes part in its numbers.
+
 Parity is pinned against the golden values hard-coded in the reference's own tests
 (test/FillZY_test.jl:45-46,77-78, test/PGF_test.jl:40-44,56-60, test/RWGData_test.jl:46-48,56-58,
 collected in tests/golden/reference_golden.json) and the analytic grating of
@@ -272,23 +277,22 @@ def analyze(strata, flist, steering):
     own (``select.py``: ``choose_gblocks``, ``choose_layer_modes!``, ``get_gbldup``, pinned to
     the reference's golden values of test/GSMs_test.jl and test/Modes_test.jl), and so is
     everything numeric: modal constants, incident GSMs and transmission-line Green's
-    functions, source and projection factors (``host.py``), the fill and basis transforms
-    (``pssfss_oracle.c``), LAPACK's LU, the cascade.  Only the basis-function topology comes
-    from the package (``setup_rwg`` through its planner, pinned by test/RWGData_test.jl).
-    Returns the package's ``Result`` containers so outputs can be taken from them."""
+    functions, source and projection factors (``host.py``), the basis-function topology
+    (``rwg.py``: ``setup_rwg``, pinned by test/RWGData_test.jl), the fill and basis transforms
+    (``pssfss_oracle.c``), LAPACK's LU, the cascade.  Nothing of the package runs; only its
+    ``Result`` and ``GSM`` containers hold the output, so outputs can be taken from them."""
     import importlib
     from . import host
+    from . import rwg as R
     from . import select as S
-    A = importlib.import_module("pssfss_b200.analyze")
     O = importlib.import_module("pssfss_b200.outputs")
     Gm = importlib.import_module("pssfss_b200.gsms")
-    plan = A.make_plan(strata, flist, steering)  # basis topology only (plan.rwgdat)
     freqs = [float(f) for f in np.atleast_1d(np.asarray(flist, float))]
     junc1, gbls, modes, gbldup = S.select(strata, freqs, lambda x: not hasattr(x, "style"))
     junc = junc1[1:]
     layers = [x for x in strata if not hasattr(x, "style")]
     sheets = [x for x in strata if hasattr(x, "style")]
-    assert all(a is b for a, b in zip(sheets, plan.sheets)) and len(sheets) == len(plan.sheets)
+    rwgdat = [None if sh.style == "NULL" else R.setup(sh) for sh in sheets]
     none = {"modes": [], "b1": np.zeros(2), "b2": np.zeros(2)}
     base = []
     for l, m in zip(layers, modes[1:]):
@@ -318,7 +322,7 @@ def analyze(strata, flist, steering):
                 gb = (host.electric_gblock if sheet.cls == "J" else host.magnetic_gblock)(region, s, k0)[0]
             else:
                 upm = sheet.units.units_per_meter
-                rwg = plan.rwgdat[junc[gj - 1] - 1]
+                rwg = rwgdat[junc[gj - 1] - 1]
                 b00 = points[p][3]
                 psi1 = float(b00 @ np.asarray(sheet.s1, float)) / upm
                 psi2 = float(b00 @ np.asarray(sheet.s2, float)) / upm

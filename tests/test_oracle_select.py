@@ -1,12 +1,13 @@
-"""The oracle's restatement of the selection steps (oracle/select.py: Gblocks, layer modes,
-duplicate Gblocks) against the reference's golden values, then against the package's
-planner on the CPU.
+"""The oracle's restatements of the steps before the numerics - Gblocks, layer modes and
+duplicate Gblocks (oracle/select.py), the basis-function topology (oracle/rwg.py) - against
+the reference's golden values, then against the package on the CPU.
 
-oracle/select.py imports nothing from the package, so the second group compares two
-separately written restatements of choose_gblocks (GSMs.jl:771-868), choose_layer_modes!
-(Modes.jl:49-275, with fill_mmax_pmn! and select_pmn!, :367-431) and get_gbldup
-(PSSFSS.jl:675-704): the Gblock ranges and sheet junctions, every layer's mode list (p, m,
-n in order) and reciprocal lattice, and the duplicate map must be identical.
+Neither oracle file imports the package, so the second group compares two separately
+written restatements of choose_gblocks (GSMs.jl:771-868), choose_layer_modes! (Modes.jl:49-275,
+with fill_mmax_pmn! and select_pmn!, :367-431), get_gbldup (PSSFSS.jl:675-704) and setup_rwg
+(RWG.jl:90-324): the Gblock ranges and sheet junctions, every layer's mode list (p, m, n in
+order) and reciprocal lattice, the duplicate map, the basis functions, boundary codes and
+face-pair classes must be identical.
 """
 import math
 
@@ -175,3 +176,47 @@ def test_selection_matches_the_planner_on_parity_workloads():
             assert (len(L.P) == 0 if m is None else
                     [(int(p), int(a), int(b)) for p, a, b in zip(L.P, L.M, L.N)] == m["modes"])
         assert list(plan.gbldup) == dup
+
+
+def test_rwg_topology_golden():
+    """test/RWGData_test.jl: the 2 x 1 strip's basis functions and face-pair classes, through
+    the oracle's own setup_rwg (oracle/rwg.py)."""
+    from oracle import rwg as R
+    from pssfss_b200.elements import rectstrip
+    for fufp in (True, False):
+        r = R.setup(rectstrip(Lx=1, Ly=1, Px=1, Py=1, Nx=2, Ny=1, units=mm, fufp=fufp))
+        assert r.bfe.tolist() == [[8, 6, 9, 1, 2, 5], [8, 6, 9, 3, 4, 7]]
+        assert r.bff.tolist() == [[1, 2, 3, 2, 4, 1], [2, 3, 4, 1, 3, 4]]
+        assert r.ebf.tolist() == [4, 5, 4, 5, 6, 2, 6, 1, 3]
+        assert r.eci.tolist() == [3, 3, 4, 4, 1, 0, 2, 0, 0]
+        if fufp:
+            assert r.ufpm.tolist() == [[1, 5, 9, 11], [2, 6, 10, 12], [3, 7, 1, 5], [4, 8, 2, 6]]
+            assert r.ufp_rep.tolist() == [1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 13, 14] and r.nufp == 12
+        else:
+            assert (r.ufpm.ravel(order="F") == np.arange(1, 17)).all() and r.nufp == 16
+
+
+def test_rwg_topology_matches_the_package():
+    """The oracle's setup_rwg against the package's on the sheets of the parity workloads and
+    on the other structured meshes (diagonal strip, fine grating): identical basis functions,
+    boundary codes and face-pair classes."""
+    from oracle import rwg as R
+    from pssfss_b200.elements import diagstrip, meander, rectstrip
+    from pssfss_b200.rwg import setup_rwg
+    from pssfss_b200.sheets import RWGSheet
+    sheets = []
+    for strata, _, _ in _parity_workloads():
+        sheets += [s for s in strata if isinstance(s, RWGSheet) and s.style != "NULL"]
+    sheets += [diagstrip(P=10, w=1, orient=45.0, Nl=20, Nw=4, units=mm),
+               diagstrip(P=10, w=1, orient=-45.0, Nl=12, Nw=3, units=mm),
+               meander(a=5, b=10, h=6, w1=0.3, w2=0.25, ntri=300, units=mm),
+               rectstrip(Lx=8, Ly=8, Px=10, Py=10, Nx=6, Ny=6, units=mm, fufp=False)]
+    seen = set()
+    for sh in sheets:
+        if id(sh) in seen:
+            continue
+        seen.add(id(sh))
+        a, b = setup_rwg(sh), R.setup(sh)
+        for f in ("bfe", "bff", "ebf", "eci", "ufpm", "ufp_rep"):
+            assert np.array_equal(getattr(a, f), getattr(b, f)), (sh.style, f)
+        assert a.nufp == b.nufp
