@@ -55,90 +55,98 @@ def get_ie_xieta(ie, sheet):
     return xi0, xi1, eta0, eta1
 
 
+def _edge_xieta(sheet):
+    """(xi, eta) of every edge's initial and terminal node (``get_ie_ξη``, ``RWG.jl:388-398``),
+    as four arrays over the edges, computed as ``_xieta`` does node by node."""
+    rho = np.asarray(sheet.rho, float)
+    b1, b2 = sheet.beta1, sheet.beta2
+    p0 = rho[np.asarray(sheet.e1, np.int64) - 1]
+    p1 = rho[np.asarray(sheet.e2, np.int64) - 1]
+    tp = 2 * math.pi
+    return ((b1[0] * p0[:, 0] + b1[1] * p0[:, 1]) / tp, (b1[0] * p1[:, 0] + b1[1] * p1[:, 1]) / tp,
+            (b2[0] * p0[:, 0] + b2[1] * p0[:, 1]) / tp, (b2[0] * p1[:, 0] + b2[1] * p1[:, 1]) / tp)
+
+
 def setup_rwg(sheet):
     """Basis functions, boundary codes and unique face pairs of ``sheet`` (``RWG.jl:90``)."""
     tol = 1.0e-5
     nface = sheet.nface
     nedge = sheet.nedge
-    fe = sheet.fe
-    eci = np.zeros(nedge, np.int64)
-    ie_xi0, ie_xi1, ie_eta0, ie_eta1 = [], [], [], []
+    fe = np.asarray(sheet.fe, np.int64)
 
     # Interior basis functions: each pair of faces (fp < fm) sharing an edge, ordered by
     # (fp, fm, local edge slot in fp, local edge slot in fm) like the reference's loops.
-    edge_faces = [[] for _ in range(nedge + 1)]
-    for f in range(nface):
-        for k in range(3):
-            edge_faces[int(fe[k, f])].append((f + 1, k))
-    pairs = []
-    for e in range(1, nedge + 1):
-        fl = edge_faces[e]
-        for a in range(len(fl)):
-            for b in range(a + 1, len(fl)):
-                (fa, ka), (fb, kb) = fl[a], fl[b]
-                if fa > fb:
-                    (fa, ka), (fb, kb) = (fb, kb), (fa, ka)
-                pairs.append((fa, fb, ka, kb, e))
-    pairs.sort()
-    nbf_int = len(pairs)
+    # The 3 nface (face, slot, edge) incidences sorted by edge, face, slot: an edge of two
+    # faces gives one pair; an edge of more faces gives every pair of distinct faces.
+    face = np.repeat(np.arange(1, nface + 1, dtype=np.int64), 3)
+    slot = np.tile(np.arange(3, dtype=np.int64), nface)
+    edge = fe.T.ravel()
+    order = np.lexsort((slot, face, edge))
+    e_s, f_s, k_s = edge[order], face[order], slot[order]
+    start = np.flatnonzero(np.r_[True, e_s[1:] != e_s[:-1]])
+    size = np.diff(np.r_[start, len(e_s)])
+    two = start[size == 2]
+    rows = [np.stack([f_s[two], f_s[two + 1], k_s[two], k_s[two + 1], e_s[two]], axis=1)]
+    for s0, n in zip(start[size > 2], size[size > 2]):  # an edge of three or more faces
+        rows.append(np.array([(f_s[a], f_s[b], k_s[a], k_s[b], e_s[a]) for a in range(s0, s0 + n)
+                              for b in range(a + 1, s0 + n)], np.int64).reshape(-1, 5))
+    rows = np.concatenate(rows)
+    rows = rows[rows[:, 0] < rows[:, 1]]
+    rows = rows[np.lexsort((rows[:, 3], rows[:, 2], rows[:, 1], rows[:, 0]))]
+    pf, mf, pe = rows[:, 0], rows[:, 1], rows[:, 4]
+    nbf_int = len(rows)
 
-    nbf = nbf_int
+    # Unit-cell boundary edges (codes 1: xi = 0, 2: xi = 1, 3: eta = 0, 4: eta = 1, tested in
+    # that order); the xi = 0 and eta = 0 edges each add a basis function.
+    eci = np.zeros(nedge, np.int64)
     if sheet.xi_eta_check:
-        for gep in range(1, nedge + 1):
-            xi0, xi1, eta0, eta1 = get_ie_xieta(gep, sheet)
-            if abs(xi0) < tol and abs(xi1) < tol:
-                nbf += 1
-                eci[gep - 1] = 1
-                ie_xi0.append(gep)
-            elif abs(xi0 - 1) < tol and abs(xi1 - 1) < tol:
-                eci[gep - 1] = 2
-                ie_xi1.append(gep)
-            elif abs(eta0) < tol and abs(eta1) < tol:
-                nbf += 1
-                eci[gep - 1] = 3
-                ie_eta0.append(gep)
-            elif abs(eta0 - 1) < tol and abs(eta1 - 1) < tol:
-                eci[gep - 1] = 4
-                ie_eta1.append(gep)
+        xi0, xi1, eta0, eta1 = _edge_xieta(sheet)
+        conds = [(np.abs(xi0) < tol) & (np.abs(xi1) < tol), (np.abs(xi0 - 1) < tol) & (np.abs(xi1 - 1) < tol),
+                 (np.abs(eta0) < tol) & (np.abs(eta1) < tol), (np.abs(eta0 - 1) < tol) & (np.abs(eta1 - 1) < tol)]
+        eci = np.select(conds, [1, 2, 3, 4], 0).astype(np.int64)
+    ie_xi0, ie_xi1 = np.flatnonzero(eci == 1) + 1, np.flatnonzero(eci == 2) + 1
+    ie_eta0, ie_eta1 = np.flatnonzero(eci == 3) + 1, np.flatnonzero(eci == 4) + 1
     if len(ie_xi0) != len(ie_xi1):
         raise ValueError("Inconsistent # edges at ξ=0 and ξ=1")
     if len(ie_eta0) != len(ie_eta1):
         raise ValueError("Inconsistent # edges at η=0 and η=1")
+    nbf = nbf_int + len(ie_xi0) + len(ie_eta0)
 
     bfe = np.zeros((2, nbf), np.int64)
     bff = np.zeros((2, nbf), np.int64)
     ebf = np.zeros(nedge, np.int64)
-    for i, (fa, fb, ka, kb, e) in enumerate(pairs):
-        bfe[:, i] = (e, e)
-        bff[:, i] = (fa, fb)
-        ebf[e - 1] = i + 1
+    bfe[0, :nbf_int] = pe
+    bfe[1, :nbf_int] = pe
+    bff[0, :nbf_int] = pf
+    bff[1, :nbf_int] = mf
+    if np.all(size <= 2):
+        ebf[pe - 1] = np.arange(1, nbf_int + 1)
+    else:
+        for k, e in enumerate(pe):  # an edge in several pairs keeps its last one
+            ebf[e - 1] = k + 1
     i = nbf_int
 
-    def first_face(ge):
-        fl = edge_faces[ge]
-        if not fl:
-            return 0
-        return min(f for f, _ in fl)
+    # first (lowest-numbered) face holding each edge, 0 for none: the head of its sorted run
+    first = np.zeros(nedge + 1, np.int64)
+    first[e_s[start]] = f_s[start]
 
     def pair_boundary(list0, list1, use_xi):
         nonlocal i
+        if len(list0) == 0:
+            return
+        xi0, xi1, eta0, eta1 = _edge_xieta(sheet)
+        a, b = (xi0, xi1) if use_xi else (eta0, eta1)
+        lo1, hi1 = np.minimum(a[list1 - 1], b[list1 - 1]), np.maximum(a[list1 - 1], b[list1 - 1])
         for ge0 in list0:
-            face0 = first_face(ge0)
+            face0 = first[ge0]
             if face0 == 0:
                 raise ValueError(f"Unable to locate face containing boundary edge {ge0}")
-            x0 = get_ie_xieta(ge0, sheet)
-            v0 = (x0[0], x0[1]) if use_xi else (x0[2], x0[3])
-            mn0, mx0 = min(v0), max(v0)
-            ge1 = 0
-            for ge in list1:
-                x1 = get_ie_xieta(ge, sheet)
-                v1 = (x1[0], x1[1]) if use_xi else (x1[2], x1[3])
-                if abs(min(v1) - mn0) < tol and abs(max(v1) - mx0) < tol:
-                    ge1 = ge
-                    break
-            if ge1 == 0:
+            mn0, mx0 = min(a[ge0 - 1], b[ge0 - 1]), max(a[ge0 - 1], b[ge0 - 1])
+            hit = np.flatnonzero((np.abs(lo1 - mn0) < tol) & (np.abs(hi1 - mx0) < tol))
+            if len(hit) == 0:
                 raise ValueError(f"Unable to locate edge corresponding to edge {ge0}")
-            face1 = first_face(ge1)
+            ge1 = int(list1[hit[0]])
+            face1 = first[ge1]
             if face1 == 0:
                 raise ValueError(f"Unable to locate face containing boundary edge {ge1}")
             bfe[:, i] = (ge0, ge1)
