@@ -19,11 +19,12 @@ GPU arm drops its cached integrals before every step, the CPU arm adds one J/K p
 
 At one GPU the line also carries the 6000-unknown targets (target_sweep: the meanderline at
 ntri = 4000, N = 5610, 201 frequencies, FP32 + refinement against the FP64 form; grads: the
-adjoint gradient of that sweep's objective in trace width, pitch and eps_r, grads/s) and the
-two-sheet oblique cascade (cascade_sweep: Jerusalem cross on a lossy substrate, air gap,
-square aperture; 51 frequencies, theta = 30, phi = 45, so the face-pair integrals run at every
-point; through analyze, in a child process of its own so that its outcome cannot touch this
-line's other numbers).
+adjoint gradient of that sweep's objective in trace width, pitch and eps_r, grads/s), the
+square patch (patch_sweep: N = 736, 11 frequencies) and the two-sheet oblique cascade
+(cascade_sweep: Jerusalem cross on a lossy substrate, air gap, square aperture; 51
+frequencies, theta = 30, phi = 45, so the face-pair integrals run at every point), both
+through analyze in a child process of their own so that their outcome cannot touch this
+line's other numbers.
 
 --impl reference: the CPU oracle (C restatement + LAPACK) on the host cores, one point
 per step with the sweep's J/K pass amortised over the 101 points.
@@ -377,18 +378,12 @@ def run_grads(args, rank):
     print(json.dumps(line), flush=True)
 
 
-def cascade_sweep():
-    """The two-sheet cascade (workloads.jerusalem_aperture_cascade: a Jerusalem cross of about
-    1500 triangles on 0.5 mm eps_r = 3, tan d = 0.002, a 2 mm air gap, a 6 mm square aperture of
-    about 1200 triangles; 51 frequencies 5-25 GHz at theta = 30, phi = 45): points/s through
-    ``analyze`` (wall clock with the device synchronised on both sides: host planning, both
-    sheets' sweeps with their face-pair integrals at every point, and the GSM cascade), FP64
-    and FP32 + refinement, one warm-up each, and max |S| difference between the two forms."""
+def _analyze_rates(strata, flist, steer):
+    """Points/s of ``analyze`` on one workload (wall clock with the device synchronised on both
+    sides: host planning, every sheet's sweep, the GSM cascade), FP64 and FP32 + refinement
+    after one warm-up each, and the largest |S| difference between the two forms."""
     import torch
-    load_package()
-    from pssfss_b200 import workloads
     from pssfss_b200.analyze import analyze
-    strata, flist, steer = workloads.jerusalem_aperture_cascade()
 
     def run(prec):
         torch.cuda.synchronize()
@@ -405,11 +400,28 @@ def cascade_sweep():
     npts = len(r64)
     dmax = max(float(np.max(np.abs(a.gsm[k] - b.gsm[k]))) for a, b in zip(r32, r64)
                for k in ((1, 1), (1, 2), (2, 1), (2, 2)))
-    return {"workload": "Jerusalem cross (%d faces) on 0.5 mm eps_r=3 tan d=0.002, 2 mm air gap, square "
-                        "aperture (%d faces), 51 freqs 5-25 GHz, theta=30 phi=45" % (strata[1].nface, strata[4].nface),
-            "fp64_value": npts / t64, "fp32r_value": npts / t32, "unit": "freq-points/s",
-            "timed": "analyze() wall clock after one warm-up per form: host planning, face-pair integrals at "
-                     "every point, both sheets' sweeps, cascade", "max_abs_S_fp32r_vs_fp64": dmax}
+    return {"fp64_value": npts / t64, "fp32r_value": npts / t32, "unit": "freq-points/s",
+            "timed": "analyze() wall clock after one warm-up per form (host planning, sweeps, cascade)",
+            "max_abs_S_fp32r_vs_fp64": dmax}
+
+
+def config_sweeps():
+    """The two smaller configurations through ``analyze``: the free-standing square patch
+    (8 mm in a 10 mm cell, 512 triangles, N = 736; 11 frequencies 10-20 GHz, normal incidence)
+    and the two-sheet cascade (workloads.jerusalem_aperture_cascade: a Jerusalem cross of about
+    1500 triangles on 0.5 mm eps_r = 3, tan d = 0.002, a 2 mm air gap, a 6 mm square aperture of
+    about 1200 triangles; 51 frequencies 5-25 GHz at theta = 30, phi = 45, so both sheets'
+    face-pair integrals run at every point)."""
+    load_package()
+    from pssfss_b200 import workloads
+    strata, flist, steer = workloads.square_patch_sweep()
+    patch = dict(workload="square patch 8 mm in a 10 mm cell (%d faces), free-standing, 11 freqs 10-20 GHz, "
+                          "normal incidence" % strata[1].nface, **_analyze_rates(strata, flist, steer))
+    strata, flist, steer = workloads.jerusalem_aperture_cascade()
+    casc = dict(workload="Jerusalem cross (%d faces) on 0.5 mm eps_r=3 tan d=0.002, 2 mm air gap, square "
+                         "aperture (%d faces), 51 freqs 5-25 GHz, theta=30 phi=45" % (strata[1].nface, strata[4].nface),
+                **_analyze_rates(strata, flist, steer))
+    return {"patch_sweep": patch, "cascade_sweep": casc}
 
 
 def target_sweep(fp64_steps=1):
@@ -442,18 +454,19 @@ def target_sweep(fp64_steps=1):
             "refine_fallbacks": int(sum(1 for x in s32 if x & 32))}
 
 
-def cascade_sweep_child(timeout=240):
-    """``cascade_sweep`` in a child process (``bench.py --cascade``); its JSON, or the reason
-    there is none."""
+def config_sweeps_child(timeout=240):
+    """``config_sweeps`` in a child process (``bench.py --configs``): its two entries, or the
+    reason there are none."""
     try:
-        p = subprocess.run([sys.executable, os.path.abspath(__file__), "--cascade"], capture_output=True,
+        p = subprocess.run([sys.executable, os.path.abspath(__file__), "--configs"], capture_output=True,
                            text=True, timeout=timeout, cwd=ROOT)
         lines = [ln for ln in p.stdout.splitlines() if ln.startswith("{")]
         if p.returncode == 0 and lines:
             return json.loads(lines[-1])
-        return {"error": f"exit {p.returncode}: " + (p.stderr or p.stdout)[-300:]}
+        err = {"error": f"exit {p.returncode}: " + (p.stderr or p.stdout)[-300:]}
     except Exception as e:  # report, never fake
-        return {"error": str(e)[:200]}
+        err = {"error": str(e)[:200]}
+    return {"patch_sweep": err, "cascade_sweep": err}
 
 
 def main():
@@ -472,9 +485,9 @@ def main():
                     help="frequencies of the gradient workload (default: all 201)")
     ap.add_argument("--rings", action="store_true",
                     help="time the seeded batch of 64 ring problems of differing size instead")
-    ap.add_argument("--cascade", action="store_true",
-                    help="time the two-sheet oblique cascade alone (one JSON line; the default run "
-                         "adds it to its line)")
+    ap.add_argument("--configs", action="store_true",
+                    help="time the square patch and the two-sheet oblique cascade through analyze "
+                         "(one JSON line; the default run adds both to its line)")
     ap.add_argument("--no-targets", action="store_true",
                     help="skip the 6000-unknown target sweep and the gradient (profiling runs)")
     ap.add_argument("--no-tuning", action="store_true", help="--rings with the library defaults")
@@ -490,10 +503,10 @@ def main():
         return run_grads(args, rank)
     if args.rings:
         return run_rings(args, rank, world, local)
-    if args.cascade:
+    if args.configs:
         import torch
         torch.cuda.set_device(0)
-        print(json.dumps(cascade_sweep()), flush=True)
+        print(json.dumps(config_sweeps()), flush=True)
         return None
     if args.autotune:
         return run_autotune(args, rank)
@@ -646,7 +659,7 @@ def main():
                                  "planning included"}
             except Exception as e:
                 line["grads"] = {"error": str(e)[:200]}
-            line["cascade_sweep"] = cascade_sweep_child()
+            line.update(config_sweeps_child())
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
