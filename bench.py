@@ -249,6 +249,25 @@ def cpu_baseline_sample(case):
                                       f"({t_jk:.1f} s) amortised over {NFREQ} points", **ci}, NFREQ // 2, dS_ref
 
 
+def patch_cpu_baseline():
+    """The square-patch configuration (the one the reference itself runs on a CPU) whole
+    through the CPU oracle's ``analyze`` on the host cores: every step of the 11-point sweep
+    (J/K pass, fill, LAPACK LU and solves, projection, cascade), one warm-up run first."""
+    sys.path.insert(0, ROOT)
+    import oracle
+    load_package()
+    from pssfss_b200 import workloads
+    strata, flist, steer = workloads.square_patch_sweep()
+    oracle.analyze(strata, flist, steer)
+    t = time.perf_counter()
+    res = oracle.analyze(strata, flist, steer)
+    sec = time.perf_counter() - t
+    ci = cpu_info()
+    cores = max(ci["omp_threads"] or 0, ci["blas_threads"] or 0) or os.cpu_count()
+    return {"value": len(res) / sec, "unit": "freq-points/s", "cores": cores, "kind": "port",
+            "sample": f"the whole {len(res)}-point sweep through the oracle's analyze ({sec:.2f} s)"}
+
+
 def run_rings(args, rank, world=1, local=0):
     """Freq-points/s over the seeded batch of 64 ring problems (period 6-12 mm, 300-3000
     triangles, so unknown counts 480-4800; theta in {0, 15, 30, 45}; 21 frequencies each;
@@ -660,6 +679,11 @@ def main():
             except Exception as e:
                 line["grads"] = {"error": str(e)[:200]}
             line.update(config_sweeps_child())
+            if not args.no_cpu_baseline and "error" not in line["patch_sweep"]:
+                try:
+                    line["patch_sweep"]["cpu_baseline"] = patch_cpu_baseline()
+                except Exception as e:  # report, never fake
+                    line["patch_sweep"]["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
